@@ -1,0 +1,274 @@
+/*
+ * qm_gpu.h — C ABI of the B200 filter -> hash GROUP BY aggregate path.
+ *
+ * This is the drop-in boundary that replaces QueryMode's per-batch WASM calls
+ * and JS aggregation on the `.filter().groupBy()` / `.sql("... GROUP BY ...")`
+ * path.  Every entry point below names the reference interface it replaces.
+ * Reference paths are relative to the QueryMode repository root.
+ *
+ * Conventions (mirroring the WASM boundary, src/wasm-engine.ts:21-187, and the
+ * native Node ABI, wasm/src/nodejs.zig:20-40):
+ *   - every function returns an int status (QM_OK == 0); on failure the
+ *     context keeps a message readable with qm_ctx_last_error();
+ *   - handles are opaque and explicitly destroyed;
+ *   - a context is used by one host thread at a time (the reference keeps one
+ *     single-threaded engine per Durable Object, src/wasm-engine.ts:181-186);
+ *     distinct contexts may run concurrently;
+ *   - there is no CPU fallback: if no CUDA device or the kernel image is
+ *     unavailable, qm_ctx_create fails with QM_ERR_NO_DEVICE / QM_ERR_CUDA.
+ *
+ * Semantics follow the reference's JS operator path (the parity target):
+ *   predicates  src/decode.ts:478-578 (coerceCompare, matchesFilter,
+ *               rowPassesFilters), op codes src/operators.ts:422-432;
+ *   aggregates  src/partial-agg.ts:38-352 (SUM/COUNT/MIN/MAX/AVG state,
+ *               update, merge, finalize), group keys src/types.ts:10-18;
+ *   batch merge src/operators.ts:1646-1710 (AggregateOperator.next).
+ */
+#ifndef QM_GPU_H
+#define QM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define QM_OK 0
+#define QM_ERR_INVALID 1     /* malformed descriptor / argument            */
+#define QM_ERR_UNSUPPORTED 2 /* query shape outside the GPU path           */
+#define QM_ERR_CUDA 3        /* CUDA runtime error                          */
+#define QM_ERR_OOM 4         /* device allocation or HBM budget refused     */
+#define QM_ERR_NOT_FOUND 5   /* unknown column name                         */
+#define QM_ERR_CAPACITY 6    /* caller-provided output capacity too small   */
+#define QM_ERR_TIMEOUT 7     /* a bounded device-side wait gave up          */
+#define QM_ERR_NO_DEVICE 8   /* no CUDA device                              */
+#define QM_ERR_CANCELLED 9   /* serving: request cancelled before running   */
+
+/* ---- dtypes: QMCB tags (src/columnar.ts:22-33) ------------------------- */
+#define QM_F64 0
+#define QM_I64 1
+#define QM_I32 6
+#define QM_F32 7
+/* result-only: exact 128-bit two's-complement integer stored as (lo u64,
+ * hi i64) pairs; carries SUM over int64 columns, which the reference keeps
+ * as an arbitrary-precision BigInt (src/partial-agg.ts:89-95). */
+#define QM_I128 64
+
+/* ---- filter ops: src/types.ts:130-133, codes 0-5 as src/operators.ts:422-432 */
+#define QM_OP_EQ 0
+#define QM_OP_NEQ 1
+#define QM_OP_LT 2
+#define QM_OP_LTE 3
+#define QM_OP_GT 4
+#define QM_OP_GTE 5
+#define QM_OP_BETWEEN 6     /* inclusive, src/decode.ts:528-534            */
+#define QM_OP_NOT_BETWEEN 7 /* src/decode.ts:535-541                       */
+#define QM_OP_IS_NULL 8
+#define QM_OP_IS_NOT_NULL 9
+
+/* filter value kinds: a JS `number` or a JS `bigint` (FilterOp.value) */
+#define QM_VAL_NUMBER 0
+#define QM_VAL_BIGINT 1
+
+/* ---- aggregate fns: src/types.ts:137-145 (numeric subset) -------------- */
+#define QM_AGG_SUM 0
+#define QM_AGG_AVG 1
+#define QM_AGG_MIN 2
+#define QM_AGG_MAX 3
+#define QM_AGG_COUNT 4
+
+/* ---- query flags --------------------------------------------------------- */
+/* Emit groups in hash-table order instead of the reference's Map
+ * first-seen order (src/partial-agg.ts:320-349).  Saves one sort. */
+#define QM_FLAG_UNORDERED 1
+/* Evaluate numeric filters the way the scan-time WASM filter does
+ * (src/operators.ts:550-666): NULLs read as 0 and int32 thresholds pass
+ * through ToInt32.  Default is the JS matchesFilter semantics. */
+#define QM_FLAG_WASM_SCAN_SEMANTICS 2
+
+typedef struct qm_ctx qm_ctx;
+typedef struct qm_table qm_table;
+typedef struct qm_agg qm_agg;
+typedef struct qm_result qm_result;
+
+/* One input column.  `null_bitmap` follows QMCB: bit (row & 7) of byte
+ * (row >> 3) set = NULL (src/columnar.ts:752-754).  With on_device == 0 the
+ * library copies host memory into HBM it owns; with on_device == 1 `data` and
+ * `null_bitmap` are device pointers of the context's device, borrowed (not
+ * freed) and read in place. */
+typedef struct {
+  const char *name;
+  int32_t dtype;
+  int32_t on_device;
+  const void *data;
+  const uint8_t *null_bitmap;
+} qm_column;
+
+/* A JS filter value: `number` (kind QM_VAL_NUMBER, in `num`) or `bigint`
+ * (kind QM_VAL_BIGINT, in `big`). */
+typedef struct {
+  int32_t kind;
+  int32_t reserved;
+  double num;
+  int64_t big;
+} qm_value;
+
+/* FilterOp {column, op, value} (src/types.ts:130-134).  BETWEEN uses
+ * value (low) and value2 (high). */
+typedef struct {
+  const char *column;
+  int32_t op;
+  int32_t reserved;
+  qm_value value;
+  qm_value value2;
+} qm_filter;
+
+/* AggregateOp {fn, column, alias} (src/types.ts:137-145); column "*" is
+ * COUNT(*).  A NULL alias means the reference default `${fn}_${column}`
+ * (src/partial-agg.ts:136-138). */
+typedef struct {
+  int32_t fn;
+  int32_t reserved;
+  const char *column;
+  const char *alias;
+} qm_aggregate;
+
+/* The filter/groupBy/aggregates part of QueryDescriptor
+ * (src/client.ts:1254-1277).  OR groups (QueryDescriptor.filterGroups) are
+ * flattened: group g owns or_group_sizes[g] consecutive entries of
+ * or_filters.  The row passes if every `filters` entry passes and, when
+ * n_or_groups > 0, every entry of at least one group passes
+ * (src/decode.ts:558-578). */
+typedef struct {
+  const qm_filter *filters;
+  int32_t n_filters;
+  int32_t n_or_groups;
+  const int32_t *or_group_sizes;
+  const qm_filter *or_filters;
+  const char *const *group_by;
+  int32_t n_group_by;
+  int32_t n_aggregates;
+  const qm_aggregate *aggregates;
+  int32_t flags;
+  int32_t reserved;
+} qm_query;
+
+/* One output column.  `data` is host memory owned by the result; dtype is
+ * QM_I32/QM_I64/QM_F64 or QM_I128 (2 x 8 bytes per row).  `null_bitmap`
+ * is NULL or QMCB-style (bit set = NULL: a NULL group key, or an aggregate
+ * whose group saw no non-null value, src/partial-agg.ts:109-111). */
+typedef struct {
+  const char *name;
+  int32_t dtype;
+  int32_t is_key;
+  int64_t n_rows;
+  const void *data;
+  const uint8_t *null_bitmap;
+} qm_result_col;
+
+/* Per-run counters (the reference reports scanMs / bytesRead / wasmExecMs,
+ * src/operators.ts:180-182, src/types.ts:262-300). */
+typedef struct {
+  int64_t rows_scanned;
+  int64_t rows_selected;
+  int64_t groups;
+  int64_t bytes_scanned;  /* algorithmic: rows x widths of referenced columns */
+  double device_ms;       /* CUDA-event time of the device work of the run  */
+  int32_t strategy;       /* 0 direct-mapped, 1 block-local + global hash,
+                             2 global hash only, 3 hash-partitioned          */
+  int32_t table_capacity; /* log2 of the group table's slot count           */
+  int32_t retries;        /* table regrowths after a capacity overflow      */
+  int32_t launches;       /* kernels of this library launched by the run   */
+  double scan_ms;         /* CUDA-event time of the fused scan kernel(s)    */
+} qm_stats;
+
+/* ---- library / context ---------------------------------------------------- */
+const char *qm_version(void);
+
+/* Replaces WebAssembly.instantiate + WasmEngine construction
+ * (src/wasm-engine.ts:151-187, src/local-executor.ts:85-98).  `device` is a
+ * CUDA ordinal; the context owns a stream and a device memory pool. */
+int qm_ctx_create(int32_t device, qm_ctx **out);
+int qm_ctx_destroy(qm_ctx *ctx);
+/* Replaces WasmEngine.getLastError (src/wasm-engine.ts:272-279). */
+const char *qm_ctx_last_error(const qm_ctx *ctx);
+/* Order the context's device work on a caller's stream (a cudaStream_t of
+ * the context's device, e.g. torch.cuda.current_stream().cuda_stream);
+ * NULL restores the context's own stream.  No reference counterpart: the
+ * WASM engine has no streams; this lets a host framework time or overlap
+ * the path with its own work. */
+int qm_ctx_set_stream(qm_ctx *ctx, void *stream);
+/* Device properties the host planner and tests read. */
+int qm_ctx_device_info(const qm_ctx *ctx, int32_t *sm_count, int64_t *hbm_bytes);
+
+/* ---- tables ---------------------------------------------------------------- */
+/* Register a table of numeric columns resident in HBM.  Replaces the
+ * per-page copy into WASM linear memory (src/operators.ts:558-583) and the
+ * in-memory table of MaterializedExecutor (src/client.ts:996-1127). */
+int qm_table_create(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
+                    const qm_column *cols, qm_table **out);
+/* Register a table from one QMCB buffer (src/columnar.ts:438-516).
+ * Numeric columns (F64/I64/I32/F32) are uploaded; others are ignored. */
+int qm_table_from_qmcb(qm_ctx *ctx, const uint8_t *buf, size_t len,
+                       qm_table **out);
+int qm_table_destroy(qm_table *table);
+int qm_table_num_rows(const qm_table *table, int64_t *out);
+
+/* ---- one-shot query over a registered table ---------------------------- */
+/* filter -> GROUP BY -> finalize over all rows of `table` as one batch.
+ * Replaces MaterializedExecutor.execute's rowPassesFilters +
+ * computePartialAgg + finalizePartialAgg (src/client.ts:1023-1054). */
+int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *query,
+                 qm_result **out);
+
+/* ---- streaming aggregation (AggregateOperator drop-in) ------------------ */
+/* Begin an aggregation whose input arrives batch by batch, as
+ * AggregateOperator.next drains upstream.nextColumnar
+ * (src/operators.ts:1656-1681).  Filters in `query` are fused into the
+ * aggregation kernel (the scan-time filter of src/operators.ts:439-547 plus
+ * FilterOperator, src/operators.ts:1406-1496). */
+int qm_agg_begin(qm_ctx *ctx, const qm_query *query, qm_agg **out);
+/* Feed one batch: n_rows rows of n_cols columns (host or device).  If
+ * `selection` is non-NULL it lists n_selected ascending row indices that are
+ * alive (ColumnarBatch.selection, src/operators.ts:57-64); only those rows
+ * are filtered and aggregated.  Row order across pushes is the batch order
+ * the reference merges partials in. */
+int qm_agg_push(qm_agg *agg, int64_t n_rows, int32_t n_cols,
+                const qm_column *cols, const uint32_t *selection,
+                int64_t n_selected);
+/* Finalize into a result (src/partial-agg.ts:306-352). */
+int qm_agg_finish(qm_agg *agg, qm_result **out);
+int qm_agg_destroy(qm_agg *agg);
+
+/* ---- filter-only selection (FilterOperator / WASM filter drop-in) ------- */
+/* Evaluate the filters of `query` (aggregates and group_by ignored) over one
+ * batch and write the ascending indices of passing rows into out_indices
+ * (capacity max_out).  Replaces filterFloat64Buffer / filterInt64Buffer /
+ * filterInt32Buffer / *Range / *NotRange + intersectIndices / unionIndices
+ * (wasm/src/wasm/aggregates.zig:605-1066) as composed by applyAndFilters /
+ * scanFilterIndices (src/operators.ts:439-547).  If more than max_out rows
+ * pass, *out_count is the full count and QM_ERR_CAPACITY is returned. */
+int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
+                     const qm_column *cols, const qm_query *query,
+                     uint32_t *out_indices, int64_t max_out,
+                     int64_t *out_count);
+
+/* ---- results ------------------------------------------------------------- */
+int qm_result_num_rows(const qm_result *res, int64_t *out);
+int qm_result_num_columns(const qm_result *res, int32_t *out);
+int qm_result_column(const qm_result *res, int32_t index,
+                     qm_result_col *out);
+int qm_result_stats(const qm_result *res, qm_stats *out);
+/* Encode the result as a QMCB buffer (src/columnar.ts:523-613), owned by
+ * the result.  QM_I128 sums are written as I64 when every value fits, else
+ * QM_ERR_UNSUPPORTED. */
+int qm_result_qmcb(const qm_result *res, const uint8_t **buf, size_t *len);
+int qm_result_destroy(qm_result *res);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QM_GPU_H */

@@ -1,0 +1,167 @@
+"""ctypes mirror of include/qm_gpu.h and the loader for libqm_gpu.so.
+
+The structures here are byte-for-byte the C ABI declared in include/qm_gpu.h;
+the product library and the CPU oracle both take them.  Loading the product
+library fails loudly when the built .so is missing: there is no CPU fallback
+on this path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+# status codes
+QM_OK = 0
+QM_ERR_INVALID = 1
+QM_ERR_UNSUPPORTED = 2
+QM_ERR_CUDA = 3
+QM_ERR_OOM = 4
+QM_ERR_NOT_FOUND = 5
+QM_ERR_CAPACITY = 6
+QM_ERR_TIMEOUT = 7
+QM_ERR_NO_DEVICE = 8
+QM_ERR_CANCELLED = 9
+
+STATUS_NAMES = {
+    0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "OOM", 5: "NOT_FOUND",
+    6: "CAPACITY", 7: "TIMEOUT", 8: "NO_DEVICE", 9: "CANCELLED",
+}
+
+# dtypes (QMCB tags, src/columnar.ts:22-33) + the result-only 128-bit integer
+QM_F64 = 0
+QM_I64 = 1
+QM_I32 = 6
+QM_F32 = 7
+QM_I128 = 64
+
+# filter ops (src/operators.ts:422-432 codes 0-5)
+QM_OP_EQ, QM_OP_NEQ, QM_OP_LT, QM_OP_LTE, QM_OP_GT, QM_OP_GTE = range(6)
+QM_OP_BETWEEN = 6
+QM_OP_NOT_BETWEEN = 7
+QM_OP_IS_NULL = 8
+QM_OP_IS_NOT_NULL = 9
+
+OP_CODES = {
+    "eq": QM_OP_EQ, "neq": QM_OP_NEQ, "lt": QM_OP_LT, "lte": QM_OP_LTE,
+    "gt": QM_OP_GT, "gte": QM_OP_GTE, "between": QM_OP_BETWEEN,
+    "not_between": QM_OP_NOT_BETWEEN, "is_null": QM_OP_IS_NULL,
+    "is_not_null": QM_OP_IS_NOT_NULL,
+}
+
+QM_VAL_NUMBER = 0
+QM_VAL_BIGINT = 1
+
+QM_AGG_SUM, QM_AGG_AVG, QM_AGG_MIN, QM_AGG_MAX, QM_AGG_COUNT = range(5)
+AGG_CODES = {"sum": QM_AGG_SUM, "avg": QM_AGG_AVG, "min": QM_AGG_MIN,
+             "max": QM_AGG_MAX, "count": QM_AGG_COUNT}
+
+QM_FLAG_UNORDERED = 1
+QM_FLAG_WASM_SCAN_SEMANTICS = 2
+
+
+class QmColumn(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("on_device", C.c_int32),
+                ("data", C.c_void_p), ("null_bitmap", C.c_void_p)]
+
+
+class QmValue(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("num", C.c_double),
+                ("big", C.c_int64)]
+
+
+class QmFilter(C.Structure):
+    _fields_ = [("column", C.c_char_p), ("op", C.c_int32), ("reserved", C.c_int32),
+                ("value", QmValue), ("value2", QmValue)]
+
+
+class QmAggregate(C.Structure):
+    _fields_ = [("fn", C.c_int32), ("reserved", C.c_int32), ("column", C.c_char_p),
+                ("alias", C.c_char_p)]
+
+
+class QmQuery(C.Structure):
+    _fields_ = [("filters", C.POINTER(QmFilter)), ("n_filters", C.c_int32),
+                ("n_or_groups", C.c_int32), ("or_group_sizes", C.POINTER(C.c_int32)),
+                ("or_filters", C.POINTER(QmFilter)), ("group_by", C.POINTER(C.c_char_p)),
+                ("n_group_by", C.c_int32), ("n_aggregates", C.c_int32),
+                ("aggregates", C.POINTER(QmAggregate)), ("flags", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class QmResultCol(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("is_key", C.c_int32),
+                ("n_rows", C.c_int64), ("data", C.c_void_p), ("null_bitmap", C.c_void_p)]
+
+
+class QmStats(C.Structure):
+    _fields_ = [("rows_scanned", C.c_int64), ("rows_selected", C.c_int64),
+                ("groups", C.c_int64), ("bytes_scanned", C.c_int64),
+                ("device_ms", C.c_double), ("strategy", C.c_int32),
+                ("table_capacity", C.c_int32), ("retries", C.c_int32),
+                ("launches", C.c_int32), ("scan_ms", C.c_double)]
+
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libqm_gpu.so")
+
+# (name, restype, argtypes) for every entry point of include/qm_gpu.h
+_P = C.c_void_p
+_PP = C.POINTER(C.c_void_p)
+SIGNATURES = [
+    ("qm_version", C.c_char_p, []),
+    ("qm_ctx_create", C.c_int, [C.c_int32, _PP]),
+    ("qm_ctx_destroy", C.c_int, [_P]),
+    ("qm_ctx_last_error", C.c_char_p, [_P]),
+    ("qm_ctx_set_stream", C.c_int, [_P, C.c_void_p]),
+    ("qm_ctx_device_info", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    ("qm_table_create", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn), _PP]),
+    ("qm_table_from_qmcb", C.c_int, [_P, C.c_void_p, C.c_size_t, _PP]),
+    ("qm_table_destroy", C.c_int, [_P]),
+    ("qm_table_num_rows", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("qm_query_run", C.c_int, [_P, _P, C.POINTER(QmQuery), _PP]),
+    ("qm_agg_begin", C.c_int, [_P, C.POINTER(QmQuery), _PP]),
+    ("qm_agg_push", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn),
+                              C.POINTER(C.c_uint32), C.c_int64]),
+    ("qm_agg_finish", C.c_int, [_P, _PP]),
+    ("qm_agg_destroy", C.c_int, [_P]),
+    ("qm_filter_select", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn),
+                                   C.POINTER(QmQuery), C.POINTER(C.c_uint32), C.c_int64,
+                                   C.POINTER(C.c_int64)]),
+    ("qm_result_num_rows", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("qm_result_num_columns", C.c_int, [_P, C.POINTER(C.c_int32)]),
+    ("qm_result_column", C.c_int, [_P, C.c_int32, C.POINTER(QmResultCol)]),
+    ("qm_result_stats", C.c_int, [_P, C.POINTER(QmStats)]),
+    ("qm_result_qmcb", C.c_int, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    ("qm_result_destroy", C.c_int, [_P]),
+]
+
+_lib = None
+
+
+class QmError(RuntimeError):
+    """A non-OK status from the C ABI, with the context's last-error text."""
+
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"QM_ERR_{name}: {message}" if message else f"QM_ERR_{name}")
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Load libqm_gpu.so (built in-tree).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"libqm_gpu.so not found at {p}; build it with "
+            "`python -m querymode_b200.build` (there is no CPU fallback)")
+    lib = C.CDLL(p)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

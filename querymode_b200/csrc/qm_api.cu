@@ -1,0 +1,1758 @@
+// qm_api.cu — the C ABI of include/qm_gpu.h: contexts, HBM-resident tables,
+// the planner that lowers a query, execution, finalize, results.
+//
+// The planner folds the reference's JS comparison coercions into the kernel's
+// bounds:
+//   * int64 column vs number t: coerceCompare turns t into BigInt(trunc(t))
+//     (src/decode.ts:480-485), so the test is an exact integer comparison
+//     with trunc(t);
+//   * int32 / float column vs number: plain JS number comparison — exact for
+//     int32 cells, IEEE for float cells (NaN compares false, != is true);
+//   * bigint t: exact integer comparison (int columns) or
+//     BigInt(trunc(v)) <op> t (float columns).
+// Every integer test becomes one inclusive range or its complement, clamped
+// to the column type; empty / full ranges become constants.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qm_gpu.h"
+#include "qm_launch.h"
+#include "qm_plan.h"
+
+typedef __int128 i128;
+
+namespace {
+
+// ------------------------------------------------------------ device buffers
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct HostBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct qm_ctx {
+  int device = 0;
+  int sm_count = 0;
+  int64_t hbm_bytes = 0;
+  cudaStream_t stream = nullptr;      // where work is ordered
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs0 = nullptr, evs1 = nullptr;
+  int launches = 0;  // kernels of this library launched since the last reset
+  std::string err;
+  // grow-only scratch reused across runs of this context
+  DevBuf table, status, keys, slots, keys2, slots2, sort_temp, counter, out, hll;
+  DevBuf masks, counts, offsets, sel_out, sel_in;
+  std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
+  HostBuf hout, hstatus;
+};
+
+namespace {
+
+int set_err(qm_ctx *ctx, int code, const char *fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return set_err(ctx, QM_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+int ensure(qm_ctx *ctx, DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes && b.p) return QM_OK;
+  if (b.p) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, QM_ERR_OOM, "cudaMalloc(%zu): %s", want, cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  return QM_OK;
+}
+
+int ensure_host(qm_ctx *ctx, HostBuf &b, size_t bytes) {
+  if (b.bytes >= bytes && b.p) return QM_OK;
+  if (b.p) cudaFreeHost(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  size_t want = std::max<size_t>(bytes, 4096);
+  cudaError_t e = cudaMallocHost(&b.p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, QM_ERR_OOM, "cudaMallocHost(%zu): %s", want, cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  return QM_OK;
+}
+
+void release(DevBuf &b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+int64_t qm_f2ord_host(double d) {
+  int64_t b;
+  memcpy(&b, &d, 8);
+  return b >= 0 ? b : (b ^ 0x7fffffffffffffffLL);
+}
+
+size_t dtype_size(int d) { return d == QM_I32 || d == QM_F32 ? 4 : (d == QM_I128 ? 16 : 8); }
+bool is_int(int d) { return d == QM_I32 || d == QM_I64; }
+bool valid_dtype(int d) { return d == QM_I32 || d == QM_I64 || d == QM_F32 || d == QM_F64; }
+
+// ------------------------------------------------------------ columns
+struct DevCol {
+  std::string name;
+  int dtype = QM_F64;
+  void *data = nullptr;
+  uint32_t *nulls = nullptr;
+  bool own_data = false, own_nulls = false;
+  bool has_minmax = false;
+  long long mn = 0, mx = 0;
+  bool has_hll = false;
+  double hll = 0;
+};
+
+}  // namespace
+
+struct qm_table {
+  qm_ctx *ctx = nullptr;
+  int64_t n_rows = 0;
+  std::vector<DevCol> cols;
+};
+
+namespace {
+
+void free_col(DevCol &c) {
+  if (c.own_data && c.data) cudaFree(c.data);
+  if (c.own_nulls && c.nulls) cudaFree(c.nulls);
+  c.data = nullptr;
+  c.nulls = nullptr;
+}
+
+// Copy a QMCB-style byte bitmap into a 32-bit-word device bitmap.
+int upload_nulls(qm_ctx *ctx, const uint8_t *host_bits, int64_t n, uint32_t **out) {
+  size_t words = (size_t)((n + 31) / 32) + 1;
+  uint32_t *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, words * 4);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, QM_ERR_OOM, "null bitmap alloc: %s", cudaGetErrorString(e));
+  }
+  CK(cudaMemsetAsync(d, 0, words * 4, ctx->stream));
+  if (n > 0) CK(cudaMemcpyAsync(d, host_bits, (size_t)((n + 7) / 8), cudaMemcpyHostToDevice, ctx->stream));
+  *out = d;
+  return QM_OK;
+}
+
+int make_col(qm_ctx *ctx, int64_t n, const qm_column &src, DevCol &c) {
+  if (!src.name) return set_err(ctx, QM_ERR_INVALID, "column without a name");
+  if (!valid_dtype(src.dtype))
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dtype %d is not numeric", src.name, src.dtype);
+  c.name = src.name;
+  c.dtype = src.dtype;
+  if (n > 0 && !src.data) return set_err(ctx, QM_ERR_INVALID, "column %s: no data", src.name);
+  if (src.on_device) {
+    c.data = const_cast<void *>(src.data);
+    if (src.null_bitmap) {
+      // a device bitmap must already be readable as 32-bit words: copy it
+      // into an owned, word-padded buffer
+      size_t words = (size_t)((n + 31) / 32) + 1;
+      uint32_t *d = nullptr;
+      cudaError_t e = cudaMalloc(&d, words * 4);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, QM_ERR_OOM, "null bitmap alloc");
+      }
+      CK(cudaMemsetAsync(d, 0, words * 4, ctx->stream));
+      if (n > 0)
+        CK(cudaMemcpyAsync(d, src.null_bitmap, (size_t)((n + 7) / 8), cudaMemcpyDeviceToDevice, ctx->stream));
+      c.nulls = d;
+      c.own_nulls = true;
+    }
+    return QM_OK;
+  }
+  size_t bytes = (size_t)n * dtype_size(src.dtype);
+  void *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, QM_ERR_OOM, "column %s: cudaMalloc(%zu): %s", src.name, bytes, cudaGetErrorString(e));
+  }
+  c.data = d;
+  c.own_data = true;
+  if (bytes) CK(cudaMemcpyAsync(d, src.data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if (src.null_bitmap) {
+    int rc = upload_nulls(ctx, src.null_bitmap, n, &c.nulls);
+    if (rc) return rc;
+    c.own_nulls = true;
+  }
+  return QM_OK;
+}
+
+// ------------------------------------------------------------ planning
+struct ColView {  // what the planner needs to know of a column
+  const DevCol *col;
+  int64_t n;
+};
+
+struct OutMeta {
+  std::string name;
+  int dtype;
+  int is_key;
+  bool nullable;
+};
+
+struct Plan {
+  qm_pred pred{};
+  qm_keyspec key{};
+  qm_aggspec agg{};
+  qm_outspec outs{};
+  std::vector<OutMeta> meta;
+  int64_t bytes_per_row = 0;  // algorithmic: widths of referenced columns
+  bool ordered = true;
+  int key_col_dtype = 0;
+};
+
+const i128 BIG = (i128)1 << 100;
+
+i128 clamp_d(double d) {  // integer-valued double -> i128, saturating
+  if (d >= 1e30) return BIG;
+  if (d <= -1e30) return -BIG;
+  return (i128)d;
+}
+
+// A JS comparison threshold as seen from an integer cell.  kind: 0 finite
+// (floor/ceil exact integers), 1 NaN.  ±Infinity are finite beyond any
+// int64 (±2^101).
+struct Thr {
+  int nan = 0;
+  i128 fl = 0, ce = 0;
+};
+
+Thr thr_of_number_exact(double t) {  // int32 cell (a JS number) vs number t
+  Thr r;
+  if (std::isnan(t)) {
+    r.nan = 1;
+    return r;
+  }
+  if (std::isinf(t)) {
+    r.fl = r.ce = t > 0 ? BIG * 2 : -BIG * 2;
+    return r;
+  }
+  r.fl = clamp_d(std::floor(t));
+  r.ce = clamp_d(std::ceil(t));
+  return r;
+}
+
+Thr thr_of_int(i128 T) {
+  Thr r;
+  r.fl = r.ce = T;
+  return r;
+}
+
+// ECMAScript ToInt32 (a number passed as a WASM i32 parameter).
+int32_t to_int32(double x) {
+  if (!std::isfinite(x)) return 0;
+  double t = std::trunc(x);
+  double m = std::fmod(t, 4294967296.0);
+  if (m < 0) m += 4294967296.0;
+  return (int32_t)(uint32_t)m;
+}
+
+// safeBigInt then ToBigInt64 (a bigint passed as a WASM i64 parameter).
+int64_t to_wasm_i64(double x) {
+  if (!std::isfinite(x)) return 0;
+  double t = std::trunc(x);
+  if (std::fabs(t) < 9.2e18) return (int64_t)t;
+  double m = std::fmod(t, 18446744073709551616.0);
+  if (m < 0) m += 18446744073709551616.0;
+  uint64_t u = m >= 9223372036854775808.0 ? (uint64_t)(m - 9223372036854775808.0) + 9223372036854775808ULL
+                                           : (uint64_t)m;
+  return (int64_t)u;
+}
+
+// The threshold an integer cell is compared with, after JS coercion.
+Thr int_threshold(int dtype, const qm_value &v, bool wasm) {
+  if (v.kind == QM_VAL_BIGINT) return thr_of_int((i128)v.big);
+  if (wasm) {
+    if (dtype == QM_I32) return thr_of_int((i128)to_int32(v.num));
+    return thr_of_int((i128)to_wasm_i64(v.num));
+  }
+  if (dtype == QM_I64) {
+    // bigint cell: BigInt(Math.trunc(t)) for finite t, else the number
+    if (std::isfinite(v.num)) return thr_of_int(clamp_d(std::trunc(v.num)));
+    return thr_of_number_exact(v.num);
+  }
+  return thr_of_number_exact(v.num);
+}
+
+struct IRange {
+  int konst = -1;  // -1: a range test; 0 / 1: constant result
+  bool negate = false;
+  i128 lo = 0, hi = 0;
+};
+
+IRange int_range_for(int op, const Thr &t) {
+  IRange r;
+  if (t.nan) {
+    r.konst = op == QM_OP_NEQ ? 1 : 0;
+    return r;
+  }
+  const i128 MIN = -BIG * 4, MAX = BIG * 4;
+  switch (op) {
+    case QM_OP_EQ: if (t.fl != t.ce) { r.konst = 0; return r; } r.lo = r.hi = t.fl; break;
+    case QM_OP_NEQ: if (t.fl != t.ce) { r.konst = 1; return r; } r.lo = r.hi = t.fl; r.negate = true; break;
+    case QM_OP_LT: r.lo = MIN; r.hi = t.ce - 1; break;
+    case QM_OP_LTE: r.lo = MIN; r.hi = t.fl; break;
+    case QM_OP_GT: r.lo = t.fl + 1; r.hi = MAX; break;
+    default: r.lo = t.ce; r.hi = MAX; break;  // GTE
+  }
+  return r;
+}
+
+bool range_test0(const IRange &r) {  // does the test pass for the value 0?
+  if (r.konst >= 0) return r.konst;
+  bool in = r.lo <= 0 && 0 <= r.hi;
+  return r.negate ? !in : in;
+}
+
+void lower_irange(const IRange &r0, int dtype, qm_term &t) {
+  IRange r = r0;
+  const i128 dmin = dtype == QM_I32 ? (i128)INT32_MIN : (i128)INT64_MIN;
+  const i128 dmax = dtype == QM_I32 ? (i128)INT32_MAX : (i128)INT64_MAX;
+  if (r.konst >= 0) {
+    t.kind = r.konst ? QT_TRUE : QT_FALSE;
+    return;
+  }
+  i128 lo = std::max(r.lo, dmin), hi = std::min(r.hi, dmax);
+  bool empty = lo > hi;
+  bool full = !empty && lo == dmin && hi == dmax;
+  if (!r.negate) {
+    if (empty) { t.kind = QT_FALSE; return; }
+    if (full) { t.kind = QT_TRUE; return; }
+    t.kind = QT_IRANGE;
+  } else {
+    if (empty) { t.kind = QT_TRUE; return; }
+    if (full) { t.kind = QT_FALSE; return; }
+    t.kind = QT_INRANGE;
+  }
+  t.lo = (int64_t)lo;
+  t.hi = (int64_t)hi;
+}
+
+// Does the scan-time WASM filter (applyAndFilters, src/operators.ts:469-547)
+// take its WASM branch for this filter?
+bool wasm_route(int dtype, const qm_filter &f) {
+  if (f.op <= QM_OP_GTE) {
+    if (f.value.kind != QM_VAL_NUMBER) return false;
+    if (dtype == QM_I64 && !std::isfinite(f.value.num)) return false;
+    return true;
+  }
+  if (f.op == QM_OP_BETWEEN || f.op == QM_OP_NOT_BETWEEN) {
+    if (f.value.kind != QM_VAL_NUMBER || f.value2.kind != QM_VAL_NUMBER) return false;
+    if (dtype == QM_I64 && (!std::isfinite(f.value.num) || !std::isfinite(f.value2.num))) return false;
+    return true;
+  }
+  return false;
+}
+
+bool fcmp_host(double v, int op, double t) {
+  switch (op) {
+    case 0: return v == t; case 1: return v != t; case 2: return v < t;
+    case 3: return v <= t; case 4: return v > t; default: return v >= t;
+  }
+}
+
+int lower_filter(qm_ctx *ctx, const qm_filter &f, const ColView &cv, bool wasm_flag, qm_term &t) {
+  const DevCol &c = *cv.col;
+  memset(&t, 0, sizeof t);
+  t.data = c.data;
+  t.nulls = c.nulls;
+  t.dtype = c.dtype;
+  t.null_pass = 0;
+  if (f.op == QM_OP_IS_NULL) { t.kind = QT_FALSE; t.null_pass = 1; return QM_OK; }
+  if (f.op == QM_OP_IS_NOT_NULL) { t.kind = QT_TRUE; t.null_pass = 0; return QM_OK; }
+  if (f.op < 0 || f.op > QM_OP_NOT_BETWEEN)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "filter op %d on %s is not on the GPU path", f.op, c.name.c_str());
+  if (f.value.kind != QM_VAL_NUMBER && f.value.kind != QM_VAL_BIGINT)
+    return set_err(ctx, QM_ERR_INVALID, "filter on %s: bad value kind", c.name.c_str());
+  const bool wasm = wasm_flag && wasm_route(c.dtype, f);
+  const bool range = f.op == QM_OP_BETWEEN || f.op == QM_OP_NOT_BETWEEN;
+  if (is_int(c.dtype)) {
+    IRange r;
+    if (!range) {
+      r = int_range_for(f.op, int_threshold(c.dtype, f.value, wasm));
+    } else {
+      if (f.value2.kind != QM_VAL_NUMBER && f.value2.kind != QM_VAL_BIGINT)
+        return set_err(ctx, QM_ERR_INVALID, "filter on %s: bad BETWEEN bound", c.name.c_str());
+      Thr a = int_threshold(c.dtype, f.value, wasm), b = int_threshold(c.dtype, f.value2, wasm);
+      if (f.op == QM_OP_BETWEEN) {  // v >= a && v <= b (inclusive)
+        if (a.nan || b.nan) r.konst = 0;
+        else { r.lo = a.ce; r.hi = b.fl; }
+      } else {                      // v < a || v > b
+        if (a.nan && b.nan) r.konst = 0;
+        else if (a.nan) { r.lo = b.fl + 1; r.hi = BIG * 4; }
+        else if (b.nan) { r.lo = -BIG * 4; r.hi = a.ce - 1; }
+        else { r.lo = a.ce; r.hi = b.fl; r.negate = true; }
+      }
+    }
+    lower_irange(r, c.dtype, t);
+    if (wasm) t.null_pass = range_test0(r) ? 1 : 0;  // WASM reads a NULL cell as 0
+    return QM_OK;
+  }
+  // float column (JS number cells)
+  if (!range) {
+    if (f.value.kind == QM_VAL_BIGINT) {
+      t.kind = QT_FBIG;
+      t.op = f.op;
+      t.lo = f.value.big;
+      return QM_OK;
+    }
+    t.kind = QT_FCMP;
+    t.op = f.op;
+    t.f0 = f.value.num;
+    if (wasm) t.null_pass = fcmp_host(0.0, f.op, t.f0) ? 1 : 0;
+    return QM_OK;
+  }
+  if (f.value.kind != QM_VAL_NUMBER || f.value2.kind != QM_VAL_NUMBER)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "BETWEEN with bigint bounds on float column %s", c.name.c_str());
+  t.kind = f.op == QM_OP_BETWEEN ? QT_FBETWEEN : QT_FNBETWEEN;
+  t.f0 = f.value.num;
+  t.f1 = f.value2.num;
+  if (wasm) {
+    bool p = f.op == QM_OP_BETWEEN ? (0.0 >= t.f0 && 0.0 <= t.f1) : (0.0 < t.f0 || 0.0 > t.f1);
+    t.null_pass = p ? 1 : 0;
+  }
+  return QM_OK;
+}
+
+typedef const ColView *(*Resolver)(void *env, const char *name);
+
+struct ColEnv {
+  std::vector<ColView> views;
+  const ColView *find(const char *name) const {
+    for (auto &v : views)
+      if (v.col->name == name) return &v;
+    return nullptr;
+  }
+};
+
+int build_pred(qm_ctx *ctx, const qm_query *q, const ColEnv &env, qm_pred &P, int64_t &bytes_per_row,
+               std::vector<const DevCol *> &touched) {
+  memset(&P, 0, sizeof P);
+  const bool wasm = (q->flags & QM_FLAG_WASM_SCAN_SEMANTICS) != 0;
+  int nt = 0;
+  if (q->n_filters < 0 || q->n_or_groups < 0) return set_err(ctx, QM_ERR_INVALID, "negative filter count");
+  auto add = [&](const qm_filter &f) -> int {
+    if (nt >= QM_MAX_TERMS) return set_err(ctx, QM_ERR_UNSUPPORTED, "more than %d filter terms", QM_MAX_TERMS);
+    if (!f.column) return set_err(ctx, QM_ERR_INVALID, "filter without a column");
+    const ColView *cv = env.find(f.column);
+    if (!cv) return set_err(ctx, QM_ERR_NOT_FOUND, "unknown filter column %s", f.column);
+    int rc = lower_filter(ctx, f, *cv, wasm, P.t[nt]);
+    if (rc) return rc;
+    if (std::find(touched.begin(), touched.end(), cv->col) == touched.end()) touched.push_back(cv->col);
+    nt++;
+    return QM_OK;
+  };
+  for (int i = 0; i < q->n_filters; i++) {
+    int rc = add(q->filters[i]);
+    if (rc) return rc;
+  }
+  P.n_and = nt;
+  int off = 0;
+  for (int g = 0; g < q->n_or_groups; g++) {
+    int sz = q->or_group_sizes[g];
+    if (sz < 0) return set_err(ctx, QM_ERR_INVALID, "negative OR group size");
+    for (int i = 0; i < sz; i++) {
+      int rc = add(q->or_filters[off + i]);
+      if (rc) return rc;
+    }
+    off += sz;
+    P.group_end[g] = nt;
+  }
+  P.n_groups = q->n_or_groups;
+  if (P.n_groups > QM_MAX_TERMS) return set_err(ctx, QM_ERR_UNSUPPORTED, "too many OR groups");
+  (void)bytes_per_row;
+  return QM_OK;
+}
+
+const char *agg_name(int fn) {
+  static const char *n[] = {"sum", "avg", "min", "max", "count"};
+  return (fn >= 0 && fn <= 4) ? n[fn] : "?";
+}
+
+// Builds the key spec (without the mode), the accumulators and the outputs.
+int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::vector<const DevCol *> &touched) {
+  qm_keyspec &K = pl.key;
+  qm_aggspec &A = pl.agg;
+  memset(&K, 0, sizeof K);
+  memset(&A, 0, sizeof A);
+  pl.meta.clear();
+  if (q->n_group_by < 0 || q->n_aggregates < 0) return set_err(ctx, QM_ERR_INVALID, "negative counts");
+  if (q->n_group_by > 2) return set_err(ctx, QM_ERR_UNSUPPORTED, "GROUP BY over more than 2 columns");
+  const DevCol *kc[2] = {nullptr, nullptr};
+  for (int i = 0; i < q->n_group_by; i++) {
+    if (!q->group_by[i]) return set_err(ctx, QM_ERR_INVALID, "group column without a name");
+    const ColView *cv = env.find(q->group_by[i]);
+    if (!cv) return set_err(ctx, QM_ERR_NOT_FOUND, "unknown group column %s", q->group_by[i]);
+    kc[i] = cv->col;
+    if (std::find(touched.begin(), touched.end(), cv->col) == touched.end()) touched.push_back(cv->col);
+  }
+  K.n_cols = q->n_group_by;
+  if (K.n_cols == 2) {
+    if (kc[0]->dtype != QM_I32 || kc[1]->dtype != QM_I32 || kc[0]->nulls || kc[1]->nulls)
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "two-column GROUP BY needs two non-null int32 columns");
+  }
+  for (int i = 0; i < K.n_cols; i++) {
+    K.data[i] = kc[i]->data;
+    K.nulls[i] = kc[i]->nulls;
+    K.dtype[i] = kc[i]->dtype;
+  }
+  // accumulators
+  auto add_acc = [&](int kind, int vcol, int wide) -> int {
+    for (int i = 0; i < A.n_accs; i++)
+      if (A.acc[i].kind == kind && A.acc[i].vcol == vcol) return i;
+    if (A.n_accs >= QM_MAX_ACCS) return -1;
+    int width = (kind == QA_ISUM || kind == QA_FSUM) ? 2 : 1;
+    if (A.n_words + width > QM_MAX_WORDS) return -1;
+    qm_acc &a = A.acc[A.n_accs];
+    a.kind = kind;
+    a.vcol = vcol;
+    a.word = A.n_words;
+    a.wide = wide;
+    uint64_t init = 0;
+    switch (kind) {
+      case QA_FIRST: case QA_FZERO: init = ~0ULL; break;
+      case QA_IMIN: init = (uint64_t)INT64_MAX; break;
+      case QA_IMAX: init = (uint64_t)INT64_MIN; break;
+      case QA_FMIN: init = (uint64_t)qm_f2ord_host(INFINITY); break;
+      case QA_FMAX: init = (uint64_t)qm_f2ord_host(-INFINITY); break;
+      default: init = 0;
+    }
+    for (int w = 0; w < width; w++) A.init[A.n_words + w] = init;
+    A.n_words += width;
+    return A.n_accs++;
+  };
+  A.acc_count = add_acc(QA_COUNT, -1, 0);
+  pl.ordered = (q->flags & QM_FLAG_UNORDERED) == 0;
+  A.acc_first = pl.ordered && K.n_cols > 0 ? add_acc(QA_FIRST, -1, 0) : -1;
+  std::vector<const DevCol *> vcols;
+  auto vcol_of = [&](const DevCol *c) -> int {
+    for (size_t i = 0; i < vcols.size(); i++)
+      if (vcols[i] == c) return (int)i;
+    if ((int)vcols.size() >= QM_MAX_VCOLS) return -1;
+    vcols.push_back(c);
+    A.vcol[vcols.size() - 1].data = c->data;
+    A.vcol[vcols.size() - 1].nulls = c->nulls;
+    A.vcol[vcols.size() - 1].dtype = c->dtype;
+    return (int)vcols.size() - 1;
+  };
+  // outputs: keys, then aggregates in query order
+  qm_outspec &O = pl.outs;
+  memset(&O, 0, sizeof O);
+  for (int i = 0; i < K.n_cols; i++) {
+    qm_out &o = O.o[O.n_out++];
+    o.kind = QO_KEY;
+    o.src = i;
+    o.dtype = kc[i]->dtype == QM_F32 ? QM_F64 : kc[i]->dtype;
+    o.zero_word = -1;
+    pl.meta.push_back({q->group_by[i], o.dtype, 1, kc[i]->nulls != nullptr});
+  }
+  if (K.n_cols + q->n_aggregates > QM_MAX_OUT) return set_err(ctx, QM_ERR_UNSUPPORTED, "too many output columns");
+  for (int i = 0; i < q->n_aggregates; i++) {
+    const qm_aggregate &ag = q->aggregates[i];
+    if (!ag.column) return set_err(ctx, QM_ERR_INVALID, "aggregate without a column");
+    if (ag.fn < QM_AGG_SUM || ag.fn > QM_AGG_COUNT)
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "aggregate fn %d is not on the GPU path", ag.fn);
+    std::string name = ag.alias ? std::string(ag.alias) : std::string(agg_name(ag.fn)) + "_" + ag.column;
+    qm_out &o = O.o[O.n_out++];
+    memset(&o, 0, sizeof o);
+    o.zero_word = -1;
+    o.nn_word = A.acc[A.acc_count].word;
+    const bool star = strcmp(ag.column, "*") == 0;
+    if (star) {
+      if (ag.fn != QM_AGG_COUNT) return set_err(ctx, QM_ERR_INVALID, "%s(*) is not an aggregate", agg_name(ag.fn));
+      o.kind = QO_COUNT;
+      o.dtype = QM_I64;
+      o.word = A.acc[A.acc_count].word;
+      pl.meta.push_back({name, o.dtype, 0, false});
+      continue;
+    }
+    const ColView *cv = env.find(ag.column);
+    if (!cv) return set_err(ctx, QM_ERR_NOT_FOUND, "unknown aggregate column %s", ag.column);
+    const DevCol *c = cv->col;
+    if (std::find(touched.begin(), touched.end(), c) == touched.end()) touched.push_back(c);
+    int vc = vcol_of(c);
+    if (vc < 0) return set_err(ctx, QM_ERR_UNSUPPORTED, "more than %d aggregated columns", QM_MAX_VCOLS);
+    int nn_acc = c->nulls ? add_acc(QA_NN, vc, 0) : A.acc_count;
+    if (nn_acc < 0) return set_err(ctx, QM_ERR_UNSUPPORTED, "too many accumulators");
+    o.nn_word = A.acc[nn_acc].word;
+    int acc = -1;
+    switch (ag.fn) {
+      case QM_AGG_COUNT:
+        o.kind = QO_COUNT;
+        o.dtype = QM_I64;
+        o.word = o.nn_word;
+        break;
+      case QM_AGG_SUM:
+      case QM_AGG_AVG:
+        if (is_int(c->dtype)) {
+          acc = add_acc(QA_ISUM, vc, c->dtype == QM_I64);
+          if (c->dtype == QM_I64) {
+            o.kind = ag.fn == QM_AGG_SUM ? QO_SUM_I128 : QO_AVG_BIG;
+            o.dtype = ag.fn == QM_AGG_SUM ? QM_I128 : QM_F64;
+          } else {
+            o.kind = ag.fn == QM_AGG_SUM ? QO_SUM_I2F : QO_AVG_I2F;
+            o.dtype = QM_F64;
+          }
+        } else {
+          acc = add_acc(QA_FSUM, vc, 0);
+          o.kind = ag.fn == QM_AGG_SUM ? QO_SUM_F : QO_AVG_F;
+          o.dtype = QM_F64;
+        }
+        break;
+      case QM_AGG_MIN:
+      case QM_AGG_MAX:
+        if (is_int(c->dtype)) {
+          acc = add_acc(ag.fn == QM_AGG_MIN ? QA_IMIN : QA_IMAX, vc, 0);
+          o.kind = ag.fn == QM_AGG_MIN ? QO_MIN_I : QO_MAX_I;
+          o.dtype = c->dtype;
+        } else {
+          acc = add_acc(ag.fn == QM_AGG_MIN ? QA_FMIN : QA_FMAX, vc, 0);
+          int z = add_acc(QA_FZERO, vc, 0);
+          if (z < 0) return set_err(ctx, QM_ERR_UNSUPPORTED, "too many accumulators");
+          o.zero_word = A.acc[z].word;
+          o.kind = ag.fn == QM_AGG_MIN ? QO_MIN_F : QO_MAX_F;
+          o.dtype = QM_F64;
+        }
+        break;
+    }
+    if (ag.fn != QM_AGG_COUNT) {
+      if (acc < 0) return set_err(ctx, QM_ERR_UNSUPPORTED, "too many accumulators");
+      o.word = A.acc[acc].word;
+    }
+    pl.meta.push_back({name, o.dtype, 0, ag.fn != QM_AGG_COUNT});
+  }
+  A.n_vcols = (int)vcols.size();
+  return QM_OK;
+}
+
+// ------------------------------------------------------------ execution
+struct Exec {
+  int64_t n_slots = 1;  // QK_DIRECT size / QK_HASH capacity
+  int log2cap = 0;
+  int64_t total_slots = 1;
+  int stride = 1;
+  int local_slots = 0;
+  int local_hash = 0;
+  int dedupe = 1;
+  int strategy = 0;
+};
+
+int64_t special_slots(int mode) { return mode == QK_HASH ? 2 : (mode == QK_DIRECT ? 1 : 0); }
+
+int ilog2_ceil(int64_t x) {
+  int l = 0;
+  while (((int64_t)1 << l) < x) l++;
+  return l;
+}
+
+constexpr size_t LOCAL_BUDGET = 96 * 1024;  // bytes of the block-local table
+
+void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex) {
+  const int words = pl.agg.n_words;
+  ex.stride = 1 + words;
+  ex.total_slots = ex.n_slots + special_slots(pl.key.mode);
+  const int64_t per_slot = (int64_t)words * 8;
+  if (pl.key.mode == QK_NONE) {
+    ex.local_slots = 1;
+    ex.local_hash = 0;
+    ex.dedupe = 1;
+    ex.strategy = 0;
+    return;
+  }
+  if (pl.key.mode == QK_DIRECT && (ex.n_slots + 1) * per_slot <= (int64_t)LOCAL_BUDGET) {
+    ex.local_slots = (int)(ex.n_slots + 1);
+    ex.local_hash = 0;
+    ex.dedupe = 1;
+    ex.strategy = 0;
+    return;
+  }
+  if (est_groups <= ((int64_t)1 << 20)) {
+    int L = 1;
+    while ((int64_t)(L * 2) * (per_slot + 8) <= (int64_t)LOCAL_BUDGET) L *= 2;
+    ex.local_slots = L;
+    ex.local_hash = 1;
+    ex.dedupe = 1;
+    ex.strategy = 1;
+    return;
+  }
+  ex.local_slots = 0;
+  ex.local_hash = 0;
+  ex.dedupe = 0;
+  ex.strategy = 2;
+}
+
+std::mutex g_cfg_mu;
+size_t g_cfg_smem = 0;
+
+int scan_blocks(qm_ctx *ctx, size_t smem, int64_t n) {
+  int bps = 1;
+  {
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    size_t want = std::max(smem, g_cfg_smem);
+    if (qm_scan_configure(want, &bps) != cudaSuccess) {
+      cudaGetLastError();
+      bps = 1;
+    }
+    g_cfg_smem = want;
+    if (qm_scan_configure(smem, &bps) != cudaSuccess) {
+      cudaGetLastError();
+      bps = 1;
+    }
+  }
+  if (bps < 1) bps = 1;
+  int64_t tiles = (n + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  int64_t warps = QM_SCAN_THREADS / 32;
+  int64_t need = (tiles + warps - 1) / warps;
+  int64_t blocks = std::min<int64_t>((int64_t)ctx->sm_count * bps, std::max<int64_t>(need, 1));
+  return (int)blocks;
+}
+
+double hll_estimate(const uint32_t *regs) {
+  const int m = 1 << QM_HLL_P;
+  double sum = 0;
+  int zeros = 0;
+  for (int i = 0; i < m; i++) {
+    sum += std::ldexp(1.0, -(int)regs[i]);
+    zeros += regs[i] == 0;
+  }
+  double alpha = 0.7213 / (1.0 + 1.079 / m);
+  double E = alpha * m * (double)m / sum;
+  if (E <= 2.5 * m && zeros > 0) E = m * std::log((double)m / zeros);
+  return E;
+}
+
+// Distinct-key estimate of `n` rows under key spec K (HyperLogLog).
+int estimate_groups(qm_ctx *ctx, const qm_keyspec &K, int64_t n, double *out) {
+  int rc = ensure(ctx, ctx->hll, sizeof(uint32_t) << QM_HLL_P);
+  if (rc) return rc;
+  rc = ensure_host(ctx, ctx->hout, sizeof(uint32_t) << QM_HLL_P);
+  if (rc) return rc;
+  CK(qm_launch_hll(K, n, (uint32_t *)ctx->hll.p, ctx->sm_count, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hout.p, ctx->hll.p, sizeof(uint32_t) << QM_HLL_P, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *out = hll_estimate((const uint32_t *)ctx->hout.p);
+  return QM_OK;
+}
+
+int column_minmax(qm_ctx *ctx, DevCol &c, int64_t n) {
+  if (c.has_minmax) return QM_OK;
+  int rc = ensure(ctx, ctx->counter, 64);
+  if (rc) return rc;
+  rc = ensure_host(ctx, ctx->hstatus, 64);
+  if (rc) return rc;
+  CK(qm_launch_minmax(c.data, c.dtype, c.nulls, n, (long long *)ctx->counter.p, ctx->sm_count, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->counter.p, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  c.mn = ((long long *)ctx->hstatus.p)[0];
+  c.mx = ((long long *)ctx->hstatus.p)[1];
+  c.has_minmax = true;
+  return QM_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ results
+struct qm_result {
+  int64_t n_rows = 0;
+  struct Col {
+    std::string name;
+    int dtype;
+    int is_key;
+    std::vector<uint8_t> data;
+    std::vector<uint8_t> nulls;
+    bool has_nulls = false;
+  };
+  std::vector<Col> cols;
+  qm_stats stats{};
+  std::vector<uint8_t> qmcb;
+  bool qmcb_built = false;
+};
+
+namespace {
+
+// Group table state of one aggregation (one-shot query or a stream of pushes).
+struct GroupTable {
+  Plan pl;
+  Exec ex;
+  DevBuf own;            // streaming aggregations own their table
+  uint64_t *table = nullptr;
+  int64_t rows_done = 0;  // global row index of the next pushed row
+  int64_t groups_upper = 0;
+  int retries = 0;
+  unsigned long long selected = 0;
+  bool scan_pending = false;  // evs0/evs1 bracket a scan not yet timed
+  double scan_ms = 0;         // accumulated scan-kernel time
+};
+
+int read_status(qm_ctx *ctx, qm_status *out) {
+  int rc = ensure_host(ctx, ctx->hstatus, sizeof(qm_status));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->status.p, sizeof(qm_status), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  memcpy(out, ctx->hstatus.p, sizeof(qm_status));
+  return QM_OK;
+}
+
+// After a synchronize: fold the bracketed scan time into the table's total.
+void take_scan_time(qm_ctx *ctx, GroupTable &gt, bool keep) {
+  if (!gt.scan_pending) return;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, ctx->evs0, ctx->evs1) != cudaSuccess) {
+    cudaGetLastError();
+    ms = 0;
+  }
+  gt.scan_pending = false;
+  if (keep) gt.scan_ms += ms;
+}
+
+int init_table(qm_ctx *ctx, GroupTable &gt) {
+  CK(qm_launch_init_table(gt.table, gt.ex.total_slots, gt.ex.stride, gt.pl.key.mode == QK_HASH, gt.pl.agg,
+                          ctx->sm_count, ctx->stream));
+  ctx->launches++;
+  return QM_OK;
+}
+
+void fill_args(const GroupTable &gt, qm_scan_args &a, qm_status *st) {
+  memset(&a, 0, sizeof a);
+  a.pred = gt.pl.pred;
+  a.key = gt.pl.key;
+  a.agg = gt.pl.agg;
+  a.table = gt.table;
+  a.n_slots = gt.ex.n_slots;
+  a.stride = gt.ex.stride;
+  a.log2cap = gt.ex.log2cap;
+  a.local_slots = gt.ex.local_slots;
+  a.local_hash = gt.ex.local_hash;
+  a.dedupe = gt.ex.dedupe;
+  a.max_probe = 1 << 12;
+  a.status = st;
+}
+
+// Finalize the group table into a qm_result (compaction, first-seen order,
+// per-group finalize on the device, one copy back).
+int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far) {
+  const Plan &pl = gt.pl;
+  const Exec &ex = gt.ex;
+  int64_t G = 0;
+  const uint32_t *slots = nullptr;
+  if (pl.key.mode == QK_NONE) {
+    G = 1;  // ungrouped: exactly one row (src/partial-agg.ts:313-320)
+  } else {
+    int rc;
+    if ((rc = ensure(ctx, ctx->keys, ex.total_slots * 8)) || (rc = ensure(ctx, ctx->slots, ex.total_slots * 4)) ||
+        (rc = ensure(ctx, ctx->counter, 64)) || (rc = ensure_host(ctx, ctx->hstatus, 64)))
+      return rc;
+    CK(cudaMemsetAsync(ctx->counter.p, 0, 8, ctx->stream));
+    const int first_word = pl.agg.acc_first >= 0 ? pl.agg.acc[pl.agg.acc_first].word : -1;
+    CK(qm_launch_compact(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word,
+                         (uint64_t *)ctx->keys.p, (uint32_t *)ctx->slots.p, (unsigned long long *)ctx->counter.p,
+                         ctx->sm_count, ctx->stream));
+    ctx->launches++;
+    CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->counter.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    G = (int64_t)*(unsigned long long *)ctx->hstatus.p;
+    slots = (const uint32_t *)ctx->slots.p;
+    if (G > 1 && first_word >= 0) {
+      if ((rc = ensure(ctx, ctx->keys2, G * 8)) || (rc = ensure(ctx, ctx->slots2, G * 4))) return rc;
+      int end_bit = 1;
+      while (end_bit < 64 && ((uint64_t)1 << end_bit) <= (uint64_t)std::max<int64_t>(gt.rows_done, 1)) end_bit++;
+      size_t tb = 0;
+      CK(qm_sort_pairs(nullptr, &tb, (uint64_t *)ctx->keys.p, (uint64_t *)ctx->keys2.p, (uint32_t *)ctx->slots.p,
+                       (uint32_t *)ctx->slots2.p, G, end_bit, ctx->stream));
+      if ((rc = ensure(ctx, ctx->sort_temp, tb))) return rc;
+      tb = ctx->sort_temp.bytes;
+      CK(qm_sort_pairs(ctx->sort_temp.p, &tb, (uint64_t *)ctx->keys.p, (uint64_t *)ctx->keys2.p,
+                       (uint32_t *)ctx->slots.p, (uint32_t *)ctx->slots2.p, G, end_bit, ctx->stream));
+      slots = (const uint32_t *)ctx->slots2.p;
+    }
+  }
+  // output buffer layout
+  qm_outspec O = pl.outs;
+  size_t off = 0;
+  const size_t null_words_bytes = (size_t)((G + 31) / 32) * 4;
+  for (int k = 0; k < O.n_out; k++) {
+    O.o[k].offset = (int64_t)off;
+    off += ((size_t)G * dtype_size(O.o[k].dtype) + 15) & ~(size_t)15;
+    if (pl.meta[k].nullable) {
+      O.o[k].null_offset = (int64_t)off;
+      off += (null_words_bytes + 15) & ~(size_t)15;
+    } else {
+      O.o[k].null_offset = -1;
+    }
+  }
+  int rc;
+  if ((rc = ensure(ctx, ctx->out, off + 16)) || (rc = ensure_host(ctx, ctx->hout, off + 16))) return rc;
+  CK(cudaMemsetAsync(ctx->out.p, 0, off + 16, ctx->stream));
+  CK(qm_launch_emit(gt.table, ex.stride, slots, G, pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p,
+                    ctx->sm_count, ctx->stream));
+  if (G > 0) ctx->launches++;
+  CK(cudaMemcpyAsync(ctx->hout.p, ctx->out.p, off, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float tail_ms = 0;
+  cudaEventElapsedTime(&tail_ms, ctx->ev0, ctx->ev1);
+
+  qm_result *R = new qm_result();
+  R->n_rows = G;
+  const uint8_t *h = (const uint8_t *)ctx->hout.p;
+  for (int k = 0; k < O.n_out; k++) {
+    qm_result::Col c;
+    c.name = pl.meta[k].name;
+    c.dtype = O.o[k].dtype;
+    c.is_key = pl.meta[k].is_key;
+    size_t bytes = (size_t)G * dtype_size(c.dtype);
+    c.data.assign(h + O.o[k].offset, h + O.o[k].offset + bytes);
+    if (O.o[k].null_offset >= 0) {
+      size_t nb = (size_t)((G + 7) / 8);
+      c.nulls.assign(h + O.o[k].null_offset, h + O.o[k].null_offset + nb);
+      for (uint8_t b : c.nulls)
+        if (b) {
+          c.has_nulls = true;
+          break;
+        }
+    }
+    R->cols.push_back(std::move(c));
+  }
+  R->stats.groups = G;
+  R->stats.strategy = ex.strategy;
+  R->stats.table_capacity = ilog2_ceil(std::max<int64_t>(ex.n_slots, 1));
+  R->stats.retries = gt.retries;
+  R->stats.rows_selected = (int64_t)gt.selected;
+  R->stats.device_ms = (double)(scan_ms_so_far > tail_ms ? scan_ms_so_far : tail_ms);
+  R->stats.scan_ms = gt.scan_ms;
+  R->stats.launches = ctx->launches;
+  *out = R;
+  return QM_OK;
+}
+
+// Sizes the table for `est_groups` groups and allocates it (from ctx for a
+// one-shot run, owned for a stream).
+int setup_table(qm_ctx *ctx, GroupTable &gt, int64_t est_groups, int64_t direct_size, bool owned) {
+  Plan &pl = gt.pl;
+  Exec &ex = gt.ex;
+  if (pl.key.mode == QK_NONE) {
+    ex.n_slots = 1;
+  } else if (pl.key.mode == QK_DIRECT) {
+    ex.n_slots = direct_size;
+  } else {
+    int64_t want = std::max<int64_t>(1024, est_groups * 2 + est_groups / 8);
+    ex.log2cap = ilog2_ceil(want);
+    if (ex.log2cap > 31) ex.log2cap = 31;
+    ex.n_slots = (int64_t)1 << ex.log2cap;
+  }
+  choose_layout(pl, est_groups, ex);
+  size_t bytes = (size_t)ex.total_slots * ex.stride * 8;
+  DevBuf &buf = owned ? gt.own : ctx->table;
+  int rc = ensure(ctx, buf, bytes);
+  if (rc) return rc;
+  gt.table = (uint64_t *)buf.p;
+  return init_table(ctx, gt);
+}
+
+int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel) {
+  qm_scan_args a;
+  fill_args(gt, a, (qm_status *)ctx->status.p);
+  a.n = n;
+  a.sel = sel;
+  a.row_offset = gt.rows_done;
+  size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words);
+  int blocks = scan_blocks(ctx, smem, n);
+  CK(cudaEventRecord(ctx->evs0, ctx->stream));
+  CK(qm_launch_scan(a, blocks, smem, ctx->stream));
+  CK(cudaEventRecord(ctx->evs1, ctx->stream));
+  if (n > 0) ctx->launches++;
+  gt.scan_pending = true;
+  return QM_OK;
+}
+
+struct TableSource {  // a registered table's columns as the planner sees them
+  ColEnv env;
+};
+
+int plan_query(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl) {
+  if (!q) return set_err(ctx, QM_ERR_INVALID, "null query");
+  std::vector<const DevCol *> touched;
+  int64_t bpr = 0;
+  int rc = build_pred(ctx, q, env, pl.pred, bpr, touched);
+  if (rc) return rc;
+  rc = build_agg(ctx, q, env, pl, touched);
+  if (rc) return rc;
+  pl.bytes_per_row = 0;
+  for (auto *c : touched) pl.bytes_per_row += (int64_t)dtype_size(c->dtype);
+  return QM_OK;
+}
+
+}  // namespace
+
+
+// ================================================================== C ABI
+extern "C" {
+
+const char *qm_version(void) { return "querymode-b200 0.1 (sm_100a)"; }
+
+int qm_ctx_create(int32_t device, qm_ctx **out) {
+  if (!out) return QM_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return QM_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return QM_ERR_INVALID;
+  qm_ctx *ctx = new qm_ctx();
+  ctx->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  ctx->stream = ctx->own_stream;
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->evs0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->evs1);
+  cudaDeviceProp prop;
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return QM_ERR_CUDA;
+  }
+  ctx->sm_count = prop.multiProcessorCount;
+  ctx->hbm_bytes = (int64_t)prop.totalGlobalMem;
+  if (ensure(ctx, ctx->status, sizeof(qm_status))) {
+    delete ctx;
+    return QM_ERR_OOM;
+  }
+  *out = ctx;
+  return QM_OK;
+}
+
+int qm_ctx_destroy(qm_ctx *ctx) {
+  if (!ctx) return QM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  DevBuf *bufs[] = {&ctx->table, &ctx->status, &ctx->keys, &ctx->slots, &ctx->keys2, &ctx->slots2,
+                    &ctx->sort_temp, &ctx->counter, &ctx->out, &ctx->hll, &ctx->masks, &ctx->counts,
+                    &ctx->offsets, &ctx->sel_out, &ctx->sel_in};
+  for (DevBuf *b : bufs) release(*b);
+  for (auto &b : ctx->staged) release(b);
+  if (ctx->hout.p) cudaFreeHost(ctx->hout.p);
+  if (ctx->hstatus.p) cudaFreeHost(ctx->hstatus.p);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->evs0) cudaEventDestroy(ctx->evs0);
+  if (ctx->evs1) cudaEventDestroy(ctx->evs1);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return QM_OK;
+}
+
+int qm_ctx_set_stream(qm_ctx *ctx, void *stream) {
+  if (!ctx) return QM_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return QM_OK;
+}
+
+const char *qm_ctx_last_error(const qm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int qm_ctx_device_info(const qm_ctx *ctx, int32_t *sm_count, int64_t *hbm_bytes) {
+  if (!ctx) return QM_ERR_INVALID;
+  if (sm_count) *sm_count = ctx->sm_count;
+  if (hbm_bytes) *hbm_bytes = ctx->hbm_bytes;
+  return QM_OK;
+}
+
+int qm_table_create(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column *cols, qm_table **out) {
+  if (!ctx || !out || n_rows < 0 || n_cols < 0 || (n_cols > 0 && !cols))
+    return set_err(ctx, QM_ERR_INVALID, "qm_table_create: bad arguments");
+  if (n_rows > 0xffffffffLL)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "tables are limited to 2^32-1 rows (QMCB rowCount is u32)");
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  qm_table *t = new qm_table();
+  t->ctx = ctx;
+  t->n_rows = n_rows;
+  for (int i = 0; i < n_cols; i++) {
+    for (auto &c : t->cols)
+      if (c.name == cols[i].name) {
+        qm_table_destroy(t);
+        return set_err(ctx, QM_ERR_INVALID, "duplicate column %s", cols[i].name);
+      }
+    DevCol c;
+    int rc = make_col(ctx, n_rows, cols[i], c);
+    if (rc) {
+      free_col(c);
+      qm_table_destroy(t);
+      return rc;
+    }
+    t->cols.push_back(c);
+  }
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    qm_table_destroy(t);
+    return set_err(ctx, QM_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+  }
+  *out = t;
+  return QM_OK;
+}
+
+int qm_table_from_qmcb(qm_ctx *ctx, const uint8_t *buf, size_t len, qm_table **out) {
+  if (!ctx || !buf || !out) return set_err(ctx, QM_ERR_INVALID, "qm_table_from_qmcb: bad arguments");
+  // decodeColumnarBatch layout (src/columnar.ts:438-516)
+  if (len < 10) return set_err(ctx, QM_ERR_INVALID, "QMCB buffer shorter than its header");
+  uint32_t magic, rows;
+  uint16_t ncol;
+  memcpy(&magic, buf, 4);
+  memcpy(&rows, buf + 4, 4);
+  memcpy(&ncol, buf + 8, 2);
+  if (magic != 0x42434D51u) return set_err(ctx, QM_ERR_INVALID, "bad QMCB magic");
+  struct D {
+    std::string name;
+    int dtype;
+    bool nulls;
+  };
+  std::vector<D> descs;
+  size_t pos = 10;
+  for (int c = 0; c < ncol; c++) {
+    if (pos + 2 > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB descriptor");
+    uint16_t nl;
+    memcpy(&nl, buf + pos, 2);
+    pos += 2;
+    if (pos + nl + 2 > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB descriptor");
+    D d;
+    d.name.assign((const char *)buf + pos, nl);
+    pos += nl;
+    d.dtype = buf[pos++];
+    d.nulls = buf[pos++] != 0;
+    descs.push_back(d);
+  }
+  std::vector<qm_column> cols;
+  std::vector<std::string> names;
+  names.reserve(descs.size());
+  for (auto &d : descs) {
+    const uint8_t *nb = nullptr;
+    if (d.nulls) {
+      size_t nbl = ((size_t)rows + 7) / 8;
+      if (pos + nbl > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB null bitmap");
+      nb = buf + pos;
+      pos += nbl;
+    }
+    size_t sz = 0;
+    switch (d.dtype) {
+      case QM_F64: case QM_I64: sz = (size_t)rows * 8; break;
+      case QM_I32: case QM_F32: sz = (size_t)rows * 4; break;
+      case 2: {  // UTF8: total length, offsets, bytes
+        if (pos + 4 > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB utf8 column");
+        uint32_t tl;
+        memcpy(&tl, buf + pos, 4);
+        sz = 4 + ((size_t)rows + 1) * 4 + tl;
+        break;
+      }
+      case 3: sz = ((size_t)rows + 7) / 8; break;  // BOOL
+      case 4: {                                     // F32VEC: dim, data
+        if (pos + 4 > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB vector column");
+        uint32_t dim;
+        memcpy(&dim, buf + pos, 4);
+        sz = 4 + (size_t)rows * dim * 4;
+        break;
+      }
+      default: sz = 0;
+    }
+    if (pos + sz > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB column %s", d.name.c_str());
+    if (valid_dtype(d.dtype)) {
+      names.push_back(d.name);
+      qm_column c;
+      c.name = names.back().c_str();
+      c.dtype = d.dtype;
+      c.on_device = 0;
+      c.data = buf + pos;
+      c.null_bitmap = nb;
+      cols.push_back(c);
+    }
+    pos += sz;
+  }
+  return qm_table_create(ctx, (int64_t)rows, (int32_t)cols.size(), cols.data(), out);
+}
+
+int qm_table_destroy(qm_table *t) {
+  if (!t) return QM_OK;
+  if (t->ctx) cudaSetDevice(t->ctx->device);
+  if (t->ctx) cudaStreamSynchronize(t->ctx->stream);
+  for (auto &c : t->cols) free_col(c);
+  delete t;
+  return QM_OK;
+}
+
+int qm_table_num_rows(const qm_table *t, int64_t *out) {
+  if (!t || !out) return QM_ERR_INVALID;
+  *out = t->n_rows;
+  return QM_OK;
+}
+
+int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_result **out) {
+  if (!ctx || !table || !q || !out) return set_err(ctx, QM_ERR_INVALID, "qm_query_run: bad arguments");
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  qm_table *t = const_cast<qm_table *>(table);
+  ctx->launches = 0;
+  ColEnv env;
+  for (auto &c : t->cols) env.views.push_back({&c, t->n_rows});
+  GroupTable gt;
+  int rc = plan_query(ctx, q, env, gt.pl);
+  if (rc) return rc;
+  Plan &pl = gt.pl;
+  // key mode and size
+  int64_t est = 1, direct_size = 0;
+  if (pl.key.n_cols == 0) {
+    pl.key.mode = QK_NONE;
+  } else {
+    const ColView *kv = env.find(q->group_by[0]);
+    DevCol &kc = *const_cast<DevCol *>(kv->col);
+    bool direct = false;
+    if (pl.key.n_cols == 1 && is_int(kc.dtype)) {
+      if ((rc = column_minmax(ctx, kc, t->n_rows))) return rc;
+      if (kc.mx >= kc.mn) {
+        unsigned long long range = (unsigned long long)kc.mx - (unsigned long long)kc.mn + 1ULL;
+        if (range != 0 && range <= (1ULL << 25) && (int64_t)range <= std::max<int64_t>(4 * t->n_rows, 1 << 16)) {
+          direct = true;
+          direct_size = (int64_t)range;
+          pl.key.base = kc.mn;
+        }
+      } else {
+        direct = true;  // no non-null key: only the NULL slot is used
+        direct_size = 1;
+        pl.key.base = 0;
+      }
+    }
+    if (direct) {
+      pl.key.mode = QK_DIRECT;
+      est = direct_size;
+      if (!kc.has_hll && direct_size > (1 << 16)) {
+        qm_keyspec K = pl.key;
+        K.mode = QK_HASH;
+        double e;
+        if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
+        kc.hll = e;
+        kc.has_hll = true;
+      }
+      if (kc.has_hll) est = std::min<int64_t>(est, (int64_t)(kc.hll * 1.05) + 16);
+    } else {
+      pl.key.mode = QK_HASH;
+      if (pl.key.n_cols == 1 && kc.has_hll) {
+        est = (int64_t)(kc.hll * 1.05) + 16;
+      } else {
+        qm_keyspec K = pl.key;
+        double e;
+        if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
+        est = (int64_t)(e * 1.05) + 16;
+        if (pl.key.n_cols == 1) {
+          kc.hll = e;
+          kc.has_hll = true;
+        }
+      }
+      est = std::min<int64_t>(est, std::max<int64_t>(t->n_rows, 1));
+    }
+  }
+  gt.rows_done = 0;
+  for (int attempt = 0;; attempt++) {
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((rc = setup_table(ctx, gt, est, direct_size, false))) return rc;
+    if ((rc = run_scan(ctx, gt, t->n_rows, nullptr))) return rc;
+    qm_status st;
+    if ((rc = read_status(ctx, &st))) return rc;
+    take_scan_time(ctx, gt, st.error == QM_DEV_OK);
+    if (st.error == QM_DEV_OK) {
+      gt.selected = st.rows_selected;
+      break;
+    }
+    if (attempt >= 4) return set_err(ctx, QM_ERR_CUDA, "group table overflow after %d regrowths", attempt);
+    gt.retries++;
+    if (st.error == QM_DEV_RANGE || pl.key.mode == QK_DIRECT) {
+      pl.key.mode = QK_HASH;
+    }
+    est = std::max<int64_t>(est * 4, (int64_t)st.groups_inserted * 2);
+  }
+  gt.rows_done = t->n_rows;
+  rc = finish_table(ctx, gt, out, 0.f);
+  if (rc) return rc;
+  (*out)->stats.rows_scanned = t->n_rows;
+  (*out)->stats.bytes_scanned = pl.bytes_per_row * t->n_rows;
+  return QM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ streaming
+struct qm_agg {
+  qm_ctx *ctx = nullptr;
+  std::vector<std::string> strs;  // owned copies of every name in the query
+  std::vector<qm_filter> filters, or_filters;
+  std::vector<int32_t> or_sizes;
+  std::vector<const char *> group_by;
+  std::vector<qm_aggregate> aggs;
+  qm_query q{};
+  GroupTable gt;
+  bool planned = false;
+  std::vector<std::pair<std::string, int>> schema;
+  double device_ms = 0;
+  bool failed = false;
+};
+
+namespace {
+
+const char *keep_str(qm_agg *a, const char *s) {
+  if (!s) return nullptr;
+  a->strs.emplace_back(s);
+  return nullptr;
+}
+
+// Stage one batch's columns on the device: host columns are copied into
+// grow-only per-column buffers of the context, null bitmaps into word-padded
+// buffers.  Views point at the staged copies.
+int stage_batch(qm_ctx *ctx, int64_t n, int32_t n_cols, const qm_column *cols, std::vector<DevCol> &out) {
+  out.clear();
+  if ((int)ctx->staged.size() < 2 * n_cols) ctx->staged.resize(2 * n_cols);
+  for (int i = 0; i < n_cols; i++) {
+    const qm_column &c = cols[i];
+    if (!c.name) return set_err(ctx, QM_ERR_INVALID, "column without a name");
+    if (!valid_dtype(c.dtype)) return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dtype %d is not numeric", c.name, c.dtype);
+    if (n > 0 && !c.data) return set_err(ctx, QM_ERR_INVALID, "column %s: no data", c.name);
+    DevCol d;
+    d.name = c.name;
+    d.dtype = c.dtype;
+    const size_t bytes = (size_t)n * dtype_size(c.dtype);
+    if (c.on_device) {
+      d.data = const_cast<void *>(c.data);
+    } else {
+      int rc = ensure(ctx, ctx->staged[2 * i], bytes + 16);
+      if (rc) return rc;
+      if (bytes) CK(cudaMemcpyAsync(ctx->staged[2 * i].p, c.data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      d.data = ctx->staged[2 * i].p;
+    }
+    if (c.null_bitmap) {
+      const size_t words = (size_t)((n + 31) / 32) + 1;
+      int rc = ensure(ctx, ctx->staged[2 * i + 1], words * 4);
+      if (rc) return rc;
+      CK(cudaMemsetAsync(ctx->staged[2 * i + 1].p, 0, words * 4, ctx->stream));
+      if (n > 0)
+        CK(cudaMemcpyAsync(ctx->staged[2 * i + 1].p, c.null_bitmap, (size_t)((n + 7) / 8),
+                           c.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+      d.nulls = (uint32_t *)ctx->staged[2 * i + 1].p;
+    }
+    out.push_back(d);
+  }
+  return QM_OK;
+}
+
+int stage_selection(qm_ctx *ctx, const uint32_t *sel, int64_t n_sel, const uint32_t **dsel) {
+  *dsel = nullptr;
+  if (!sel) return QM_OK;
+  int rc = ensure(ctx, ctx->sel_in, (size_t)n_sel * 4 + 16);
+  if (rc) return rc;
+  cudaPointerAttributes at;
+  bool on_dev = cudaPointerGetAttributes(&at, sel) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+  cudaGetLastError();
+  if (on_dev) {
+    *dsel = sel;
+    return QM_OK;
+  }
+  if (n_sel) CK(cudaMemcpyAsync(ctx->sel_in.p, sel, (size_t)n_sel * 4, cudaMemcpyHostToDevice, ctx->stream));
+  *dsel = (const uint32_t *)ctx->sel_in.p;
+  return QM_OK;
+}
+
+// Grow a streaming hash table so that `upper` groups keep the load <= ~0.5.
+int grow_table(qm_ctx *ctx, GroupTable &gt, int64_t upper) {
+  Exec &ex = gt.ex;
+  if (gt.pl.key.mode != QK_HASH || upper * 2 + upper / 8 <= ex.n_slots) return QM_OK;
+  Exec nx = ex;
+  nx.log2cap = ilog2_ceil(std::max<int64_t>(1024, upper * 2 + upper / 8));
+  if (nx.log2cap > 31) return set_err(ctx, QM_ERR_OOM, "group table would exceed 2^31 slots");
+  nx.n_slots = (int64_t)1 << nx.log2cap;
+  nx.total_slots = nx.n_slots + 2;
+  DevBuf nb;
+  int rc = ensure(ctx, nb, (size_t)nx.total_slots * nx.stride * 8);
+  if (rc) return rc;
+  GroupTable tmp;
+  tmp.pl = gt.pl;
+  tmp.ex = nx;
+  tmp.table = (uint64_t *)nb.p;
+  if ((rc = init_table(ctx, tmp))) {
+    release(nb);
+    return rc;
+  }
+  CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+  CK(qm_launch_rehash(gt.table, ex.n_slots, ex.stride, gt.pl.agg.acc[gt.pl.agg.acc_count].word, tmp.table,
+                      nx.log2cap, (qm_status *)ctx->status.p, ctx->sm_count, ctx->stream));
+  // the two reserved slots (sentinel-valued key, NULL key) move as they are
+  CK(cudaMemcpyAsync(tmp.table + nx.n_slots * nx.stride, gt.table + ex.n_slots * ex.stride,
+                     (size_t)2 * ex.stride * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  qm_status st;
+  if ((rc = read_status(ctx, &st))) {
+    release(nb);
+    return rc;
+  }
+  if (st.error) {
+    release(nb);
+    return set_err(ctx, QM_ERR_CUDA, "rehash overflow");
+  }
+  release(gt.own);
+  gt.own = nb;
+  gt.table = tmp.table;
+  // local-table choice may change with the new size
+  choose_layout(gt.pl, upper, nx);
+  gt.ex = nx;
+  return QM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qm_agg_begin(qm_ctx *ctx, const qm_query *q, qm_agg **out) {
+  if (!ctx || !q || !out) return set_err(ctx, QM_ERR_INVALID, "qm_agg_begin: bad arguments");
+  *out = nullptr;
+  qm_agg *a = new qm_agg();
+  a->ctx = ctx;
+  // deep copy (names live in a->strs; reserve so c_str() stays valid)
+  int n_or = 0;
+  for (int g = 0; g < q->n_or_groups; g++) n_or += q->or_group_sizes[g];
+  a->strs.reserve(2 + q->n_filters + n_or + q->n_group_by + 2 * q->n_aggregates);
+  auto dup = [&](const char *s) -> const char * {
+    if (!s) return nullptr;
+    a->strs.emplace_back(s);
+    return a->strs.back().c_str();
+  };
+  for (int i = 0; i < q->n_filters; i++) {
+    qm_filter f = q->filters[i];
+    f.column = dup(f.column);
+    a->filters.push_back(f);
+  }
+  for (int i = 0; i < n_or; i++) {
+    qm_filter f = q->or_filters[i];
+    f.column = dup(f.column);
+    a->or_filters.push_back(f);
+  }
+  for (int g = 0; g < q->n_or_groups; g++) a->or_sizes.push_back(q->or_group_sizes[g]);
+  for (int i = 0; i < q->n_group_by; i++) a->group_by.push_back(dup(q->group_by[i]));
+  for (int i = 0; i < q->n_aggregates; i++) {
+    qm_aggregate ag = q->aggregates[i];
+    ag.column = dup(ag.column);
+    ag.alias = dup(ag.alias);
+    a->aggs.push_back(ag);
+  }
+  a->q = *q;
+  a->q.filters = a->filters.data();
+  a->q.or_filters = a->or_filters.data();
+  a->q.or_group_sizes = a->or_sizes.data();
+  a->q.group_by = a->group_by.data();
+  a->q.aggregates = a->aggs.data();
+  (void)keep_str;
+  *out = a;
+  return QM_OK;
+}
+
+int qm_agg_push(qm_agg *a, int64_t n_rows, int32_t n_cols, const qm_column *cols, const uint32_t *selection,
+                int64_t n_selected) {
+  if (!a) return QM_ERR_INVALID;
+  qm_ctx *ctx = a->ctx;
+  if (a->failed) return set_err(ctx, QM_ERR_INVALID, "aggregation already failed");
+  if (n_rows < 0 || n_cols < 0 || (n_cols > 0 && !cols) || (selection && n_selected < 0))
+    return set_err(ctx, QM_ERR_INVALID, "qm_agg_push: bad arguments");
+  if (n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
+  cudaSetDevice(ctx->device);
+  // schema is fixed by the first push
+  if (!a->planned) {
+    for (int i = 0; i < n_cols; i++) a->schema.push_back({cols[i].name ? cols[i].name : "", cols[i].dtype});
+  } else {
+    for (int i = 0; i < n_cols; i++) {
+      bool ok = false;
+      for (auto &sc : a->schema)
+        if (cols[i].name && sc.first == cols[i].name) ok = sc.second == cols[i].dtype;
+      if (!ok) return set_err(ctx, QM_ERR_INVALID, "column %s changed type or was not in the first batch",
+                              cols[i].name ? cols[i].name : "?");
+    }
+  }
+  std::vector<DevCol> dcols;
+  int rc = stage_batch(ctx, n_rows, n_cols, cols, dcols);
+  if (rc) return rc;
+  const uint32_t *dsel = nullptr;
+  if ((rc = stage_selection(ctx, selection, n_selected, &dsel))) return rc;
+  if (dsel && n_selected > 0) {
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+    CK(qm_launch_check_selection(dsel, n_selected, n_rows, (qm_status *)ctx->status.p, ctx->sm_count, ctx->stream));
+    qm_status cst;
+    if ((rc = read_status(ctx, &cst))) return rc;
+    if (cst.error) return set_err(ctx, QM_ERR_INVALID, "selection is not strictly ascending row indices below %lld",
+                                  (long long)n_rows);
+  }
+  const int64_t n_elems = selection ? n_selected : n_rows;
+  ColEnv env;
+  for (auto &c : dcols) env.views.push_back({&c, n_rows});
+  GroupTable &gt = a->gt;
+  Plan pl;
+  if ((rc = plan_query(ctx, &a->q, env, pl))) return rc;
+  pl.key.mode = pl.key.n_cols == 0 ? QK_NONE : QK_HASH;
+  if (!a->planned) {
+    gt.pl = pl;
+    int64_t est = 1;
+    if (pl.key.mode == QK_HASH) {
+      est = n_elems;
+      if (n_elems > (1 << 16)) {
+        double e;
+        if ((rc = estimate_groups(ctx, pl.key, n_rows, &e))) return rc;
+        est = std::min<int64_t>(est, (int64_t)(e * 1.1) + 1024);
+      }
+    }
+    if ((rc = setup_table(ctx, gt, std::max<int64_t>(est, 1), 0, true))) return rc;
+    a->planned = true;
+  } else {
+    // same structure, this batch's column pointers
+    pl.key.base = gt.pl.key.base;
+    gt.pl.pred = pl.pred;
+    gt.pl.agg = pl.agg;
+    memcpy(gt.pl.key.data, pl.key.data, sizeof pl.key.data);
+    memcpy(gt.pl.key.nulls, pl.key.nulls, sizeof pl.key.nulls);
+    if (gt.pl.key.mode == QK_HASH) {
+      int64_t add = n_elems;
+      if (n_elems > (1 << 16)) {
+        double e;
+        if ((rc = estimate_groups(ctx, gt.pl.key, n_rows, &e))) return rc;
+        add = std::min<int64_t>(add, (int64_t)(e * 1.1) + 1024);
+      }
+      if ((rc = grow_table(ctx, gt, gt.groups_upper + add))) return rc;
+    }
+  }
+  CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  if ((rc = run_scan(ctx, gt, n_elems, dsel))) return rc;
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  qm_status st;
+  if ((rc = read_status(ctx, &st))) return rc;
+  take_scan_time(ctx, gt, true);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  a->device_ms += ms;
+  if (st.error) {
+    a->failed = true;
+    return set_err(ctx, QM_ERR_CUDA, "group table overflow in a streamed batch (device status %d)", st.error);
+  }
+  gt.groups_upper += (int64_t)st.groups_inserted;
+  gt.selected += st.rows_selected;
+  gt.rows_done += n_rows;
+  return QM_OK;
+}
+
+int qm_agg_finish(qm_agg *a, qm_result **out) {
+  if (!a || !out) return QM_ERR_INVALID;
+  qm_ctx *ctx = a->ctx;
+  *out = nullptr;
+  if (a->failed) return set_err(ctx, QM_ERR_INVALID, "aggregation failed earlier");
+  cudaSetDevice(ctx->device);
+  if (!a->planned) {
+    // no batch at all: plan against an empty schema is impossible when the
+    // query names columns; an ungrouped COUNT(*) still has its one row
+    std::vector<DevCol> none;
+    ColEnv env;
+    GroupTable &gt = a->gt;
+    int rc = plan_query(ctx, &a->q, env, gt.pl);
+    if (rc) return rc;
+    gt.pl.key.mode = gt.pl.key.n_cols == 0 ? QK_NONE : QK_HASH;
+    if ((rc = setup_table(ctx, gt, 1, 0, true))) return rc;
+    a->planned = true;
+  }
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  int rc = finish_table(ctx, a->gt, out, 0.f);
+  if (rc) return rc;
+  (*out)->stats.rows_scanned = a->gt.rows_done;
+  (*out)->stats.bytes_scanned = a->gt.pl.bytes_per_row * a->gt.rows_done;
+  (*out)->stats.device_ms += a->device_ms;
+  return QM_OK;
+}
+
+int qm_agg_destroy(qm_agg *a) {
+  if (!a) return QM_OK;
+  cudaSetDevice(a->ctx->device);
+  cudaStreamSynchronize(a->ctx->stream);
+  release(a->gt.own);
+  delete a;
+  return QM_OK;
+}
+
+int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column *cols, const qm_query *q,
+                     uint32_t *out_indices, int64_t max_out, int64_t *out_count) {
+  if (!ctx || !q || !out_count || n_rows < 0 || (n_cols > 0 && !cols) || max_out < 0 || (max_out > 0 && !out_indices))
+    return set_err(ctx, QM_ERR_INVALID, "qm_filter_select: bad arguments");
+  if (n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
+  cudaSetDevice(ctx->device);
+  *out_count = 0;
+  std::vector<DevCol> dcols;
+  int rc = stage_batch(ctx, n_rows, n_cols, cols, dcols);
+  if (rc) return rc;
+  ColEnv env;
+  for (auto &c : dcols) env.views.push_back({&c, n_rows});
+  qm_pred P;
+  std::vector<const DevCol *> touched;
+  int64_t bpr = 0;
+  if ((rc = build_pred(ctx, q, env, P, bpr, touched))) return rc;
+  if (n_rows == 0) return QM_OK;
+  const int64_t n_tiles = (n_rows + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  if ((rc = ensure(ctx, ctx->masks, (size_t)n_tiles * QM_R * 4)) || (rc = ensure(ctx, ctx->counts, (size_t)n_tiles * 4 + 4)) ||
+      (rc = ensure(ctx, ctx->offsets, (size_t)(n_tiles + 1) * 8)) || (rc = ensure_host(ctx, ctx->hstatus, 64)))
+    return rc;
+  CK(qm_launch_select_masks(P, n_rows, nullptr, (uint32_t *)ctx->masks.p, (uint32_t *)ctx->counts.p, ctx->sm_count,
+                            ctx->stream));
+  size_t tb = 0;
+  CK(qm_exclusive_scan_u32(nullptr, &tb, (uint32_t *)ctx->counts.p, (uint64_t *)ctx->offsets.p, n_tiles + 1,
+                           ctx->stream));
+  if ((rc = ensure(ctx, ctx->sort_temp, tb))) return rc;
+  tb = ctx->sort_temp.bytes;
+  // counts[n_tiles] = 0 so offsets[n_tiles] is the total
+  CK(cudaMemsetAsync((uint32_t *)ctx->counts.p + n_tiles, 0, 4, ctx->stream));
+  CK(qm_exclusive_scan_u32(ctx->sort_temp.p, &tb, (uint32_t *)ctx->counts.p, (uint64_t *)ctx->offsets.p,
+                           n_tiles + 1, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hstatus.p, (uint64_t *)ctx->offsets.p + n_tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const int64_t total = (int64_t)*(uint64_t *)ctx->hstatus.p;
+  *out_count = total;
+  const int64_t n_write = std::min(total, max_out);
+  if (n_write > 0) {
+    if ((rc = ensure(ctx, ctx->sel_out, (size_t)n_write * 4 + 16))) return rc;
+    CK(qm_launch_select_write(n_tiles, nullptr, (uint32_t *)ctx->masks.p, (uint64_t *)ctx->offsets.p,
+                              (uint32_t *)ctx->sel_out.p, n_write, ctx->sm_count, ctx->stream));
+    CK(cudaMemcpyAsync(out_indices, ctx->sel_out.p, (size_t)n_write * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  if (total > max_out) return set_err(ctx, QM_ERR_CAPACITY, "%lld rows pass, capacity %lld", (long long)total, (long long)max_out);
+  return QM_OK;
+}
+
+int qm_result_num_rows(const qm_result *r, int64_t *out) {
+  if (!r || !out) return QM_ERR_INVALID;
+  *out = r->n_rows;
+  return QM_OK;
+}
+
+int qm_result_num_columns(const qm_result *r, int32_t *out) {
+  if (!r || !out) return QM_ERR_INVALID;
+  *out = (int32_t)r->cols.size();
+  return QM_OK;
+}
+
+int qm_result_column(const qm_result *r, int32_t i, qm_result_col *out) {
+  if (!r || !out || i < 0 || i >= (int32_t)r->cols.size()) return QM_ERR_INVALID;
+  const auto &c = r->cols[i];
+  out->name = c.name.c_str();
+  out->dtype = c.dtype;
+  out->is_key = c.is_key;
+  out->n_rows = r->n_rows;
+  out->data = c.data.data();
+  out->null_bitmap = c.has_nulls ? c.nulls.data() : nullptr;
+  return QM_OK;
+}
+
+int qm_result_stats(const qm_result *r, qm_stats *out) {
+  if (!r || !out) return QM_ERR_INVALID;
+  *out = r->stats;
+  return QM_OK;
+}
+
+int qm_result_qmcb(const qm_result *cr, const uint8_t **buf, size_t *len) {
+  if (!cr || !buf || !len) return QM_ERR_INVALID;
+  qm_result *r = const_cast<qm_result *>(cr);
+  if (!r->qmcb_built) {
+    // encodeColumnarBatch layout (src/columnar.ts:523-613)
+    std::vector<uint8_t> &o = r->qmcb;
+    o.clear();
+    auto put = [&](const void *p, size_t n) { o.insert(o.end(), (const uint8_t *)p, (const uint8_t *)p + n); };
+    uint32_t magic = 0x42434D51u, rows = (uint32_t)r->n_rows;
+    uint16_t nc = (uint16_t)r->cols.size();
+    put(&magic, 4);
+    put(&rows, 4);
+    put(&nc, 2);
+    std::vector<int> tags;
+    for (auto &c : r->cols) {
+      int tag = c.dtype;
+      if (c.dtype == QM_I128) {
+        for (int64_t i = 0; i < r->n_rows; i++) {
+          uint64_t lo;
+          int64_t hi;
+          memcpy(&lo, c.data.data() + 16 * i, 8);
+          memcpy(&hi, c.data.data() + 16 * i + 8, 8);
+          if (hi != ((int64_t)lo < 0 ? -1 : 0)) return QM_ERR_UNSUPPORTED;
+        }
+        tag = QM_I64;
+      }
+      tags.push_back(tag);
+      uint16_t nl = (uint16_t)c.name.size();
+      put(&nl, 2);
+      put(c.name.data(), nl);
+      uint8_t t8 = (uint8_t)tag, hn = c.has_nulls ? 1 : 0;
+      put(&t8, 1);
+      put(&hn, 1);
+    }
+    for (size_t k = 0; k < r->cols.size(); k++) {
+      auto &c = r->cols[k];
+      if (c.has_nulls) put(c.nulls.data(), (size_t)((r->n_rows + 7) / 8));
+      if (c.dtype == QM_I128) {
+        for (int64_t i = 0; i < r->n_rows; i++) put(c.data.data() + 16 * i, 8);
+      } else {
+        put(c.data.data(), c.data.size());
+      }
+    }
+    r->qmcb_built = true;
+  }
+  *buf = r->qmcb.data();
+  *len = r->qmcb.size();
+  return QM_OK;
+}
+
+int qm_result_destroy(qm_result *r) {
+  delete r;
+  return QM_OK;
+}
+
+}  // extern "C"

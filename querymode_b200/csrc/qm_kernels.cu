@@ -1,0 +1,562 @@
+// qm_kernels.cu — kernels of the filter -> GROUP BY path and their launchers.
+//
+//   qm_scan_kernel      fused filter + compaction + group-by aggregation
+//   qm_init_table       fill the group table with empty keys / initial words
+//   qm_compact_groups   list occupied slots with their first-seen row
+//   qm_emit_groups      finalize each group's row (src/partial-agg.ts:306-352)
+//   qm_select_masks /   filter-only selection vector (ascending row indices)
+//   qm_select_write
+//   qm_minmax_kernel    integer column min / max (planning statistics)
+#include <cub/cub.cuh>
+
+#include "qm_kernels.cuh"
+#include "qm_launch.h"
+
+namespace qm {
+
+// Shared memory of one block: the block-local group table (keys, then the
+// accumulator words structure-of-arrays), then one compaction list per warp.
+struct smem_layout {
+  int L;
+  size_t keys_off, words_off, lists_off, bytes;
+};
+
+__host__ __device__ inline smem_layout make_smem_layout(int local_slots, int local_hash, int n_words,
+                                                        int warps) {
+  smem_layout s;
+  s.L = local_slots;
+  s.keys_off = 0;
+  size_t kb = (local_slots > 0 && local_hash) ? (size_t)local_slots * 8 : 0;
+  s.words_off = kb;
+  size_t wb = (size_t)local_slots * n_words * 8;
+  s.lists_off = s.words_off + wb;
+  s.bytes = s.lists_off + (size_t)warps * QM_TILE_ROWS * sizeof(uint16_t);
+  return s;
+}
+
+template <bool SEL>
+__global__ void __launch_bounds__(QM_SCAN_THREADS)
+    qm_scan_kernel(const __grid_constant__ qm_scan_args a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  const qm_aggspec &A = a.agg;
+  const smem_layout lay = make_smem_layout(a.local_slots, a.local_hash, A.n_words, warps);
+  const int L = lay.L;
+  uint64_t *lkeys = reinterpret_cast<uint64_t *>(smem + lay.keys_off);
+  uint64_t *lw = reinterpret_cast<uint64_t *>(smem + lay.words_off);
+  uint16_t *list = reinterpret_cast<uint16_t *>(smem + lay.lists_off) + warp * QM_TILE_ROWS;
+  __shared__ unsigned long long blk_selected;
+
+  if (threadIdx.x == 0) blk_selected = 0;
+  if (L > 0) {
+    if (a.local_hash)
+      for (int s = threadIdx.x; s < L; s += blockDim.x) lkeys[s] = QM_EMPTY_KEY;
+    for (int i = threadIdx.x; i < L * A.n_words; i += blockDim.x) lw[i] = A.init[i / L];
+  }
+  __syncthreads();
+
+  const int64_t n_tiles = (a.n + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  const int64_t gwarps = (int64_t)gridDim.x * warps;
+  unsigned long long my_selected = 0;
+
+  for (int64_t tile = (int64_t)blockIdx.x * warps + warp; tile < n_tiles; tile += gwarps) {
+    const int64_t e0 = tile * QM_TILE_ROWS;
+    // element -> row
+    int64_t rowv[QM_R];
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) {
+      int64_t e = e0 + j * 32 + lane;
+      bool in = e < a.n;
+      m |= (uint32_t)in << j;
+      if (SEL) rowv[j] = in ? (int64_t)__ldg(a.sel + e) : 0;
+      else rowv[j] = e;
+    }
+    auto rowf = [&](int j) { return rowv[j]; };
+    m = eval_pred(a.pred, rowf, m);
+
+    // compaction: survivors in ascending row order
+    uint32_t tot = 0;
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) {
+      uint32_t b = __ballot_sync(QM_FULL, (m >> j) & 1);
+      if ((m >> j) & 1) list[tot + __popc(b & lt)] = (uint16_t)(j * 32 + lane);
+      tot += __popc(b);
+    }
+    __syncwarp();
+    my_selected += tot;
+
+    for (uint32_t c0 = 0; c0 < tot; c0 += 32) {
+      const bool active = c0 + lane < tot;
+      const unsigned act = __ballot_sync(QM_FULL, active);
+      if (active) {
+        const int off = list[c0 + lane];
+        const int64_t row = SEL ? (int64_t)__ldg(a.sel + e0 + off) : e0 + off;
+        const uint64_t grow = (uint64_t)(a.row_offset + row);
+        int special;
+        const uint64_t key = row_key(a.key, row, special);
+        uint64_t vb[QM_MAX_VCOLS];
+        uint32_t vnull = 0;
+#pragma unroll
+        for (int c = 0; c < QM_MAX_VCOLS; ++c) {
+          vb[c] = 0;
+          if (c < A.n_vcols) {
+            const qm_vcol &vc = A.vcol[c];
+            if (cell_null(vc.nulls, row)) {
+              vnull |= 1u << c;
+            } else if (vc.dtype == QM_I32 || vc.dtype == QM_I64) {
+              vb[c] = (uint64_t)ld_int(vc.data, vc.dtype, row);
+            } else {
+              vb[c] = (uint64_t)__double_as_longlong(ld_flt(vc.data, vc.dtype, row));
+            }
+          }
+        }
+        unsigned peers = 1u << lane;
+        if (a.dedupe) {
+          peers = __match_any_sync(act, key);
+          if (__any_sync(act, special != 0)) peers &= __match_any_sync(act, special);
+        }
+        const bool leader = lane == __ffs(peers) - 1;
+        uint64_t *tp = nullptr;
+        int ws = 1;
+        bool local = false;
+        if (leader) {
+          int ls = -1;
+          if (L > 0) {
+            if (!a.local_hash) ls = (int)global_slot(a, key, special);
+            else if (special == 0) ls = local_find(lkeys, L, key);
+          }
+          if (ls >= 0) {
+            tp = lw + ls;
+            ws = L;
+            local = true;
+          } else if (!(L > 0 && !a.local_hash)) {
+            int64_t gs = global_slot(a, key, special);
+            if (gs >= 0) tp = a.table + gs * a.stride + 1;
+          }
+        }
+        apply_row(A, tp, ws, local, peers, lane, grow, vb, vnull);
+      }
+    }
+    __syncwarp();
+  }
+
+  // per-block selected count
+  for (int o = 16; o > 0; o >>= 1) my_selected += __shfl_xor_sync(QM_FULL, my_selected, o);
+  if (lane == 0 && my_selected) atomicAdd(&blk_selected, my_selected);
+  __syncthreads();
+  if (threadIdx.x == 0 && blk_selected) atomicAdd(&a.status->rows_selected, blk_selected);
+
+  // merge the block-local table into the global table
+  if (L > 0) {
+    const int cw = A.acc[A.acc_count].word;
+    for (int s = threadIdx.x; s < L; s += blockDim.x) {
+      if (lw[(int64_t)cw * L + s] == 0) continue;
+      int64_t gs;
+      if (a.local_hash) gs = global_slot(a, lkeys[s], 0);
+      else gs = s;
+      if (gs < 0) continue;
+      merge_local(A, lw + s, L, a.table + gs * a.stride + 1);
+    }
+  }
+}
+
+__global__ void qm_init_table(uint64_t *t, int64_t n_slots_total, int stride, int hash_keys,
+                              const __grid_constant__ qm_aggspec A) {
+  const int64_t n = n_slots_total * stride;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(i % stride);
+    t[i] = w == 0 ? (hash_keys ? QM_EMPTY_KEY : 0ULL) : A.init[w - 1];
+  }
+}
+
+// Occupied slots (COUNT word > 0) with their sort key: the first-seen row
+// (or the slot itself when no order is needed).
+__global__ void qm_compact_groups(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
+                                  int first_word, uint64_t *keys_out, uint32_t *slots_out,
+                                  unsigned long long *counter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < n_slots_total; s0 += step) {
+    const int64_t s = s0 + lane;
+    const bool occ = s < n_slots_total && t[s * stride + 1 + count_word] > 0;
+    const unsigned b = __ballot_sync(QM_FULL, occ);
+    if (!b) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, (unsigned long long)__popc(b));
+    base = __shfl_sync(QM_FULL, base, 0);
+    if (occ) {
+      const unsigned long long pos = base + __popc(b & lanemask_lt());
+      keys_out[pos] = first_word >= 0 ? t[s * stride + 1 + first_word] : (uint64_t)s;
+      slots_out[pos] = (uint32_t)s;
+    }
+  }
+}
+
+// Move the occupied hash slots of a table into a larger one (keys are
+// unique, so each new slot has one writer and the words are plain copies).
+__global__ void qm_rehash(const uint64_t *old_t, int64_t old_cap, int stride, int count_word, uint64_t *new_t,
+                          int log2cap, qm_status *st) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < old_cap; s += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t *src = old_t + s * stride;
+    if (src[1 + count_word] == 0) continue;
+    const int64_t ns = global_find(new_t, stride, log2cap, src[0], 1 << 12, st);
+    if (ns < 0) {
+      set_error(st, QM_DEV_OVERFLOW);
+      continue;
+    }
+    uint64_t *dst = new_t + ns * stride;
+    for (int w = 1; w < stride; ++w) dst[w] = src[w];
+  }
+}
+
+// Number(bigint): round to nearest, ties to even.
+__device__ __forceinline__ double i128_to_f64(uint64_t lo, int64_t hi) {
+  const bool neg = hi < 0;
+  if (neg) {  // negate the 128-bit value
+    lo = ~lo + 1;
+    hi = ~hi + (lo == 0 ? 1 : 0);
+  }
+  const uint64_t uhi = (uint64_t)hi;
+  double r;
+  if (uhi == 0) {
+    r = __ull2double_rn(lo);
+  } else {
+    const int shift = 64 - __clzll((long long)uhi);  // drop `shift` bits
+    const uint64_t top = (uhi << (64 - shift)) | (lo >> shift);
+    const bool sticky = (lo << (64 - shift)) != 0;
+    uint64_t keep = top >> 11;
+    const uint64_t rem = top & 0x7ff;
+    const bool guard = (rem >> 10) & 1;
+    const bool st = sticky || (rem & 0x3ff);
+    if (guard && (st || (keep & 1))) keep++;
+    r = ldexp((double)keep, shift + 11);
+  }
+  return neg ? -r : r;
+}
+
+__device__ __forceinline__ void set_null(unsigned char *out, int64_t null_offset, int64_t i) {
+  atomicOr(reinterpret_cast<unsigned *>(out + null_offset) + (i >> 5), 1u << (i & 31));
+}
+
+__global__ void qm_emit_groups(const uint64_t *t, int stride, const uint32_t *slots, int64_t G,
+                               const __grid_constant__ qm_keyspec K, int64_t n_slots,
+                               const __grid_constant__ qm_outspec O, unsigned char *out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = slots ? slots[i] : (uint64_t)i;
+    const uint64_t *w = t + s * stride + 1;
+    // reconstruct the key word
+    bool knull = false;
+    uint64_t key = 0;
+    if (K.mode == QK_DIRECT) {
+      if ((int64_t)s == n_slots) knull = true;
+      else key = (uint64_t)K.base + s;
+    } else if (K.mode == QK_HASH) {
+      if ((int64_t)s == n_slots) key = QM_EMPTY_KEY;
+      else if ((int64_t)s == n_slots + 1) knull = true;
+      else key = t[s * stride];
+    }
+    for (int k = 0; k < O.n_out; ++k) {
+      const qm_out &o = O.o[k];
+      unsigned char *col = out + o.offset;
+      if (o.kind == QO_KEY) {
+        if (knull) {
+          set_null(out, o.null_offset, i);
+          continue;
+        }
+        if (K.n_cols == 2) {
+          reinterpret_cast<int32_t *>(col)[i] = (int32_t)(o.src == 0 ? (key >> 32) : key);
+        } else if (o.dtype == QM_I32) {
+          reinterpret_cast<int32_t *>(col)[i] = (int32_t)(int64_t)key;
+        } else {
+          reinterpret_cast<uint64_t *>(col)[i] = key;
+        }
+        continue;
+      }
+      if (o.kind == QO_COUNT) {
+        reinterpret_cast<int64_t *>(col)[i] = (int64_t)w[o.word];
+        continue;
+      }
+      const uint64_t nn = w[o.nn_word];
+      if (nn == 0) {
+        set_null(out, o.null_offset, i);
+        continue;
+      }
+      switch (o.kind) {
+        case QO_SUM_F:
+        case QO_AVG_F: {
+          double s2 = __longlong_as_double((long long)w[o.word]) + __longlong_as_double((long long)w[o.word + 1]);
+          reinterpret_cast<double *>(col)[i] = o.kind == QO_SUM_F ? s2 : s2 / (double)nn;
+          break;
+        }
+        case QO_SUM_I2F:
+        case QO_AVG_I2F: {
+          double s2 = i128_to_f64(w[o.word], (int64_t)w[o.word + 1]);
+          reinterpret_cast<double *>(col)[i] = o.kind == QO_SUM_I2F ? s2 : s2 / (double)nn;
+          break;
+        }
+        case QO_SUM_I128:
+          reinterpret_cast<uint64_t *>(col)[2 * i] = w[o.word];
+          reinterpret_cast<uint64_t *>(col)[2 * i + 1] = w[o.word + 1];
+          break;
+        case QO_AVG_BIG: {
+          // bigAvg(bigSum, 0, count): Number(sum / n) + Number(sum % n) / n
+          const __int128 sum = (__int128)(((unsigned __int128)(uint64_t)w[o.word + 1] << 64) | w[o.word]);
+          const __int128 q = sum / (__int128)nn, r = sum % (__int128)nn;
+          const double qd = i128_to_f64((uint64_t)q, (int64_t)(q >> 64));
+          const double rd = i128_to_f64((uint64_t)r, (int64_t)(r >> 64));
+          reinterpret_cast<double *>(col)[i] = qd + (rd + 0.0) / (double)nn;
+          break;
+        }
+        case QO_MIN_I:
+        case QO_MAX_I:
+          if (o.dtype == QM_I32) reinterpret_cast<int32_t *>(col)[i] = (int32_t)(int64_t)w[o.word];
+          else reinterpret_cast<int64_t *>(col)[i] = (int64_t)w[o.word];
+          break;
+        case QO_MIN_F:
+        case QO_MAX_F: {
+          const int64_t ov = (int64_t)w[o.word];
+          double d = ord2f(ov);
+          // a zero result takes the sign of the first zero seen (strict
+          // '<' / '>' keep the first of -0 and 0, src/partial-agg.ts:80-81)
+          if (ov == 0 && o.zero_word >= 0 && w[o.zero_word] != ~0ULL && (w[o.zero_word] & 1)) d = -0.0;
+          reinterpret_cast<double *>(col)[i] = d;
+          break;
+        }
+      }
+    }
+  }
+}
+
+// Filter-only pass 1: per warp tile, the 32-bit survivor masks and counts.
+template <bool SEL>
+__global__ void __launch_bounds__(QM_SCAN_THREADS)
+    qm_select_masks(const __grid_constant__ qm_pred P, int64_t n, const uint32_t *sel, uint32_t *masks,
+                    uint32_t *counts) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  const int64_t n_tiles = (n + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  for (int64_t tile = (int64_t)blockIdx.x * warps + (threadIdx.x >> 5); tile < n_tiles;
+       tile += (int64_t)gridDim.x * warps) {
+    const int64_t e0 = tile * QM_TILE_ROWS;
+    int64_t rowv[QM_R];
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) {
+      int64_t e = e0 + j * 32 + lane;
+      bool in = e < n;
+      m |= (uint32_t)in << j;
+      rowv[j] = SEL ? (in ? (int64_t)__ldg(sel + e) : 0) : e;
+    }
+    auto rowf = [&](int j) { return rowv[j]; };
+    m = eval_pred(P, rowf, m);
+    uint32_t tot = 0;
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) {
+      uint32_t b = __ballot_sync(QM_FULL, (m >> j) & 1);
+      if (lane == j) masks[tile * QM_R + j] = b;
+      tot += __popc(b);
+    }
+    if (lane == 0) counts[tile] = tot;
+  }
+}
+
+// Filter-only pass 2: ascending row indices at each tile's exclusive offset.
+__global__ void qm_select_write(int64_t n_tiles, const uint32_t *sel, const uint32_t *masks,
+                                const uint64_t *offsets, uint32_t *out, int64_t max_out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  const uint32_t lt = lanemask_lt();
+  for (int64_t tile = (int64_t)blockIdx.x * warps + (threadIdx.x >> 5); tile < n_tiles;
+       tile += (int64_t)gridDim.x * warps) {
+    uint64_t pos = offsets[tile];
+    const int64_t e0 = tile * QM_TILE_ROWS;
+    for (int j = 0; j < QM_R; ++j) {
+      const uint32_t b = masks[tile * QM_R + j];
+      if ((b >> lane) & 1) {
+        const uint64_t p = pos + __popc(b & lt);
+        const int64_t e = e0 + j * 32 + lane;
+        if ((int64_t)p < max_out) out[p] = sel ? __ldg(sel + e) : (uint32_t)e;
+      }
+      pos += __popc(b);
+    }
+  }
+}
+
+// min / max of a (possibly nullable) integer column.
+__global__ void qm_minmax_kernel(const void *p, int dtype, const uint32_t *nulls, int64_t n,
+                                 long long *out) {
+  long long mn = LLONG_MAX, mx = LLONG_MIN;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (cell_null(nulls, i)) continue;
+    long long v = dtype == QM_I32 ? (long long)__ldg((const int *)p + i) : __ldg((const long long *)p + i);
+    mn = min(mn, v);
+    mx = max(mx, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(QM_FULL, mn, o));
+    mx = max(mx, __shfl_xor_sync(QM_FULL, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out, mn);
+    atomicMax(out + 1, mx);
+  }
+}
+
+// A selection vector must list strictly ascending row indices below n_rows.
+__global__ void qm_check_selection(const uint32_t *sel, int64_t n_sel, int64_t n_rows, qm_status *st) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_sel; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = sel[i];
+    if ((int64_t)v >= n_rows || (i > 0 && sel[i - 1] >= v)) set_error(st, QM_DEV_RANGE);
+  }
+}
+
+// HyperLogLog registers (2^QM_HLL_P) of the group keys: the planner's
+// distinct-count estimate that sizes hash tables.
+__global__ void qm_hll_kernel(const __grid_constant__ qm_keyspec K, int64_t n, uint32_t *regs) {
+  __shared__ uint32_t r[1 << QM_HLL_P];
+  for (int i = threadIdx.x; i < (1 << QM_HLL_P); i += blockDim.x) r[i] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int special;
+    uint64_t key = row_key(K, i, special);
+    if (special == 2) key = 0x6e756c6c6e756c6cULL;
+    const uint64_t h = fmix64(key ^ 0x9e3779b97f4a7c15ULL);
+    const uint32_t idx = (uint32_t)(h >> (64 - QM_HLL_P));
+    const uint64_t w = h << QM_HLL_P;
+    const uint32_t rank = w ? (uint32_t)__clzll((long long)w) + 1 : (uint32_t)(65 - QM_HLL_P);
+    atomicMax(&r[idx], rank);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (1 << QM_HLL_P); i += blockDim.x)
+    if (r[i]) atomicMax(&regs[i], r[i]);
+}
+
+__global__ void qm_minmax_init(long long *out) {
+  out[0] = LLONG_MAX;
+  out[1] = LLONG_MIN;
+}
+
+}  // namespace qm
+
+// ---------------------------------------------------------------- launchers
+using namespace qm;
+
+size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words) {
+  return make_smem_layout(local_slots, local_hash, n_words, QM_SCAN_THREADS / 32).bytes;
+}
+
+cudaError_t qm_scan_configure(size_t smem_bytes, int *blocks_per_sm) {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(qm_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(qm_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false>, QM_SCAN_THREADS,
+                                                       smem_bytes);
+}
+
+cudaError_t qm_launch_scan(const qm_scan_args &a, int blocks, size_t smem_bytes, cudaStream_t st) {
+  if (a.n <= 0) return cudaSuccess;
+  if (a.sel) qm_scan_kernel<true><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  else qm_scan_kernel<false><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_init_table(uint64_t *t, int64_t n_slots_total, int stride, int hash_keys,
+                                 const qm_aggspec &A, int sm_count, cudaStream_t st) {
+  int64_t n = n_slots_total * stride;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 16);
+  if (blocks < 1) blocks = 1;
+  qm_init_table<<<blocks, 256, 0, st>>>(t, n_slots_total, stride, hash_keys, A);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_compact(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
+                              int first_word, uint64_t *keys_out, uint32_t *slots_out,
+                              unsigned long long *counter, int sm_count, cudaStream_t st) {
+  int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
+  if (blocks < 1) blocks = 1;
+  qm_compact_groups<<<blocks, 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, keys_out,
+                                            slots_out, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_sort_pairs(void *temp, size_t *temp_bytes, const uint64_t *kin, uint64_t *kout,
+                          const uint32_t *vin, uint32_t *vout, int64_t n, int end_bit, cudaStream_t st) {
+  return cub::DeviceRadixSort::SortPairs(temp, *temp_bytes, kin, kout, vin, vout, (int)n, 0, end_bit, st);
+}
+
+cudaError_t qm_launch_emit(const uint64_t *t, int stride, const uint32_t *slots, int64_t G,
+                           const qm_keyspec &K, int64_t n_slots, const qm_outspec &O, unsigned char *out,
+                           int sm_count, cudaStream_t st) {
+  if (G <= 0) return cudaSuccess;
+  int blocks = (int)std::min<int64_t>((G + 255) / 256, (int64_t)sm_count * 8);
+  qm_emit_groups<<<blocks, 256, 0, st>>>(t, stride, slots, G, K, n_slots, O, out);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *sel, uint32_t *masks,
+                                   uint32_t *counts, int sm_count, cudaStream_t st) {
+  int64_t n_tiles = (n + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  int warps = QM_SCAN_THREADS / 32;
+  int blocks = (int)std::min<int64_t>((n_tiles + warps - 1) / warps, (int64_t)sm_count * 4);
+  if (blocks < 1) return cudaSuccess;
+  if (sel) qm_select_masks<true><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
+  else qm_select_masks<false><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_exclusive_scan_u32(void *temp, size_t *temp_bytes, const uint32_t *in, uint64_t *out, int64_t n,
+                                  cudaStream_t st) {
+  return cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, in, out, (int)n, st);
+}
+
+cudaError_t qm_launch_select_write(int64_t n_tiles, const uint32_t *sel, const uint32_t *masks,
+                                   const uint64_t *offsets, uint32_t *out, int64_t max_out, int sm_count,
+                                   cudaStream_t st) {
+  int warps = 256 / 32;
+  int blocks = (int)std::min<int64_t>((n_tiles + warps - 1) / warps, (int64_t)sm_count * 8);
+  if (blocks < 1) return cudaSuccess;
+  qm_select_write<<<blocks, 256, 0, st>>>(n_tiles, sel, masks, offsets, out, max_out);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_check_selection(const uint32_t *sel, int64_t n_sel, int64_t n_rows, qm_status *st,
+                                      int sm_count, cudaStream_t stream) {
+  if (n_sel <= 0) return cudaSuccess;
+  int blocks = (int)std::min<int64_t>((n_sel + 255) / 256, (int64_t)sm_count * 4);
+  qm_check_selection<<<blocks, 256, 0, stream>>>(sel, n_sel, n_rows, st);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(regs, 0, sizeof(uint32_t) << QM_HLL_P, st);
+  if (e != cudaSuccess || n <= 0) return e;
+  int blocks = (int)std::min<int64_t>((n + 1023) / 1024, (int64_t)sm_count * 2);
+  qm_hll_kernel<<<blocks, 512, 0, st>>>(K, n, regs);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_rehash(const uint64_t *old_t, int64_t old_cap, int stride, int count_word, uint64_t *new_t,
+                             int log2cap, qm_status *st, int sm_count, cudaStream_t stream) {
+  if (old_cap <= 0) return cudaSuccess;
+  int blocks = (int)std::min<int64_t>((old_cap + 255) / 256, (int64_t)sm_count * 8);
+  qm_rehash<<<blocks, 256, 0, stream>>>(old_t, old_cap, stride, count_word, new_t, log2cap, st);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_minmax(const void *p, int dtype, const uint32_t *nulls, int64_t n, long long *out,
+                             int sm_count, cudaStream_t st) {
+  qm_minmax_init<<<1, 1, 0, st>>>(out);
+  if (n > 0) {
+    int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 4);
+    qm_minmax_kernel<<<blocks, 256, 0, st>>>(p, dtype, nulls, n, out);
+  }
+  return cudaGetLastError();
+}

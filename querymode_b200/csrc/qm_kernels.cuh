@@ -1,0 +1,494 @@
+// qm_kernels.cuh — device code of the fused filter -> GROUP BY path.
+//
+// One warp owns a tile of QM_TILE_ROWS consecutive rows (or selection
+// entries).  Per tile:
+//   1. predicates: each lane tests QM_R rows (lane, lane+32, ...), one term at
+//      a time; a term's column is read only for rows still alive, so a
+//      selective first term skips the sectors of later columns;
+//   2. compaction: __ballot_sync masks + popcount prefix sums put the
+//      surviving row offsets, in ascending row order, into a per-warp list;
+//   3. aggregation: 32 survivors at a time, the lane gathers its row's key and
+//      value cells, equal keys in the warp are merged with __match_any_sync
+//      (one update per distinct key), and the leader updates the block-local
+//      shared-memory table (or the global table when the key misses it).
+// At block end the shared-memory table is merged into the global table with
+// atomics.  Float sums are compensated (TwoSum of every atomic add: the old
+// value returned by atomicAdd gives the exact rounding error, which goes to a
+// second word), integer sums are exact 128-bit, MIN/MAX are integer atomics
+// on an order-preserving image of the value.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/qm_gpu.h"
+#include "qm_plan.h"
+
+#define QM_FULL 0xffffffffu
+#define QM_LOCAL_PROBE 16
+
+namespace qm {
+
+// murmur3 fmix64 finaliser — the hash the reference's LinearHashTable uses
+// (wasm/src/query/vector_engine.zig:209-250)
+__host__ __device__ __forceinline__ uint64_t fmix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---- column access ----------------------------------------------------------
+// Column cells are read once per query: cache-streaming loads keep the group
+// table (read-modify-written by atomics) resident in L2.
+template <typename T>
+__device__ __forceinline__ T ldcs(const void *p, int64_t r) {
+  return __ldcs(reinterpret_cast<const T *>(p) + r);
+}
+
+__device__ __forceinline__ bool cell_null(const uint32_t *nb, int64_t r) {
+  return nb != nullptr && ((__ldg(nb + (r >> 5)) >> (r & 31)) & 1u);
+}
+
+__device__ __forceinline__ int64_t ld_int(const void *p, int dtype, int64_t r) {
+  return dtype == QM_I32 ? (int64_t)ldcs<int>(p, r) : (int64_t)ldcs<long long>(p, r);
+}
+
+__device__ __forceinline__ double ld_flt(const void *p, int dtype, int64_t r) {
+  return dtype == QM_F32 ? (double)ldcs<float>(p, r) : ldcs<double>(p, r);
+}
+
+// order-preserving image of a double in int64 (after -0 -> +0)
+__host__ __device__ __forceinline__ int64_t f2ord(double d) {
+  int64_t b;
+#ifdef __CUDA_ARCH__
+  b = __double_as_longlong(d);
+#else
+  memcpy(&b, &d, 8);
+#endif
+  return b >= 0 ? b : (b ^ 0x7fffffffffffffffLL);
+}
+
+__host__ __device__ __forceinline__ double ord2f(int64_t o) {
+  int64_t b = o >= 0 ? o : (o ^ 0x7fffffffffffffffLL);
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(b);
+#else
+  double d;
+  memcpy(&d, &b, 8);
+  return d;
+#endif
+}
+
+// ---- predicates -------------------------------------------------------------
+__device__ __forceinline__ bool fcmp(double v, int op, double t) {
+  switch (op) {
+    case QC_EQ: return v == t;
+    case QC_NEQ: return v != t;
+    case QC_LT: return v < t;
+    case QC_LTE: return v <= t;
+    case QC_GT: return v > t;
+    default: return v >= t;
+  }
+}
+
+// JS: coerceCompare(number v, bigint b) -> BigInt(trunc(v)) <op> b, with a
+// non-finite v compared as a number (src/decode.ts:480-485).
+__device__ __forceinline__ bool fbig(double v, int op, int64_t b) {
+  if (isnan(v)) return op == QC_NEQ;
+  int c;
+  if (isinf(v)) {
+    c = v > 0 ? 1 : -1;
+    if (op == QC_EQ) return false;
+    if (op == QC_NEQ) return true;
+  } else {
+    double t = trunc(v);
+    if (t >= 9223372036854775808.0) c = 1;
+    else if (t < -9223372036854775808.0) c = -1;
+    else {
+      long long ti = (long long)t;
+      c = ti < b ? -1 : (ti > b ? 1 : 0);
+    }
+  }
+  switch (op) {
+    case QC_EQ: return c == 0;
+    case QC_NEQ: return c != 0;
+    case QC_LT: return c < 0;
+    case QC_LTE: return c <= 0;
+    case QC_GT: return c > 0;
+    default: return c >= 0;
+  }
+}
+
+__device__ __forceinline__ bool fterm(const qm_term &t, double v) {
+  switch (t.kind) {
+    case QT_FCMP: return fcmp(v, t.op, t.f0);
+    case QT_FBETWEEN: return v >= t.f0 && v <= t.f1;
+    case QT_FNBETWEEN: return v < t.f0 || v > t.f1;
+    default: return fbig(v, t.op, t.lo);
+  }
+}
+
+// Tests term `t` on the lane's alive rows (bit j of m = row[j] alive).
+template <typename ROWS>
+__device__ __forceinline__ uint32_t eval_term(const qm_term &t, const ROWS &row, uint32_t m) {
+  uint32_t pass = 0;
+  if (t.kind <= QT_FALSE) {
+    pass = t.kind == QT_TRUE ? ((1u << QM_R) - 1) : 0u;
+  } else if (t.dtype == QM_I32 || t.dtype == QM_I64) {
+    int64_t v[QM_R];
+    if (t.dtype == QM_I32) {
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = ((m >> j) & 1) ? (int64_t)ldcs<int>(t.data, row(j)) : 0;
+    } else {
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = ((m >> j) & 1) ? (int64_t)ldcs<long long>(t.data, row(j)) : 0;
+    }
+    const bool inr = t.kind == QT_IRANGE;
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) {
+      bool in = v[j] >= t.lo && v[j] <= t.hi;
+      pass |= (uint32_t)(in == inr) << j;
+    }
+  } else {
+    double v[QM_R];
+    if (t.dtype == QM_F32) {
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = ((m >> j) & 1) ? (double)ldcs<float>(t.data, row(j)) : 0.0;
+    } else {
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = ((m >> j) & 1) ? ldcs<double>(t.data, row(j)) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)fterm(t, v[j]) << j;
+  }
+  if (t.nulls != nullptr) {
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j)
+      if (((m >> j) & 1) && cell_null(t.nulls, row(j)))
+        pass = (pass & ~(1u << j)) | ((uint32_t)t.null_pass << j);
+  }
+  return m & pass;
+}
+
+// AND terms, then the OR of the groups' AND chains (src/decode.ts:558-578).
+template <typename ROWS>
+__device__ __forceinline__ uint32_t eval_pred(const qm_pred &P, const ROWS &row, uint32_t m) {
+  for (int i = 0; i < P.n_and; ++i) {
+    if (!__any_sync(QM_FULL, m)) return 0;
+    m = eval_term(P.t[i], row, m);
+  }
+  if (P.n_groups > 0) {
+    uint32_t any = 0;
+    int b = P.n_and;
+    for (int g = 0; g < P.n_groups; ++g) {
+      uint32_t mg = m & ~any;
+      const int e = P.group_end[g];
+      for (int i = b; i < e; ++i) {
+        if (!__any_sync(QM_FULL, mg)) break;
+        mg = eval_term(P.t[i], row, mg);
+      }
+      any |= mg;
+      b = e;
+    }
+    m = any;
+  }
+  return m;
+}
+
+// ---- group keys -------------------------------------------------------------
+// Key word of one row.  special: 0 ordinary, 1 the key equals the empty-slot
+// sentinel (hash mode), 2 NULL key.
+__device__ __forceinline__ uint64_t row_key(const qm_keyspec &K, int64_t r, int &special) {
+  special = 0;
+  if (K.n_cols == 0) return 0;
+  if (K.n_cols == 2) {
+    uint32_t a = (uint32_t)ldcs<int>(K.data[0], r), b = (uint32_t)ldcs<int>(K.data[1], r);
+    uint64_t k = ((uint64_t)a << 32) | b;
+    if (K.mode == QK_HASH && k == QM_EMPTY_KEY) special = 1;
+    return k;
+  }
+  if (cell_null(K.nulls[0], r)) {
+    special = 2;
+    return 0;
+  }
+  uint64_t k;
+  switch (K.dtype[0]) {
+    case QM_I32: k = (uint64_t)(int64_t)ldcs<int>(K.data[0], r); break;
+    case QM_I64: k = (uint64_t)ldcs<long long>(K.data[0], r); break;
+    default: {
+      // String(v) identity: -0 and 0 share "0", every NaN is "NaN"
+      double d = ld_flt(K.data[0], K.dtype[0], r);
+      if (d == 0.0) d = 0.0;
+      k = isnan(d) ? 0x7ff8000000000000ULL : (uint64_t)__double_as_longlong(d);
+    }
+  }
+  if (K.mode == QK_HASH && k == QM_EMPTY_KEY) special = 1;
+  return k;
+}
+
+__device__ __forceinline__ void set_error(qm_status *st, int code) {
+  atomicCAS(&st->error, 0, code);
+}
+
+// Linear probing with a CAS claim of the key word.  Accumulator words are
+// pre-initialised, so a claimed slot is immediately usable.
+__device__ __forceinline__ int64_t global_find(uint64_t *table, int stride, int log2cap,
+                                               uint64_t key, int max_probe, qm_status *st) {
+  const uint64_t mask = (1ULL << log2cap) - 1;
+  uint64_t s = fmix64(key) & mask;
+  for (int p = 0; p < max_probe; ++p) {
+    unsigned long long *kp = reinterpret_cast<unsigned long long *>(table + s * stride);
+    uint64_t k = *reinterpret_cast<volatile unsigned long long *>(kp);
+    if (k == key) return (int64_t)s;
+    if (k == QM_EMPTY_KEY) {
+      uint64_t prev = atomicCAS(kp, QM_EMPTY_KEY, key);
+      if (prev == QM_EMPTY_KEY) {
+        atomicAdd(&st->groups_inserted, 1ULL);
+        return (int64_t)s;
+      }
+      if (prev == key) return (int64_t)s;
+    }
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int64_t global_slot(const qm_scan_args &a, uint64_t key, int special) {
+  if (a.key.mode == QK_NONE) return 0;
+  if (a.key.mode == QK_DIRECT) {
+    if (special == 2) return a.n_slots;
+    uint64_t d = key - (uint64_t)a.key.base;
+    if (d >= (uint64_t)a.n_slots) {
+      set_error(a.status, QM_DEV_RANGE);
+      return -1;
+    }
+    return (int64_t)d;
+  }
+  if (special) return a.n_slots + special - 1;
+  int64_t s = global_find(a.table, a.stride, a.log2cap, key, a.max_probe, a.status);
+  if (s < 0) set_error(a.status, QM_DEV_OVERFLOW);
+  return s;
+}
+
+__device__ __forceinline__ int local_find(uint64_t *lkeys, int L, uint64_t key) {
+  uint32_t s = (uint32_t)fmix64(key) & (uint32_t)(L - 1);
+  for (int p = 0; p < QM_LOCAL_PROBE; ++p) {
+    uint64_t k = reinterpret_cast<volatile uint64_t *>(lkeys)[s];
+    if (k == key) return (int)s;
+    if (k == QM_EMPTY_KEY) {
+      uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long *>(lkeys + s), QM_EMPTY_KEY, key);
+      if (prev == QM_EMPTY_KEY || prev == key) return (int)s;
+    }
+    s = (s + 1) & (uint32_t)(L - 1);
+  }
+  return -1;
+}
+
+// ---- accumulator updates ------------------------------------------------------
+__device__ __forceinline__ void add128(uint64_t *lo, uint64_t *hi, uint64_t vlo, int64_t vhi) {
+  if (vlo != 0) {
+    uint64_t old = atomicAdd(reinterpret_cast<unsigned long long *>(lo), (unsigned long long)vlo);
+    if (old + vlo < old) vhi += 1;
+  }
+  if (vhi != 0) atomicAdd(reinterpret_cast<unsigned long long *>(hi), (unsigned long long)vhi);
+}
+
+// Compensated atomic add: atomicAdd returns the old value, so the rounding
+// error of old + x is recovered exactly (TwoSum) and added, with the
+// contribution's own low part xc, to the low word.
+__device__ __forceinline__ void fsum_add(uint64_t *hp, uint64_t *lp, double x, double xc) {
+  if (x == 0.0 && xc == 0.0) return;
+  double old = atomicAdd(reinterpret_cast<double *>(hp), x);
+  double s = old + x;
+  if (!isfinite(s)) return;
+  double bb = s - old;
+  double err = (old - (s - bb)) + (x - bb);
+  double add = xc + err;
+  if (add != 0.0) atomicAdd(reinterpret_cast<double *>(lp), add);
+}
+
+__device__ __forceinline__ void two_sum_acc(double &s, double &c, double x) {
+  double t = s + x;
+  if (isfinite(t)) {
+    double bb = t - s;
+    c += (s - (t - bb)) + (x - bb);
+  }
+  s = t;
+}
+
+__device__ __forceinline__ uint64_t pick(const uint64_t (&v)[QM_MAX_VCOLS], int i) {
+  uint64_t r = 0;
+#pragma unroll
+  for (int c = 0; c < QM_MAX_VCOLS; ++c)
+    if (c == i) r = v[c];
+  return r;
+}
+
+// Apply one compacted row (merged with its equal-key peers) to a slot whose
+// accumulator word w lives at tp[w * ws].  Every peer executes this (the
+// shuffles need them); only the leader, with tp != nullptr, writes.
+__device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
+                                          unsigned peers, int lane, uint64_t grow,
+                                          const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
+  const bool solo = (peers & (peers - 1)) == 0;
+  for (int i = 0; i < A.n_accs; ++i) {
+    const qm_acc ac = A.acc[i];
+    uint64_t *w0 = tp ? tp + (int64_t)ac.word * ws : nullptr;
+    uint64_t *w1 = tp ? tp + (int64_t)(ac.word + 1) * ws : nullptr;
+    if (ac.kind == QA_COUNT) {
+      if (tp) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)__popc(peers));
+      continue;
+    }
+    if (ac.kind == QA_FIRST) {
+      if (tp) atomicMin(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)grow);
+      continue;
+    }
+    const bool valid = !((vnull >> ac.vcol) & 1);
+    const uint64_t raw = pick(vb, ac.vcol);
+    switch (ac.kind) {
+      case QA_NN: {
+        unsigned nn = solo ? (unsigned)valid : __popc(__ballot_sync(peers, valid));
+        if (tp && nn) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)nn);
+        break;
+      }
+      case QA_ISUM: {
+        int64_t v = valid ? (int64_t)raw : 0;
+        if (!ac.wide) {
+          int64_t s = v;
+          if (!solo)
+            for (unsigned m = peers; m; m &= m - 1) {
+              int src = __ffs(m) - 1;
+              int64_t x = __shfl_sync(peers, v, src);
+              if (src != lane) s += x;
+            }
+          if (tp && s != 0) {
+            if (local) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)s);
+            else add128(w0, w1, (uint64_t)s, s < 0 ? -1 : 0);
+          }
+        } else {
+          // 128-bit sum of up to 32 int64 cells
+          uint64_t lo = (uint64_t)v;
+          int64_t hi = v < 0 ? -1 : 0;
+          if (!solo)
+            for (unsigned m = peers; m; m &= m - 1) {
+              int src = __ffs(m) - 1;
+              int64_t x = __shfl_sync(peers, v, src);
+              if (src != lane) {
+                uint64_t nlo = lo + (uint64_t)x;
+                hi += (x < 0 ? -1 : 0) + (nlo < lo ? 1 : 0);
+                lo = nlo;
+              }
+            }
+          if (tp && (lo != 0 || hi != 0)) add128(w0, w1, lo, hi);
+        }
+        break;
+      }
+      case QA_FSUM: {
+        double v = valid ? __longlong_as_double((long long)raw) : 0.0;
+        double s = v, c = 0.0;
+        if (!solo)
+          for (unsigned m = peers; m; m &= m - 1) {
+            int src = __ffs(m) - 1;
+            double x = __shfl_sync(peers, v, src);
+            if (src != lane) two_sum_acc(s, c, x);
+          }
+        if (tp) fsum_add(w0, w1, s, c);
+        break;
+      }
+      case QA_IMIN:
+      case QA_IMAX: {
+        const bool mx = ac.kind == QA_IMAX;
+        int64_t v = valid ? (int64_t)raw : (mx ? INT64_MIN : INT64_MAX);
+        if (!solo)
+          for (unsigned m = peers; m; m &= m - 1) {
+            int src = __ffs(m) - 1;
+            int64_t x = __shfl_sync(peers, v, src);
+            v = mx ? max(v, x) : min(v, x);
+          }
+        if (tp && v != (mx ? INT64_MIN : INT64_MAX)) {
+          if (mx) atomicMax(reinterpret_cast<long long *>(w0), (long long)v);
+          else atomicMin(reinterpret_cast<long long *>(w0), (long long)v);
+        }
+        break;
+      }
+      case QA_FMIN:
+      case QA_FMAX: {
+        const bool mx = ac.kind == QA_FMAX;
+        double d = __longlong_as_double((long long)raw);
+        bool ok = valid && !isnan(d); // NaN never wins '<' / '>' (src/partial-agg.ts:80-81)
+        int64_t o = ok ? f2ord(d == 0.0 ? 0.0 : d) : (mx ? INT64_MIN : INT64_MAX);
+        if (!solo)
+          for (unsigned m = peers; m; m &= m - 1) {
+            int src = __ffs(m) - 1;
+            int64_t x = __shfl_sync(peers, o, src);
+            o = mx ? max(o, x) : min(o, x);
+          }
+        if (tp && o != (mx ? INT64_MIN : INT64_MAX)) {
+          if (mx) atomicMax(reinterpret_cast<long long *>(w0), (long long)o);
+          else atomicMin(reinterpret_cast<long long *>(w0), (long long)o);
+        }
+        break;
+      }
+      case QA_FZERO: {
+        double d = __longlong_as_double((long long)raw);
+        bool z = valid && d == 0.0;
+        uint64_t code = z ? ((grow << 1) | (raw >> 63)) : ~0ULL;
+        if (!solo) {
+          if (__any_sync(peers, z))
+            for (unsigned m = peers; m; m &= m - 1) {
+              int src = __ffs(m) - 1;
+              uint64_t x = __shfl_sync(peers, code, src);
+              code = min(code, x);
+            }
+        }
+        if (tp && code != ~0ULL) atomicMin(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)code);
+        break;
+      }
+    }
+  }
+}
+
+// Merge one block-local slot (words at lp[w * L]) into global slot words gp.
+__device__ __forceinline__ void merge_local(const qm_aggspec &A, const uint64_t *lp, int L, uint64_t *gp) {
+  for (int i = 0; i < A.n_accs; ++i) {
+    const qm_acc ac = A.acc[i];
+    const uint64_t v0 = lp[(int64_t)ac.word * L];
+    uint64_t *g0 = gp + ac.word, *g1 = gp + ac.word + 1;
+    switch (ac.kind) {
+      case QA_COUNT:
+      case QA_NN:
+        if (v0) atomicAdd(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
+        break;
+      case QA_FIRST:
+      case QA_FZERO:
+        if (v0 != ~0ULL) atomicMin(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
+        break;
+      case QA_ISUM:
+        if (ac.wide) add128(g0, g1, v0, (int64_t)lp[(int64_t)(ac.word + 1) * L]);
+        else if (v0) add128(g0, g1, v0, (int64_t)v0 < 0 ? -1 : 0);
+        break;
+      case QA_FSUM:
+        fsum_add(g0, g1, __longlong_as_double((long long)v0),
+                 __longlong_as_double((long long)lp[(int64_t)(ac.word + 1) * L]));
+        break;
+      case QA_IMIN:
+      case QA_FMIN:
+        if ((int64_t)v0 != (int64_t)A.init[ac.word]) atomicMin(reinterpret_cast<long long *>(g0), (long long)v0);
+        break;
+      case QA_IMAX:
+      case QA_FMAX:
+        if ((int64_t)v0 != (int64_t)A.init[ac.word]) atomicMax(reinterpret_cast<long long *>(g0), (long long)v0);
+        break;
+    }
+  }
+}
+
+}  // namespace qm

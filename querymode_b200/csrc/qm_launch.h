@@ -1,0 +1,38 @@
+// qm_launch.h — host-callable launchers of the kernels in qm_kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "qm_plan.h"
+
+#define QM_SCAN_THREADS 512
+#define QM_HLL_P 12
+
+size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words);
+cudaError_t qm_scan_configure(size_t smem_bytes, int *blocks_per_sm);
+cudaError_t qm_launch_scan(const qm_scan_args &a, int blocks, size_t smem_bytes, cudaStream_t st);
+cudaError_t qm_launch_init_table(uint64_t *t, int64_t n_slots_total, int stride, int hash_keys,
+                                 const qm_aggspec &A, int sm_count, cudaStream_t st);
+cudaError_t qm_launch_compact(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
+                              int first_word, uint64_t *keys_out, uint32_t *slots_out,
+                              unsigned long long *counter, int sm_count, cudaStream_t st);
+cudaError_t qm_sort_pairs(void *temp, size_t *temp_bytes, const uint64_t *kin, uint64_t *kout,
+                          const uint32_t *vin, uint32_t *vout, int64_t n, int end_bit, cudaStream_t st);
+cudaError_t qm_launch_emit(const uint64_t *t, int stride, const uint32_t *slots, int64_t G,
+                           const qm_keyspec &K, int64_t n_slots, const qm_outspec &O, unsigned char *out,
+                           int sm_count, cudaStream_t st);
+cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *sel, uint32_t *masks,
+                                   uint32_t *counts, int sm_count, cudaStream_t st);
+cudaError_t qm_exclusive_scan_u32(void *temp, size_t *temp_bytes, const uint32_t *in, uint64_t *out, int64_t n,
+                                  cudaStream_t st);
+cudaError_t qm_launch_select_write(int64_t n_tiles, const uint32_t *sel, const uint32_t *masks,
+                                   const uint64_t *offsets, uint32_t *out, int64_t max_out, int sm_count,
+                                   cudaStream_t st);
+cudaError_t qm_launch_minmax(const void *p, int dtype, const uint32_t *nulls, int64_t n, long long *out,
+                             int sm_count, cudaStream_t st);
+cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st);
+cudaError_t qm_launch_rehash(const uint64_t *old_t, int64_t old_cap, int stride, int count_word, uint64_t *new_t,
+                             int log2cap, qm_status *st, int sm_count, cudaStream_t stream);
+cudaError_t qm_launch_check_selection(const uint32_t *sel, int64_t n_sel, int64_t n_rows, qm_status *st,
+                                      int sm_count, cudaStream_t stream);

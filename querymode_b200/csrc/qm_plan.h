@@ -1,0 +1,177 @@
+// qm_plan.h — the lowered query plan shared by the host planner and the
+// kernels.  Plain-old-data only: it is passed by value as a kernel parameter
+// (single query) or copied into device memory (batched queries).
+//
+// A query is lowered into
+//   * predicate terms  — filters normalised so the kernel evaluates each as
+//     one integer range test or one IEEE comparison (the JS coercions of
+//     src/decode.ts:480-541 are folded into the bounds on the host);
+//   * a group key      — one 64-bit word per row (src/types.ts:10-18 builds a
+//     string; for numeric columns string equality is equality of this word);
+//   * accumulators     — the per-group state words of PartialAggState
+//     (src/partial-agg.ts:13-36) that the query's aggregates read.
+#pragma once
+#include <stdint.h>
+
+#define QM_MAX_TERMS 16
+#define QM_MAX_VCOLS 8
+#define QM_MAX_ACCS 16
+#define QM_MAX_WORDS 24
+#define QM_MAX_OUT 24
+#define QM_R 8                   // rows per lane per warp tile
+#define QM_TILE_ROWS (QM_R * 32) // rows per warp tile
+
+// ---- predicate terms -------------------------------------------------------
+enum qm_term_kind : int32_t {
+  QT_TRUE = 0,      // constant pass (still subject to the NULL rule)
+  QT_FALSE = 1,     // constant fail
+  QT_IRANGE = 2,    // integer column: lo <= v <= hi
+  QT_INRANGE = 3,   // integer column: v < lo || v > hi
+  QT_FCMP = 4,      // float column: v <op> f0 (IEEE, NaN compares false)
+  QT_FBETWEEN = 5,  // float column: v >= f0 && v <= f1
+  QT_FNBETWEEN = 6, // float column: v < f0 || v > f1
+  QT_FBIG = 7,      // float column vs bigint: BigInt(trunc(v)) <op> lo
+  QT_ISNULL = 8,
+  QT_NOTNULL = 9,
+};
+
+enum qm_cmp_op : int32_t { QC_EQ = 0, QC_NEQ, QC_LT, QC_LTE, QC_GT, QC_GTE };
+
+struct qm_term {
+  const void *data;
+  const uint32_t *nulls; // QMCB null bitmap viewed as 32-bit words, or null
+  int32_t dtype;         // QM_I32 / QM_I64 / QM_F32 / QM_F64
+  int32_t kind;          // qm_term_kind
+  int32_t op;            // qm_cmp_op for QT_FCMP / QT_FBIG
+  int32_t null_pass;     // result for a NULL cell: 0 (JS), or the result of
+                         // the test on 0 (WASM scan reads NULL as 0)
+  int64_t lo, hi;
+  double f0, f1;
+};
+
+struct qm_pred {
+  int32_t n_and;                   // terms [0, n_and) are ANDed
+  int32_t n_groups;                // OR groups after the AND terms
+  int32_t group_end[QM_MAX_TERMS]; // group g = terms [end[g-1], end[g])
+  qm_term t[QM_MAX_TERMS];
+};
+
+// ---- group key --------------------------------------------------------------
+enum qm_key_mode : int32_t {
+  QK_NONE = 0,   // no GROUP BY: one group
+  QK_DIRECT = 1, // slot = key - base, for a dense integer key range
+  QK_HASH = 2,   // open addressing on the 64-bit key
+};
+
+struct qm_keyspec {
+  int32_t n_cols;   // 0, 1 or 2 (two int32 columns pack into one word)
+  int32_t mode;     // qm_key_mode
+  const void *data[2];
+  const uint32_t *nulls[2];
+  int32_t dtype[2];
+  int64_t base;     // QK_DIRECT: smallest key
+};
+
+// ---- accumulators ----------------------------------------------------------
+enum qm_acc_kind : int32_t {
+  QA_COUNT = 0,  // rows in the group (COUNT(*)), u64
+  QA_FIRST = 1,  // smallest global row index, u64 (first-seen order)
+  QA_NN = 2,     // non-NULL cells of a column, u64
+  QA_ISUM = 3,   // exact integer sum, 2 words: lo u64, hi i64
+  QA_FSUM = 4,   // compensated float sum, 2 words: hi f64, lo f64
+  QA_IMIN = 5,   // i64
+  QA_IMAX = 6,   // i64
+  QA_FMIN = 7,   // order-preserving i64 image of a double (-0 as +0)
+  QA_FMAX = 8,
+  QA_FZERO = 9,  // min over zero cells of (row << 1 | sign bit), u64
+};
+
+struct qm_acc {
+  int32_t kind;
+  int32_t vcol;  // value column index, -1 for COUNT / FIRST
+  int32_t word;  // first word of the accumulator within a slot (after key)
+  int32_t wide;  // QA_ISUM over int64 cells (128-bit even block-locally)
+};
+
+struct qm_vcol {
+  const void *data;
+  const uint32_t *nulls;
+  int32_t dtype;
+  int32_t pad;
+};
+
+struct qm_aggspec {
+  int32_t n_accs;
+  int32_t n_words;   // accumulator words per slot (excluding the key word)
+  int32_t n_vcols;
+  int32_t acc_count; // index of QA_COUNT / QA_FIRST in accs
+  int32_t acc_first;
+  int32_t pad;
+  qm_acc acc[QM_MAX_ACCS];
+  qm_vcol vcol[QM_MAX_VCOLS];
+  uint64_t init[QM_MAX_WORDS]; // initial value of each accumulator word
+};
+
+// ---- outputs ---------------------------------------------------------------
+enum qm_out_kind : int32_t {
+  QO_KEY = 0,       // group key column `src`
+  QO_COUNT = 1,     // u64 word -> int64
+  QO_SUM_F = 2,     // FSUM -> double (NULL when nn == 0)
+  QO_AVG_F = 3,     // FSUM / nn
+  QO_SUM_I2F = 4,   // ISUM -> double (int32 column: JS number)
+  QO_AVG_I2F = 5,   // ISUM / nn (int32 column)
+  QO_SUM_I128 = 6,  // ISUM -> 128-bit (int64 column: JS bigint)
+  QO_AVG_BIG = 7,   // bigAvg (src/partial-agg.ts:38-44), int64 column
+  QO_MIN_I = 8,     // IMIN -> i64 or i32
+  QO_MAX_I = 9,
+  QO_MIN_F = 10,    // FMIN (+FZERO for the sign of a zero) -> double
+  QO_MAX_F = 11,
+};
+
+struct qm_out {
+  int32_t kind;
+  int32_t dtype;    // result dtype (QM_I32 / QM_I64 / QM_F64 / QM_I128)
+  int32_t word;     // main accumulator word
+  int32_t nn_word;  // count word deciding NULL (and the AVG divisor)
+  int32_t zero_word;// QA_FZERO word for float MIN/MAX, else -1
+  int32_t src;      // key column index for QO_KEY
+  int64_t offset;   // byte offset of the column in the output buffer
+  int64_t null_offset; // byte offset of its 32-bit-word null bitmap, or -1
+};
+
+struct qm_outspec {
+  int32_t n_out;
+  int32_t pad;
+  qm_out o[QM_MAX_OUT];
+};
+
+// ---- one launch of the fused filter + aggregate kernel ----------------------
+#define QM_EMPTY_KEY 0x8000000000000000ULL // free hash slot; a real key equal
+                                           // to it lives in a reserved slot
+struct qm_status {
+  int32_t error;      // QM_DEV_* below, first writer wins
+  int32_t pad;
+  unsigned long long rows_selected;
+  unsigned long long groups_inserted; // new keys claimed in the global table
+};
+#define QM_DEV_OK 0
+#define QM_DEV_OVERFLOW 1  // hash probe limit hit: regrow and re-run
+#define QM_DEV_RANGE 2     // direct-mapped key outside the planned range
+
+struct qm_scan_args {
+  qm_pred pred;
+  qm_keyspec key;
+  qm_aggspec agg;
+  int64_t n;             // elements: rows, or selection entries when sel != 0
+  const uint32_t *sel;   // ascending alive row indices, or null
+  int64_t row_offset;    // global index of row 0 (batch order across pushes)
+  uint64_t *table;       // group table: slot s = words [s*stride, (s+1)*stride)
+  int64_t n_slots;       // QK_HASH capacity (power of two) / QK_DIRECT size
+  int32_t stride;        // 1 key word + agg.n_words
+  int32_t log2cap;       // QK_HASH
+  int32_t local_slots;   // block-local table slots (0: none)
+  int32_t local_hash;    // block-local table is hashed (else direct-indexed)
+  int32_t dedupe;        // warp-level pre-aggregation of equal keys
+  int32_t max_probe;     // bound on linear probing in the global table
+  qm_status *status;
+};

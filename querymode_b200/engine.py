@@ -1,0 +1,371 @@
+"""Host-side handles over the C ABI: Context, Table, Result, AggStream.
+
+Everything here calls libqm_gpu.so through ctypes; there is no CPU compute
+path.  Columns are numpy arrays (int32 / int64 / float32 / float64) with an
+optional boolean NULL mask, or torch CUDA tensors already resident in HBM
+(passed by device pointer, read in place).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Any, Mapping
+
+import numpy as np
+
+from . import _abi as A
+from .query import CQuery, QueryDescriptor
+
+_NP_DTYPES = {
+    np.dtype(np.int32): A.QM_I32,
+    np.dtype(np.int64): A.QM_I64,
+    np.dtype(np.float32): A.QM_F32,
+    np.dtype(np.float64): A.QM_F64,
+}
+_QM_TO_NP = {A.QM_I32: np.int32, A.QM_I64: np.int64, A.QM_F32: np.float32, A.QM_F64: np.float64}
+
+
+def _check(lib, ctx_ptr, status: int) -> None:
+    if status != A.QM_OK:
+        msg = lib.qm_ctx_last_error(ctx_ptr) if ctx_ptr else b""
+        raise A.QmError(status, (msg or b"").decode(errors="replace"))
+
+
+def pack_nulls(mask: np.ndarray | None) -> np.ndarray | None:
+    """Boolean NULL mask -> QMCB bitmap (bit set = NULL, LSB first)."""
+    if mask is None:
+        return None
+    mask = np.asarray(mask, dtype=bool)
+    if not mask.any():
+        return None
+    return np.packbits(mask, bitorder="little")
+
+
+def unpack_nulls(bits: np.ndarray, n: int) -> np.ndarray:
+    return np.unpackbits(bits, count=n, bitorder="little").astype(bool)
+
+
+@dataclass
+class Column:
+    """One input column: values plus an optional NULL mask (True = NULL)."""
+    values: Any
+    nulls: np.ndarray | None = None
+
+
+class _ColumnSet:
+    """Builds the qm_column array for a mapping of name -> array / Column and
+    keeps every referenced buffer alive while the C side may read it."""
+
+    def __init__(self, columns: Mapping[str, Any]):
+        self.keep: list = []
+        cols = []
+        n_rows = None
+        for name, v in columns.items():
+            nulls = None
+            if isinstance(v, Column):
+                v, nulls = v.values, v.nulls
+            c = A.QmColumn()
+            nm = name.encode()
+            self.keep.append(nm)
+            c.name = nm
+            if _is_torch_cuda(v):
+                import torch  # noqa: F401  (plumbing for device-resident input)
+                if not v.is_contiguous():
+                    v = v.contiguous()
+                dt = _torch_dtype(v)
+                c.dtype = dt
+                c.on_device = 1
+                c.data = v.data_ptr()
+                n = v.numel()
+                self.keep.append(v)
+                if nulls is not None:
+                    raise ValueError("device-resident columns take no host NULL mask")
+            else:
+                arr = np.ascontiguousarray(v)
+                if arr.dtype not in _NP_DTYPES:
+                    raise TypeError(f"column {name}: dtype {arr.dtype} is not on the GPU path")
+                c.dtype = _NP_DTYPES[arr.dtype]
+                c.on_device = 0
+                c.data = arr.ctypes.data if arr.size else None
+                n = arr.size
+                self.keep.append(arr)
+                nb = pack_nulls(nulls)
+                if nb is not None:
+                    if len(nulls) != n:
+                        raise ValueError(f"column {name}: NULL mask length {len(nulls)} != {n}")
+                    self.keep.append(nb)
+                    c.null_bitmap = nb.ctypes.data
+            if n_rows is None:
+                n_rows = n
+            elif n != n_rows:
+                raise ValueError(f"column {name} has {n} rows, expected {n_rows}")
+            cols.append(c)
+        self.n_rows = n_rows or 0
+        self.array = (A.QmColumn * max(1, len(cols)))(*cols)
+        self.count = len(cols)
+
+
+def _is_torch_cuda(v) -> bool:
+    mod = type(v).__module__
+    return mod.startswith("torch") and getattr(v, "is_cuda", False)
+
+
+def _torch_dtype(t) -> int:
+    import torch
+    m = {torch.int32: A.QM_I32, torch.int64: A.QM_I64, torch.float32: A.QM_F32,
+         torch.float64: A.QM_F64}
+    if t.dtype not in m:
+        raise TypeError(f"tensor dtype {t.dtype} is not on the GPU path")
+    return m[t.dtype]
+
+
+@dataclass
+class ResultColumn:
+    name: str
+    dtype: int
+    is_key: bool
+    values: np.ndarray       # I128 columns: shape (n, 2) int64 [lo, hi]
+    nulls: np.ndarray | None  # bool, True = NULL
+
+    def pyvalues(self) -> list:
+        """Python values: int for integer results, float for float ones,
+        None for NULL."""
+        n = len(self.values)
+        if self.dtype == A.QM_I128:
+            lo = self.values[:, 0].astype(np.uint64)
+            hi = self.values[:, 1]
+            out = [(int(h) << 64) | int(l) for l, h in zip(lo, hi)]
+        elif self.dtype == A.QM_F64:
+            out = [float(x) for x in self.values]
+        else:
+            out = [int(x) for x in self.values]
+        if self.nulls is not None:
+            out = [None if self.nulls[i] else out[i] for i in range(n)]
+        return out
+
+
+@dataclass
+class Stats:
+    rows_scanned: int
+    rows_selected: int
+    groups: int
+    bytes_scanned: int
+    device_ms: float
+    strategy: int
+    table_capacity: int
+    retries: int
+    launches: int
+    scan_ms: float
+
+
+class Result:
+    """Typed result columns (keys first, then aggregates in query order)."""
+
+    def __init__(self, columns: list[ResultColumn], n_rows: int, stats: Stats | None = None,
+                 qmcb: bytes | None = None):
+        self.columns = columns
+        self.n_rows = n_rows
+        self.stats = stats
+        self.qmcb = qmcb
+
+    def column(self, name: str) -> ResultColumn:
+        for c in self.columns:
+            if c.name == name:
+                return c
+        raise KeyError(name)
+
+    @property
+    def names(self) -> list[str]:
+        return [c.name for c in self.columns]
+
+    @classmethod
+    def from_handle(cls, lib, handle: C.c_void_p, with_qmcb: bool = False) -> "Result":
+        n = C.c_int64()
+        nc = C.c_int32()
+        lib.qm_result_num_rows(handle, C.byref(n))
+        lib.qm_result_num_columns(handle, C.byref(nc))
+        cols = []
+        for i in range(nc.value):
+            rc = A.QmResultCol()
+            lib.qm_result_column(handle, i, C.byref(rc))
+            cols.append(_read_col(rc, n.value))
+        st = A.QmStats()
+        lib.qm_result_stats(handle, C.byref(st))
+        stats = Stats(st.rows_scanned, st.rows_selected, st.groups, st.bytes_scanned, st.device_ms,
+                      st.strategy, st.table_capacity, st.retries, st.launches, st.scan_ms)
+        qmcb = None
+        if with_qmcb:
+            p = C.c_void_p()
+            ln = C.c_size_t()
+            if lib.qm_result_qmcb(handle, C.byref(p), C.byref(ln)) == A.QM_OK:
+                qmcb = C.string_at(p, ln.value)
+        return cls(cols, n.value, stats, qmcb)
+
+
+def _read_col(rc: A.QmResultCol, n: int) -> ResultColumn:
+    name = rc.name.decode()
+    if rc.dtype == A.QM_I128:
+        buf = C.string_at(rc.data, 16 * n) if n else b""
+        vals = np.frombuffer(buf, dtype=np.int64).reshape(n, 2).copy()
+    else:
+        dt = _QM_TO_NP[rc.dtype]
+        size = np.dtype(dt).itemsize
+        buf = C.string_at(rc.data, size * n) if n else b""
+        vals = np.frombuffer(buf, dtype=dt).copy()
+    nulls = None
+    if rc.null_bitmap:
+        bits = np.frombuffer(C.string_at(rc.null_bitmap, (n + 7) // 8), dtype=np.uint8)
+        nulls = unpack_nulls(bits, n)
+    return ResultColumn(name, rc.dtype, bool(rc.is_key), vals, nulls)
+
+
+class Context:
+    """A qm_ctx: one CUDA device, one stream, cached scratch memory.
+
+    Like the reference's per-Durable-Object engine, a context serves one host
+    thread at a time."""
+
+    def __init__(self, device: int = 0, lib: C.CDLL | None = None):
+        self.lib = lib or A.load_library()
+        h = C.c_void_p()
+        st = self.lib.qm_ctx_create(device, C.byref(h))
+        if st != A.QM_OK:
+            raise A.QmError(st, f"qm_ctx_create(device={device})")
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.qm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def check(self, status: int) -> None:
+        _check(self.lib, self.h, status)
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        """Order this context's work on a CUDA stream handle (e.g.
+        ``torch.cuda.current_stream().cuda_stream``); None restores the
+        context's own stream."""
+        self.check(self.lib.qm_ctx_set_stream(self.h, stream_handle or None))
+
+    def device_info(self) -> tuple[int, int]:
+        sm = C.c_int32()
+        hbm = C.c_int64()
+        self.check(self.lib.qm_ctx_device_info(self.h, C.byref(sm), C.byref(hbm)))
+        return sm.value, hbm.value
+
+    # -- tables --------------------------------------------------------------
+    def table(self, columns: Mapping[str, Any]) -> "Table":
+        cs = _ColumnSet(columns)
+        h = C.c_void_p()
+        self.check(self.lib.qm_table_create(self.h, cs.n_rows, cs.count, cs.array, C.byref(h)))
+        return Table(self, h, cs.n_rows, list(columns.keys()), keep=cs.keep)
+
+    def table_from_qmcb(self, buf: bytes) -> "Table":
+        b = bytes(buf)
+        h = C.c_void_p()
+        self.check(self.lib.qm_table_from_qmcb(self.h, b, len(b), C.byref(h)))
+        n = C.c_int64()
+        self.lib.qm_table_num_rows(h, C.byref(n))
+        return Table(self, h, n.value, [])
+
+    # -- filter-only ---------------------------------------------------------
+    def filter_select(self, columns: Mapping[str, Any], query: QueryDescriptor) -> np.ndarray:
+        """Ascending indices of the rows passing query's filters."""
+        cs = _ColumnSet(columns)
+        cq = CQuery(query)
+        cap = cs.n_rows
+        out = np.empty(max(cap, 1), dtype=np.uint32)
+        cnt = C.c_int64()
+        self.check(self.lib.qm_filter_select(
+            self.h, cs.n_rows, cs.count, cs.array, cq.ref,
+            out.ctypes.data_as(C.POINTER(C.c_uint32)), cap, C.byref(cnt)))
+        return out[:cnt.value].copy()
+
+    def aggregate(self, query: QueryDescriptor) -> "AggStream":
+        return AggStream(self, query)
+
+
+class Table:
+    """A qm_table: numeric columns resident in HBM."""
+
+    def __init__(self, ctx: Context, h: C.c_void_p, n_rows: int, names: list[str], keep=None):
+        self.ctx = ctx
+        self.h = h
+        self.n_rows = n_rows
+        self.names = names
+        self._keep = keep  # device-resident inputs are read in place
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.ctx.lib.qm_table_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, query: QueryDescriptor, with_qmcb: bool = False) -> Result:
+        cq = CQuery(query)
+        r = C.c_void_p()
+        self.ctx.check(self.ctx.lib.qm_query_run(self.ctx.h, self.h, cq.ref, C.byref(r)))
+        try:
+            return Result.from_handle(self.ctx.lib, r, with_qmcb)
+        finally:
+            self.ctx.lib.qm_result_destroy(r)
+
+
+class AggStream:
+    """Streaming aggregation: push batches in order, then finish
+    (AggregateOperator.next's drain loop, src/operators.ts:1656-1681)."""
+
+    def __init__(self, ctx: Context, query: QueryDescriptor):
+        self.ctx = ctx
+        self.cq = CQuery(query)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.qm_agg_begin(ctx.h, self.cq.ref, C.byref(h)))
+        self.h = h
+
+    def push(self, columns: Mapping[str, Any], selection: np.ndarray | None = None) -> None:
+        cs = _ColumnSet(columns)
+        sel_ptr = None
+        n_sel = 0
+        if selection is not None:
+            sel = np.ascontiguousarray(selection, dtype=np.uint32)
+            cs.keep.append(sel)
+            sel_ptr = sel.ctypes.data_as(C.POINTER(C.c_uint32))
+            n_sel = sel.size
+        self.ctx.check(self.ctx.lib.qm_agg_push(self.h, cs.n_rows, cs.count, cs.array, sel_ptr, n_sel))
+
+    def finish(self, with_qmcb: bool = False) -> Result:
+        r = C.c_void_p()
+        self.ctx.check(self.ctx.lib.qm_agg_finish(self.h, C.byref(r)))
+        try:
+            return Result.from_handle(self.ctx.lib, r, with_qmcb)
+        finally:
+            self.ctx.lib.qm_result_destroy(r)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.ctx.lib.qm_agg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,262 @@
+"""GPU path vs the CPU oracle, through the C ABI (libqm_gpu.so via ctypes).
+
+Bit-exact: group keys and their first-seen order, COUNT, integer SUM / MIN /
+MAX, float MIN / MAX (the sign of a zero included).  Float SUM / AVG: within
+1e-12 relative (tests/helpers.py states the fallback for cancelling sums).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from querymode_b200 import _abi as A
+from querymode_b200 import datagen
+from querymode_b200.engine import Column
+from querymode_b200.query import AggregateOp, BigInt, FilterOp, QueryDescriptor
+from tests.helpers import assert_same
+from tests.test_oracle_golden import golden_columns, golden_query, load_golden
+from tests.test_oracle_jsref import make_table, rand_query
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(ctx, cols, q, batch_rows=0):
+    t = ctx.table(cols)
+    g = t.run(q)
+    r = oracle.run(cols, q, batch_rows=batch_rows)
+    return g, r
+
+
+def test_orders_1m(ctx):
+    cols = datagen.orders()
+    g, r = run_both(ctx, cols, datagen.orders_query())
+    assert g.n_rows == 16
+    assert_same(g, r)
+    assert g.stats.rows_selected == int((cols["status"] == 1).sum())
+
+
+def test_events_4m(ctx):
+    cols = datagen.events(4_000_000, seed=11)
+    q = datagen.events_query()
+    g, r = run_both(ctx, cols, q)
+    assert g.n_rows > 1000
+    assert_same(g, r)
+
+
+def test_wide_keys_filtered_and_full(ctx):
+    cols = datagen.wide_keys(6_000_000, seed=12, n_keys=1 << 20)
+    for filtered in (True, False):
+        g, r = run_both(ctx, cols, datagen.wide_keys_query(filtered))
+        assert_same(g, r, ctx_msg=f"filtered={filtered}")
+
+
+def test_generate_rows_conformance(ctx):
+    cols = datagen.generate_rows(5_000_000)
+    q = QueryDescriptor(group_by=["region"], aggregates=[
+        AggregateOp("sum", "amount", "sum_amount"), AggregateOp("avg", "amount", "avg_amount"),
+        AggregateOp("min", "amount", "min_amount"), AggregateOp("max", "amount", "max_amount"),
+        AggregateOp("count", "amount", "cnt")])
+    g, r = run_both(ctx, cols, q, batch_rows=4096)
+    assert_same(g, r)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_queries(ctx, seed):
+    rng = np.random.default_rng(1000 + seed)
+    cols = make_table(rng, n=int(rng.choice([300, 5000, 70000])))
+    q = rand_query(rng)
+    g, r = run_both(ctx, cols, q)
+    assert_same(g, r, ctx_msg=str(q))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_streamed_batches_and_selection(ctx, seed):
+    rng = np.random.default_rng(7000 + seed)
+    n = 20000
+    cols = make_table(rng, n=n)
+    q = rand_query(rng)
+    batch = int(rng.choice([1000, 4096, 7777]))
+    # reference: AggregateOperator over batches whose selection vectors keep
+    # every third row (a scan that already filtered)
+    keep = np.arange(n) % 3 != 1
+    ref_cols = {k: Column(v.values[keep], None if v.nulls is None else v.nulls[keep]) for k, v in cols.items()}
+    s = ctx.aggregate(q)
+    for b0 in range(0, n, batch):
+        b1 = min(n, b0 + batch)
+        part = {k: Column(v.values[b0:b1], None if v.nulls is None else v.nulls[b0:b1]) for k, v in cols.items()}
+        sel = np.nonzero(keep[b0:b1])[0].astype(np.uint32)
+        s.push(part, selection=sel)
+    g = s.finish()
+    s.close()
+    r = oracle.run(ref_cols, q, batch_rows=0)
+    assert_same(g, r, ctx_msg=str(q))
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_filter_select_random(ctx, seed):
+    rng = np.random.default_rng(5000 + seed)
+    cols = make_table(rng, n=int(rng.choice([300, 10000, 100000])))
+    q = rand_query(rng)
+    assert ctx.filter_select(cols, q).tolist() == oracle.filter_select(cols, q).tolist()
+
+
+@pytest.mark.parametrize("case", load_golden()["cases"], ids=lambda c: c["name"])
+def test_filter_fixtures_gpu(ctx, case):
+    g = load_golden()
+    got = ctx.filter_select(golden_columns(g), golden_query(case))
+    assert got.tolist() == case["expected_rows"], case["query"]
+
+
+def test_empty_and_all_filtered(ctx):
+    cols = {"k": np.array([1, 2, 3], np.int64), "v": np.array([1.0, 2.0, 3.0])}
+    q = QueryDescriptor(filters=[FilterOp("v", "gt", 10)], group_by=["k"],
+                        aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")])
+    g, r = run_both(ctx, cols, q)
+    assert g.n_rows == 0 and r.n_rows == 0
+    q2 = QueryDescriptor(filters=[FilterOp("v", "gt", 10)],
+                         aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")])
+    g, r = run_both(ctx, cols, q2)
+    assert g.n_rows == 1 and g.column("count_*").pyvalues() == [0] and g.column("sum_v").pyvalues() == [None]
+    assert_same(g, r)
+    empty = {"k": np.zeros(0, np.int64), "v": np.zeros(0)}
+    g, r = run_both(ctx, empty, q)
+    assert g.n_rows == 0 and r.n_rows == 0
+
+
+def test_extreme_int64_keys_and_sums(ctx):
+    imin, imax = np.iinfo(np.int64).min, np.iinfo(np.int64).max
+    keys = np.array([imin, imax, 0, imin, -1, imax, imin] * 1000, np.int64)
+    vals = np.array([imax, imax, imin, imin, 5, imax, -3] * 1000, np.int64)
+    cols = {"k": keys, "v": vals}
+    q = QueryDescriptor(group_by=["k"], aggregates=[
+        AggregateOp("sum", "v"), AggregateOp("avg", "v"), AggregateOp("min", "v"), AggregateOp("max", "v"),
+        AggregateOp("count", "*")])
+    g, r = run_both(ctx, cols, q)
+    assert_same(g, r)
+    sums = g.column("sum_v").pyvalues()
+    assert max(abs(s) for s in sums) > 2**63  # beyond int64: exact 128-bit
+
+
+def test_random_int64_keys_hash_mode(ctx):
+    rng = np.random.default_rng(3)
+    universe = rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, 300_000, dtype=np.int64)
+    keys = universe[rng.integers(0, universe.size, 3_000_000)]
+    cols = {"k": keys, "v": rng.normal(0, 1, keys.size), "w": rng.integers(-100, 100, keys.size).astype(np.int32)}
+    q = QueryDescriptor(filters=[FilterOp("w", "gte", -50)], group_by=["k"],
+                        aggregates=[AggregateOp("sum", "v"), AggregateOp("min", "w"), AggregateOp("max", "v"),
+                                    AggregateOp("count", "*"), AggregateOp("avg", "w")])
+    g, r = run_both(ctx, cols, q)
+    assert g.stats.strategy in (1, 2)
+    assert_same(g, r)
+
+
+def test_signed_zero_first_seen_min_max(ctx):
+    # strict '<' / '>' keep the first of -0 and 0 (src/partial-agg.ts:80-81)
+    v = np.array([0.0, -0.0, 0.0, 5.0, -0.0, 0.0, -0.0, 0.0], np.float64)
+    k = np.array([0, 0, 1, 1, 2, 2, 3, 3], np.int32)
+    q = QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("min", "v"), AggregateOp("max", "v"),
+                                                    AggregateOp("sum", "v")])
+    big_v = np.tile(v, 5000)
+    big_k = np.tile(k, 5000) + np.repeat(np.arange(5000, dtype=np.int32) * 4, 8)
+    for cols in ({"k": k, "v": v}, {"k": big_k, "v": big_v}):
+        g, r = run_both(ctx, cols, q)
+        assert_same(g, r)
+    mins = g.column("min_v").values
+    assert np.signbit(mins[0]) == False and np.signbit(mins[3]) == True  # noqa: E712
+
+
+def test_nan_inf_values_and_keys(ctx):
+    v = np.array([math.nan, 1.0, math.inf, -math.inf, 2.0, math.nan, math.inf, 3.0])
+    k = np.array([math.nan, math.nan, 0.0, -0.0, math.inf, 1.0, 1.0, -math.inf])
+    q = QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("sum", "v"), AggregateOp("min", "v"),
+                                                    AggregateOp("max", "v"), AggregateOp("avg", "v"),
+                                                    AggregateOp("count", "v")])
+    g, r = run_both(ctx, {"k": k, "v": v}, q)
+    assert_same(g, r)
+
+
+def test_nullable_keys_and_values(ctx):
+    rng = np.random.default_rng(9)
+    n = 200_000
+    cols = {"k": Column(rng.integers(0, 50, n).astype(np.int64), rng.random(n) < 0.05),
+            "x": Column(rng.normal(size=n), rng.random(n) < 0.2),
+            "y": Column(rng.integers(-9, 9, n).astype(np.int32), rng.random(n) < 0.3)}
+    q = QueryDescriptor(filters=[FilterOp("y", "is_not_null")], group_by=["k"],
+                        aggregates=[AggregateOp("count", "x"), AggregateOp("sum", "x"), AggregateOp("min", "y"),
+                                    AggregateOp("avg", "y"), AggregateOp("count", "*")])
+    g, r = run_both(ctx, cols, q)
+    assert_same(g, r)
+
+
+def test_two_int32_keys_and_f32(ctx):
+    rng = np.random.default_rng(4)
+    n = 300_000
+    cols = {"a": rng.integers(-3, 3, n).astype(np.int32), "b": rng.integers(0, 1000, n).astype(np.int32),
+            "f": rng.normal(size=n).astype(np.float32)}
+    q = QueryDescriptor(filters=[FilterOp("f", "lt", 0.5)], group_by=["a", "b"],
+                        aggregates=[AggregateOp("sum", "f"), AggregateOp("max", "f"), AggregateOp("count", "*")])
+    g, r = run_both(ctx, cols, q)
+    assert_same(g, r)
+
+
+def test_wasm_scan_semantics(ctx):
+    rng = np.random.default_rng(5)
+    n = 50_000
+    cols = {"i": Column(rng.integers(-10, 10, n).astype(np.int32), rng.random(n) < 0.1),
+            "f": Column(rng.normal(size=n), rng.random(n) < 0.1),
+            "k": rng.integers(0, 7, n).astype(np.int32)}
+    for flt in ([FilterOp("i", "lt", 2.5)], [FilterOp("f", "eq", 0)], [FilterOp("i", "between", [-0.5, 3.7])],
+                [FilterOp("i", "gt", 3e9)], [FilterOp("f", "not_between", [-0.1, 0.1])]):
+        q = QueryDescriptor(filters=flt, group_by=["k"], aggregates=[AggregateOp("count", "*")],
+                            flags=A.QM_FLAG_WASM_SCAN_SEMANTICS)
+        g, r = run_both(ctx, cols, q)
+        assert_same(g, r, ctx_msg=str(flt))
+
+
+def test_bigint_thresholds(ctx):
+    cols = {"i": np.arange(-50, 50, dtype=np.int64), "f": np.linspace(-5.5, 5.5, 100),
+            "k": np.zeros(100, np.int32)}
+    for flt in ([FilterOp("i", "gt", BigInt(7))], [FilterOp("f", "lte", BigInt(2))], [FilterOp("f", "eq", BigInt(0))],
+                [FilterOp("i", "between", [BigInt(-3), 4.5])], [FilterOp("i", "lt", -2.5)]):
+        q = QueryDescriptor(filters=flt, group_by=["k"], aggregates=[AggregateOp("count", "*")])
+        g, r = run_both(ctx, cols, q)
+        assert_same(g, r, ctx_msg=str(flt))
+
+
+def test_unordered_flag_same_groups(ctx):
+    cols = datagen.events(1_000_000, seed=21)
+    q = datagen.events_query()
+    q.flags = A.QM_FLAG_UNORDERED
+    g = ctx.table(cols).run(q)
+    q2 = datagen.events_query()
+    r = oracle.run(cols, q2)
+    assert_same(g, r, ordered=False)
+
+
+def test_qmcb_roundtrip(ctx):
+    from querymode_b200 import qmcb
+    rng = np.random.default_rng(6)
+    n = 10_000
+    cols = {"k": Column(rng.integers(0, 9, n).astype(np.int32), rng.random(n) < 0.1),
+            "v": rng.normal(size=n), "w": rng.integers(0, 10, n).astype(np.int64)}
+    buf = qmcb.encode(cols)
+    t = ctx.table_from_qmcb(buf)
+    q = QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("sum", "v"), AggregateOp("sum", "w"),
+                                                    AggregateOp("count", "*")])
+    g = t.run(q, with_qmcb=True)
+    r = oracle.run(cols, q)
+    assert_same(g, r)
+    dec = qmcb.decode(g.qmcb)
+    assert dec.names == g.names
+    assert np.array_equal(dec.column("sum_v").values, g.column("sum_v").values)
+
+
+def test_device_resident_columns(ctx):
+    import torch
+    cols = datagen.events(2_000_000, seed=31)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in cols.items()}
+    q = datagen.events_query()
+    g = ctx.table(dev).run(q)
+    r = oracle.run(cols, q)
+    assert_same(g, r)
