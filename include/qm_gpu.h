@@ -184,6 +184,17 @@ typedef struct {
   double scan_ms;         /* CUDA-event time of the fused scan kernel(s)    */
 } qm_stats;
 
+/* Launch-shape knobs of the fused scan kernel, chosen by the autotuner
+ * (querymode_b200/autotune.py).  Zero / negative fields mean "planner's
+ * choice".  No reference counterpart (the WASM engine has no launch shape). */
+typedef struct {
+  int32_t local_slots;   /* block-local table slots: 0 auto, -1 none, else a power of two */
+  int32_t dedupe;        /* warp-level merge of equal keys: -1 auto, 0 off, 1 on */
+  int32_t blocks_per_sm; /* resident blocks per SM: 0 auto (occupancy), else a cap */
+  int32_t stage_depth;   /* filter-column tiles in flight per warp (bulk async
+                            copies into shared memory): 0 auto, -1 off, 2..4 */
+} qm_tuning;
+
 /* ---- library / context ---------------------------------------------------- */
 const char *qm_version(void);
 
@@ -200,6 +211,8 @@ const char *qm_ctx_last_error(const qm_ctx *ctx);
  * WASM engine has no streams; this lets a host framework time or overlap
  * the path with its own work. */
 int qm_ctx_set_stream(qm_ctx *ctx, void *stream);
+/* Set (tuning != NULL) or clear (NULL) the context's launch-shape knobs. */
+int qm_ctx_set_tuning(qm_ctx *ctx, const qm_tuning *tuning);
 /* Device properties the host planner and tests read. */
 int qm_ctx_device_info(const qm_ctx *ctx, int32_t *sm_count, int64_t *hbm_bytes);
 

@@ -88,6 +88,11 @@ class QmQuery(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class QmTuning(C.Structure):
+    _fields_ = [("local_slots", C.c_int32), ("dedupe", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("stage_depth", C.c_int32)]
+
+
 class QmResultCol(C.Structure):
     _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("is_key", C.c_int32),
                 ("n_rows", C.c_int64), ("data", C.c_void_p), ("null_bitmap", C.c_void_p)]
@@ -113,6 +118,7 @@ SIGNATURES = [
     ("qm_ctx_destroy", C.c_int, [_P]),
     ("qm_ctx_last_error", C.c_char_p, [_P]),
     ("qm_ctx_set_stream", C.c_int, [_P, C.c_void_p]),
+    ("qm_ctx_set_tuning", C.c_int, [_P, C.c_void_p]),
     ("qm_ctx_device_info", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("qm_table_create", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn), _PP]),
     ("qm_table_from_qmcb", C.c_int, [_P, C.c_void_p, C.c_size_t, _PP]),

@@ -52,6 +52,7 @@ struct qm_ctx {
   cudaStream_t own_stream = nullptr;  // the context's own stream
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs0 = nullptr, evs1 = nullptr;
   int launches = 0;  // kernels of this library launched since the last reset
+  qm_tuning tuning{0, -1, 0, 0};  // local_slots, dedupe, blocks_per_sm, stage_depth
   std::string err;
   // grow-only scratch reused across runs of this context
   DevBuf table, status, keys, slots, keys2, slots2, sort_temp, counter, out, hll;
@@ -240,6 +241,7 @@ struct Plan {
   int64_t bytes_per_row = 0;  // algorithmic: widths of referenced columns
   bool ordered = true;
   int key_col_dtype = 0;
+  const DevCol *keycols[QM_MAX_KEYS] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 const i128 BIG = (i128)1 << 100;
@@ -437,17 +439,38 @@ int lower_filter(qm_ctx *ctx, const qm_filter &f, const ColView &cv, bool wasm_f
       t.lo = f.value.big;
       return QM_OK;
     }
-    t.kind = QT_FCMP;
-    t.op = f.op;
-    t.f0 = f.value.num;
-    if (wasm) t.null_pass = fcmp_host(0.0, f.op, t.f0) ? 1 : 0;
+    const double v = f.value.num;
+    if (wasm) t.null_pass = fcmp_host(0.0, f.op, v) ? 1 : 0;
+    if (f.op == QM_OP_NEQ) {
+      t.kind = QT_FCMP;
+      t.op = f.op;
+      t.f0 = v;
+      return QM_OK;
+    }
+    if (std::isnan(v)) {  // every comparison with NaN is false
+      t.kind = QT_FALSE;
+      return QM_OK;
+    }
+    t.kind = QT_FRANGE;
+    t.f0 = -INFINITY;
+    t.f1 = INFINITY;
+    t.op = 3;
+    switch (f.op) {
+      case QM_OP_EQ: t.f0 = t.f1 = v; break;
+      case QM_OP_LT: t.f1 = v; t.op = 1; break;
+      case QM_OP_LTE: t.f1 = v; break;
+      case QM_OP_GT: t.f0 = v; t.op = 2; break;
+      default: t.f0 = v; break;  // GTE
+    }
     return QM_OK;
   }
   if (f.value.kind != QM_VAL_NUMBER || f.value2.kind != QM_VAL_NUMBER)
     return set_err(ctx, QM_ERR_UNSUPPORTED, "BETWEEN with bigint bounds on float column %s", c.name.c_str());
-  t.kind = f.op == QM_OP_BETWEEN ? QT_FBETWEEN : QT_FNBETWEEN;
+  t.kind = f.op == QM_OP_BETWEEN ? QT_FRANGE : QT_FNBETWEEN;
+  t.op = 3;
   t.f0 = f.value.num;
   t.f1 = f.value2.num;
+  if (f.op == QM_OP_BETWEEN && (std::isnan(t.f0) || std::isnan(t.f1))) t.kind = QT_FALSE;
   if (wasm) {
     bool p = f.op == QM_OP_BETWEEN ? (0.0 >= t.f0 && 0.0 <= t.f1) : (0.0 < t.f0 || 0.0 > t.f1);
     t.null_pass = p ? 1 : 0;
@@ -486,6 +509,31 @@ int build_pred(qm_ctx *ctx, const qm_query *q, const ColEnv &env, qm_pred &P, in
   for (int i = 0; i < q->n_filters; i++) {
     int rc = add(q->filters[i]);
     if (rc) return rc;
+    // AND-ed range tests on one column become one test (one read per row)
+    qm_term &nw = P.t[nt - 1];
+    for (int j = 0; j < nt - 1; j++) {
+      qm_term &o = P.t[j];
+      if (o.data != nw.data || o.kind != nw.kind || o.dtype != nw.dtype) continue;
+      if (nw.kind == QT_IRANGE) {
+        o.lo = std::max(o.lo, nw.lo);
+        o.hi = std::min(o.hi, nw.hi);
+        if (o.lo > o.hi) o.kind = QT_FALSE;
+      } else if (nw.kind == QT_FRANGE) {
+        if (nw.f0 > o.f0 || (nw.f0 == o.f0 && !(nw.op & 1))) {
+          o.f0 = nw.f0;
+          o.op = (o.op & ~1) | (nw.op & 1);
+        }
+        if (nw.f1 < o.f1 || (nw.f1 == o.f1 && !(nw.op & 2))) {
+          o.f1 = nw.f1;
+          o.op = (o.op & ~2) | (nw.op & 2);
+        }
+      } else {
+        continue;
+      }
+      o.null_pass = o.null_pass && nw.null_pass;
+      nt--;
+      break;
+    }
   }
   P.n_and = nt;
   int off = 0;
@@ -518,8 +566,9 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
   memset(&A, 0, sizeof A);
   pl.meta.clear();
   if (q->n_group_by < 0 || q->n_aggregates < 0) return set_err(ctx, QM_ERR_INVALID, "negative counts");
-  if (q->n_group_by > 2) return set_err(ctx, QM_ERR_UNSUPPORTED, "GROUP BY over more than 2 columns");
-  const DevCol *kc[2] = {nullptr, nullptr};
+  if (q->n_group_by > QM_MAX_KEYS)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "GROUP BY over more than %d columns", QM_MAX_KEYS);
+  const DevCol *kc[QM_MAX_KEYS] = {nullptr, nullptr, nullptr, nullptr};
   for (int i = 0; i < q->n_group_by; i++) {
     if (!q->group_by[i]) return set_err(ctx, QM_ERR_INVALID, "group column without a name");
     const ColView *cv = env.find(q->group_by[i]);
@@ -528,15 +577,13 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
     if (std::find(touched.begin(), touched.end(), cv->col) == touched.end()) touched.push_back(cv->col);
   }
   K.n_cols = q->n_group_by;
-  if (K.n_cols == 2) {
-    if (kc[0]->dtype != QM_I32 || kc[1]->dtype != QM_I32 || kc[0]->nulls || kc[1]->nulls)
-      return set_err(ctx, QM_ERR_UNSUPPORTED, "two-column GROUP BY needs two non-null int32 columns");
-  }
   for (int i = 0; i < K.n_cols; i++) {
     K.data[i] = kc[i]->data;
     K.nulls[i] = kc[i]->nulls;
     K.dtype[i] = kc[i]->dtype;
+    pl.keycols[i] = kc[i];
   }
+  K.pack = QP_RAW;  // multi-column packing is chosen with the key mode
   // accumulators
   auto add_acc = [&](int kind, int vcol, int wide) -> int {
     for (int i = 0; i < A.n_accs; i++)
@@ -663,6 +710,26 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
     pl.meta.push_back({name, o.dtype, 0, ag.fn != QM_AGG_COUNT});
   }
   A.n_vcols = (int)vcols.size();
+  A.w_count = A.acc[A.acc_count].word;
+  A.w_first = A.acc_first >= 0 ? A.acc[A.acc_first].word : -1;
+  for (int c = 0; c < A.n_vcols; c++) {
+    qm_vcol &vc = A.vcol[c];
+    vc.flags = 0;
+    vc.w_nn = vc.w_sum = vc.w_min = vc.w_max = vc.w_zero = -1;
+  }
+  for (int i = 0; i < A.n_accs; i++) {
+    const qm_acc &ac = A.acc[i];
+    if (ac.vcol < 0) continue;
+    qm_vcol &vc = A.vcol[ac.vcol];
+    switch (ac.kind) {
+      case QA_NN: vc.flags |= VF_NN; vc.w_nn = ac.word; break;
+      case QA_ISUM: vc.flags |= VF_SUM | (ac.wide ? VF_WIDE : 0); vc.w_sum = ac.word; break;
+      case QA_FSUM: vc.flags |= VF_SUM; vc.w_sum = ac.word; break;
+      case QA_IMIN: case QA_FMIN: vc.flags |= VF_MIN; vc.w_min = ac.word; break;
+      case QA_IMAX: case QA_FMAX: vc.flags |= VF_MAX; vc.w_max = ac.word; break;
+      case QA_FZERO: vc.flags |= VF_ZERO; vc.w_zero = ac.word; break;
+    }
+  }
   return QM_OK;
 }
 
@@ -686,9 +753,9 @@ int ilog2_ceil(int64_t x) {
   return l;
 }
 
-constexpr size_t LOCAL_BUDGET = 96 * 1024;  // bytes of the block-local table
+constexpr size_t LOCAL_BUDGET = 40 * 1024;  // bytes of the block-local table
 
-void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex) {
+void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning &tu) {
   const int words = pl.agg.n_words;
   ex.stride = 1 + words;
   ex.total_slots = ex.n_slots + special_slots(pl.key.mode);
@@ -700,53 +767,84 @@ void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex) {
     ex.strategy = 0;
     return;
   }
-  if (pl.key.mode == QK_DIRECT && (ex.n_slots + 1) * per_slot <= (int64_t)LOCAL_BUDGET) {
+  if (pl.key.mode == QK_DIRECT && tu.local_slots >= 0 && (ex.n_slots + 1) * per_slot <= (int64_t)LOCAL_BUDGET) {
     ex.local_slots = (int)(ex.n_slots + 1);
     ex.local_hash = 0;
-    ex.dedupe = 1;
+    ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : (ex.n_slots <= 256 ? 1 : 0);
     ex.strategy = 0;
     return;
   }
-  if (est_groups <= ((int64_t)1 << 20)) {
+  if (tu.local_slots > 0 || (tu.local_slots == 0 && est_groups <= ((int64_t)1 << 20))) {
     int L = 1;
     while ((int64_t)(L * 2) * (per_slot + 8) <= (int64_t)LOCAL_BUDGET) L *= 2;
+    if (tu.local_slots > 0) {
+      L = tu.local_slots;
+      while (L > 1 && (int64_t)L * (per_slot + 8) > (int64_t)200 * 1024) L /= 2;  // fit shared memory
+    }
     ex.local_slots = L;
     ex.local_hash = 1;
-    ex.dedupe = 1;
+    ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : 0;
     ex.strategy = 1;
     return;
   }
   ex.local_slots = 0;
   ex.local_hash = 0;
-  ex.dedupe = 0;
+  ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : 0;
   ex.strategy = 2;
 }
 
 std::mutex g_cfg_mu;
-size_t g_cfg_smem = 0;
 
-int scan_blocks(qm_ctx *ctx, size_t smem, int64_t n) {
+int scan_blocks(qm_ctx *ctx, size_t smem, int64_t n, bool staged) {
   int bps = 1;
   {
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    size_t want = std::max(smem, g_cfg_smem);
-    if (qm_scan_configure(want, &bps) != cudaSuccess) {
-      cudaGetLastError();
-      bps = 1;
-    }
-    g_cfg_smem = want;
-    if (qm_scan_configure(smem, &bps) != cudaSuccess) {
+    if (qm_scan_configure(smem, staged, &bps) != cudaSuccess) {
       cudaGetLastError();
       bps = 1;
     }
   }
   if (bps < 1) bps = 1;
+  if (ctx->tuning.blocks_per_sm > 0 && ctx->tuning.blocks_per_sm < bps) bps = ctx->tuning.blocks_per_sm;
   int64_t tiles = (n + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
   int64_t warps = QM_SCAN_THREADS / 32;
   int64_t need = (tiles + warps - 1) / warps;
   int64_t blocks = std::min<int64_t>((int64_t)ctx->sm_count * bps, std::max<int64_t>(need, 1));
   return (int)blocks;
 }
+
+// Filter columns to stream through shared memory: every column a term reads,
+// at most QM_MAX_STAGED, each 16-byte aligned (bulk copies need it).
+bool setup_staging(qm_pred &P, qm_staging &S, int depth) {
+  memset(&S, 0, sizeof S);
+  const int nt = P.n_groups > 0 ? P.group_end[P.n_groups - 1] : P.n_and;
+  int off = 0;
+  for (int i = 0; i < nt; i++) {
+    qm_term &t = P.t[i];
+    t.sidx = -1;
+    if (t.kind <= QT_FALSE) continue;
+    int c = 0;
+    while (c < S.n && S.data[c] != t.data) c++;
+    if (c == S.n) {
+      if (S.n == QM_MAX_STAGED || ((uintptr_t)t.data & 15)) {
+        S.n = 0;
+        return false;
+      }
+      S.data[c] = t.data;
+      S.elem[c] = (int)dtype_size(t.dtype);
+      S.off[c] = off;
+      off += QM_TILE_ROWS * S.elem[c];
+      S.n++;
+    }
+    t.sidx = c;
+  }
+  if (S.n == 0) return false;
+  S.tile_bytes = off;
+  S.depth = depth;
+  return true;
+}
+
+constexpr size_t SMEM_LIMIT = 227 * 1024;
 
 double hll_estimate(const uint32_t *regs) {
   const int m = 1 << QM_HLL_P;
@@ -788,6 +886,62 @@ int column_minmax(qm_ctx *ctx, DevCol &c, int64_t n) {
   c.mx = ((long long *)ctx->hstatus.p)[1];
   c.has_minmax = true;
   return QM_OK;
+}
+
+// Multi-column keys: integer columns as mixed-radix digits of one 64-bit
+// word (NULL is digit 0 of a nullable column) when the column ranges are
+// known and the product fits; two non-null int32 columns concatenate
+// otherwise.  Returns the number of distinct key words (0 = unbounded).
+int plan_key_packing(qm_ctx *ctx, Plan &pl, int64_t n_rows, bool have_stats, uint64_t *space) {
+  qm_keyspec &K = pl.key;
+  *space = 0;
+  if (K.n_cols <= 1) {
+    K.pack = QP_RAW;
+    return QM_OK;
+  }
+  bool all_int = true;
+  for (int i = 0; i < K.n_cols; i++) all_int = all_int && is_int(K.dtype[i]);
+  if (all_int && have_stats) {
+    unsigned __int128 prod = 1;
+    bool fits = true;
+    for (int i = 0; i < K.n_cols && fits; i++) {
+      DevCol &c = *const_cast<DevCol *>(pl.keycols[i]);
+      int rc = column_minmax(ctx, c, n_rows);
+      if (rc) return rc;
+      const int nullable = c.nulls ? 1 : 0;
+      uint64_t radix;
+      if (c.mx >= c.mn) {
+        unsigned __int128 r = (unsigned __int128)((__int128)c.mx - (__int128)c.mn) + 1 + nullable;
+        if (r > ((unsigned __int128)1 << 62)) fits = false;
+        radix = (uint64_t)r;
+        K.kbase[i] = c.mn;
+      } else {  // no non-null value
+        radix = 1 + nullable;
+        K.kbase[i] = 0;
+      }
+      K.knullable[i] = nullable;
+      K.kradix[i] = radix;
+      prod *= radix;
+      if (prod > ((unsigned __int128)1 << 62)) fits = false;
+    }
+    if (fits) {
+      uint64_t m = 1;
+      for (int i = K.n_cols - 1; i >= 0; i--) {
+        K.kmul[i] = m;
+        m *= K.kradix[i];
+      }
+      K.pack = QP_DIGITS;
+      *space = (uint64_t)prod;
+      return QM_OK;
+    }
+  }
+  if (K.n_cols == 2 && K.dtype[0] == QM_I32 && K.dtype[1] == QM_I32 && !K.nulls[0] && !K.nulls[1]) {
+    K.pack = QP_CONCAT;
+    return QM_OK;
+  }
+  return set_err(ctx, QM_ERR_UNSUPPORTED,
+                 "GROUP BY over %d columns needs integer columns whose value ranges pack into 62 bits%s",
+                 K.n_cols, have_stats ? "" : " (streamed batches: two non-null int32 columns)");
 }
 
 }  // namespace
@@ -867,6 +1021,10 @@ void fill_args(const GroupTable &gt, qm_scan_args &a, qm_status *st) {
   a.dedupe = gt.ex.dedupe;
   a.max_probe = 1 << 12;
   a.status = st;
+  a.vec_ok = 1;
+  const int nt = gt.pl.pred.n_groups > 0 ? gt.pl.pred.group_end[gt.pl.pred.n_groups - 1] : gt.pl.pred.n_and;
+  for (int i = 0; i < nt; i++)
+    if (((uintptr_t)gt.pl.pred.t[i].data & 15) != 0) a.vec_ok = 0;
 }
 
 // Finalize the group table into a qm_result (compaction, first-seen order,
@@ -981,7 +1139,7 @@ int setup_table(qm_ctx *ctx, GroupTable &gt, int64_t est_groups, int64_t direct_
     if (ex.log2cap > 31) ex.log2cap = 31;
     ex.n_slots = (int64_t)1 << ex.log2cap;
   }
-  choose_layout(pl, est_groups, ex);
+  choose_layout(pl, est_groups, ex, ctx->tuning);
   size_t bytes = (size_t)ex.total_slots * ex.stride * 8;
   DevBuf &buf = owned ? gt.own : ctx->table;
   int rc = ensure(ctx, buf, bytes);
@@ -996,8 +1154,22 @@ int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel) {
   a.n = n;
   a.sel = sel;
   a.row_offset = gt.rows_done;
-  size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words);
-  int blocks = scan_blocks(ctx, smem, n);
+  int depth = ctx->tuning.stage_depth == 0 ? 3 : ctx->tuning.stage_depth;
+  if (depth > QM_STAGE_MAX_DEPTH) depth = QM_STAGE_MAX_DEPTH;
+  bool staged = false;
+  size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, 0, 0);
+  if (!sel && depth >= 2 && n >= (int64_t)QM_TILE_ROWS * 256) {
+    for (; depth >= 2 && !staged; depth--) {
+      if (!setup_staging(a.pred, a.stage, depth)) break;
+      size_t sm = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, a.stage.tile_bytes, depth);
+      if (sm <= SMEM_LIMIT) {
+        smem = sm;
+        staged = true;
+      }
+    }
+  }
+  if (!staged) memset(&a.stage, 0, sizeof a.stage);
+  int blocks = scan_blocks(ctx, smem, n, staged);
   CK(cudaEventRecord(ctx->evs0, ctx->stream));
   CK(qm_launch_scan(a, blocks, smem, ctx->stream));
   CK(cudaEventRecord(ctx->evs1, ctx->stream));
@@ -1084,6 +1256,19 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   if (ctx->evs1) cudaEventDestroy(ctx->evs1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
+  return QM_OK;
+}
+
+int qm_ctx_set_tuning(qm_ctx *ctx, const qm_tuning *t) {
+  if (!ctx) return QM_ERR_INVALID;
+  if (!t) {
+    ctx->tuning = qm_tuning{0, -1, 0, 0};
+    return QM_OK;
+  }
+  if (t->local_slots > 0 && (t->local_slots & (t->local_slots - 1)))
+    return set_err(ctx, QM_ERR_INVALID, "local_slots must be a power of two");
+  if (t->local_slots > (1 << 14)) return set_err(ctx, QM_ERR_INVALID, "local_slots too large");
+  ctx->tuning = *t;
   return QM_OK;
 }
 
@@ -1245,13 +1430,21 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
   Plan &pl = gt.pl;
   // key mode and size
   int64_t est = 1, direct_size = 0;
+  uint64_t space = 0;
+  if ((rc = plan_key_packing(ctx, pl, t->n_rows, true, &space))) return rc;
   if (pl.key.n_cols == 0) {
     pl.key.mode = QK_NONE;
   } else {
     const ColView *kv = env.find(q->group_by[0]);
     DevCol &kc = *const_cast<DevCol *>(kv->col);
     bool direct = false;
-    if (pl.key.n_cols == 1 && is_int(kc.dtype)) {
+    if (pl.key.pack == QP_DIGITS) {
+      if (space <= (1ULL << 25) && (int64_t)space <= std::max<int64_t>(4 * t->n_rows, 1 << 16)) {
+        direct = true;
+        direct_size = (int64_t)space;
+        pl.key.base = 0;
+      }
+    } else if (pl.key.n_cols == 1 && is_int(kc.dtype)) {
       if ((rc = column_minmax(ctx, kc, t->n_rows))) return rc;
       if (kc.mx >= kc.mn) {
         unsigned long long range = (unsigned long long)kc.mx - (unsigned long long)kc.mn + 1ULL;
@@ -1266,21 +1459,28 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
         pl.key.base = 0;
       }
     }
+    const bool single = pl.key.n_cols == 1;
     if (direct) {
       pl.key.mode = QK_DIRECT;
       est = direct_size;
-      if (!kc.has_hll && direct_size > (1 << 16)) {
-        qm_keyspec K = pl.key;
-        K.mode = QK_HASH;
-        double e;
-        if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
-        kc.hll = e;
-        kc.has_hll = true;
+      if (direct_size > (1 << 16)) {
+        double e = 0;
+        if (single && kc.has_hll) {
+          e = kc.hll;
+        } else {
+          qm_keyspec K = pl.key;
+          K.mode = QK_HASH;
+          if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
+          if (single) {
+            kc.hll = e;
+            kc.has_hll = true;
+          }
+        }
+        est = std::min<int64_t>(est, (int64_t)(e * 1.05) + 16);
       }
-      if (kc.has_hll) est = std::min<int64_t>(est, (int64_t)(kc.hll * 1.05) + 16);
     } else {
       pl.key.mode = QK_HASH;
-      if (pl.key.n_cols == 1 && kc.has_hll) {
+      if (single && kc.has_hll) {
         est = (int64_t)(kc.hll * 1.05) + 16;
       } else {
         qm_keyspec K = pl.key;
@@ -1443,7 +1643,7 @@ int grow_table(qm_ctx *ctx, GroupTable &gt, int64_t upper) {
   gt.own = nb;
   gt.table = tmp.table;
   // local-table choice may change with the new size
-  choose_layout(gt.pl, upper, nx);
+  choose_layout(gt.pl, upper, nx, ctx->tuning);
   gt.ex = nx;
   return QM_OK;
 }
@@ -1535,6 +1735,8 @@ int qm_agg_push(qm_agg *a, int64_t n_rows, int32_t n_cols, const qm_column *cols
   GroupTable &gt = a->gt;
   Plan pl;
   if ((rc = plan_query(ctx, &a->q, env, pl))) return rc;
+  uint64_t space = 0;
+  if ((rc = plan_key_packing(ctx, pl, n_rows, false, &space))) return rc;
   pl.key.mode = pl.key.n_cols == 0 ? QK_NONE : QK_HASH;
   if (!a->planned) {
     gt.pl = pl;

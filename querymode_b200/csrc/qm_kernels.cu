@@ -15,144 +15,248 @@
 namespace qm {
 
 // Shared memory of one block: the block-local group table (keys, then the
-// accumulator words structure-of-arrays), then one compaction list per warp.
+// accumulator words structure-of-arrays), then one survivor queue per warp.
+#define QM_WQ (QM_TILE_ROWS + 32)  // per-warp queue: a tile's survivors + < 32 left over
+
 struct smem_layout {
   int L;
-  size_t keys_off, words_off, lists_off, bytes;
+  size_t keys_off, words_off, queue_off, stage_off, stage_warp_bytes, bytes;
 };
 
-__host__ __device__ inline smem_layout make_smem_layout(int local_slots, int local_hash, int n_words,
-                                                        int warps) {
+// Per warp staging region: QM_STAGE_MAX_DEPTH mbarriers (32 bytes), then
+// `depth` tile buffers of tile_bytes each.
+__host__ __device__ inline smem_layout make_smem_layout(int local_slots, int local_hash, int n_words, int warps,
+                                                        int stage_tile_bytes = 0, int stage_depth = 0) {
   smem_layout s;
   s.L = local_slots;
   s.keys_off = 0;
   size_t kb = (local_slots > 0 && local_hash) ? (size_t)local_slots * 8 : 0;
   s.words_off = kb;
   size_t wb = (size_t)local_slots * n_words * 8;
-  s.lists_off = s.words_off + wb;
-  s.bytes = s.lists_off + (size_t)warps * QM_TILE_ROWS * sizeof(uint16_t);
+  s.queue_off = (s.words_off + wb + 15) & ~(size_t)15;
+  s.stage_off = (s.queue_off + (size_t)warps * QM_WQ * sizeof(uint32_t) + 127) & ~(size_t)127;
+  s.stage_warp_bytes = stage_depth > 0 ? (size_t)(32 + stage_depth * stage_tile_bytes + 127) & ~(size_t)127 : 0;
+  s.bytes = s.stage_off + (size_t)warps * s.stage_warp_bytes;
   return s;
 }
 
+// Aggregates one survivor per lane (lanes with active = false sit out).
 template <bool SEL>
+__device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
+                                            int *l_used, int lane, bool active, int64_t row) {
+  const qm_aggspec &A = a.agg;
+  if (a.dedupe) {
+    const unsigned act = __ballot_sync(QM_FULL, active);
+    if (!active) return;
+    const uint64_t grow = (uint64_t)(a.row_offset + row);
+    int special;
+    const uint64_t key = row_key(a.key, row, special);
+    uint64_t vb[QM_MAX_VCOLS];
+    uint32_t vnull;
+    gather_values(A, row, vb, vnull);
+    unsigned peers = __match_any_sync(act, key);
+    if (__any_sync(act, special != 0)) peers &= __match_any_sync(act, special);
+    const bool leader = lane == __ffs(peers) - 1;
+    uint64_t *tp = nullptr;
+    int ws = 1;
+    bool local = false;
+    if (leader) {
+      int ls = -1;
+      if (L > 0) {
+        if (!a.local_hash) ls = (int)global_slot(a, key, special);
+        else if (special == 0) ls = local_find(lkeys, L, key, l_used);
+      }
+      if (ls >= 0) {
+        tp = lw + ls;
+        ws = L;
+        local = true;
+      } else if (!(L > 0 && !a.local_hash)) {
+        const int64_t gs = global_slot(a, key, special);
+        if (gs >= 0) tp = a.table + gs * a.stride + 1;
+      }
+    }
+    apply_row(A, tp, ws, local, peers, lane, grow, vb, vnull);
+    return;
+  }
+  if (!active) return;
+  const uint64_t grow = (uint64_t)(a.row_offset + row);
+  int special;
+  const uint64_t key = row_key(a.key, row, special);
+  uint64_t vb[QM_MAX_VCOLS];
+  uint32_t vnull;
+  gather_values(A, row, vb, vnull);
+  int ls = -1;
+  if (L > 0) {
+    if (!a.local_hash) ls = (int)global_slot(a, key, special);
+    else if (special == 0) ls = local_find(lkeys, L, key, l_used);
+  }
+  if (ls >= 0) {
+    agg_row(A, lw + ls, L, true, grow, vb, vnull);
+  } else if (!(L > 0 && !a.local_hash)) {
+    const int64_t gs = global_slot(a, key, special);
+    if (gs >= 0) agg_row(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull);
+  }
+}
+
+// The fused scan.  Each warp takes tiles of QM_TILE_ROWS rows round robin,
+// filters them, appends the survivors' row indices to its own queue in
+// shared memory and aggregates 32 survivors at a time (one per lane): gather
+// the key and value cells, find the slot in the block-local table (else the
+// global table) and update the accumulators.  With STAGED, the filter
+// columns of the warp's next tiles stream into its shared-memory buffers by
+// bulk async copies (lane 0 issues, an mbarrier per buffer counts the bytes)
+// while the current tile is evaluated.
+template <bool SEL, bool STAGED>
 __global__ void __launch_bounds__(QM_SCAN_THREADS)
     qm_scan_kernel(const __grid_constant__ qm_scan_args a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int warps = blockDim.x >> 5;
   const qm_aggspec &A = a.agg;
-  const smem_layout lay = make_smem_layout(a.local_slots, a.local_hash, A.n_words, warps);
+  const qm_staging &S = a.stage;
+  const smem_layout lay =
+      make_smem_layout(a.local_slots, a.local_hash, A.n_words, warps, STAGED ? S.tile_bytes : 0, STAGED ? S.depth : 0);
   const int L = lay.L;
   uint64_t *lkeys = reinterpret_cast<uint64_t *>(smem + lay.keys_off);
   uint64_t *lw = reinterpret_cast<uint64_t *>(smem + lay.words_off);
-  uint16_t *list = reinterpret_cast<uint16_t *>(smem + lay.lists_off) + warp * QM_TILE_ROWS;
+  uint32_t *queue = reinterpret_cast<uint32_t *>(smem + lay.queue_off) + warp * QM_WQ;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + lay.stage_off + warp * lay.stage_warp_bytes);
+  uint8_t *sbuf = smem + lay.stage_off + warp * lay.stage_warp_bytes + 32;
+  __shared__ int l_used;
   __shared__ unsigned long long blk_selected;
 
-  if (threadIdx.x == 0) blk_selected = 0;
+  if (threadIdx.x == 0) {
+    l_used = 0;
+    blk_selected = 0;
+  }
   if (L > 0) {
     if (a.local_hash)
       for (int s = threadIdx.x; s < L; s += blockDim.x) lkeys[s] = QM_EMPTY_KEY;
     for (int i = threadIdx.x; i < L * A.n_words; i += blockDim.x) lw[i] = A.init[i / L];
   }
+  if (STAGED && lane == 0) {
+    for (int d = 0; d < S.depth; ++d) mbar_init(&mbar[d], 1);
+    fence_async_shared();
+  }
   __syncthreads();
 
   const int64_t n_tiles = (a.n + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  const int64_t full_tiles = a.n / QM_TILE_ROWS;
   const int64_t gwarps = (int64_t)gridDim.x * warps;
-  unsigned long long my_selected = 0;
+  const int64_t first = (int64_t)blockIdx.x * warps + warp;
+  const uint32_t lt = lanemask_lt();
+  int qn = 0;  // warp-uniform queue length
+  unsigned long long selected = 0;
+  int64_t issued = 0;  // STAGED: tiles whose copies were issued (in order)
+  bool failed = false;
 
-  for (int64_t tile = (int64_t)blockIdx.x * warps + warp; tile < n_tiles; tile += gwarps) {
+  // lane 0 issues the copies of the warp's k-th tile into buffer k % depth
+  auto issue = [&](int64_t k) {
+    const int64_t tile = first + k * gwarps;
+    if (tile >= full_tiles) return;
+    if (lane == 0) {
+      fence_async_shared();
+      const int b = (int)(k % S.depth);
+      uint8_t *dst = sbuf + b * S.tile_bytes;
+      mbar_expect_tx(&mbar[b], (uint32_t)S.tile_bytes);
+      for (int c = 0; c < S.n; ++c)
+        bulk_g2s(dst + S.off[c], reinterpret_cast<const uint8_t *>(S.data[c]) + tile * QM_TILE_ROWS * S.elem[c],
+                 (uint32_t)(QM_TILE_ROWS * S.elem[c]), &mbar[b]);
+    }
+    issued = k + 1;
+  };
+  if (STAGED)
+    for (int64_t k = 0; k < S.depth - 1; ++k) issue(k);
+
+  int64_t k = 0;
+  for (int64_t tile = first; tile < n_tiles; tile += gwarps, ++k) {
     const int64_t e0 = tile * QM_TILE_ROWS;
-    // element -> row
-    int64_t rowv[QM_R];
     uint32_t m = 0;
-#pragma unroll
-    for (int j = 0; j < QM_R; ++j) {
-      int64_t e = e0 + j * 32 + lane;
-      bool in = e < a.n;
-      m |= (uint32_t)in << j;
-      if (SEL) rowv[j] = in ? (int64_t)__ldg(a.sel + e) : 0;
-      else rowv[j] = e;
-    }
-    auto rowf = [&](int j) { return rowv[j]; };
-    m = eval_pred(a.pred, rowf, m);
-
-    // compaction: survivors in ascending row order
-    uint32_t tot = 0;
-    const uint32_t lt = lanemask_lt();
-#pragma unroll
-    for (int j = 0; j < QM_R; ++j) {
-      uint32_t b = __ballot_sync(QM_FULL, (m >> j) & 1);
-      if ((m >> j) & 1) list[tot + __popc(b & lt)] = (uint16_t)(j * 32 + lane);
-      tot += __popc(b);
-    }
-    __syncwarp();
-    my_selected += tot;
-
-    for (uint32_t c0 = 0; c0 < tot; c0 += 32) {
-      const bool active = c0 + lane < tot;
-      const unsigned act = __ballot_sync(QM_FULL, active);
-      if (active) {
-        const int off = list[c0 + lane];
-        const int64_t row = SEL ? (int64_t)__ldg(a.sel + e0 + off) : e0 + off;
-        const uint64_t grow = (uint64_t)(a.row_offset + row);
-        int special;
-        const uint64_t key = row_key(a.key, row, special);
-        uint64_t vb[QM_MAX_VCOLS];
-        uint32_t vnull = 0;
-#pragma unroll
-        for (int c = 0; c < QM_MAX_VCOLS; ++c) {
-          vb[c] = 0;
-          if (c < A.n_vcols) {
-            const qm_vcol &vc = A.vcol[c];
-            if (cell_null(vc.nulls, row)) {
-              vnull |= 1u << c;
-            } else if (vc.dtype == QM_I32 || vc.dtype == QM_I64) {
-              vb[c] = (uint64_t)ld_int(vc.data, vc.dtype, row);
-            } else {
-              vb[c] = (uint64_t)__double_as_longlong(ld_flt(vc.data, vc.dtype, row));
-            }
-          }
-        }
-        unsigned peers = 1u << lane;
-        if (a.dedupe) {
-          peers = __match_any_sync(act, key);
-          if (__any_sync(act, special != 0)) peers &= __match_any_sync(act, special);
-        }
-        const bool leader = lane == __ffs(peers) - 1;
-        uint64_t *tp = nullptr;
-        int ws = 1;
-        bool local = false;
-        if (leader) {
-          int ls = -1;
-          if (L > 0) {
-            if (!a.local_hash) ls = (int)global_slot(a, key, special);
-            else if (special == 0) ls = local_find(lkeys, L, key);
-          }
-          if (ls >= 0) {
-            tp = lw + ls;
-            ws = L;
-            local = true;
-          } else if (!(L > 0 && !a.local_hash)) {
-            int64_t gs = global_slot(a, key, special);
-            if (gs >= 0) tp = a.table + gs * a.stride + 1;
-          }
-        }
-        apply_row(A, tp, ws, local, peers, lane, grow, vb, vnull);
+    if (STAGED && tile < full_tiles) {
+      __syncwarp();
+      issue(k + S.depth - 1);
+      const int b = (int)(k % S.depth);
+      if (!mbar_wait(&mbar[b], (uint32_t)((k / S.depth) & 1))) {
+        set_error(a.status, QM_DEV_TIMEOUT);
+        failed = true;
+        break;
       }
+      m = eval_pred_staged(a.pred, S, sbuf + b * S.tile_bytes, e0, lane, (1u << QM_R) - 1);
+      // append survivors (rows e0 + j*32 + lane)
+      uint32_t base = (uint32_t)qn;
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) {
+        const uint32_t bal = __ballot_sync(QM_FULL, (m >> j) & 1);
+        if ((m >> j) & 1) queue[base + __popc(bal & lt)] = (uint32_t)(e0 + j * 32 + lane);
+        base += __popc(bal);
+      }
+      const int tot = (int)base - qn;
+      qn = (int)base;
+      selected += tot;
+    } else {
+      const int64_t r0 = e0 + (int64_t)lane * QM_R;  // this lane's first element
+      int64_t rowv[QM_R];
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) {
+        const bool in = r0 + j < a.n;
+        m |= (uint32_t)in << j;
+        rowv[j] = r0 + j;
+      }
+      if (!SEL && a.vec_ok && e0 + QM_TILE_ROWS <= a.n) {
+        m = eval_pred_contig(a.pred, r0, m);
+      } else {
+        if (SEL) {
+#pragma unroll
+          for (int j = 0; j < QM_R; ++j) rowv[j] = ((m >> j) & 1) ? (int64_t)__ldg(a.sel + r0 + j) : 0;
+        }
+        auto rowf = [&](int j) { return rowv[j]; };
+        m = eval_pred(a.pred, rowf, m);
+      }
+      // append survivors (order inside the queue does not matter: FIRST is a min)
+      const uint32_t cnt = __popc(m);
+      uint32_t off = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(QM_FULL, off, o);
+        if (lane >= o) off += x;
+      }
+      const uint32_t tot = __shfl_sync(QM_FULL, off, 31);
+      off -= cnt;  // exclusive prefix
+      uint32_t q = qn + off;
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j)
+        if ((m >> j) & 1) queue[q++] = (uint32_t)rowv[j];
+      qn += (int)tot;
+      selected += tot;
     }
     __syncwarp();
+    while (qn >= 32) {
+      const int64_t row = queue[qn - 32 + lane];
+      __syncwarp();
+      qn -= 32;
+      drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, true, row);
+    }
+  }
+  if (STAGED && failed) {
+    // let every copy still in flight land before the block's memory goes
+    for (int64_t j = k; j < issued; ++j)
+      if (!mbar_wait(&mbar[j % S.depth], (uint32_t)((j / S.depth) & 1))) break;
+  }
+  if (qn > 0) {
+    const bool active = lane < qn;
+    const int64_t row = active ? (int64_t)queue[lane] : 0;
+    __syncwarp();
+    drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, active, row);
   }
 
-  // per-block selected count
-  for (int o = 16; o > 0; o >>= 1) my_selected += __shfl_xor_sync(QM_FULL, my_selected, o);
-  if (lane == 0 && my_selected) atomicAdd(&blk_selected, my_selected);
+  if (lane == 0 && selected) atomicAdd(&blk_selected, selected);
   __syncthreads();
   if (threadIdx.x == 0 && blk_selected) atomicAdd(&a.status->rows_selected, blk_selected);
 
   // merge the block-local table into the global table
   if (L > 0) {
-    const int cw = A.acc[A.acc_count].word;
+    const int cw = A.w_count;
     for (int s = threadIdx.x; s < L; s += blockDim.x) {
       if (lw[(int64_t)cw * L + s] == 0) continue;
       int64_t gs;
@@ -269,8 +373,18 @@ __global__ void qm_emit_groups(const uint64_t *t, int stride, const uint32_t *sl
           set_null(out, o.null_offset, i);
           continue;
         }
-        if (K.n_cols == 2) {
+        if (K.pack == QP_CONCAT) {
           reinterpret_cast<int32_t *>(col)[i] = (int32_t)(o.src == 0 ? (key >> 32) : key);
+        } else if (K.pack == QP_DIGITS) {
+          const int c = o.src;
+          const uint64_t d = (key / K.kmul[c]) % K.kradix[c];
+          if (K.knullable[c] && d == 0) {
+            set_null(out, o.null_offset, i);
+            continue;
+          }
+          const int64_t v = K.kbase[c] + (int64_t)(d - (uint64_t)K.knullable[c]);
+          if (o.dtype == QM_I32) reinterpret_cast<int32_t *>(col)[i] = (int32_t)v;
+          else reinterpret_cast<int64_t *>(col)[i] = v;
         } else if (o.dtype == QM_I32) {
           reinterpret_cast<int32_t *>(col)[i] = (int32_t)(int64_t)key;
         } else {
@@ -447,24 +561,31 @@ __global__ void qm_minmax_init(long long *out) {
 // ---------------------------------------------------------------- launchers
 using namespace qm;
 
-size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words) {
-  return make_smem_layout(local_slots, local_hash, n_words, QM_SCAN_THREADS / 32).bytes;
+size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth) {
+  return make_smem_layout(local_slots, local_hash, n_words, QM_SCAN_THREADS / 32, stage_tile_bytes, stage_depth).bytes;
 }
 
-cudaError_t qm_scan_configure(size_t smem_bytes, int *blocks_per_sm) {
+cudaError_t qm_scan_configure(size_t smem_bytes, bool staged, int *blocks_per_sm) {
   cudaError_t e;
-  e = cudaFuncSetAttribute(qm_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (staged) {
+    e = cudaFuncSetAttribute(qm_scan_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false, true>, QM_SCAN_THREADS,
+                                                         smem_bytes);
+  }
+  e = cudaFuncSetAttribute(qm_scan_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(qm_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  e = cudaFuncSetAttribute(qm_scan_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false>, QM_SCAN_THREADS,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false, false>, QM_SCAN_THREADS,
                                                        smem_bytes);
 }
 
 cudaError_t qm_launch_scan(const qm_scan_args &a, int blocks, size_t smem_bytes, cudaStream_t st) {
   if (a.n <= 0) return cudaSuccess;
-  if (a.sel) qm_scan_kernel<true><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
-  else qm_scan_kernel<false><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  if (a.sel) qm_scan_kernel<true, false><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  else if (a.stage.n > 0) qm_scan_kernel<false, true><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  else qm_scan_kernel<false, false><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -24,7 +24,7 @@
 #include "qm_plan.h"
 
 #define QM_FULL 0xffffffffu
-#define QM_LOCAL_PROBE 16
+#define QM_LOCAL_PROBE 8
 
 namespace qm {
 
@@ -129,6 +129,8 @@ __device__ __forceinline__ bool fbig(double v, int op, int64_t b) {
 
 __device__ __forceinline__ bool fterm(const qm_term &t, double v) {
   switch (t.kind) {
+    case QT_FRANGE:
+      return ((t.op & 1) ? v >= t.f0 : v > t.f0) && ((t.op & 2) ? v <= t.f1 : v < t.f1);
     case QT_FCMP: return fcmp(v, t.op, t.f0);
     case QT_FBETWEEN: return v >= t.f0 && v <= t.f1;
     case QT_FNBETWEEN: return v < t.f0 || v > t.f1;
@@ -178,6 +180,196 @@ __device__ __forceinline__ uint32_t eval_term(const qm_term &t, const ROWS &row,
   return m & pass;
 }
 
+// Full dense tile, lane owns rows e0 + 8*lane + j (j < 8): one or two
+// 16-byte loads per column per lane, NULL bits as one byte per lane.
+template <typename V, typename T, int PER>
+__device__ __forceinline__ void load_contig(const void *data, int64_t r0, uint32_t m, T (&v)[QM_R]) {
+  const V *p = reinterpret_cast<const V *>(reinterpret_cast<const T *>(data) + r0);
+#pragma unroll
+  for (int k = 0; k < QM_R / PER; ++k) {
+    if ((m >> (k * PER)) & ((1u << PER) - 1)) {
+      const V x = __ldcs(p + k);
+      const T *xs = reinterpret_cast<const T *>(&x);
+#pragma unroll
+      for (int i = 0; i < PER; ++i) v[k * PER + i] = xs[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < PER; ++i) v[k * PER + i] = T(0);
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t eval_term_contig(const qm_term &t, int64_t r0, uint32_t m) {
+  uint32_t pass = 0;
+  if (t.kind <= QT_FALSE) {
+    pass = t.kind == QT_TRUE ? ((1u << QM_R) - 1) : 0u;
+  } else if (t.dtype == QM_I32 || t.dtype == QM_I64) {
+    int64_t v[QM_R];
+    if (t.dtype == QM_I32) {
+      int w[QM_R];
+      load_contig<int4, int, 4>(t.data, r0, m, w);
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = w[j];
+    } else {
+      long long w[QM_R];
+      load_contig<longlong2, long long, 2>(t.data, r0, m, w);
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = w[j];
+    }
+    const bool inr = t.kind == QT_IRANGE;
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)((v[j] >= t.lo && v[j] <= t.hi) == inr) << j;
+  } else {
+    double v[QM_R];
+    if (t.dtype == QM_F32) {
+      float w[QM_R];
+      load_contig<float4, float, 4>(t.data, r0, m, w);
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) v[j] = w[j];
+    } else {
+      load_contig<double2, double, 2>(t.data, r0, m, v);
+    }
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)fterm(t, v[j]) << j;
+  }
+  if (t.nulls != nullptr) {
+    // r0 is a multiple of 8: the lane's 8 NULL bits are one byte
+    const uint32_t nb = (__ldg(t.nulls + (r0 >> 5)) >> (r0 & 31)) & 0xffu;
+    const uint32_t np = t.null_pass ? 0xffu : 0u;
+    pass = (pass & ~nb) | (np & nb);
+  }
+  return m & pass;
+}
+
+__device__ __forceinline__ uint32_t eval_pred_contig(const qm_pred &P, int64_t r0, uint32_t m) {
+  for (int i = 0; i < P.n_and; ++i) {
+    if (!__any_sync(QM_FULL, m)) return 0;
+    m = eval_term_contig(P.t[i], r0, m);
+  }
+  if (P.n_groups > 0) {
+    uint32_t any = 0;
+    int b = P.n_and;
+    for (int g = 0; g < P.n_groups; ++g) {
+      uint32_t mg = m & ~any;
+      const int e = P.group_end[g];
+      for (int i = b; i < e; ++i) {
+        if (!__any_sync(QM_FULL, mg)) break;
+        mg = eval_term_contig(P.t[i], r0, mg);
+      }
+      any |= mg;
+      b = e;
+    }
+    m = any;
+  }
+  return m;
+}
+
+// ---- bulk async copies into shared memory (cp.async.bulk + mbarrier) ------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// global -> shared bulk copy; dst, src and bytes are multiples of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+#define QM_WAIT_LIMIT (1 << 22)
+
+// Bounded wait for a phase of an mbarrier; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (int i = 0; i < QM_WAIT_LIMIT; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Term evaluation on a staged tile: rows e0 + j*32 + lane, cells read from
+// the shared-memory copy (consecutive lanes, consecutive addresses).
+__device__ __forceinline__ uint32_t eval_term_staged(const qm_term &t, const qm_staging &S, const uint8_t *buf,
+                                                     int64_t e0, int lane, uint32_t m) {
+  uint32_t pass = 0;
+  if (t.kind <= QT_FALSE) {
+    pass = t.kind == QT_TRUE ? ((1u << QM_R) - 1) : 0u;
+  } else {
+    const uint8_t *col = buf + S.off[t.sidx];
+    if (t.dtype == QM_I32 || t.dtype == QM_I64) {
+      const bool inr = t.kind == QT_IRANGE;
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) {
+        const int64_t v = t.dtype == QM_I32 ? (int64_t)reinterpret_cast<const int *>(col)[j * 32 + lane]
+                                            : (int64_t)reinterpret_cast<const long long *>(col)[j * 32 + lane];
+        pass |= (uint32_t)((v >= t.lo && v <= t.hi) == inr) << j;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) {
+        const double v = t.dtype == QM_F32 ? (double)reinterpret_cast<const float *>(col)[j * 32 + lane]
+                                           : reinterpret_cast<const double *>(col)[j * 32 + lane];
+        pass |= (uint32_t)fterm(t, v) << j;
+      }
+    }
+  }
+  if (t.nulls != nullptr) {
+#pragma unroll
+    for (int j = 0; j < QM_R; ++j) {
+      const uint32_t w = __ldg(t.nulls + ((e0 >> 5) + j));
+      if ((w >> lane) & 1) pass = (pass & ~(1u << j)) | ((uint32_t)t.null_pass << j);
+    }
+  }
+  return m & pass;
+}
+
+__device__ __forceinline__ uint32_t eval_pred_staged(const qm_pred &P, const qm_staging &S, const uint8_t *buf,
+                                                     int64_t e0, int lane, uint32_t m) {
+  for (int i = 0; i < P.n_and; ++i) {
+    if (!__any_sync(QM_FULL, m)) return 0;
+    m = eval_term_staged(P.t[i], S, buf, e0, lane, m);
+  }
+  if (P.n_groups > 0) {
+    uint32_t any = 0;
+    int b = P.n_and;
+    for (int g = 0; g < P.n_groups; ++g) {
+      uint32_t mg = m & ~any;
+      const int e = P.group_end[g];
+      for (int i = b; i < e; ++i) {
+        if (!__any_sync(QM_FULL, mg)) break;
+        mg = eval_term_staged(P.t[i], S, buf, e0, lane, mg);
+      }
+      any |= mg;
+      b = e;
+    }
+    m = any;
+  }
+  return m;
+}
+
 // AND terms, then the OR of the groups' AND chains (src/decode.ts:558-578).
 template <typename ROWS>
 __device__ __forceinline__ uint32_t eval_pred(const qm_pred &P, const ROWS &row, uint32_t m) {
@@ -209,25 +401,32 @@ __device__ __forceinline__ uint32_t eval_pred(const qm_pred &P, const ROWS &row,
 __device__ __forceinline__ uint64_t row_key(const qm_keyspec &K, int64_t r, int &special) {
   special = 0;
   if (K.n_cols == 0) return 0;
-  if (K.n_cols == 2) {
-    uint32_t a = (uint32_t)ldcs<int>(K.data[0], r), b = (uint32_t)ldcs<int>(K.data[1], r);
-    uint64_t k = ((uint64_t)a << 32) | b;
-    if (K.mode == QK_HASH && k == QM_EMPTY_KEY) special = 1;
-    return k;
-  }
-  if (cell_null(K.nulls[0], r)) {
-    special = 2;
-    return 0;
-  }
   uint64_t k;
-  switch (K.dtype[0]) {
-    case QM_I32: k = (uint64_t)(int64_t)ldcs<int>(K.data[0], r); break;
-    case QM_I64: k = (uint64_t)ldcs<long long>(K.data[0], r); break;
-    default: {
-      // String(v) identity: -0 and 0 share "0", every NaN is "NaN"
-      double d = ld_flt(K.data[0], K.dtype[0], r);
-      if (d == 0.0) d = 0.0;
-      k = isnan(d) ? 0x7ff8000000000000ULL : (uint64_t)__double_as_longlong(d);
+  if (K.pack == QP_CONCAT) {
+    uint32_t a = (uint32_t)ldcs<int>(K.data[0], r), b = (uint32_t)ldcs<int>(K.data[1], r);
+    k = ((uint64_t)a << 32) | b;
+  } else if (K.pack == QP_DIGITS) {
+    k = 0;
+    for (int i = 0; i < K.n_cols; ++i) {
+      uint64_t d;
+      if (K.knullable[i] && cell_null(K.nulls[i], r)) d = 0;
+      else d = (uint64_t)(ld_int(K.data[i], K.dtype[i], r) - K.kbase[i]) + (uint64_t)K.knullable[i];
+      k += d * K.kmul[i];
+    }
+  } else {
+    if (cell_null(K.nulls[0], r)) {
+      special = 2;
+      return 0;
+    }
+    switch (K.dtype[0]) {
+      case QM_I32: k = (uint64_t)(int64_t)ldcs<int>(K.data[0], r); break;
+      case QM_I64: k = (uint64_t)ldcs<long long>(K.data[0], r); break;
+      default: {
+        // String(v) identity: -0 and 0 share "0", every NaN is "NaN"
+        double d = ld_flt(K.data[0], K.dtype[0], r);
+        if (d == 0.0) d = 0.0;
+        k = isnan(d) ? 0x7ff8000000000000ULL : (uint64_t)__double_as_longlong(d);
+      }
     }
   }
   if (K.mode == QK_HASH && k == QM_EMPTY_KEY) special = 1;
@@ -278,14 +477,22 @@ __device__ __forceinline__ int64_t global_slot(const qm_scan_args &a, uint64_t k
   return s;
 }
 
-__device__ __forceinline__ int local_find(uint64_t *lkeys, int L, uint64_t key) {
+// Block-local lookup.  New keys are admitted only while the table is at
+// most half full (`used` counts admissions), so a miss meets an empty slot
+// within a few probes and goes to the global table.
+__device__ __forceinline__ int local_find(uint64_t *lkeys, int L, uint64_t key, int *used) {
   uint32_t s = (uint32_t)fmix64(key) & (uint32_t)(L - 1);
   for (int p = 0; p < QM_LOCAL_PROBE; ++p) {
     uint64_t k = reinterpret_cast<volatile uint64_t *>(lkeys)[s];
     if (k == key) return (int)s;
     if (k == QM_EMPTY_KEY) {
+      if (*reinterpret_cast<volatile int *>(used) >= (L >> 1)) return -1;
       uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long *>(lkeys + s), QM_EMPTY_KEY, key);
-      if (prev == QM_EMPTY_KEY || prev == key) return (int)s;
+      if (prev == QM_EMPTY_KEY) {
+        atomicAdd(used, 1);
+        return (int)s;
+      }
+      if (prev == key) return (int)s;
     }
     s = (s + 1) & (uint32_t)(L - 1);
   }
@@ -332,6 +539,18 @@ __device__ __forceinline__ uint64_t pick(const uint64_t (&v)[QM_MAX_VCOLS], int 
   return r;
 }
 
+// Monotone updates: the word only ever decreases (min) or increases (max),
+// so a plain read that already beats the value makes the atomic redundant.
+__device__ __forceinline__ void min_u64(uint64_t *p, uint64_t v) {
+  if (v < *reinterpret_cast<volatile uint64_t *>(p)) atomicMin(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
+}
+__device__ __forceinline__ void min_i64(uint64_t *p, int64_t v) {
+  if (v < (int64_t)*reinterpret_cast<volatile uint64_t *>(p)) atomicMin(reinterpret_cast<long long *>(p), (long long)v);
+}
+__device__ __forceinline__ void max_i64(uint64_t *p, int64_t v) {
+  if (v > (int64_t)*reinterpret_cast<volatile uint64_t *>(p)) atomicMax(reinterpret_cast<long long *>(p), (long long)v);
+}
+
 // Apply one compacted row (merged with its equal-key peers) to a slot whose
 // accumulator word w lives at tp[w * ws].  Every peer executes this (the
 // shuffles need them); only the leader, with tp != nullptr, writes.
@@ -348,7 +567,13 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
       continue;
     }
     if (ac.kind == QA_FIRST) {
-      if (tp) atomicMin(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)grow);
+      uint64_t first = grow;
+      if (!solo)
+        for (unsigned m = peers; m; m &= m - 1) {
+          const uint64_t x = __shfl_sync(peers, grow, __ffs(m) - 1);
+          first = min(first, x);
+        }
+      if (tp) min_u64(w0, first);
       continue;
     }
     const bool valid = !((vnull >> ac.vcol) & 1);
@@ -452,6 +677,61 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
         if (tp && code != ~0ULL) atomicMin(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)code);
         break;
       }
+    }
+  }
+}
+
+// One row's update of the slot whose word w lives at tp[w * ws]: straight
+// line per value column, values already gathered into vb (NULL bits in
+// vnull) so the cell loads overlap the key lookup.
+__device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
+                                        uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)A.w_count * ws), 1ULL);
+  if (A.w_first >= 0) min_u64(tp + (int64_t)A.w_first * ws, grow);
+#pragma unroll
+  for (int c = 0; c < QM_MAX_VCOLS; ++c) {
+    if (c >= A.n_vcols) break;
+    if ((vnull >> c) & 1) continue;
+    const qm_vcol &vc = A.vcol[c];
+    const int f = vc.flags;
+    if (f & VF_NN) atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)vc.w_nn * ws), 1ULL);
+    if (vc.dtype == QM_I32 || vc.dtype == QM_I64) {
+      const int64_t v = (int64_t)vb[c];
+      if ((f & VF_SUM) && v != 0) {
+        uint64_t *w0 = tp + (int64_t)vc.w_sum * ws;
+        if (local && !(f & VF_WIDE)) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)v);
+        else add128(w0, w0 + ws, (uint64_t)v, v < 0 ? -1 : 0);
+      }
+      if (f & VF_MIN) min_i64(tp + (int64_t)vc.w_min * ws, v);
+      if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * ws, v);
+    } else {
+      const double d = __longlong_as_double((long long)vb[c]);
+      if (f & VF_SUM) {
+        uint64_t *w0 = tp + (int64_t)vc.w_sum * ws;
+        fsum_add(w0, w0 + ws, d, 0.0);
+      }
+      if ((f & (VF_MIN | VF_MAX)) && !isnan(d)) {  // NaN never wins '<' / '>'
+        const int64_t o = f2ord(d == 0.0 ? 0.0 : d);
+        if (f & VF_MIN) min_i64(tp + (int64_t)vc.w_min * ws, o);
+        if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * ws, o);
+      }
+      if ((f & VF_ZERO) && d == 0.0) min_u64(tp + (int64_t)vc.w_zero * ws, (grow << 1) | (vb[c] >> 63));
+    }
+  }
+}
+
+// Gather a row's value cells (float32 widened to double, as JS numbers).
+__device__ __forceinline__ void gather_values(const qm_aggspec &A, int64_t row, uint64_t (&vb)[QM_MAX_VCOLS],
+                                              uint32_t &vnull) {
+  vnull = 0;
+#pragma unroll
+  for (int c = 0; c < QM_MAX_VCOLS; ++c) {
+    vb[c] = 0;
+    if (c < A.n_vcols) {
+      const qm_vcol &vc = A.vcol[c];
+      if (cell_null(vc.nulls, row)) vnull |= 1u << c;
+      else if (vc.dtype == QM_I32 || vc.dtype == QM_I64) vb[c] = (uint64_t)ld_int(vc.data, vc.dtype, row);
+      else vb[c] = (uint64_t)__double_as_longlong(ld_flt(vc.data, vc.dtype, row));
     }
   }
 }

@@ -31,6 +31,8 @@ enum qm_term_kind : int32_t {
   QT_FBETWEEN = 5,  // float column: v >= f0 && v <= f1
   QT_FNBETWEEN = 6, // float column: v < f0 || v > f1
   QT_FBIG = 7,      // float column vs bigint: BigInt(trunc(v)) <op> lo
+  QT_FRANGE = 10,   // float column: v in (f0 | [f0) .. (f1 | f1]): op bit 0 = f0
+                    // inclusive, bit 1 = f1 inclusive (NaN fails)
   QT_ISNULL = 8,
   QT_NOTNULL = 9,
 };
@@ -45,6 +47,8 @@ struct qm_term {
   int32_t op;            // qm_cmp_op for QT_FCMP / QT_FBIG
   int32_t null_pass;     // result for a NULL cell: 0 (JS), or the result of
                          // the test on 0 (WASM scan reads NULL as 0)
+  int32_t sidx;          // staged column holding this term's cells, or -1
+  int32_t pad;
   int64_t lo, hi;
   double f0, f1;
 };
@@ -63,13 +67,29 @@ enum qm_key_mode : int32_t {
   QK_HASH = 2,   // open addressing on the 64-bit key
 };
 
+#define QM_MAX_KEYS 4
+
+// How the key columns form the 64-bit key word.
+enum qm_key_pack : int32_t {
+  QP_RAW = 0,     // one column: its value (float: normalised bits)
+  QP_CONCAT = 1,  // two non-null int32 columns: (u32)a << 32 | (u32)b
+  QP_DIGITS = 2,  // integer columns as mixed-radix digits: digit_i = v - kbase_i
+                  // (+1 when nullable, 0 = NULL), key = sum digit_i * kmul_i
+};
+
 struct qm_keyspec {
-  int32_t n_cols;   // 0, 1 or 2 (two int32 columns pack into one word)
+  int32_t n_cols;   // 0 .. QM_MAX_KEYS
   int32_t mode;     // qm_key_mode
-  const void *data[2];
-  const uint32_t *nulls[2];
-  int32_t dtype[2];
-  int64_t base;     // QK_DIRECT: smallest key
+  int32_t pack;     // qm_key_pack
+  int32_t pad;
+  const void *data[QM_MAX_KEYS];
+  const uint32_t *nulls[QM_MAX_KEYS];
+  int32_t dtype[QM_MAX_KEYS];
+  int32_t knullable[QM_MAX_KEYS];
+  int64_t kbase[QM_MAX_KEYS];
+  uint64_t kmul[QM_MAX_KEYS];
+  uint64_t kradix[QM_MAX_KEYS];
+  int64_t base;     // QK_DIRECT: smallest key word
 };
 
 // ---- accumulators ----------------------------------------------------------
@@ -93,11 +113,21 @@ struct qm_acc {
   int32_t wide;  // QA_ISUM over int64 cells (128-bit even block-locally)
 };
 
+// Per value column: which accumulators read it (VF_* bits) and where their
+// words live, so a row updates its slot in straight-line code.
+#define VF_NN 1     // non-NULL count word
+#define VF_SUM 2    // QA_ISUM (integer column) or QA_FSUM (float column)
+#define VF_MIN 4
+#define VF_MAX 8
+#define VF_ZERO 16  // QA_FZERO (float MIN / MAX)
+#define VF_WIDE 32  // 128-bit integer sum even block-locally (int64 cells)
+
 struct qm_vcol {
   const void *data;
   const uint32_t *nulls;
   int32_t dtype;
-  int32_t pad;
+  int32_t flags;
+  int32_t w_nn, w_sum, w_min, w_max, w_zero, pad;
 };
 
 struct qm_aggspec {
@@ -106,6 +136,8 @@ struct qm_aggspec {
   int32_t n_vcols;
   int32_t acc_count; // index of QA_COUNT / QA_FIRST in accs
   int32_t acc_first;
+  int32_t w_count;   // word of QA_COUNT
+  int32_t w_first;   // word of QA_FIRST, or -1
   int32_t pad;
   qm_acc acc[QM_MAX_ACCS];
   qm_vcol vcol[QM_MAX_VCOLS];
@@ -157,6 +189,21 @@ struct qm_status {
 #define QM_DEV_OK 0
 #define QM_DEV_OVERFLOW 1  // hash probe limit hit: regrow and re-run
 #define QM_DEV_RANGE 2     // direct-mapped key outside the planned range
+#define QM_DEV_TIMEOUT 3   // a bounded wait on an asynchronous copy gave up
+
+// Filter columns copied tile by tile into shared memory with bulk async
+// copies (cp.async.bulk + mbarrier), double buffered per warp.
+#define QM_MAX_STAGED 4
+#define QM_STAGE_MAX_DEPTH 4
+struct qm_staging {
+  int32_t n;                       // staged columns (0: read filters from global)
+  int32_t tile_bytes;              // bytes of one tile of all staged columns
+  int32_t depth;                   // tile buffers per warp (2..QM_STAGE_MAX_DEPTH)
+  int32_t pad;
+  const void *data[QM_MAX_STAGED];
+  int32_t elem[QM_MAX_STAGED];     // 4 or 8
+  int32_t off[QM_MAX_STAGED];      // byte offset of the column inside a tile buffer
+};
 
 struct qm_scan_args {
   qm_pred pred;
@@ -172,6 +219,8 @@ struct qm_scan_args {
   int32_t local_slots;   // block-local table slots (0: none)
   int32_t local_hash;    // block-local table is hashed (else direct-indexed)
   int32_t dedupe;        // warp-level pre-aggregation of equal keys
+  int32_t vec_ok;          // every term column is 16-byte aligned: vector loads
   int32_t max_probe;     // bound on linear probing in the global table
   qm_status *status;
+  qm_staging stage;
 };

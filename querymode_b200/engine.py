@@ -260,6 +260,14 @@ class Context:
         context's own stream."""
         self.check(self.lib.qm_ctx_set_stream(self.h, stream_handle or None))
 
+    def set_tuning(self, local_slots: int = 0, dedupe: int = -1, blocks_per_sm: int = 0,
+                   stage_depth: int = 0) -> None:
+        """Launch-shape knobs of the fused scan (see qm_tuning); the
+        defaults restore the planner's choices."""
+        t = A.QmTuning(local_slots, dedupe, blocks_per_sm, stage_depth)
+        self._tuning = t
+        self.check(self.lib.qm_ctx_set_tuning(self.h, C.byref(t)))
+
     def device_info(self) -> tuple[int, int]:
         sm = C.c_int32()
         hbm = C.c_int64()

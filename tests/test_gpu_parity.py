@@ -75,7 +75,7 @@ def test_streamed_batches_and_selection(ctx, seed):
     rng = np.random.default_rng(7000 + seed)
     n = 20000
     cols = make_table(rng, n=n)
-    q = rand_query(rng)
+    q = rand_query(rng, stream_keys=True)
     batch = int(rng.choice([1000, 4096, 7777]))
     # reference: AggregateOperator over batches whose selection vectors keep
     # every third row (a scan that already filtered)

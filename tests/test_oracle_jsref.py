@@ -71,12 +71,16 @@ def rand_filter(rng):
     return FilterOp(col, op, val())
 
 
-def rand_query(rng):
+def rand_query(rng, stream_keys=False):
+    """stream_keys: only key shapes a stream of batches can group by (no
+    table statistics to pack several columns into one word)."""
     filters = [rand_filter(rng) for _ in range(rng.integers(0, 3))]
     groups = None
     if rng.random() < 0.3:
         groups = [[rand_filter(rng) for _ in range(rng.integers(1, 3))] for _ in range(rng.integers(1, 3))]
-    gb = [["g32"], ["i64"], ["gf"], ["i32"], [], ["g32", "i32"]][rng.integers(6)]
+    gb = [["g32"], ["i64"], ["gf"], ["i32"], [], ["g32", "i32"], ["i32", "g32"]][rng.integers(7)]
+    if stream_keys and len(gb) > 1:
+        gb = ["g32"]
     aggs = [AggregateOp("count", "*")]
     for _ in range(rng.integers(1, 5)):
         aggs.append(AggregateOp(str(rng.choice(["sum", "avg", "min", "max", "count"])),
