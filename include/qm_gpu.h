@@ -192,7 +192,7 @@ typedef struct {
   int32_t dedupe;        /* warp-level merge of equal keys: -1 auto, 0 off, 1 on */
   int32_t blocks_per_sm; /* resident blocks per SM: 0 auto (occupancy), else a cap */
   int32_t stage_depth;   /* filter-column tiles in flight per warp (bulk async
-                            copies into shared memory): 0 auto, -1 off, 2..4 */
+                            copies into shared memory): <= 0 off, 2..4 */
 } qm_tuning;
 
 /* ---- library / context ---------------------------------------------------- */
@@ -257,7 +257,10 @@ int qm_agg_destroy(qm_agg *agg);
 
 /* ---- filter-only selection (FilterOperator / WASM filter drop-in) ------- */
 /* Evaluate the filters of `query` (aggregates and group_by ignored) over one
- * batch and write the ascending indices of passing rows into out_indices
+ * batch — over the rows listed by `selection` (ascending, n_selected) when it
+ * is non-NULL, FilterOperator narrowing a selection vector
+ * (src/operators.ts:1425-1466) — and write the ascending indices of passing
+ * rows into out_indices
  * (capacity max_out).  Replaces filterFloat64Buffer / filterInt64Buffer /
  * filterInt32Buffer / *Range / *NotRange + intersectIndices / unionIndices
  * (wasm/src/wasm/aggregates.zig:605-1066) as composed by applyAndFilters /
@@ -265,6 +268,7 @@ int qm_agg_destroy(qm_agg *agg);
  * pass, *out_count is the full count and QM_ERR_CAPACITY is returned. */
 int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
                      const qm_column *cols, const qm_query *query,
+                     const uint32_t *selection, int64_t n_selected,
                      uint32_t *out_indices, int64_t max_out,
                      int64_t *out_count);
 

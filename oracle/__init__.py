@@ -115,7 +115,16 @@ def run(columns, query: QueryDescriptor, batch_rows: int = 0, threads: int = 1) 
         L.oracle_result_destroy(h)
 
 
-def filter_select(columns, query: QueryDescriptor) -> np.ndarray:
+def filter_select(columns, query: QueryDescriptor, selection=None) -> np.ndarray:
+    if selection is not None:
+        sel = np.asarray(selection, dtype=np.int64)
+        sub = {}
+        for k, v in columns.items():
+            if hasattr(v, "values"):
+                sub[k] = type(v)(np.asarray(v.values)[sel], None if v.nulls is None else np.asarray(v.nulls)[sel])
+            else:
+                sub[k] = np.asarray(v)[sel]
+        return sel[filter_select(sub, query)].astype(np.uint32)
     L = lib()
     cs = _ColumnSet(columns)
     cq = CQuery(query)

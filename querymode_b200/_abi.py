@@ -132,7 +132,7 @@ SIGNATURES = [
     ("qm_agg_destroy", C.c_int, [_P]),
     ("qm_filter_select", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn),
                                    C.POINTER(QmQuery), C.POINTER(C.c_uint32), C.c_int64,
-                                   C.POINTER(C.c_int64)]),
+                                   C.POINTER(C.c_uint32), C.c_int64, C.POINTER(C.c_int64)]),
     ("qm_result_num_rows", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("qm_result_num_columns", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("qm_result_column", C.c_int, [_P, C.c_int32, C.POINTER(QmResultCol)]),

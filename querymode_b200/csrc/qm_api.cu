@@ -1154,7 +1154,9 @@ int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel) {
   a.n = n;
   a.sel = sel;
   a.row_offset = gt.rows_done;
-  int depth = ctx->tuning.stage_depth == 0 ? 3 : ctx->tuning.stage_depth;
+  // staged filter columns are opt-in: measured slower than direct vector
+  // loads at the occupancy their buffers allow
+  int depth = ctx->tuning.stage_depth <= 0 ? 0 : ctx->tuning.stage_depth;
   if (depth > QM_STAGE_MAX_DEPTH) depth = QM_STAGE_MAX_DEPTH;
   bool staged = false;
   size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, 0, 0);
@@ -1825,8 +1827,10 @@ int qm_agg_destroy(qm_agg *a) {
 }
 
 int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column *cols, const qm_query *q,
-                     uint32_t *out_indices, int64_t max_out, int64_t *out_count) {
-  if (!ctx || !q || !out_count || n_rows < 0 || (n_cols > 0 && !cols) || max_out < 0 || (max_out > 0 && !out_indices))
+                     const uint32_t *selection, int64_t n_selected, uint32_t *out_indices, int64_t max_out,
+                     int64_t *out_count) {
+  if (!ctx || !q || !out_count || n_rows < 0 || (n_cols > 0 && !cols) || max_out < 0 || (max_out > 0 && !out_indices) ||
+      (selection && n_selected < 0))
     return set_err(ctx, QM_ERR_INVALID, "qm_filter_select: bad arguments");
   if (n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
   cudaSetDevice(ctx->device);
@@ -1840,12 +1844,23 @@ int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_colum
   std::vector<const DevCol *> touched;
   int64_t bpr = 0;
   if ((rc = build_pred(ctx, q, env, P, bpr, touched))) return rc;
-  if (n_rows == 0) return QM_OK;
-  const int64_t n_tiles = (n_rows + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+  const uint32_t *dsel = nullptr;
+  if ((rc = stage_selection(ctx, selection, n_selected, &dsel))) return rc;
+  if (dsel && n_selected > 0) {
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+    CK(qm_launch_check_selection(dsel, n_selected, n_rows, (qm_status *)ctx->status.p, ctx->sm_count, ctx->stream));
+    qm_status cst;
+    if ((rc = read_status(ctx, &cst))) return rc;
+    if (cst.error) return set_err(ctx, QM_ERR_INVALID, "selection is not strictly ascending row indices below %lld",
+                                  (long long)n_rows);
+  }
+  const int64_t n_elems = selection ? n_selected : n_rows;
+  if (n_elems == 0) return QM_OK;
+  const int64_t n_tiles = (n_elems + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
   if ((rc = ensure(ctx, ctx->masks, (size_t)n_tiles * QM_R * 4)) || (rc = ensure(ctx, ctx->counts, (size_t)n_tiles * 4 + 4)) ||
       (rc = ensure(ctx, ctx->offsets, (size_t)(n_tiles + 1) * 8)) || (rc = ensure_host(ctx, ctx->hstatus, 64)))
     return rc;
-  CK(qm_launch_select_masks(P, n_rows, nullptr, (uint32_t *)ctx->masks.p, (uint32_t *)ctx->counts.p, ctx->sm_count,
+  CK(qm_launch_select_masks(P, n_elems, dsel, (uint32_t *)ctx->masks.p, (uint32_t *)ctx->counts.p, ctx->sm_count,
                             ctx->stream));
   size_t tb = 0;
   CK(qm_exclusive_scan_u32(nullptr, &tb, (uint32_t *)ctx->counts.p, (uint64_t *)ctx->offsets.p, n_tiles + 1,
@@ -1863,7 +1878,7 @@ int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_colum
   const int64_t n_write = std::min(total, max_out);
   if (n_write > 0) {
     if ((rc = ensure(ctx, ctx->sel_out, (size_t)n_write * 4 + 16))) return rc;
-    CK(qm_launch_select_write(n_tiles, nullptr, (uint32_t *)ctx->masks.p, (uint64_t *)ctx->offsets.p,
+    CK(qm_launch_select_write(n_tiles, dsel, (uint32_t *)ctx->masks.p, (uint64_t *)ctx->offsets.p,
                               (uint32_t *)ctx->sel_out.p, n_write, ctx->sm_count, ctx->stream));
     CK(cudaMemcpyAsync(out_indices, ctx->sel_out.p, (size_t)n_write * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

@@ -290,15 +290,23 @@ class Context:
         return Table(self, h, n.value, [])
 
     # -- filter-only ---------------------------------------------------------
-    def filter_select(self, columns: Mapping[str, Any], query: QueryDescriptor) -> np.ndarray:
-        """Ascending indices of the rows passing query's filters."""
+    def filter_select(self, columns: Mapping[str, Any], query: QueryDescriptor,
+                      selection: np.ndarray | None = None) -> np.ndarray:
+        """Ascending indices of the rows (of `selection`, if given) passing
+        query's filters."""
         cs = _ColumnSet(columns)
         cq = CQuery(query)
-        cap = cs.n_rows
+        sel_ptr, n_sel = None, 0
+        if selection is not None:
+            sel = np.ascontiguousarray(selection, dtype=np.uint32)
+            cs.keep.append(sel)
+            sel_ptr = sel.ctypes.data_as(C.POINTER(C.c_uint32))
+            n_sel = sel.size
+        cap = n_sel if selection is not None else cs.n_rows
         out = np.empty(max(cap, 1), dtype=np.uint32)
         cnt = C.c_int64()
         self.check(self.lib.qm_filter_select(
-            self.h, cs.n_rows, cs.count, cs.array, cq.ref,
+            self.h, cs.n_rows, cs.count, cs.array, cq.ref, sel_ptr, n_sel,
             out.ctypes.data_as(C.POINTER(C.c_uint32)), cap, C.byref(cnt)))
         return out[:cnt.value].copy()
 
