@@ -272,6 +272,36 @@ int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
                      uint32_t *out_indices, int64_t max_out,
                      int64_t *out_count);
 
+/* ---- filter -> GROUP BY without allocating --------------------------------- */
+/* Bytes of the fixed device scratch array behind qm_query_run_noalloc. */
+#define QM_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* No counterpart in the reference (its WASM engine owns a bump allocator).
+ * For callers that cannot allocate device memory — code running inside
+ * another framework's memory arena or allocator, or where cudaMalloc is not
+ * available to it — this runs the query of qm_query_run over device-resident
+ * columns without any device or pinned allocation: the group table and
+ * every temporary live in one static device array of
+ * QM_NOALLOC_SCRATCH_BYTES, held by each device from the first call on it
+ * until the process exits.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Every call shares and re-initialises the array, so calls
+ * that overlap on the GPU race: serialise them.
+ *   cols         device columns only (on_device = 1); a NULL bitmap must be
+ *                4-byte aligned and readable as ceil(n_rows/32) 32-bit words
+ *   max_groups   capacity of the outputs; queries whose groups (or whose
+ *                scratch need) exceed it fail with QM_ERR_CAPACITY
+ *   out_columns  one device buffer per result column (keys, then aggregates),
+ *                max_groups rows of the column's dtype (QM_I128 = 16 bytes)
+ *   out_null_words  NULL or, per column, NULL or a device buffer of
+ *                ceil(max_groups/32) 32-bit words receiving bit set = NULL
+ *   out_dtypes   NULL or a host array receiving each result column's dtype
+ *   out_groups   receives the number of groups written
+ * Groups come in hash-table order, not first-seen order. */
+int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column *cols,
+                         const qm_query *query, int64_t max_groups, void *const *out_columns,
+                         uint32_t *const *out_null_words, int32_t *out_dtypes, int64_t *out_groups);
+
 /* ---- results ------------------------------------------------------------- */
 int qm_result_num_rows(const qm_result *res, int64_t *out);
 int qm_result_num_columns(const qm_result *res, int32_t *out);

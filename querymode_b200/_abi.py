@@ -55,6 +55,8 @@ QM_AGG_SUM, QM_AGG_AVG, QM_AGG_MIN, QM_AGG_MAX, QM_AGG_COUNT = range(5)
 AGG_CODES = {"sum": QM_AGG_SUM, "avg": QM_AGG_AVG, "min": QM_AGG_MIN,
              "max": QM_AGG_MAX, "count": QM_AGG_COUNT}
 
+QM_NOALLOC_SCRATCH_BYTES = 32 << 20
+
 QM_FLAG_UNORDERED = 1
 QM_FLAG_WASM_SCAN_SEMANTICS = 2
 
@@ -133,6 +135,9 @@ SIGNATURES = [
     ("qm_filter_select", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn),
                                    C.POINTER(QmQuery), C.POINTER(C.c_uint32), C.c_int64,
                                    C.POINTER(C.c_uint32), C.c_int64, C.POINTER(C.c_int64)]),
+    ("qm_query_run_noalloc", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn), C.POINTER(QmQuery),
+                                       C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("qm_result_num_rows", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("qm_result_num_columns", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("qm_result_column", C.c_int, [_P, C.c_int32, C.POINTER(QmResultCol)]),

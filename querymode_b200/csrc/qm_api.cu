@@ -1973,3 +1973,176 @@ int qm_result_destroy(qm_result *r) {
 }
 
 }  // extern "C"
+
+// ================================================================ no-alloc
+// qm_query_run_noalloc: the filter -> GROUP BY of qm_query_run for callers
+// that cannot allocate device memory — code running inside another
+// framework's memory manager or arena, or while the device allocator is
+// unavailable to it.  Every temporary (group table, device status word,
+// compaction lists, staged result columns) lives in one file-scope static
+// device array of QM_NOALLOC_SCRATCH_BYTES that each device holds from the
+// library's first use until the process exits.  The host code of this file
+// reaches it through cudaGetSymbolAddress, once per device (the array's
+// name is only a host-side stand-in).  Calls share the array: overlapping
+// calls on the GPU race and must be serialised by the caller.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[128];
+bool g_noalloc_ready[128];
+
+// The device address of the scratch array on the current device (set up on
+// the first call per device; that call must come before any stream capture).
+int noalloc_scratch(qm_ctx *ctx, unsigned char **out) {
+  if (ctx->device < 0 || ctx->device >= 128) return set_err(ctx, QM_ERR_INVALID, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ready[ctx->device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return set_err(ctx, QM_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    }
+    g_noalloc_addr[ctx->device] = p;
+    g_noalloc_ready[ctx->device] = true;
+  }
+  *out = (unsigned char *)g_noalloc_addr[ctx->device];
+  return QM_OK;
+}
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column *cols,
+                                    const qm_query *q, int64_t max_groups, void *const *out_columns,
+                                    uint32_t *const *out_null_words, int32_t *out_dtypes, int64_t *out_groups) {
+  if (!ctx || !q || !out_columns || !out_groups || n_rows < 0 || n_cols < 0 || (n_cols > 0 && !cols) ||
+      max_groups <= 0)
+    return set_err(ctx, QM_ERR_INVALID, "qm_query_run_noalloc: bad arguments");
+  if (n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
+  *out_groups = 0;
+  cudaSetDevice(ctx->device);
+  unsigned char *scratch = nullptr;
+  int rc = noalloc_scratch(ctx, &scratch);
+  if (rc) return rc;
+  // columns are read in place: device memory only, NULL bitmaps readable as
+  // ceil(n_rows / 32) 32-bit words
+  std::vector<DevCol> dcols(n_cols);
+  for (int i = 0; i < n_cols; i++) {
+    const qm_column &c = cols[i];
+    if (!c.name || !valid_dtype(c.dtype)) return set_err(ctx, QM_ERR_INVALID, "column %d: name / dtype", i);
+    if (!c.on_device) return set_err(ctx, QM_ERR_INVALID, "column %s: qm_query_run_noalloc reads device columns only", c.name);
+    if (n_rows > 0 && !c.data) return set_err(ctx, QM_ERR_INVALID, "column %s: no data", c.name);
+    if (c.null_bitmap && ((uintptr_t)c.null_bitmap & 3))
+      return set_err(ctx, QM_ERR_INVALID, "column %s: NULL bitmap must be 4-byte aligned", c.name);
+    dcols[i].name = c.name;
+    dcols[i].dtype = c.dtype;
+    dcols[i].data = const_cast<void *>(c.data);
+    dcols[i].nulls = (uint32_t *)c.null_bitmap;
+  }
+  ColEnv env;
+  for (auto &c : dcols) env.views.push_back({&c, n_rows});
+  GroupTable gt;
+  if ((rc = plan_query(ctx, q, env, gt.pl))) return rc;
+  Plan &pl = gt.pl;
+  uint64_t space = 0;
+  if ((rc = plan_key_packing(ctx, pl, n_rows, false, &space))) return rc;
+  pl.key.mode = pl.key.n_cols == 0 ? QK_NONE : QK_HASH;
+  if (out_dtypes)
+    for (int k = 0; k < pl.outs.n_out; k++) out_dtypes[k] = pl.outs.o[k].dtype;
+  for (int k = 0; k < pl.outs.n_out; k++)
+    if (!out_columns[k]) return set_err(ctx, QM_ERR_INVALID, "output column %d has no buffer", k);
+  // sizes inside the scratch array
+  Exec &ex = gt.ex;
+  if (pl.key.mode == QK_NONE) {
+    ex.n_slots = 1;
+  } else {
+    ex.log2cap = ilog2_ceil(std::max<int64_t>(1024, max_groups * 2 + max_groups / 8));
+    if (ex.log2cap > 30) return set_err(ctx, QM_ERR_CAPACITY, "max_groups too large for the scratch array");
+    ex.n_slots = (int64_t)1 << ex.log2cap;
+  }
+  choose_layout(pl, max_groups, ex, ctx->tuning);
+  const int64_t G_cap = pl.key.mode == QK_NONE ? 1 : max_groups;
+  const size_t status_off = 0;
+  const size_t table_off = 256;
+  const size_t table_bytes = up256((size_t)ex.total_slots * ex.stride * 8);
+  const size_t keys_off = table_off + table_bytes;
+  const size_t slots_off = keys_off + up256((size_t)ex.total_slots * 8);
+  const size_t out_off = slots_off + up256((size_t)ex.total_slots * 4);
+  qm_outspec O = pl.outs;
+  size_t off = 0;
+  const size_t null_words_bytes = (size_t)((G_cap + 31) / 32) * 4;
+  for (int k = 0; k < O.n_out; k++) {
+    O.o[k].offset = (int64_t)off;
+    off += up256((size_t)G_cap * dtype_size(O.o[k].dtype));
+    if (pl.meta[k].nullable) {
+      O.o[k].null_offset = (int64_t)off;
+      off += up256(null_words_bytes);
+    } else {
+      O.o[k].null_offset = -1;
+    }
+  }
+  const size_t need = out_off + off;
+  if (need > (size_t)QM_NOALLOC_SCRATCH_BYTES)
+    return set_err(ctx, QM_ERR_CAPACITY,
+                   "query needs %zu bytes of scratch for %lld groups; the fixed scratch array holds %u bytes",
+                   need, (long long)max_groups, (unsigned)QM_NOALLOC_SCRATCH_BYTES);
+  qm_status *status = (qm_status *)(scratch + status_off);
+  gt.table = (uint64_t *)(scratch + table_off);
+  // status starts at zero; the group table is re-initialised every call
+  CK(cudaMemsetAsync(status, 0, sizeof(qm_status), ctx->stream));
+  if ((rc = init_table(ctx, gt))) return rc;
+  if (n_rows > 0) {
+    qm_scan_args a;
+    fill_args(gt, a, status);
+    a.n = n_rows;
+    a.sel = nullptr;
+    a.row_offset = 0;
+    const size_t smem = qm_scan_smem_bytes(ex.local_slots, ex.local_hash, pl.agg.n_words, 0, 0);
+    const int blocks = scan_blocks(ctx, smem, n_rows, false);
+    CK(qm_launch_scan(a, blocks, smem, ctx->stream));
+  }
+  qm_status st;
+  CK(cudaMemcpyAsync(&st, status, sizeof st, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (st.error == QM_DEV_OVERFLOW)
+    return set_err(ctx, QM_ERR_CAPACITY, "more groups than max_groups = %lld", (long long)max_groups);
+  if (st.error) return set_err(ctx, QM_ERR_CUDA, "device status %d", st.error);
+  int64_t G = 1;
+  const uint32_t *slots = nullptr;
+  if (pl.key.mode != QK_NONE) {
+    unsigned long long *counter = (unsigned long long *)((unsigned char *)status + offsetof(qm_status, groups_inserted));
+    CK(cudaMemsetAsync(counter, 0, 8, ctx->stream));
+    CK(qm_launch_compact(gt.table, ex.total_slots, ex.stride, pl.agg.w_count, -1, (uint64_t *)(scratch + keys_off),
+                         (uint32_t *)(scratch + slots_off), counter, ctx->sm_count, ctx->stream));
+    unsigned long long g = 0;
+    CK(cudaMemcpyAsync(&g, counter, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    G = (int64_t)g;
+    if (G > max_groups) return set_err(ctx, QM_ERR_CAPACITY, "%lld groups exceed max_groups = %lld", (long long)G,
+                                       (long long)max_groups);
+    slots = (const uint32_t *)(scratch + slots_off);
+  }
+  unsigned char *outbase = scratch + out_off;
+  CK(cudaMemsetAsync(outbase, 0, off, ctx->stream));
+  CK(qm_launch_emit(gt.table, ex.stride, slots, G, pl.key, ex.n_slots, O, outbase, ctx->sm_count, ctx->stream));
+  for (int k = 0; k < O.n_out; k++) {
+    if (G > 0)
+      CK(cudaMemcpyAsync(out_columns[k], outbase + O.o[k].offset, (size_t)G * dtype_size(O.o[k].dtype),
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+    if (out_null_words && out_null_words[k]) {
+      const size_t nw = (size_t)((G + 31) / 32) * 4;
+      if (O.o[k].null_offset >= 0) {
+        if (nw) CK(cudaMemcpyAsync(out_null_words[k], outbase + O.o[k].null_offset, nw, cudaMemcpyDeviceToDevice, ctx->stream));
+      } else if (nw) {
+        CK(cudaMemsetAsync(out_null_words[k], 0, nw, ctx->stream));
+      }
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  *out_groups = G;
+  return QM_OK;
+}
