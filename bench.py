@@ -48,7 +48,7 @@ BYTES_PER_ROW = 28  # ts int64 + qty int32 + key int64 + price float64
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--rows", type=int, default=100_000_000)
@@ -78,55 +78,64 @@ def profiled_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML from a
+    thread during the timed region (read-only queries)."""
 
-    def __init__(self, device: int):
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device = device
-        self.proc = None
-        self.lines: list[str] = []
+        self.period = period_s
+        self.samples: list[tuple[int, int]] = []
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.handle = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.device)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _run(self):
+        import pynvml
+        while not self.stop.is_set():
+            try:
+                mhz = pynvml.nvmlDeviceGetClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+                reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((mhz, reasons))
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            self.handle = self._handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+        except Exception:
+            self.handle = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.handle is not None:
+            self.thread.join(timeout=2)
 
     def summary(self):
-        rows = []
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
-            except ValueError:
-                continue
-        if not rows:
+        if not self.samples:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(r & bit for _, r in self.samples))
+        return {"sm_mhz": float(np.median([m for m, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml"}
 
 
 def dist_setup():
@@ -236,6 +245,7 @@ def main():
 
     from querymode_b200 import datagen
     from querymode_b200.engine import Context
+    from querymode_b200.query import CQuery
 
     torch.cuda.set_device(local)
     n = args.rows
@@ -245,11 +255,12 @@ def main():
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
     table = ctx.table(cols)
+    cq = CQuery(q)  # lowered once, like a prepared statement
     bytes_per_query = n * BYTES_PER_ROW
 
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
-            res = table.run(q)
+            res = table.run(cq)
         barrier(world)
         torch.cuda.synchronize()
         ev0 = torch.cuda.Event(enable_timing=True)
@@ -259,7 +270,7 @@ def main():
         with ClockSampler(local) as clocks:
             ev0.record(stream)
             for _ in range(args.steps):
-                res = table.run(q)
+                res = table.run(cq)
                 scan_ms.append(res.stats.scan_ms)
                 launches += res.stats.launches
             ev1.record(stream)

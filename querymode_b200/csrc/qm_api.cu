@@ -19,6 +19,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -42,6 +43,47 @@ struct HostBuf {
   size_t bytes = 0;
 };
 
+// Pinned host buffers handed to results and recycled when they are
+// destroyed (shared by the context and its results, which may outlive it).
+struct PinnedPool {
+  std::mutex mu;
+  std::vector<HostBuf> free;
+  ~PinnedPool() {
+    for (auto &b : free) cudaFreeHost(b.p);
+  }
+  bool acquire(size_t bytes, HostBuf &out) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      int best = -1;
+      for (int i = 0; i < (int)free.size(); i++)
+        if (free[i].bytes >= bytes && (best < 0 || free[i].bytes < free[best].bytes)) best = i;
+      if (best >= 0) {
+        out = free[best];
+        free.erase(free.begin() + best);
+        return true;
+      }
+    }
+    size_t want = std::max<size_t>(bytes, 64 * 1024);
+    if (cudaMallocHost(&out.p, want) != cudaSuccess) {
+      cudaGetLastError();
+      out = HostBuf();
+      return false;
+    }
+    out.bytes = want;
+    return true;
+  }
+  void release(HostBuf &b) {
+    if (!b.p) return;
+    std::lock_guard<std::mutex> lk(mu);
+    if (free.size() < 8) {
+      free.push_back(b);
+    } else {
+      cudaFreeHost(b.p);
+    }
+    b = HostBuf();
+  }
+};
+
 }  // namespace
 
 struct qm_ctx {
@@ -59,6 +101,7 @@ struct qm_ctx {
   DevBuf masks, counts, offsets, sel_out, sel_in;
   std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
   HostBuf hout, hstatus;
+  std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
 };
 
 namespace {
@@ -140,6 +183,8 @@ struct DevCol {
   long long mn = 0, mx = 0;
   bool has_hll = false;
   double hll = 0;
+  bool has_maxabs = false;
+  double maxabs = 0;  // max |x| over finite non-NULL cells (float columns)
 };
 
 }  // namespace
@@ -242,6 +287,7 @@ struct Plan {
   bool ordered = true;
   int key_col_dtype = 0;
   const DevCol *keycols[QM_MAX_KEYS] = {nullptr, nullptr, nullptr, nullptr};
+  const DevCol *vcolsrc[QM_MAX_VCOLS] = {};
 };
 
 const i128 BIG = (i128)1 << 100;
@@ -451,15 +497,23 @@ int lower_filter(qm_ctx *ctx, const qm_filter &f, const ColView &cv, bool wasm_f
       t.kind = QT_FALSE;
       return QM_OK;
     }
+    // float ranges are kept inclusive: for a non-NaN cell, v > x is
+    // v >= nextafter(x, +inf) and v < x is v <= nextafter(x, -inf)
     t.kind = QT_FRANGE;
     t.f0 = -INFINITY;
     t.f1 = INFINITY;
     t.op = 3;
     switch (f.op) {
       case QM_OP_EQ: t.f0 = t.f1 = v; break;
-      case QM_OP_LT: t.f1 = v; t.op = 1; break;
+      case QM_OP_LT:
+        if (v == -INFINITY) t.kind = QT_FALSE;
+        else t.f1 = std::nextafter(v, -INFINITY);
+        break;
       case QM_OP_LTE: t.f1 = v; break;
-      case QM_OP_GT: t.f0 = v; t.op = 2; break;
+      case QM_OP_GT:
+        if (v == INFINITY) t.kind = QT_FALSE;
+        else t.f0 = std::nextafter(v, INFINITY);
+        break;
       default: t.f0 = v; break;  // GTE
     }
     return QM_OK;
@@ -518,15 +572,9 @@ int build_pred(qm_ctx *ctx, const qm_query *q, const ColEnv &env, qm_pred &P, in
         o.lo = std::max(o.lo, nw.lo);
         o.hi = std::min(o.hi, nw.hi);
         if (o.lo > o.hi) o.kind = QT_FALSE;
-      } else if (nw.kind == QT_FRANGE) {
-        if (nw.f0 > o.f0 || (nw.f0 == o.f0 && !(nw.op & 1))) {
-          o.f0 = nw.f0;
-          o.op = (o.op & ~1) | (nw.op & 1);
-        }
-        if (nw.f1 < o.f1 || (nw.f1 == o.f1 && !(nw.op & 2))) {
-          o.f1 = nw.f1;
-          o.op = (o.op & ~2) | (nw.op & 2);
-        }
+      } else if (nw.kind == QT_FRANGE) {  // inclusive bounds
+        o.f0 = std::max(o.f0, nw.f0);
+        o.f1 = std::min(o.f1, nw.f1);
       } else {
         continue;
       }
@@ -618,6 +666,8 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
       if (vcols[i] == c) return (int)i;
     if ((int)vcols.size() >= QM_MAX_VCOLS) return -1;
     vcols.push_back(c);
+    pl.vcolsrc[vcols.size() - 1] = c;
+    A.vcol[vcols.size() - 1].split = 0.0;
     A.vcol[vcols.size() - 1].data = c->data;
     A.vcol[vcols.size() - 1].nulls = c->nulls;
     A.vcol[vcols.size() - 1].dtype = c->dtype;
@@ -873,6 +923,41 @@ int estimate_groups(qm_ctx *ctx, const qm_keyspec &K, int64_t n, double *out) {
   return QM_OK;
 }
 
+int column_maxabs(qm_ctx *ctx, DevCol &c, int64_t n) {
+  if (c.has_maxabs) return QM_OK;
+  int rc = ensure(ctx, ctx->counter, 64);
+  if (rc) return rc;
+  rc = ensure_host(ctx, ctx->hstatus, 64);
+  if (rc) return rc;
+  CK(qm_launch_maxabs(c.data, c.dtype, c.nulls, n, (unsigned long long *)ctx->counter.p, ctx->sm_count, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->counter.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  uint64_t b = *(uint64_t *)ctx->hstatus.p;
+  memcpy(&c.maxabs, &b, 8);
+  c.has_maxabs = true;
+  return QM_OK;
+}
+
+// Split constants of the float SUM columns of a table query (see qm_vcol).
+int plan_split_sums(qm_ctx *ctx, Plan &pl, int64_t n_rows) {
+  int bits = 1;
+  while (bits < 62 && ((int64_t)1 << bits) <= n_rows) bits++;
+  const int k = bits + 1;  // a group has fewer than 2^(k-1) rows
+  for (int c = 0; c < pl.agg.n_vcols; c++) {
+    qm_vcol &vc = pl.agg.vcol[c];
+    vc.split = 0.0;
+    if (!(vc.flags & VF_SUM) || is_int(vc.dtype) || !pl.vcolsrc[c]) continue;
+    DevCol &col = *const_cast<DevCol *>(pl.vcolsrc[c]);
+    int rc = column_maxabs(ctx, col, n_rows);
+    if (rc) return rc;
+    int e = 0;  // every finite |x| < 2^e
+    if (col.maxabs > 0) e = std::ilogb(col.maxabs) + 1;
+    if (e + k > 1000 || e + k < -960) continue;  // keep TwoSum at the ends of the range
+    vc.split = 1.5 * std::ldexp(1.0, e + k);
+  }
+  return QM_OK;
+}
+
 int column_minmax(qm_ctx *ctx, DevCol &c, int64_t n) {
   if (c.has_minmax) return QM_OK;
   int rc = ensure(ctx, ctx->counter, 64);
@@ -953,14 +1038,20 @@ struct qm_result {
     std::string name;
     int dtype;
     int is_key;
-    std::vector<uint8_t> data;
-    std::vector<uint8_t> nulls;
+    const uint8_t *data = nullptr;   // inside `buf`
+    size_t bytes = 0;
+    const uint8_t *nulls = nullptr;  // inside `buf`, QMCB bit order
     bool has_nulls = false;
   };
   std::vector<Col> cols;
   qm_stats stats{};
   std::vector<uint8_t> qmcb;
   bool qmcb_built = false;
+  std::shared_ptr<PinnedPool> pool;  // returns `buf` on destruction
+  HostBuf buf;
+  ~qm_result() {
+    if (pool) pool->release(buf);
+  }
 };
 
 namespace {
@@ -1080,35 +1171,39 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
     }
   }
   int rc;
-  if ((rc = ensure(ctx, ctx->out, off + 16)) || (rc = ensure_host(ctx, ctx->hout, off + 16))) return rc;
+  if ((rc = ensure(ctx, ctx->out, off + 16))) return rc;
+  HostBuf hbuf;
+  if (!ctx->pool->acquire(off + 16, hbuf)) return set_err(ctx, QM_ERR_OOM, "pinned result buffer (%zu bytes)", off + 16);
+  qm_result *R = new qm_result();
+  R->pool = ctx->pool;
+  R->buf = hbuf;
   CK(cudaMemsetAsync(ctx->out.p, 0, off + 16, ctx->stream));
   CK(qm_launch_emit(gt.table, ex.stride, slots, G, pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p,
                     ctx->sm_count, ctx->stream));
   if (G > 0) ctx->launches++;
-  CK(cudaMemcpyAsync(ctx->hout.p, ctx->out.p, off, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(R->buf.p, ctx->out.p, off, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  cudaError_t se = cudaStreamSynchronize(ctx->stream);
+  if (se != cudaSuccess) {
+    delete R;
+    return set_err(ctx, QM_ERR_CUDA, "finalize: %s", cudaGetErrorString(se));
+  }
   float tail_ms = 0;
   cudaEventElapsedTime(&tail_ms, ctx->ev0, ctx->ev1);
 
-  qm_result *R = new qm_result();
   R->n_rows = G;
-  const uint8_t *h = (const uint8_t *)ctx->hout.p;
+  const uint8_t *h = (const uint8_t *)R->buf.p;
   for (int k = 0; k < O.n_out; k++) {
     qm_result::Col c;
     c.name = pl.meta[k].name;
     c.dtype = O.o[k].dtype;
     c.is_key = pl.meta[k].is_key;
-    size_t bytes = (size_t)G * dtype_size(c.dtype);
-    c.data.assign(h + O.o[k].offset, h + O.o[k].offset + bytes);
+    c.bytes = (size_t)G * dtype_size(c.dtype);
+    c.data = h + O.o[k].offset;
     if (O.o[k].null_offset >= 0) {
-      size_t nb = (size_t)((G + 7) / 8);
-      c.nulls.assign(h + O.o[k].null_offset, h + O.o[k].null_offset + nb);
-      for (uint8_t b : c.nulls)
-        if (b) {
-          c.has_nulls = true;
-          break;
-        }
+      c.nulls = h + O.o[k].null_offset;
+      const size_t nb = (size_t)((G + 7) / 8);
+      for (size_t b = 0; b < nb && !c.has_nulls; b++) c.has_nulls = c.nulls[b] != 0;
     }
     R->cols.push_back(std::move(c));
   }
@@ -1434,6 +1529,7 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
   int64_t est = 1, direct_size = 0;
   uint64_t space = 0;
   if ((rc = plan_key_packing(ctx, pl, t->n_rows, true, &space))) return rc;
+  if ((rc = plan_split_sums(ctx, pl, t->n_rows))) return rc;
   if (pl.key.n_cols == 0) {
     pl.key.mode = QK_NONE;
   } else {
@@ -1906,8 +2002,8 @@ int qm_result_column(const qm_result *r, int32_t i, qm_result_col *out) {
   out->dtype = c.dtype;
   out->is_key = c.is_key;
   out->n_rows = r->n_rows;
-  out->data = c.data.data();
-  out->null_bitmap = c.has_nulls ? c.nulls.data() : nullptr;
+  out->data = c.data;
+  out->null_bitmap = c.has_nulls ? c.nulls : nullptr;
   return QM_OK;
 }
 
@@ -1937,8 +2033,8 @@ int qm_result_qmcb(const qm_result *cr, const uint8_t **buf, size_t *len) {
         for (int64_t i = 0; i < r->n_rows; i++) {
           uint64_t lo;
           int64_t hi;
-          memcpy(&lo, c.data.data() + 16 * i, 8);
-          memcpy(&hi, c.data.data() + 16 * i + 8, 8);
+          memcpy(&lo, c.data + 16 * i, 8);
+          memcpy(&hi, c.data + 16 * i + 8, 8);
           if (hi != ((int64_t)lo < 0 ? -1 : 0)) return QM_ERR_UNSUPPORTED;
         }
         tag = QM_I64;
@@ -1953,11 +2049,11 @@ int qm_result_qmcb(const qm_result *cr, const uint8_t **buf, size_t *len) {
     }
     for (size_t k = 0; k < r->cols.size(); k++) {
       auto &c = r->cols[k];
-      if (c.has_nulls) put(c.nulls.data(), (size_t)((r->n_rows + 7) / 8));
+      if (c.has_nulls) put(c.nulls, (size_t)((r->n_rows + 7) / 8));
       if (c.dtype == QM_I128) {
-        for (int64_t i = 0; i < r->n_rows; i++) put(c.data.data() + 16 * i, 8);
+        for (int64_t i = 0; i < r->n_rows; i++) put(c.data + 16 * i, 8);
       } else {
-        put(c.data.data(), c.data.size());
+        put(c.data, c.bytes);
       }
     }
     r->qmcb_built = true;

@@ -20,7 +20,7 @@ namespace qm {
 
 struct smem_layout {
   int L;
-  size_t keys_off, words_off, queue_off, stage_off, stage_warp_bytes, bytes;
+  size_t keys_off, words_off, queue_off, scratch_off, stage_off, stage_warp_bytes, bytes;
 };
 
 // Per warp staging region: QM_STAGE_MAX_DEPTH mbarriers (32 bytes), then
@@ -34,7 +34,8 @@ __host__ __device__ inline smem_layout make_smem_layout(int local_slots, int loc
   s.words_off = kb;
   size_t wb = (size_t)local_slots * n_words * 8;
   s.queue_off = (s.words_off + wb + 15) & ~(size_t)15;
-  s.stage_off = (s.queue_off + (size_t)warps * QM_WQ * sizeof(uint32_t) + 127) & ~(size_t)127;
+  s.scratch_off = (s.queue_off + (size_t)warps * QM_WQ * sizeof(uint32_t) + 15) & ~(size_t)15;
+  s.stage_off = (s.scratch_off + (size_t)warps * 64 * sizeof(uint64_t) + 127) & ~(size_t)127;
   s.stage_warp_bytes = stage_depth > 0 ? (size_t)(32 + stage_depth * stage_tile_bytes + 127) & ~(size_t)127 : 0;
   s.bytes = s.stage_off + (size_t)warps * s.stage_warp_bytes;
   return s;
@@ -43,7 +44,7 @@ __host__ __device__ inline smem_layout make_smem_layout(int local_slots, int loc
 // Aggregates one survivor per lane (lanes with active = false sit out).
 template <bool SEL>
 __device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
-                                            int *l_used, int lane, bool active, int64_t row) {
+                                            int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
   const qm_aggspec &A = a.agg;
   if (a.dedupe) {
     const unsigned act = __ballot_sync(QM_FULL, active);
@@ -78,21 +79,29 @@ __device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lke
     apply_row(A, tp, ws, local, peers, lane, grow, vb, vnull);
     return;
   }
-  if (!active) return;
-  const uint64_t grow = (uint64_t)(a.row_offset + row);
-  int special;
-  const uint64_t key = row_key(a.key, row, special);
+  uint64_t grow = 0, key = 0;
+  int special = 0;
   uint64_t vb[QM_MAX_VCOLS];
-  uint32_t vnull;
-  gather_values(A, row, vb, vnull);
+  uint32_t vnull = 0;
   int ls = -1;
-  if (L > 0) {
-    if (!a.local_hash) ls = (int)global_slot(a, key, special);
-    else if (special == 0) ls = local_find(lkeys, L, key, l_used);
+  if (active) {
+    grow = (uint64_t)(a.row_offset + row);
+    key = row_key(a.key, row, special);
+    gather_values(A, row, vb, vnull);
+    if (L > 0) {
+      if (!a.local_hash) ls = (int)global_slot(a, key, special);
+      else if (special == 0) ls = local_find(lkeys, L, key, l_used);
+    }
   }
-  if (ls >= 0) {
-    agg_row(A, lw + ls, L, true, grow, vb, vnull);
-  } else if (!(L > 0 && !a.local_hash)) {
+  const bool loc = active && ls >= 0;
+  const unsigned lmask = __ballot_sync(QM_FULL, loc);
+  unsigned peers = 0;
+  if (loc) peers = __match_any_sync(lmask, ls);
+  const bool merge = __any_sync(QM_FULL, (peers & (peers - 1)) != 0);
+  if (loc) {
+    if (merge) agg_row_merged(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr);
+    else agg_row(A, lw + ls, L, true, grow, vb, vnull);
+  } else if (active && !(L > 0 && !a.local_hash)) {
     const int64_t gs = global_slot(a, key, special);
     if (gs >= 0) agg_row(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull);
   }
@@ -121,6 +130,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
   uint64_t *lkeys = reinterpret_cast<uint64_t *>(smem + lay.keys_off);
   uint64_t *lw = reinterpret_cast<uint64_t *>(smem + lay.words_off);
   uint32_t *queue = reinterpret_cast<uint32_t *>(smem + lay.queue_off) + warp * QM_WQ;
+  uint64_t *scr = reinterpret_cast<uint64_t *>(smem + lay.scratch_off) + warp * 64;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + lay.stage_off + warp * lay.stage_warp_bytes);
   uint8_t *sbuf = smem + lay.stage_off + warp * lay.stage_warp_bytes + 32;
   __shared__ int l_used;
@@ -194,6 +204,25 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
       const int tot = (int)base - qn;
       qn = (int)base;
       selected += tot;
+    } else if (!SEL && a.vec_ok && e0 + QM_TILE_ROWS <= a.n) {
+      // full dense tile: the lane's rows are r0 .. r0+7
+      const int64_t r0 = e0 + (int64_t)lane * QM_R;
+      const int64_t nxt = (tile + gwarps) * QM_TILE_ROWS;
+      if (nxt + QM_TILE_ROWS <= a.n) prefetch_tile_l2(a.pred, nxt, lane);
+      m = eval_pred_contig(a.pred, r0, (1u << QM_R) - 1);
+      const uint32_t cnt = __popc(m);
+      uint32_t off = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(QM_FULL, off, o);
+        if (lane >= o) off += x;
+      }
+      const uint32_t tot = __shfl_sync(QM_FULL, off, 31);
+      uint32_t q = qn + off - cnt;
+      const uint32_t r0u = (uint32_t)r0;
+      for (uint32_t mm = m; mm; mm &= mm - 1) queue[q++] = r0u + (uint32_t)(__ffs(mm) - 1);
+      qn += (int)tot;
+      selected += tot;
     } else {
       const int64_t r0 = e0 + (int64_t)lane * QM_R;  // this lane's first element
       int64_t rowv[QM_R];
@@ -203,9 +232,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
         m |= (uint32_t)in << j;
         rowv[j] = r0 + j;
       }
-      if (!SEL && a.vec_ok && e0 + QM_TILE_ROWS <= a.n) {
-        m = eval_pred_contig(a.pred, r0, m);
-      } else {
+      {
         if (SEL) {
 #pragma unroll
           for (int j = 0; j < QM_R; ++j) rowv[j] = ((m >> j) & 1) ? (int64_t)__ldg(a.sel + r0 + j) : 0;
@@ -235,7 +262,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
       const int64_t row = queue[qn - 32 + lane];
       __syncwarp();
       qn -= 32;
-      drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, true, row);
+      drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, true, row, scr);
     }
   }
   if (STAGED && failed) {
@@ -247,7 +274,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
     const bool active = lane < qn;
     const int64_t row = active ? (int64_t)queue[lane] : 0;
     __syncwarp();
-    drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, active, row);
+    drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, active, row, scr);
   }
 
   if (lane == 0 && selected) atomicAdd(&blk_selected, selected);
@@ -551,6 +578,25 @@ __global__ void qm_hll_kernel(const __grid_constant__ qm_keyspec K, int64_t n, u
     if (r[i]) atomicMax(&regs[i], r[i]);
 }
 
+// max |x| over the finite non-NULL cells of a float column (as the bits of a
+// non-negative double, which order like unsigned integers).
+__global__ void qm_maxabs_kernel(const void *p, int dtype, const uint32_t *nulls, int64_t n,
+                                 unsigned long long *out) {
+  unsigned long long mx = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (cell_null(nulls, i)) continue;
+    const double v = dtype == QM_F32 ? (double)__ldg((const float *)p + i) : __ldg((const double *)p + i);
+    if (!isfinite(v)) continue;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v));
+    mx = b > mx ? b : mx;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(QM_FULL, mx, o);
+    mx = x > mx ? x : mx;
+  }
+  if ((threadIdx.x & 31) == 0 && mx) atomicMax(out, mx);
+}
+
 __global__ void qm_minmax_init(long long *out) {
   out[0] = LLONG_MAX;
   out[1] = LLONG_MIN;
@@ -669,6 +715,15 @@ cudaError_t qm_launch_rehash(const uint64_t *old_t, int64_t old_cap, int stride,
   if (old_cap <= 0) return cudaSuccess;
   int blocks = (int)std::min<int64_t>((old_cap + 255) / 256, (int64_t)sm_count * 8);
   qm_rehash<<<blocks, 256, 0, stream>>>(old_t, old_cap, stride, count_word, new_t, log2cap, st);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_maxabs(const void *p, int dtype, const uint32_t *nulls, int64_t n, unsigned long long *out,
+                             int sm_count, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, 8, st);
+  if (e != cudaSuccess || n <= 0) return e;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 4);
+  qm_maxabs_kernel<<<blocks, 256, 0, st>>>(p, dtype, nulls, n, out);
   return cudaGetLastError();
 }
 

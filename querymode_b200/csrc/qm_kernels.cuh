@@ -203,22 +203,23 @@ __device__ __forceinline__ uint32_t eval_term_contig(const qm_term &t, int64_t r
   uint32_t pass = 0;
   if (t.kind <= QT_FALSE) {
     pass = t.kind == QT_TRUE ? ((1u << QM_R) - 1) : 0u;
-  } else if (t.dtype == QM_I32 || t.dtype == QM_I64) {
-    int64_t v[QM_R];
-    if (t.dtype == QM_I32) {
-      int w[QM_R];
-      load_contig<int4, int, 4>(t.data, r0, m, w);
+  } else if (t.dtype == QM_I32) {
+    // the planner clamps int32 bounds to the int32 range: one unsigned
+    // compare per cell tests lo <= v <= hi
+    int w[QM_R];
+    load_contig<int4, int, 4>(t.data, r0, m, w);
+    const int lo = (int)t.lo;
+    const uint32_t span = (uint32_t)((int)t.hi - lo);
 #pragma unroll
-      for (int j = 0; j < QM_R; ++j) v[j] = w[j];
-    } else {
-      long long w[QM_R];
-      load_contig<longlong2, long long, 2>(t.data, r0, m, w);
+    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)((uint32_t)(w[j] - lo) <= span) << j;
+    if (t.kind == QT_INRANGE) pass = ~pass & ((1u << QM_R) - 1);
+  } else if (t.dtype == QM_I64) {
+    long long w[QM_R];
+    load_contig<longlong2, long long, 2>(t.data, r0, m, w);
+    const uint64_t span = (uint64_t)t.hi - (uint64_t)t.lo;
 #pragma unroll
-      for (int j = 0; j < QM_R; ++j) v[j] = w[j];
-    }
-    const bool inr = t.kind == QT_IRANGE;
-#pragma unroll
-    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)((v[j] >= t.lo && v[j] <= t.hi) == inr) << j;
+    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)((uint64_t)w[j] - (uint64_t)t.lo <= span) << j;
+    if (t.kind == QT_INRANGE) pass = ~pass & ((1u << QM_R) - 1);
   } else {
     double v[QM_R];
     if (t.dtype == QM_F32) {
@@ -229,8 +230,13 @@ __device__ __forceinline__ uint32_t eval_term_contig(const qm_term &t, int64_t r
     } else {
       load_contig<double2, double, 2>(t.data, r0, m, v);
     }
+    if (t.kind == QT_FRANGE) {  // bounds are inclusive after planning
 #pragma unroll
-    for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)fterm(t, v[j]) << j;
+      for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)(v[j] >= t.f0 && v[j] <= t.f1) << j;
+    } else {
+#pragma unroll
+      for (int j = 0; j < QM_R; ++j) pass |= (uint32_t)fterm(t, v[j]) << j;
+    }
   }
   if (t.nulls != nullptr) {
     // r0 is a multiple of 8: the lane's 8 NULL bits are one byte
@@ -239,6 +245,21 @@ __device__ __forceinline__ uint32_t eval_term_contig(const qm_term &t, int64_t r
     pass = (pass & ~nb) | (np & nb);
   }
   return m & pass;
+}
+
+// Pull a full tile of every filter column into L2 ahead of its evaluation
+// (one 128-byte line per lane).
+__device__ __forceinline__ void prefetch_tile_l2(const qm_pred &P, int64_t e0, int lane) {
+  const int nt = P.n_groups > 0 ? P.group_end[P.n_groups - 1] : P.n_and;
+  for (int i = 0; i < nt; ++i) {
+    const qm_term &t = P.t[i];
+    if (t.kind <= QT_FALSE) continue;
+    const int elem = (t.dtype == QM_I32 || t.dtype == QM_F32) ? 4 : 8;
+    if (lane < QM_TILE_ROWS * elem / 128) {
+      const char *p = reinterpret_cast<const char *>(t.data) + e0 * elem + lane * 128;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
+  }
 }
 
 __device__ __forceinline__ uint32_t eval_pred_contig(const qm_pred &P, int64_t r0, uint32_t m) {
@@ -522,6 +543,27 @@ __device__ __forceinline__ void fsum_add(uint64_t *hp, uint64_t *lp, double x, d
   if (add != 0.0) atomicAdd(reinterpret_cast<double *>(lp), add);
 }
 
+// Split summation: x = xh + xl exactly; the high words only ever hold
+// multiples of ulp(split) below split in magnitude, so their atomic adds are
+// exact in any order and need no returned value.  Non-finite x goes to the
+// high word as it is (Infinity / NaN propagate as in the reference's sum).
+__device__ __forceinline__ void split_parts(double x, double split, double &xh, double &xl) {
+  if (!isfinite(x)) {
+    xh = x;
+    xl = 0.0;
+    return;
+  }
+  xh = __dsub_rn(__dadd_rn(x, split), split);
+  xl = __dsub_rn(x, xh);
+}
+
+__device__ __forceinline__ void split_add(uint64_t *hp, uint64_t *lp, double x, double split) {
+  double xh, xl;
+  split_parts(x, split, xh, xl);
+  if (xh != 0.0 || isnan(xh)) atomicAdd(reinterpret_cast<double *>(hp), xh);
+  if (xl != 0.0) atomicAdd(reinterpret_cast<double *>(lp), xl);
+}
+
 __device__ __forceinline__ void two_sum_acc(double &s, double &c, double x) {
   double t = s + x;
   if (isfinite(t)) {
@@ -618,6 +660,26 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
       }
       case QA_FSUM: {
         double v = valid ? __longlong_as_double((long long)raw) : 0.0;
+        const double split = A.vcol[ac.vcol].split;
+        if (split != 0.0) {
+          double vh, vl;
+          split_parts(v, split, vh, vl);
+          double h = vh, l = vl;
+          if (!solo)
+            for (unsigned m = peers; m; m &= m - 1) {
+              int src = __ffs(m) - 1;
+              double xh = __shfl_sync(peers, vh, src), xl = __shfl_sync(peers, vl, src);
+              if (src != lane) {
+                h += xh;  // exact: multiples of ulp(split) below split
+                l += xl;
+              }
+            }
+          if (tp) {
+            if (h != 0.0 || isnan(h)) atomicAdd(reinterpret_cast<double *>(w0), h);
+            if (l != 0.0) atomicAdd(reinterpret_cast<double *>(w1), l);
+          }
+          break;
+        }
         double s = v, c = 0.0;
         if (!solo)
           for (unsigned m = peers; m; m &= m - 1) {
@@ -708,7 +770,8 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
       const double d = __longlong_as_double((long long)vb[c]);
       if (f & VF_SUM) {
         uint64_t *w0 = tp + (int64_t)vc.w_sum * ws;
-        fsum_add(w0, w0 + ws, d, 0.0);
+        if (vc.split != 0.0) split_add(w0, w0 + ws, d, vc.split);
+        else fsum_add(w0, w0 + ws, d, 0.0);
       }
       if ((f & (VF_MIN | VF_MAX)) && !isnan(d)) {  // NaN never wins '<' / '>'
         const int64_t o = f2ord(d == 0.0 ? 0.0 : d);
@@ -716,6 +779,96 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
         if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * ws, o);
       }
       if ((f & VF_ZERO) && d == 0.0) min_u64(tp + (int64_t)vc.w_zero * ws, (grow << 1) | (vb[c] >> 63));
+    }
+  }
+}
+
+// Equal-slot merge for a drain round: lanes in `peers` (same block-local
+// slot, mask `lmask` = every lane taking this path) sum their additive
+// contributions through the warp's shared scratch, and the group leader adds
+// them once; MIN / MAX / FIRST stay per lane (64-bit min/max atomics resolve
+// conflicts in hardware, and most are skipped by the read test).
+__device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp, int L, unsigned lmask, unsigned peers,
+                                               int lane, uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS],
+                                               uint32_t vnull, uint64_t *scr) {
+  const bool leader = lane == __ffs(peers) - 1;
+  if (leader) atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)A.w_count * L), (unsigned long long)__popc(peers));
+  if (A.w_first >= 0) min_u64(tp + (int64_t)A.w_first * L, grow);
+  for (int c = 0; c < A.n_vcols; ++c) {
+    const qm_vcol &vc = A.vcol[c];
+    const int f = vc.flags;
+    const bool valid = !((vnull >> c) & 1);
+    if (f & VF_NN) {
+      const unsigned nn = __popc(__ballot_sync(lmask, valid) & peers);
+      if (leader && nn) atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)vc.w_nn * L), (unsigned long long)nn);
+    }
+    const bool isint = vc.dtype == QM_I32 || vc.dtype == QM_I64;
+    const uint64_t raw = pick(vb, c);
+    if (f & VF_SUM) {
+      uint64_t *w0 = tp + (int64_t)vc.w_sum * L;
+      if (isint) {
+        scr[lane] = valid ? raw : 0;
+        __syncwarp(lmask);
+        if (leader) {
+          // 128-bit sum of up to 32 cells (int64 cells can carry out of 64 bits)
+          uint64_t lo = 0;
+          int64_t hi = 0;
+          for (unsigned m = peers; m; m &= m - 1) {
+            const int64_t x = (int64_t)scr[__ffs(m) - 1];
+            const uint64_t nlo = lo + (uint64_t)x;
+            hi += (x < 0 ? -1 : 0) + (nlo < lo ? 1 : 0);
+            lo = nlo;
+          }
+          if (f & VF_WIDE) {
+            if (lo != 0 || hi != 0) add128(w0, w0 + L, lo, hi);
+          } else if (lo != 0) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)lo);  // int32 cells: fits
+          }
+        }
+        __syncwarp(lmask);
+      } else {
+        const double d = valid ? __longlong_as_double((long long)raw) : 0.0;
+        double h, l;
+        if (vc.split != 0.0) split_parts(d, vc.split, h, l);
+        else {
+          h = d;
+          l = 0.0;
+        }
+        scr[lane] = (uint64_t)__double_as_longlong(h);
+        scr[32 + lane] = (uint64_t)__double_as_longlong(l);
+        __syncwarp(lmask);
+        if (leader) {
+          if (vc.split != 0.0) {
+            double sh = 0.0, sl = 0.0;
+            for (unsigned m = peers; m; m &= m - 1) {
+              const int src = __ffs(m) - 1;
+              sh += __longlong_as_double((long long)scr[src]);  // exact: grid multiples below split
+              sl += __longlong_as_double((long long)scr[32 + src]);
+            }
+            if (sh != 0.0) atomicAdd(reinterpret_cast<double *>(w0), sh);
+            if (sl != 0.0) atomicAdd(reinterpret_cast<double *>(w0 + L), sl);
+          } else {
+            double s = 0.0, cc = 0.0;
+            for (unsigned m = peers; m; m &= m - 1) two_sum_acc(s, cc, __longlong_as_double((long long)scr[__ffs(m) - 1]));
+            fsum_add(w0, w0 + L, s, cc);
+          }
+        }
+        __syncwarp(lmask);
+      }
+    }
+    if (!valid) continue;
+    if (isint) {
+      const int64_t v = (int64_t)raw;
+      if (f & VF_MIN) min_i64(tp + (int64_t)vc.w_min * L, v);
+      if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * L, v);
+    } else {
+      const double d = __longlong_as_double((long long)raw);
+      if ((f & (VF_MIN | VF_MAX)) && !isnan(d)) {
+        const int64_t o = f2ord(d == 0.0 ? 0.0 : d);
+        if (f & VF_MIN) min_i64(tp + (int64_t)vc.w_min * L, o);
+        if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * L, o);
+      }
+      if ((f & VF_ZERO) && d == 0.0) min_u64(tp + (int64_t)vc.w_zero * L, (grow << 1) | (raw >> 63));
     }
   }
 }
@@ -756,8 +909,15 @@ __device__ __forceinline__ void merge_local(const qm_aggspec &A, const uint64_t 
         else if (v0) add128(g0, g1, v0, (int64_t)v0 < 0 ? -1 : 0);
         break;
       case QA_FSUM:
-        fsum_add(g0, g1, __longlong_as_double((long long)v0),
-                 __longlong_as_double((long long)lp[(int64_t)(ac.word + 1) * L]));
+        if (A.vcol[ac.vcol].split != 0.0) {
+          const double h = __longlong_as_double((long long)v0);
+          const double l = __longlong_as_double((long long)lp[(int64_t)(ac.word + 1) * L]);
+          if (h != 0.0 || isnan(h)) atomicAdd(reinterpret_cast<double *>(g0), h);
+          if (l != 0.0) atomicAdd(reinterpret_cast<double *>(g1), l);
+        } else {
+          fsum_add(g0, g1, __longlong_as_double((long long)v0),
+                   __longlong_as_double((long long)lp[(int64_t)(ac.word + 1) * L]));
+        }
         break;
       case QA_IMIN:
       case QA_FMIN:

@@ -36,3 +36,5 @@ cudaError_t qm_launch_rehash(const uint64_t *old_t, int64_t old_cap, int stride,
                              int log2cap, qm_status *st, int sm_count, cudaStream_t stream);
 cudaError_t qm_launch_check_selection(const uint32_t *sel, int64_t n_sel, int64_t n_rows, qm_status *st,
                                       int sm_count, cudaStream_t stream);
+cudaError_t qm_launch_maxabs(const void *p, int dtype, const uint32_t *nulls, int64_t n, unsigned long long *out,
+                             int sm_count, cudaStream_t st);

@@ -128,6 +128,11 @@ struct qm_vcol {
   int32_t dtype;
   int32_t flags;
   int32_t w_nn, w_sum, w_min, w_max, w_zero, pad;
+  // float SUM by error-free splitting: 1.5 * 2^(e+k) where every finite
+  // |x| < 2^e and a group has fewer than 2^(k-1) rows; x splits exactly into
+  // xh = (x + split) - split, a multiple of ulp(split) whose sums are exact in
+  // any order, and xl = x - xh.  0: compensate each add with TwoSum instead.
+  double split;
 };
 
 struct qm_aggspec {

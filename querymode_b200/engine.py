@@ -179,16 +179,20 @@ class Result:
         return [c.name for c in self.columns]
 
     @classmethod
-    def from_handle(cls, lib, handle: C.c_void_p, with_qmcb: bool = False) -> "Result":
+    def from_handle(cls, lib, handle: C.c_void_p, with_qmcb: bool = False, owned: bool = False) -> "Result":
+        """Wrap a qm_result.  With owned=True the columns are zero-copy views of
+        the result's pinned host buffer and the handle is destroyed when the
+        last view goes away; otherwise the columns are copies."""
         n = C.c_int64()
         nc = C.c_int32()
         lib.qm_result_num_rows(handle, C.byref(n))
         lib.qm_result_num_columns(handle, C.byref(nc))
+        owner = _ResultOwner(lib, handle) if owned else None
         cols = []
         for i in range(nc.value):
             rc = A.QmResultCol()
             lib.qm_result_column(handle, i, C.byref(rc))
-            cols.append(_read_col(rc, n.value))
+            cols.append(_view_col(rc, n.value, owner) if owned else _read_col(rc, n.value))
         st = A.QmStats()
         lib.qm_result_stats(handle, C.byref(st))
         stats = Stats(st.rows_scanned, st.rows_selected, st.groups, st.bytes_scanned, st.device_ms,
@@ -200,6 +204,44 @@ class Result:
             if lib.qm_result_qmcb(handle, C.byref(p), C.byref(ln)) == A.QM_OK:
                 qmcb = C.string_at(p, ln.value)
         return cls(cols, n.value, stats, qmcb)
+
+
+class _ResultOwner:
+    """Destroys a qm_result once no numpy view of its buffer is alive."""
+
+    def __init__(self, lib, handle):
+        self.lib = lib
+        self.handle = C.c_void_p(handle.value if isinstance(handle, C.c_void_p) else handle)
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.lib.qm_result_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def _buffer_view(addr: int, nbytes: int, owner: _ResultOwner) -> np.ndarray:
+    buf = (C.c_uint8 * max(nbytes, 1)).from_address(addr)
+    buf._owner = owner  # the ctypes array keeps the result alive; numpy keeps the array
+    return np.frombuffer(buf, dtype=np.uint8, count=nbytes)
+
+
+def _view_col(rc: A.QmResultCol, n: int, owner: _ResultOwner) -> ResultColumn:
+    name = rc.name.decode()
+    if n == 0 or not rc.data:
+        return _read_col(rc, n)
+    if rc.dtype == A.QM_I128:
+        vals = _buffer_view(rc.data, 16 * n, owner).view(np.int64).reshape(n, 2)
+    else:
+        dt = np.dtype(_QM_TO_NP[rc.dtype])
+        vals = _buffer_view(rc.data, dt.itemsize * n, owner).view(dt)
+    nulls = None
+    if rc.null_bitmap:
+        bits = _buffer_view(rc.null_bitmap, (n + 7) // 8, owner)
+        nulls = unpack_nulls(bits, n)
+    return ResultColumn(name, rc.dtype, bool(rc.is_key), vals, nulls)
 
 
 def _read_col(rc: A.QmResultCol, n: int) -> ResultColumn:
@@ -335,14 +377,13 @@ class Table:
         except Exception:
             pass
 
-    def run(self, query: QueryDescriptor, with_qmcb: bool = False) -> Result:
-        cq = CQuery(query)
+    def run(self, query: QueryDescriptor | CQuery, with_qmcb: bool = False) -> Result:
+        """Run a query; the result's columns are zero-copy views of its
+        pinned host buffer.  A CQuery may be passed to skip re-lowering."""
+        cq = query if isinstance(query, CQuery) else CQuery(query)
         r = C.c_void_p()
         self.ctx.check(self.ctx.lib.qm_query_run(self.ctx.h, self.h, cq.ref, C.byref(r)))
-        try:
-            return Result.from_handle(self.ctx.lib, r, with_qmcb)
-        finally:
-            self.ctx.lib.qm_result_destroy(r)
+        return Result.from_handle(self.ctx.lib, r, with_qmcb, owned=True)
 
 
 class AggStream:
