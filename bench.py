@@ -56,6 +56,9 @@ def parse_args():
     p.add_argument("--cpu-sample-rows", type=int, default=8_000_000)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--batch-queries", type=int, default=256)
+    p.add_argument("--batch-reps", type=int, default=3)
     return p.parse_args()
 
 
@@ -202,6 +205,85 @@ def cpu_baseline(cols, q, sample_rows: int):
     }
 
 
+def batch_tables_on_device(specs, device: int):
+    """The batched workload's tables generated on the device (seeded torch
+    generator per query), read in place by the library."""
+    import torch
+    g = torch.Generator(device=f"cuda:{device}")
+    out = []
+    for s in specs:
+        g.manual_seed(s["seed"])
+        n, card = s["rows"], s["card"]
+        idx = torch.randint(0, card, (n,), device=f"cuda:{device}", generator=g)
+        if s["key64"]:
+            universe = torch.randint(-(1 << 62), 1 << 62, (card,), dtype=torch.int64, device=f"cuda:{device}",
+                                     generator=g)
+            key = universe[idx]
+        else:
+            key = idx.to(torch.int32)
+        del idx
+        f = torch.randint(0, 10_000, (n,), dtype=torch.int32, device=f"cuda:{device}", generator=g)
+        v = torch.empty(n, dtype=torch.float64, device=f"cuda:{device}").log_normal_(0.0, 1.0, generator=g)
+        out.append({"key": key, "f": f, "v": v})
+    return out
+
+
+def run_batched(ctx, stream, local: int, args) -> dict:
+    """256 filter -> GROUP BY queries of uneven sizes: one persistent fused
+    launch (autotuned, graph-replayed) against the same queries as sequential
+    per-query launches."""
+    import torch
+
+    from querymode_b200 import autotune, datagen
+    from querymode_b200.query import CQuery
+    specs = datagen.batch_specs(args.batch_queries, seed=3)
+    dev_tables = batch_tables_on_device(specs, local)
+    tables = [ctx.table(t) for t in dev_tables]
+    cqs = [CQuery(datagen.batch_query(s)) for s in specs]
+    batch = ctx.batch(tables, cqs)
+    tuned = autotune.tune_batch(batch, reps=1, device_name=torch.cuda.get_device_name(local))
+
+    def timed(fn, reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, (time.perf_counter() - t0) * 1e3 / reps
+
+    def plain():
+        for t, q in zip(tables, cqs):
+            t.run(q)
+
+    with torch.cuda.stream(stream):
+        plain_ms, plain_wall = timed(plain, max(1, args.batch_reps))
+        batch_ms, batch_wall = timed(batch.run, max(3, args.batch_reps))
+    st = batch.stats()
+    n = len(specs)
+    out = {
+        "queries": n, "rows": st["rows"], "bytes": st["bytes"], "chunks": st["chunks"],
+        "plain_ms": plain_ms, "batched_ms": batch_ms, "plain_qps": n / (plain_ms / 1e3),
+        "batched_qps": n / (batch_ms / 1e3), "speedup": plain_ms / batch_ms,
+        "batched_scan_gbs": st["bytes"] / (st["device_ms"] / 1e3) / 1e9,
+        "plain_wall_ms": plain_wall, "batched_wall_ms": batch_wall,
+        "autotune": {"choice": tuned["choice"], "search_s": round(tuned["search_s"], 2),
+                     "trials": len(tuned["trials"])},
+        "workload": "256 queries, rows log-uniform 1e4..5e7, cardinality log-uniform 4..1e6, int32/int64 keys, "
+                    "1-90% selectivity (seed 3)",
+    }
+    batch.close()
+    for t in tables:
+        t.close()
+    del dev_tables
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, world, rank):
     """Reference arm: the reference's algorithm (oracle port) on the host cores."""
     if rank != 0:
@@ -316,6 +398,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cols, q, min(args.cpu_sample_rows, n))
 
+    batched = None
+    if world == 1 and not args.no_batched:
+        table.close()
+        table = None
+        batched = run_batched(ctx, stream, local, args)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -330,12 +418,14 @@ def main():
                          "kernel": "qm_scan_kernel", "kernel_ms": scan_avg},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batched": batched,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "rows_per_s": n * world * args.steps / (elapsed_max / 1e3),
         }
         print(json.dumps(line), flush=True)
-    table.close()
+    if table is not None:
+        table.close()
     ctx.close()
     if world > 1:
         import torch.distributed as dist

@@ -302,6 +302,31 @@ int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_c
                          const qm_query *query, int64_t max_groups, void *const *out_columns,
                          uint32_t *const *out_null_words, int32_t *out_dtypes, int64_t *out_groups);
 
+/* ---- batched launch ------------------------------------------------------- */
+typedef struct qm_batch qm_batch;
+
+/* Plan n independent filter -> GROUP BY queries, query i over table i, for
+ * one persistent fused launch (the reference runs them as n separate
+ * executions, each a full pipeline, src/client.ts:1003-1085).  Blocks claim
+ * (query, row range) chunks of uneven queries from a shared counter; the
+ * whole run — table init, scan, first-seen ordering, finalize — is captured
+ * as a CUDA graph on the first qm_batch_run and replayed afterwards.  At
+ * most 4096 queries. */
+int qm_batch_create(qm_ctx *ctx, int32_t n, const qm_table *const *tables,
+                    const qm_query *const *queries, qm_batch **out);
+/* Run the batch; results[i] receives query i's result (destroy each). */
+int qm_batch_run(qm_batch *batch, qm_result **results);
+/* Launch-shape knobs chosen by the autotuner (querymode_b200/autotune.py):
+ * tiles of 256 rows per work chunk, block-local table budget in KiB (0:
+ * global tables only), resident blocks per SM (0: occupancy).  A negative
+ * value keeps the current setting.  Re-captures the graph on the next run. */
+int qm_batch_set_tuning(qm_batch *batch, int32_t chunk_tiles, int32_t local_kb,
+                        int32_t blocks_per_sm);
+/* Device time of the last run, total rows and algorithmic bytes, chunks. */
+int qm_batch_stats(const qm_batch *batch, double *device_ms, int64_t *rows,
+                   int64_t *bytes, int32_t *chunks);
+int qm_batch_destroy(qm_batch *batch);
+
 /* ---- results ------------------------------------------------------------- */
 int qm_result_num_rows(const qm_result *res, int64_t *out);
 int qm_result_num_columns(const qm_result *res, int32_t *out);

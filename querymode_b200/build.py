@@ -16,8 +16,8 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libqm_gpu.so")
-SOURCES = ["qm_api.cu", "qm_kernels.cu"]
-HEADERS = ["qm_plan.h", "qm_launch.h", "qm_kernels.cuh",
+SOURCES = ["qm_api.cu", "qm_kernels.cu", "qm_batch.cu"]
+HEADERS = ["qm_plan.h", "qm_launch.h", "qm_kernels.cuh", "qm_batch.h",
            os.path.join("..", "..", "include", "qm_gpu.h")]
 
 NVCC_FLAGS = [

@@ -1049,6 +1049,7 @@ struct qm_result {
   bool qmcb_built = false;
   std::shared_ptr<PinnedPool> pool;  // returns `buf` on destruction
   HostBuf buf;
+  std::shared_ptr<void> shared;      // a batch's packed buffer, shared by its results
   ~qm_result() {
     if (pool) pool->release(buf);
   }
@@ -1296,7 +1297,95 @@ int plan_query(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl) {
 
 
 // ================================================================== C ABI
+
+namespace {
+
+// Plan `q` over registered table `t`: lower it, pack its keys, pick the
+// key mode (direct when the key range from column statistics is dense, else
+// hash) and estimate the group count (HyperLogLog, cached per column).
+int plan_table_query(qm_ctx *ctx, qm_table *t, const qm_query *q, GroupTable &gt, int64_t &est,
+                     int64_t &direct_size) {
+  ColEnv env;
+  for (auto &c : t->cols) env.views.push_back({&c, t->n_rows});
+  int rc = plan_query(ctx, q, env, gt.pl);
+  if (rc) return rc;
+  Plan &pl = gt.pl;
+  est = 1;
+  direct_size = 0;
+  uint64_t space = 0;
+  if ((rc = plan_key_packing(ctx, pl, t->n_rows, true, &space))) return rc;
+  if ((rc = plan_split_sums(ctx, pl, t->n_rows))) return rc;
+  if (pl.key.n_cols == 0) {
+    pl.key.mode = QK_NONE;
+  } else {
+    const ColView *kv = env.find(q->group_by[0]);
+    DevCol &kc = *const_cast<DevCol *>(kv->col);
+    bool direct = false;
+    if (pl.key.pack == QP_DIGITS) {
+      if (space <= (1ULL << 25) && (int64_t)space <= std::max<int64_t>(4 * t->n_rows, 1 << 16)) {
+        direct = true;
+        direct_size = (int64_t)space;
+        pl.key.base = 0;
+      }
+    } else if (pl.key.n_cols == 1 && is_int(kc.dtype)) {
+      if ((rc = column_minmax(ctx, kc, t->n_rows))) return rc;
+      if (kc.mx >= kc.mn) {
+        unsigned long long range = (unsigned long long)kc.mx - (unsigned long long)kc.mn + 1ULL;
+        if (range != 0 && range <= (1ULL << 25) && (int64_t)range <= std::max<int64_t>(4 * t->n_rows, 1 << 16)) {
+          direct = true;
+          direct_size = (int64_t)range;
+          pl.key.base = kc.mn;
+        }
+      } else {
+        direct = true;  // no non-null key: only the NULL slot is used
+        direct_size = 1;
+        pl.key.base = 0;
+      }
+    }
+    const bool single = pl.key.n_cols == 1;
+    if (direct) {
+      pl.key.mode = QK_DIRECT;
+      est = direct_size;
+      if (direct_size > (1 << 16)) {
+        double e = 0;
+        if (single && kc.has_hll) {
+          e = kc.hll;
+        } else {
+          qm_keyspec K = pl.key;
+          K.mode = QK_HASH;
+          if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
+          if (single) {
+            kc.hll = e;
+            kc.has_hll = true;
+          }
+        }
+        est = std::min<int64_t>(est, (int64_t)(e * 1.05) + 16);
+      }
+    } else {
+      pl.key.mode = QK_HASH;
+      if (single && kc.has_hll) {
+        est = (int64_t)(kc.hll * 1.05) + 16;
+      } else {
+        qm_keyspec K = pl.key;
+        double e;
+        if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
+        est = (int64_t)(e * 1.05) + 16;
+        if (pl.key.n_cols == 1) {
+          kc.hll = e;
+          kc.has_hll = true;
+        }
+      }
+      est = std::min<int64_t>(est, std::max<int64_t>(t->n_rows, 1));
+    }
+  }
+  return QM_OK;
+}
+
+}  // namespace
+
 extern "C" {
+
+
 
 const char *qm_version(void) { return "querymode-b200 0.1 (sm_100a)"; }
 
@@ -1519,80 +1608,11 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
   cudaSetDevice(ctx->device);
   qm_table *t = const_cast<qm_table *>(table);
   ctx->launches = 0;
-  ColEnv env;
-  for (auto &c : t->cols) env.views.push_back({&c, t->n_rows});
   GroupTable gt;
-  int rc = plan_query(ctx, q, env, gt.pl);
+  int64_t est = 1, direct_size = 0;
+  int rc = plan_table_query(ctx, t, q, gt, est, direct_size);
   if (rc) return rc;
   Plan &pl = gt.pl;
-  // key mode and size
-  int64_t est = 1, direct_size = 0;
-  uint64_t space = 0;
-  if ((rc = plan_key_packing(ctx, pl, t->n_rows, true, &space))) return rc;
-  if ((rc = plan_split_sums(ctx, pl, t->n_rows))) return rc;
-  if (pl.key.n_cols == 0) {
-    pl.key.mode = QK_NONE;
-  } else {
-    const ColView *kv = env.find(q->group_by[0]);
-    DevCol &kc = *const_cast<DevCol *>(kv->col);
-    bool direct = false;
-    if (pl.key.pack == QP_DIGITS) {
-      if (space <= (1ULL << 25) && (int64_t)space <= std::max<int64_t>(4 * t->n_rows, 1 << 16)) {
-        direct = true;
-        direct_size = (int64_t)space;
-        pl.key.base = 0;
-      }
-    } else if (pl.key.n_cols == 1 && is_int(kc.dtype)) {
-      if ((rc = column_minmax(ctx, kc, t->n_rows))) return rc;
-      if (kc.mx >= kc.mn) {
-        unsigned long long range = (unsigned long long)kc.mx - (unsigned long long)kc.mn + 1ULL;
-        if (range != 0 && range <= (1ULL << 25) && (int64_t)range <= std::max<int64_t>(4 * t->n_rows, 1 << 16)) {
-          direct = true;
-          direct_size = (int64_t)range;
-          pl.key.base = kc.mn;
-        }
-      } else {
-        direct = true;  // no non-null key: only the NULL slot is used
-        direct_size = 1;
-        pl.key.base = 0;
-      }
-    }
-    const bool single = pl.key.n_cols == 1;
-    if (direct) {
-      pl.key.mode = QK_DIRECT;
-      est = direct_size;
-      if (direct_size > (1 << 16)) {
-        double e = 0;
-        if (single && kc.has_hll) {
-          e = kc.hll;
-        } else {
-          qm_keyspec K = pl.key;
-          K.mode = QK_HASH;
-          if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
-          if (single) {
-            kc.hll = e;
-            kc.has_hll = true;
-          }
-        }
-        est = std::min<int64_t>(est, (int64_t)(e * 1.05) + 16);
-      }
-    } else {
-      pl.key.mode = QK_HASH;
-      if (single && kc.has_hll) {
-        est = (int64_t)(kc.hll * 1.05) + 16;
-      } else {
-        qm_keyspec K = pl.key;
-        double e;
-        if ((rc = estimate_groups(ctx, K, t->n_rows, &e))) return rc;
-        est = (int64_t)(e * 1.05) + 16;
-        if (pl.key.n_cols == 1) {
-          kc.hll = e;
-          kc.has_hll = true;
-        }
-      }
-      est = std::min<int64_t>(est, std::max<int64_t>(t->n_rows, 1));
-    }
-  }
   gt.rows_done = 0;
   for (int attempt = 0;; attempt++) {
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
@@ -2242,3 +2262,371 @@ extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
   *out_groups = G;
   return QM_OK;
 }
+
+// ================================================================== batches
+// Many queries, each over its own registered table, in one persistent fused
+// launch (qm_batch.cu) captured as a CUDA graph on the first run and
+// replayed afterwards.  The work split (tiles per chunk), the block-local
+// table budget and blocks per SM are the autotuner's knobs.
+#include "qm_batch.h"
+
+namespace {
+
+// Keeps a batch run's packed pinned buffer alive for all of its results.
+struct SharedPinned {
+  std::shared_ptr<PinnedPool> pool;
+  HostBuf buf;
+  ~SharedPinned() {
+    if (pool) pool->release(buf);
+  }
+};
+
+int64_t region_bytes(int64_t G, const qm_bq &b) {
+  int64_t off = 0;
+  for (int k = 0; k < b.outs.n_out; k++) {
+    off += (G * b.width[k] + 15) & ~(int64_t)15;
+    if (b.nullable[k]) off += ((G + 31) / 32 * 4 + 15) & ~(int64_t)15;
+  }
+  return off;
+}
+
+}  // namespace
+
+struct qm_batch {
+  qm_ctx *ctx = nullptr;
+  int n = 0;
+  std::vector<GroupTable> gts;
+  std::vector<qm_bq> bq;
+  std::vector<int64_t> rows;
+  std::vector<int64_t> est;  // planner's group estimate per query
+  DevBuf arena, d_bq, d_slot0, d_chunks, d_counter, d_status, d_bitmap, d_popc, d_ranks, d_temp, d_meta,
+      d_packed, d_nullbytes;
+  HostBuf h_meta, h_status;
+  qm_batch_dev dev{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int chunk_tiles = 512;
+  int local_kb = 40;
+  int bps = 0;
+  float last_ms = 0;
+  int64_t bytes_scanned = 0;
+  int64_t total_rows = 0;
+  ~qm_batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    DevBuf *bufs[] = {&arena, &d_bq, &d_slot0, &d_chunks, &d_counter, &d_status, &d_bitmap, &d_popc, &d_ranks,
+                      &d_temp, &d_meta, &d_packed, &d_nullbytes};
+    for (DevBuf *b : bufs) release(*b);
+    if (h_meta.p) cudaFreeHost(h_meta.p);
+    if (h_status.p) cudaFreeHost(h_status.p);
+  }
+};
+
+namespace {
+
+void drop_graph(qm_batch *b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->gexec = nullptr;
+  b->graph = nullptr;
+}
+
+// (Re)build chunks, table layout and device descriptors for the current knobs.
+int batch_layout(qm_batch *b) {
+  qm_ctx *ctx = b->ctx;
+  const int n = b->n;
+  const size_t local_budget = (size_t)b->local_kb * 1024;
+  int64_t slots = 0, words = 0, bm_words = 0, packed_max = 0, nullbytes_max = 0;
+  std::vector<int64_t> slot0(n), table_off(n);
+  for (int i = 0; i < n; i++) {
+    GroupTable &gt = b->gts[i];
+    Exec &ex = gt.ex;
+    // block-local table within the batch's shared-memory budget
+    const int64_t per_slot = (int64_t)gt.pl.agg.n_words * 8;
+    if (ex.local_slots > 0) {
+      int64_t need = (int64_t)ex.local_slots * (per_slot + (ex.local_hash ? 8 : 0));
+      if (local_budget == 0) {
+        ex.local_slots = 0;
+      } else if (need > (int64_t)local_budget) {
+        int L = 1;
+        while ((int64_t)(L * 2) * (per_slot + 8) <= (int64_t)local_budget) L *= 2;
+        ex.local_slots = L >= 32 ? L : 0;
+        ex.local_hash = 1;
+      }
+    }
+    slot0[i] = slots;
+    table_off[i] = words;
+    slots += ex.total_slots;
+    words += ex.total_slots * ex.stride;
+    qm_bq &q = b->bq[i];
+    q.bm_word0 = bm_words;
+    q.bm_words = b->rows[i] / 32 + 1;
+    bm_words += q.bm_words;
+    const int64_t gmax = q.none ? 1 : std::min<int64_t>(ex.total_slots, std::max<int64_t>(b->rows[i], 1));
+    packed_max += region_bytes(gmax, q);
+    for (int k = 0; k < q.outs.n_out; k++)
+      if (q.nullable[k]) nullbytes_max += (gmax + 15) & ~(int64_t)15;
+  }
+  int rc;
+  if ((rc = ensure(ctx, b->arena, (size_t)words * 8 + 64))) return rc;
+  if ((rc = ensure(ctx, b->d_status, sizeof(qm_status) * n))) return rc;
+  for (int i = 0; i < n; i++) {
+    GroupTable &gt = b->gts[i];
+    gt.table = (uint64_t *)b->arena.p + table_off[i];
+    qm_bq &q = b->bq[i];
+    fill_args(gt, q.a, (qm_status *)b->d_status.p + i);
+    q.a.n = b->rows[i];
+    q.a.sel = nullptr;
+    q.a.row_offset = 0;
+    memset(&q.a.stage, 0, sizeof q.a.stage);
+  }
+  // chunks: each query's tiles cut into runs of chunk_tiles
+  std::vector<qm_chunk> chunks;
+  for (int i = 0; i < n; i++) {
+    const int64_t tiles = (b->rows[i] + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+    for (int64_t t0 = 0; t0 < tiles; t0 += b->chunk_tiles) {
+      qm_chunk c;
+      c.q = i;
+      c.pad = 0;
+      c.tile0 = t0;
+      c.tile1 = std::min<int64_t>(tiles, t0 + b->chunk_tiles);
+      chunks.push_back(c);
+    }
+  }
+  // the largest local table of the batch sets the kernel's shared memory
+  int local_bytes = 0;
+  for (int i = 0; i < n; i++) {
+    const Exec &ex = b->gts[i].ex;
+    if (ex.local_slots > 0)
+      local_bytes = std::max<int>(local_bytes, ex.local_slots * (b->gts[i].pl.agg.n_words * 8 + (ex.local_hash ? 8 : 0)));
+  }
+  size_t temp = 0;
+  CK(qm_batch_scan_temp_bytes(bm_words, &temp));
+  if ((rc = ensure(ctx, b->d_bq, sizeof(qm_bq) * n)) || (rc = ensure(ctx, b->d_slot0, sizeof(int64_t) * n)) ||
+      (rc = ensure(ctx, b->d_chunks, sizeof(qm_chunk) * std::max<size_t>(chunks.size(), 1))) ||
+      (rc = ensure(ctx, b->d_counter, 16)) || (rc = ensure(ctx, b->d_bitmap, sizeof(uint32_t) * (bm_words + 1))) ||
+      (rc = ensure(ctx, b->d_popc, sizeof(uint32_t) * (bm_words + 1))) ||
+      (rc = ensure(ctx, b->d_ranks, sizeof(uint64_t) * (bm_words + 1))) || (rc = ensure(ctx, b->d_temp, temp + 16)) ||
+      (rc = ensure(ctx, b->d_meta, sizeof(qm_batch_meta))) || (rc = ensure(ctx, b->d_packed, (size_t)packed_max + 64)) ||
+      (rc = ensure(ctx, b->d_nullbytes, (size_t)nullbytes_max + 64)) ||
+      (rc = ensure_host(ctx, b->h_meta, sizeof(qm_batch_meta))) || (rc = ensure_host(ctx, b->h_status, sizeof(qm_status) * n)))
+    return rc;
+  CK(cudaMemcpyAsync(b->d_bq.p, b->bq.data(), sizeof(qm_bq) * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(b->d_slot0.p, slot0.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  if (!chunks.empty())
+    CK(cudaMemcpyAsync(b->d_chunks.p, chunks.data(), sizeof(qm_chunk) * chunks.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  qm_batch_dev &d = b->dev;
+  d.n = n;
+  d.sm_count = ctx->sm_count;
+  d.bq = (qm_bq *)b->d_bq.p;
+  d.slot0 = (int64_t *)b->d_slot0.p;
+  d.total_slots = slots;
+  d.chunks = (qm_chunk *)b->d_chunks.p;
+  d.n_chunks = (int)chunks.size();
+  d.counter = (int *)b->d_counter.p;
+  d.statuses = (qm_status *)b->d_status.p;
+  d.bitmap = (uint32_t *)b->d_bitmap.p;
+  d.bm_words = bm_words;
+  d.popc = (uint32_t *)b->d_popc.p;
+  d.ranks = (uint64_t *)b->d_ranks.p;
+  d.scan_temp = b->d_temp.p;
+  d.scan_temp_bytes = temp;
+  d.meta = (qm_batch_meta *)b->d_meta.p;
+  d.meta_host = (qm_batch_meta *)b->h_meta.p;
+  d.meta_bytes = sizeof(qm_batch_meta);
+  d.packed = (unsigned char *)b->d_packed.p;
+  d.nullbytes = (unsigned char *)b->d_nullbytes.p;
+  d.local_bytes = local_bytes;
+  d.scan_smem = qm_batch_smem_bytes(local_bytes);
+  int bps = 1;
+  {
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    if (qm_batch_configure(d.scan_smem, &bps) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", d.scan_smem);
+    }
+  }
+  if (bps < 1) bps = 1;
+  if (b->bps > 0 && b->bps < bps) bps = b->bps;
+  d.scan_blocks = std::max(1, std::min(ctx->sm_count * bps, d.n_chunks));
+  drop_graph(b);
+  return QM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qm_batch_create(qm_ctx *ctx, int32_t n, const qm_table *const *tables, const qm_query *const *queries,
+                    qm_batch **out) {
+  if (!ctx || !out || n <= 0 || !tables || !queries) return set_err(ctx, QM_ERR_INVALID, "qm_batch_create: bad arguments");
+  if (n > QM_BATCH_MAX) return set_err(ctx, QM_ERR_UNSUPPORTED, "at most %d queries per batch", QM_BATCH_MAX);
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  qm_batch *b = new qm_batch();
+  b->ctx = ctx;
+  b->n = n;
+  b->gts.resize(n);
+  b->bq.resize(n);
+  b->rows.resize(n);
+  b->est.resize(n);
+  for (int i = 0; i < n; i++) {
+    if (!tables[i] || !queries[i]) {
+      delete b;
+      return set_err(ctx, QM_ERR_INVALID, "query %d: null table or query", i);
+    }
+    qm_query q = *queries[i];
+    q.flags &= ~QM_FLAG_UNORDERED;  // the batched finalize always orders by first row
+    qm_table *t = const_cast<qm_table *>(tables[i]);
+    GroupTable &gt = b->gts[i];
+    int64_t est = 1, direct_size = 0;
+    int rc = plan_table_query(ctx, t, &q, gt, est, direct_size);
+    if (rc) {
+      delete b;
+      return rc;
+    }
+    // sizes as setup_table, without allocating
+    Exec &ex = gt.ex;
+    if (gt.pl.key.mode == QK_NONE) {
+      ex.n_slots = 1;
+    } else if (gt.pl.key.mode == QK_DIRECT) {
+      ex.n_slots = direct_size;
+    } else {
+      int64_t want = std::max<int64_t>(1024, est * 2 + est / 8);
+      ex.log2cap = ilog2_ceil(want);
+      ex.n_slots = (int64_t)1 << ex.log2cap;
+    }
+    choose_layout(gt.pl, est, ex, ctx->tuning);
+    b->est[i] = est;
+    qm_bq &qb = b->bq[i];
+    memset(&qb, 0, sizeof qb);
+    qb.outs = gt.pl.outs;
+    qb.none = gt.pl.key.mode == QK_NONE;
+    for (int k = 0; k < qb.outs.n_out; k++) {
+      qb.width[k] = (int32_t)dtype_size(qb.outs.o[k].dtype);
+      qb.nullable[k] = gt.pl.meta[k].nullable ? 1 : 0;
+    }
+    b->rows[i] = t->n_rows;
+    b->total_rows += t->n_rows;
+    b->bytes_scanned += gt.pl.bytes_per_row * t->n_rows;
+  }
+  int rc = batch_layout(b);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return QM_OK;
+}
+
+int qm_batch_set_tuning(qm_batch *b, int32_t chunk_tiles, int32_t local_kb, int32_t blocks_per_sm) {
+  if (!b) return QM_ERR_INVALID;
+  if (chunk_tiles > 0) b->chunk_tiles = chunk_tiles;
+  if (local_kb >= 0) b->local_kb = std::min(local_kb, 160);
+  if (blocks_per_sm >= 0) b->bps = blocks_per_sm;
+  cudaSetDevice(b->ctx->device);
+  // rebuild block-local table choices from the planner's, then re-lay out
+  for (int i = 0; i < b->n; i++) choose_layout(b->gts[i].pl, b->est[i], b->gts[i].ex, b->ctx->tuning);
+  return batch_layout(b);
+}
+
+int qm_batch_run(qm_batch *b, qm_result **results) {
+  if (!b || !results) return QM_ERR_INVALID;
+  qm_ctx *ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  if (!b->gexec) {
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = qm_batch_launch_all(b->dev, ctx->stream);
+    cudaError_t e2 = cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n, cudaMemcpyDeviceToHost,
+                                     ctx->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e3 = cudaStreamEndCapture(ctx->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return set_err(ctx, QM_ERR_CUDA, "capturing the batched launch: %s",
+                     cudaGetErrorString(e != cudaSuccess ? e : (e2 != cudaSuccess ? e2 : e3)));
+    }
+    b->graph = g;
+    CK(cudaGraphInstantiate(&b->gexec, g, 0));
+  }
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(cudaGraphLaunch(b->gexec, ctx->stream));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  const qm_status *st = (const qm_status *)b->h_status.p;
+  for (int i = 0; i < b->n; i++)
+    if (st[i].error)
+      return set_err(ctx, st[i].error == QM_DEV_OVERFLOW ? QM_ERR_CAPACITY : QM_ERR_CUDA,
+                     "query %d of the batch: device status %d (group estimate too small)", i, st[i].error);
+  const qm_batch_meta *meta = (const qm_batch_meta *)b->h_meta.p;
+  auto holder = std::make_shared<SharedPinned>();
+  holder->pool = ctx->pool;
+  const size_t total = (size_t)meta->total;
+  if (!ctx->pool->acquire(total + 16, holder->buf)) return set_err(ctx, QM_ERR_OOM, "pinned batch results");
+  if (total) CK(cudaMemcpyAsync(holder->buf.p, b->dev.packed, total, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms2 = 0;
+  cudaEventElapsedTime(&ms2, ctx->ev0, ctx->ev1);
+  b->last_ms = ms2;
+  const uint8_t *h = (const uint8_t *)holder->buf.p;
+  for (int i = 0; i < b->n; i++) {
+    const qm_bq &qb = b->bq[i];
+    const Plan &pl = b->gts[i].pl;
+    const int64_t G = meta->groups[i];
+    qm_result *R = new qm_result();
+    R->shared = holder;
+    R->n_rows = G;
+    int64_t off = meta->base[i];
+    for (int k = 0; k < qb.outs.n_out; k++) {
+      qm_result::Col c;
+      c.name = pl.meta[k].name;
+      c.dtype = qb.outs.o[k].dtype;
+      c.is_key = pl.meta[k].is_key;
+      c.bytes = (size_t)G * qb.width[k];
+      c.data = h + off;
+      off += ((int64_t)c.bytes + 15) & ~(int64_t)15;
+      if (qb.nullable[k]) {
+        c.nulls = h + off;
+        const size_t nb = (size_t)((G + 7) / 8);
+        for (size_t x = 0; x < nb && !c.has_nulls; x++) c.has_nulls = c.nulls[x] != 0;
+        off += ((G + 31) / 32 * 4 + 15) & ~(int64_t)15;
+      }
+      R->cols.push_back(std::move(c));
+    }
+    R->stats.rows_scanned = b->rows[i];
+    R->stats.rows_selected = (int64_t)st[i].rows_selected;
+    R->stats.groups = G;
+    R->stats.bytes_scanned = b->gts[i].pl.bytes_per_row * b->rows[i];
+    R->stats.device_ms = ms2;
+    R->stats.scan_ms = ms;
+    R->stats.strategy = b->gts[i].ex.strategy;
+    R->stats.launches = 9;
+    results[i] = R;
+  }
+  return QM_OK;
+}
+
+int qm_batch_stats(const qm_batch *b, double *device_ms, int64_t *rows, int64_t *bytes, int32_t *chunks) {
+  if (!b) return QM_ERR_INVALID;
+  if (device_ms) *device_ms = b->last_ms;
+  if (rows) *rows = b->total_rows;
+  if (bytes) *bytes = b->bytes_scanned;
+  if (chunks) *chunks = b->dev.n_chunks;
+  return QM_OK;
+}
+
+int qm_batch_destroy(qm_batch *b) {
+  if (!b) return QM_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  delete b;
+  return QM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+// qm_batch.cu — many filter -> GROUP BY queries in one persistent launch.
+//
+// Each query of a batch has its own plan (qm_scan_args), group table and
+// status in device memory.  Work is cut into chunks (query, tile range);
+// every block claims chunks from an atomic counter, keeps the current
+// query's plan in shared memory, and merges its block-local table into the
+// query's global table whenever it moves to another query.
+//
+// Finalize is batched too and needs no sort: a group's first-seen rank is
+// the number of groups of its query whose first row is smaller, i.e. the
+// prefix popcount of the query's bitmap of first rows at the group's own
+// first row.  Each query's rows are written at their rank into one packed
+// buffer (columns, then NULL bitmaps), so one copy returns every result.
+#include <cub/cub.cuh>
+
+#include "qm_batch.h"
+#include "qm_launch.h"
+#include "qm_kernels.cuh"
+
+namespace qm {
+
+__device__ __forceinline__ int find_query(const int64_t *slot0, int n, int64_t gs) {
+  int lo = 0, hi = n - 1;  // last query whose slot0 <= gs
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (slot0[mid] <= gs) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void qm_batch_init(const qm_bq *bq, const int64_t *slot0, int n, int64_t total) {
+  for (int64_t gs = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gs < total; gs += (int64_t)gridDim.x * blockDim.x) {
+    const int q = find_query(slot0, n, gs);
+    const qm_scan_args &a = bq[q].a;
+    const int64_t s = gs - slot0[q];
+    uint64_t *slot = a.table + s * a.stride;
+    slot[0] = a.key.mode == QK_HASH ? QM_EMPTY_KEY : 0ULL;
+    for (int w = 1; w < a.stride; ++w) slot[w] = a.agg.init[w - 1];
+  }
+}
+
+// Shared memory: block-local table (keys, then words SoA), per-warp queues,
+// per-warp merge scratch — sized for the batch's largest local table.
+struct bsmem {
+  size_t words_off, queue_off, scratch_off, bytes;
+};
+__host__ __device__ inline bsmem batch_smem(int local_bytes, int warps) {
+  bsmem s;
+  s.words_off = 0;
+  s.queue_off = ((size_t)local_bytes + 15) & ~(size_t)15;
+  s.scratch_off = s.queue_off + (size_t)warps * (QM_TILE_ROWS + 32) * sizeof(uint32_t);
+  s.bytes = s.scratch_off + (size_t)warps * 64 * sizeof(uint64_t);
+  return s;
+}
+
+__device__ void batch_flush(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw) {
+  const int L = a.local_slots;
+  if (L <= 0) return;
+  const qm_aggspec &A = a.agg;
+  for (int s = threadIdx.x; s < L; s += blockDim.x) {
+    if (lw[(int64_t)A.w_count * L + s] == 0) continue;
+    int64_t gs;
+    if (a.local_hash) gs = global_slot(a, lkeys[s], 0);
+    else gs = s;
+    if (gs < 0) continue;
+    merge_local(A, lw + s, L, a.table + gs * a.stride + 1);
+  }
+}
+
+__global__ void __launch_bounds__(QM_SCAN_THREADS)
+    qm_batch_scan(const qm_bq *__restrict__ bq, const qm_chunk *__restrict__ chunks, int n_chunks, int *counter,
+                  int local_bytes) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ qm_scan_args P;
+  __shared__ int s_chunk;
+  __shared__ int l_used;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  const bsmem lay = batch_smem(local_bytes, warps);
+  uint32_t *queue = reinterpret_cast<uint32_t *>(smem + lay.queue_off) + warp * (QM_TILE_ROWS + 32);
+  uint64_t *scr = reinterpret_cast<uint64_t *>(smem + lay.scratch_off) + warp * 64;
+  uint64_t *lkeys = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *lw = lkeys;
+  int cur = -1;
+  unsigned long long selected = 0;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1);
+    __syncthreads();
+    const int c = s_chunk;
+    if (c >= n_chunks) break;
+    const qm_chunk ch = chunks[c];
+    if (ch.q != cur) {
+      if (cur >= 0) {
+        batch_flush(P, lkeys, lw);
+        if (lane == 0 && selected) atomicAdd(&P.status->rows_selected, selected);
+        selected = 0;
+      }
+      __syncthreads();
+      // load the next query's plan into shared memory
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(&bq[ch.q].a);
+      uint32_t *dst = reinterpret_cast<uint32_t *>(&P);
+      for (int i = threadIdx.x; i < (int)(sizeof(qm_scan_args) / 4); i += blockDim.x) dst[i] = __ldg(src + i);
+      if (threadIdx.x == 0) l_used = 0;
+      __syncthreads();
+      const int L = P.local_slots;
+      lw = lkeys + (P.local_hash ? L : 0);
+      if (L > 0) {
+        if (P.local_hash)
+          for (int s = threadIdx.x; s < L; s += blockDim.x) lkeys[s] = QM_EMPTY_KEY;
+        for (int i = threadIdx.x; i < L * P.agg.n_words; i += blockDim.x) lw[i] = P.agg.init[i / L];
+      }
+      __syncthreads();
+      cur = ch.q;
+    }
+    const int L = P.local_slots;
+    int qn = 0;
+    for (int64_t tile = ch.tile0 + warp; tile < ch.tile1; tile += warps) {
+      const int64_t e0 = tile * QM_TILE_ROWS;
+      uint32_t m;
+      const int64_t r0 = e0 + (int64_t)lane * QM_R;
+      if (P.vec_ok && e0 + QM_TILE_ROWS <= P.n) {
+        m = eval_pred_contig(P.pred, r0, (1u << QM_R) - 1);
+      } else {
+        int64_t rowv[QM_R];
+        m = 0;
+#pragma unroll
+        for (int j = 0; j < QM_R; ++j) {
+          m |= (uint32_t)(r0 + j < P.n) << j;
+          rowv[j] = r0 + j;
+        }
+        auto rowf = [&](int j) { return rowv[j]; };
+        m = eval_pred(P.pred, rowf, m);
+      }
+      const uint32_t cnt = __popc(m);
+      uint32_t off = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(QM_FULL, off, o);
+        if (lane >= o) off += x;
+      }
+      const uint32_t tot = __shfl_sync(QM_FULL, off, 31);
+      uint32_t qp = qn + off - cnt;
+      const uint32_t r0u = (uint32_t)r0;
+      for (uint32_t mm = m; mm; mm &= mm - 1) queue[qp++] = r0u + (uint32_t)(__ffs(mm) - 1);
+      qn += (int)tot;
+      selected += tot;
+      __syncwarp();
+      while (qn >= 32) {
+        const int64_t row = queue[qn - 32 + lane];
+        __syncwarp();
+        qn -= 32;
+        drain_round_any(P, lkeys, lw, L, &l_used, lane, true, row, scr);
+      }
+    }
+    if (qn > 0) {
+      const bool active = lane < qn;
+      const int64_t row = active ? (int64_t)queue[lane] : 0;
+      __syncwarp();
+      drain_round_any(P, lkeys, lw, L, &l_used, lane, active, row, scr);
+    }
+    __syncthreads();
+  }
+  if (cur >= 0) {
+    batch_flush(P, lkeys, lw);
+    if (lane == 0 && selected) atomicAdd(&P.status->rows_selected, selected);
+  }
+}
+
+// Set bit `first row` of each occupied group in its query's bitmap.
+__global__ void qm_batch_mark(const qm_bq *bq, const int64_t *slot0, int n, int64_t total, uint32_t *bitmap) {
+  for (int64_t gs = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gs < total; gs += (int64_t)gridDim.x * blockDim.x) {
+    const int q = find_query(slot0, n, gs);
+    const qm_bq &b = bq[q];
+    if (b.none) continue;
+    const uint64_t *slot = b.a.table + (gs - slot0[q]) * b.a.stride + 1;
+    if (slot[b.a.agg.w_count] == 0) continue;
+    const uint64_t first = slot[b.a.agg.w_first];
+    atomicOr(bitmap + b.bm_word0 + (int64_t)(first >> 5), 1u << (first & 31));
+  }
+}
+
+__global__ void qm_batch_popc(const uint32_t *bitmap, int64_t words, uint32_t *counts) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= words; i += (int64_t)gridDim.x * blockDim.x)
+    counts[i] = i < words ? __popc(bitmap[i]) : 0;
+}
+
+__host__ __device__ inline int64_t align16(int64_t x) { return (x + 15) & ~(int64_t)15; }
+
+// One block: each query's group count, its packed region and the offsets of
+// its output columns, NULL byte maps and NULL bitmaps.
+__global__ void qm_batch_layout(qm_bq *bq, int n, const uint64_t *ranks, qm_batch_meta *meta) {
+  if (threadIdx.x != 0) return;
+  int64_t base = 0, nbase = 0;
+  for (int q = 0; q < n; ++q) {
+    qm_bq &b = bq[q];
+    const int64_t G = b.none ? 1 : (int64_t)(ranks[b.bm_word0 + b.bm_words] - ranks[b.bm_word0]);
+    meta->groups[q] = G;
+    meta->base[q] = base;
+    int64_t off = base;
+    for (int k = 0; k < b.outs.n_out; ++k) {
+      b.outs.o[k].offset = off;
+      off += align16(G * b.width[k]);
+      if (b.nullable[k]) {
+        b.outs.o[k].null_offset = off;  // packed bits (QMCB order)
+        off += align16(((G + 31) / 32) * 4);
+        b.nullbyte_off[k] = nbase;
+        nbase += align16(G);
+      } else {
+        b.outs.o[k].null_offset = -1;
+        b.nullbyte_off[k] = -1;
+      }
+    }
+    meta->bytes[q] = off - base;
+    base = off;
+  }
+  meta->total = base;
+  meta->null_total = nbase;
+}
+
+// Write each occupied group of every query at its first-seen rank.
+__global__ void qm_batch_emit(const qm_bq *bq, const int64_t *slot0, int n, int64_t total, const uint32_t *bitmap,
+                              const uint64_t *ranks, unsigned char *packed, unsigned char *nullbytes) {
+  for (int64_t gs = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gs < total; gs += (int64_t)gridDim.x * blockDim.x) {
+    const int q = find_query(slot0, n, gs);
+    const qm_bq &b = bq[q];
+    const int64_t s = gs - slot0[q];
+    int64_t rank;
+    if (b.none) {
+      if (s != 0) continue;
+      rank = 0;
+    } else {
+      const uint64_t *slot = b.a.table + s * b.a.stride + 1;
+      if (slot[b.a.agg.w_count] == 0) continue;
+      const uint64_t first = slot[b.a.agg.w_first];
+      const int64_t w = b.bm_word0 + (int64_t)(first >> 5);
+      rank = (int64_t)(ranks[w] - ranks[b.bm_word0]) + __popc(bitmap[w] & ((1u << (first & 31)) - 1u));
+    }
+    emit_group_bytes(b.a.table, b.a.stride, (uint64_t)s, rank, b.a.key, b.a.n_slots, b.outs, packed, nullbytes,
+                     b.nullbyte_off);
+  }
+}
+
+// NULL byte maps -> QMCB bitmaps (one thread per 32 rows).
+__global__ void qm_batch_pack_nulls(const qm_bq *bq, int n, const qm_batch_meta *meta, unsigned char *packed,
+                                    const unsigned char *nullbytes) {
+  const int q = blockIdx.y;
+  if (q >= n) return;
+  const qm_bq &b = bq[q];
+  const int64_t G = meta->groups[q];
+  const int64_t words = (G + 31) / 32;
+  for (int k = 0; k < b.outs.n_out; ++k) {
+    if (!b.nullable[k]) continue;
+    const unsigned char *src = nullbytes + b.nullbyte_off[k];
+    uint32_t *dst = reinterpret_cast<uint32_t *>(packed + b.outs.o[k].null_offset);
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
+      uint32_t bits = 0;
+      for (int i = 0; i < 32; ++i) {
+        const int64_t r = w * 32 + i;
+        if (r < G && src[r]) bits |= 1u << i;
+      }
+      dst[w] = bits;
+    }
+  }
+}
+
+}  // namespace qm
+
+using namespace qm;
+
+size_t qm_batch_smem_bytes(int local_bytes) { return batch_smem(local_bytes, QM_SCAN_THREADS / 32).bytes; }
+
+cudaError_t qm_batch_configure(size_t smem, int *blocks_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(qm_batch_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_batch_scan, QM_SCAN_THREADS, smem);
+}
+
+static int grid_for(int64_t n, int sm_count, int per_sm) {
+  int64_t b = (n + 255) / 256;
+  b = std::min<int64_t>(b, (int64_t)sm_count * per_sm);
+  return (int)std::max<int64_t>(b, 1);
+}
+
+cudaError_t qm_batch_launch_all(const qm_batch_dev &d, cudaStream_t st) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(d.statuses, 0, sizeof(qm_status) * d.n, st))) return e;
+  if ((e = cudaMemsetAsync(d.counter, 0, sizeof(int), st))) return e;
+  if ((e = cudaMemsetAsync(d.bitmap, 0, sizeof(uint32_t) * (d.bm_words + 1), st))) return e;
+  qm_batch_init<<<grid_for(d.total_slots, d.sm_count, 16), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots);
+  qm_batch_scan<<<d.scan_blocks, QM_SCAN_THREADS, d.scan_smem, st>>>(d.bq, d.chunks, d.n_chunks, d.counter,
+                                                                     d.local_bytes);
+  qm_batch_mark<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap);
+  qm_batch_popc<<<grid_for(d.bm_words + 1, d.sm_count, 8), 256, 0, st>>>(d.bitmap, d.bm_words, d.popc);
+  size_t tb = d.scan_temp_bytes;
+  if ((e = cub::DeviceScan::ExclusiveSum(d.scan_temp, tb, d.popc, d.ranks, (int)(d.bm_words + 1), st))) return e;
+  qm_batch_layout<<<1, 32, 0, st>>>(d.bq, d.n, d.ranks, d.meta);
+  qm_batch_emit<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap,
+                                                                         d.ranks, d.packed, d.nullbytes);
+  dim3 pg(8, d.n);
+  qm_batch_pack_nulls<<<pg, 128, 0, st>>>(d.bq, d.n, d.meta, d.packed, d.nullbytes);
+  if ((e = cudaMemcpyAsync(d.meta_host, d.meta, d.meta_bytes, cudaMemcpyDeviceToHost, st))) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t qm_batch_scan_temp_bytes(int64_t words, size_t *bytes) {
+  return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
+                                       (int)(words + 1));
+}

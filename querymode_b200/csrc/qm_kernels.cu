@@ -41,70 +41,10 @@ __host__ __device__ inline smem_layout make_smem_layout(int local_slots, int loc
   return s;
 }
 
-// Aggregates one survivor per lane (lanes with active = false sit out).
 template <bool SEL>
 __device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
                                             int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
-  const qm_aggspec &A = a.agg;
-  if (a.dedupe) {
-    const unsigned act = __ballot_sync(QM_FULL, active);
-    if (!active) return;
-    const uint64_t grow = (uint64_t)(a.row_offset + row);
-    int special;
-    const uint64_t key = row_key(a.key, row, special);
-    uint64_t vb[QM_MAX_VCOLS];
-    uint32_t vnull;
-    gather_values(A, row, vb, vnull);
-    unsigned peers = __match_any_sync(act, key);
-    if (__any_sync(act, special != 0)) peers &= __match_any_sync(act, special);
-    const bool leader = lane == __ffs(peers) - 1;
-    uint64_t *tp = nullptr;
-    int ws = 1;
-    bool local = false;
-    if (leader) {
-      int ls = -1;
-      if (L > 0) {
-        if (!a.local_hash) ls = (int)global_slot(a, key, special);
-        else if (special == 0) ls = local_find(lkeys, L, key, l_used);
-      }
-      if (ls >= 0) {
-        tp = lw + ls;
-        ws = L;
-        local = true;
-      } else if (!(L > 0 && !a.local_hash)) {
-        const int64_t gs = global_slot(a, key, special);
-        if (gs >= 0) tp = a.table + gs * a.stride + 1;
-      }
-    }
-    apply_row(A, tp, ws, local, peers, lane, grow, vb, vnull);
-    return;
-  }
-  uint64_t grow = 0, key = 0;
-  int special = 0;
-  uint64_t vb[QM_MAX_VCOLS];
-  uint32_t vnull = 0;
-  int ls = -1;
-  if (active) {
-    grow = (uint64_t)(a.row_offset + row);
-    key = row_key(a.key, row, special);
-    gather_values(A, row, vb, vnull);
-    if (L > 0) {
-      if (!a.local_hash) ls = (int)global_slot(a, key, special);
-      else if (special == 0) ls = local_find(lkeys, L, key, l_used);
-    }
-  }
-  const bool loc = active && ls >= 0;
-  const unsigned lmask = __ballot_sync(QM_FULL, loc);
-  unsigned peers = 0;
-  if (loc) peers = __match_any_sync(lmask, ls);
-  const bool merge = __any_sync(QM_FULL, (peers & (peers - 1)) != 0);
-  if (loc) {
-    if (merge) agg_row_merged(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr);
-    else agg_row(A, lw + ls, L, true, grow, vb, vnull);
-  } else if (active && !(L > 0 && !a.local_hash)) {
-    const int64_t gs = global_slot(a, key, special);
-    if (gs >= 0) agg_row(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull);
-  }
+  drain_round_any(a, lkeys, lw, L, l_used, lane, active, row, scr);
 }
 
 // The fused scan.  Each warp takes tiles of QM_TILE_ROWS rows round robin,
@@ -345,133 +285,12 @@ __global__ void qm_rehash(const uint64_t *old_t, int64_t old_cap, int stride, in
   }
 }
 
-// Number(bigint): round to nearest, ties to even.
-__device__ __forceinline__ double i128_to_f64(uint64_t lo, int64_t hi) {
-  const bool neg = hi < 0;
-  if (neg) {  // negate the 128-bit value
-    lo = ~lo + 1;
-    hi = ~hi + (lo == 0 ? 1 : 0);
-  }
-  const uint64_t uhi = (uint64_t)hi;
-  double r;
-  if (uhi == 0) {
-    r = __ull2double_rn(lo);
-  } else {
-    const int shift = 64 - __clzll((long long)uhi);  // drop `shift` bits
-    const uint64_t top = (uhi << (64 - shift)) | (lo >> shift);
-    const bool sticky = (lo << (64 - shift)) != 0;
-    uint64_t keep = top >> 11;
-    const uint64_t rem = top & 0x7ff;
-    const bool guard = (rem >> 10) & 1;
-    const bool st = sticky || (rem & 0x3ff);
-    if (guard && (st || (keep & 1))) keep++;
-    r = ldexp((double)keep, shift + 11);
-  }
-  return neg ? -r : r;
-}
-
-__device__ __forceinline__ void set_null(unsigned char *out, int64_t null_offset, int64_t i) {
-  atomicOr(reinterpret_cast<unsigned *>(out + null_offset) + (i >> 5), 1u << (i & 31));
-}
-
 __global__ void qm_emit_groups(const uint64_t *t, int stride, const uint32_t *slots, int64_t G,
                                const __grid_constant__ qm_keyspec K, int64_t n_slots,
                                const __grid_constant__ qm_outspec O, unsigned char *out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t s = slots ? slots[i] : (uint64_t)i;
-    const uint64_t *w = t + s * stride + 1;
-    // reconstruct the key word
-    bool knull = false;
-    uint64_t key = 0;
-    if (K.mode == QK_DIRECT) {
-      if ((int64_t)s == n_slots) knull = true;
-      else key = (uint64_t)K.base + s;
-    } else if (K.mode == QK_HASH) {
-      if ((int64_t)s == n_slots) key = QM_EMPTY_KEY;
-      else if ((int64_t)s == n_slots + 1) knull = true;
-      else key = t[s * stride];
-    }
-    for (int k = 0; k < O.n_out; ++k) {
-      const qm_out &o = O.o[k];
-      unsigned char *col = out + o.offset;
-      if (o.kind == QO_KEY) {
-        if (knull) {
-          set_null(out, o.null_offset, i);
-          continue;
-        }
-        if (K.pack == QP_CONCAT) {
-          reinterpret_cast<int32_t *>(col)[i] = (int32_t)(o.src == 0 ? (key >> 32) : key);
-        } else if (K.pack == QP_DIGITS) {
-          const int c = o.src;
-          const uint64_t d = (key / K.kmul[c]) % K.kradix[c];
-          if (K.knullable[c] && d == 0) {
-            set_null(out, o.null_offset, i);
-            continue;
-          }
-          const int64_t v = K.kbase[c] + (int64_t)(d - (uint64_t)K.knullable[c]);
-          if (o.dtype == QM_I32) reinterpret_cast<int32_t *>(col)[i] = (int32_t)v;
-          else reinterpret_cast<int64_t *>(col)[i] = v;
-        } else if (o.dtype == QM_I32) {
-          reinterpret_cast<int32_t *>(col)[i] = (int32_t)(int64_t)key;
-        } else {
-          reinterpret_cast<uint64_t *>(col)[i] = key;
-        }
-        continue;
-      }
-      if (o.kind == QO_COUNT) {
-        reinterpret_cast<int64_t *>(col)[i] = (int64_t)w[o.word];
-        continue;
-      }
-      const uint64_t nn = w[o.nn_word];
-      if (nn == 0) {
-        set_null(out, o.null_offset, i);
-        continue;
-      }
-      switch (o.kind) {
-        case QO_SUM_F:
-        case QO_AVG_F: {
-          double s2 = __longlong_as_double((long long)w[o.word]) + __longlong_as_double((long long)w[o.word + 1]);
-          reinterpret_cast<double *>(col)[i] = o.kind == QO_SUM_F ? s2 : s2 / (double)nn;
-          break;
-        }
-        case QO_SUM_I2F:
-        case QO_AVG_I2F: {
-          double s2 = i128_to_f64(w[o.word], (int64_t)w[o.word + 1]);
-          reinterpret_cast<double *>(col)[i] = o.kind == QO_SUM_I2F ? s2 : s2 / (double)nn;
-          break;
-        }
-        case QO_SUM_I128:
-          reinterpret_cast<uint64_t *>(col)[2 * i] = w[o.word];
-          reinterpret_cast<uint64_t *>(col)[2 * i + 1] = w[o.word + 1];
-          break;
-        case QO_AVG_BIG: {
-          // bigAvg(bigSum, 0, count): Number(sum / n) + Number(sum % n) / n
-          const __int128 sum = (__int128)(((unsigned __int128)(uint64_t)w[o.word + 1] << 64) | w[o.word]);
-          const __int128 q = sum / (__int128)nn, r = sum % (__int128)nn;
-          const double qd = i128_to_f64((uint64_t)q, (int64_t)(q >> 64));
-          const double rd = i128_to_f64((uint64_t)r, (int64_t)(r >> 64));
-          reinterpret_cast<double *>(col)[i] = qd + (rd + 0.0) / (double)nn;
-          break;
-        }
-        case QO_MIN_I:
-        case QO_MAX_I:
-          if (o.dtype == QM_I32) reinterpret_cast<int32_t *>(col)[i] = (int32_t)(int64_t)w[o.word];
-          else reinterpret_cast<int64_t *>(col)[i] = (int64_t)w[o.word];
-          break;
-        case QO_MIN_F:
-        case QO_MAX_F: {
-          const int64_t ov = (int64_t)w[o.word];
-          double d = ord2f(ov);
-          // a zero result takes the sign of the first zero seen (strict
-          // '<' / '>' keep the first of -0 and 0, src/partial-agg.ts:80-81)
-          if (ov == 0 && o.zero_word >= 0 && w[o.zero_word] != ~0ULL && (w[o.zero_word] & 1)) d = -0.0;
-          reinterpret_cast<double *>(col)[i] = d;
-          break;
-        }
-      }
-    }
-  }
+       i += (int64_t)gridDim.x * blockDim.x)
+    emit_group<false>(t, stride, slots ? slots[i] : (uint64_t)i, i, K, n_slots, O, out, nullptr, nullptr);
 }
 
 // Filter-only pass 1: per warp tile, the 32-bit survivor masks and counts.

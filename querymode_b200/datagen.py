@@ -126,3 +126,44 @@ def generate_rows(n: int) -> dict[str, np.ndarray]:
 
 def column_bytes(columns: dict[str, np.ndarray], names) -> int:
     return int(sum(columns[c].nbytes for c in names))
+
+
+def batch_specs(n_queries: int = 256, seed: int = 3, rows_lo: float = 1e4, rows_hi: float = 5e7,
+                card_lo: float = 4, card_hi: float = 1e6) -> list[dict]:
+    """Shapes of the batched workload: per query, rows log-uniform in
+    [rows_lo, rows_hi], group cardinality log-uniform in [card_lo, card_hi],
+    int32 or int64 keys, a float64 lognormal measure and a filter threshold
+    giving 1-90% selectivity."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_queries):
+        rows = int(np.exp(rng.uniform(np.log(rows_lo), np.log(rows_hi))))
+        card = max(1, int(np.exp(rng.uniform(np.log(card_lo), np.log(card_hi)))))
+        specs.append({
+            "rows": rows, "card": card, "key64": bool(rng.random() < 0.5),
+            "selectivity": float(rng.uniform(0.01, 0.90)), "seed": int(rng.integers(1 << 31)),
+        })
+    return specs
+
+
+def batch_table(spec: dict) -> dict[str, np.ndarray]:
+    """One query's table: key (int32 codes 0..card-1, or int64 values drawn
+    from `card` random 64-bit values), f (int32 uniform 0..9999), v (float64
+    lognormal(0, 1))."""
+    rng = np.random.default_rng(spec["seed"])
+    n, card = spec["rows"], spec["card"]
+    idx = rng.integers(0, card, n)
+    if spec["key64"]:
+        universe = rng.integers(-(1 << 62), 1 << 62, card, dtype=np.int64)
+        key = universe[idx]
+    else:
+        key = idx.astype(np.int32)
+    return {"key": key, "f": rng.integers(0, 10_000, n, dtype=np.int32), "v": rng.lognormal(0.0, 1.0, n)}
+
+
+def batch_query(spec: dict) -> QueryDescriptor:
+    threshold = int(round(spec["selectivity"] * 10_000))
+    return QueryDescriptor(
+        table="batch", filters=[FilterOp("f", "lt", threshold)], group_by=["key"],
+        aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*"), AggregateOp("min", "v"),
+                    AggregateOp("max", "v"), AggregateOp("avg", "v")])

@@ -355,6 +355,9 @@ class Context:
     def aggregate(self, query: QueryDescriptor) -> "AggStream":
         return AggStream(self, query)
 
+    def batch(self, tables: list["Table"], queries: list[QueryDescriptor]) -> "Batch":
+        return Batch(self, tables, queries)
+
 
 class Table:
     """A qm_table: numeric columns resident in HBM."""
@@ -424,5 +427,82 @@ class AggStream:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """A qm_batch: many queries (query i over tables[i]) in one persistent
+    fused launch, CUDA-graph captured on the first run."""
+
+    def __init__(self, ctx: Context, tables: list[Table], queries: list[QueryDescriptor]):
+        if len(tables) != len(queries):
+            raise ValueError("one table per query")
+        self.ctx = ctx
+        self.tables = tables
+        self.cqs = [q if isinstance(q, CQuery) else CQuery(q) for q in queries]
+        n = len(queries)
+        th = (C.c_void_p * n)(*[t.h.value for t in tables])
+        qs = (C.POINTER(A.QmQuery) * n)(*[C.pointer(cq.struct) for cq in self.cqs])
+        h = C.c_void_p()
+        ctx.check(ctx.lib.qm_batch_create(ctx.h, n, th, qs, C.byref(h)))
+        self.h = h
+        self.n = n
+
+    def set_tuning(self, chunk_tiles: int = -1, local_kb: int = -1, blocks_per_sm: int = -1) -> None:
+        self.ctx.check(self.ctx.lib.qm_batch_set_tuning(self.h, chunk_tiles, local_kb, blocks_per_sm))
+
+    def run(self) -> "BatchResults":
+        out = (C.c_void_p * self.n)()
+        self.ctx.check(self.ctx.lib.qm_batch_run(self.h, out))
+        return BatchResults(self.ctx.lib, [out[i] for i in range(self.n)])
+
+    def stats(self) -> dict:
+        ms = C.c_double()
+        rows = C.c_int64()
+        nbytes = C.c_int64()
+        chunks = C.c_int32()
+        self.ctx.check(self.ctx.lib.qm_batch_stats(self.h, C.byref(ms), C.byref(rows), C.byref(nbytes),
+                                                   C.byref(chunks)))
+        return {"device_ms": ms.value, "rows": rows.value, "bytes": nbytes.value, "chunks": chunks.value}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.ctx.lib.qm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchResults:
+    """The n results of a batch run; each Result is wrapped on first access
+    (unaccessed handles are destroyed with this object)."""
+
+    def __init__(self, lib, handles: list[int]):
+        self.lib = lib
+        self.handles = handles
+        self.cache: dict[int, Result] = {}
+
+    def __len__(self) -> int:
+        return len(self.handles)
+
+    def __getitem__(self, i: int) -> Result:
+        if i not in self.cache:
+            self.cache[i] = Result.from_handle(self.lib, C.c_void_p(self.handles[i]), owned=True)
+        return self.cache[i]
+
+    def __iter__(self):
+        for i in range(len(self.handles)):
+            yield self[i]
+
+    def __del__(self):
+        try:
+            for i, h in enumerate(self.handles):
+                if i not in self.cache and h:
+                    self.lib.qm_result_destroy(C.c_void_p(h))
         except Exception:
             pass

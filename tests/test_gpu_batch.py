@@ -1,0 +1,66 @@
+"""Batched launch (qm_batch_*): every query's result equals the oracle's,
+on the first (graph-capturing) run, on a replay, and after retuning."""
+import numpy as np
+import pytest
+
+import oracle
+from querymode_b200 import datagen
+from querymode_b200.engine import Column
+from querymode_b200.query import AggregateOp, FilterOp, QueryDescriptor
+from tests.helpers import assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_batch(seed=5, n=40):
+    specs = datagen.batch_specs(n, seed=seed, rows_lo=1e3, rows_hi=3e5, card_lo=1, card_hi=5e4)
+    tables = [datagen.batch_table(s) for s in specs]
+    queries = [datagen.batch_query(s) for s in specs]
+    rng = np.random.default_rng(seed)
+    # other shapes: ungrouped, two packed keys, NULLs, int sums
+    m = 50_000
+    extra = {"a": Column(rng.integers(0, 7, m).astype(np.int32), rng.random(m) < 0.1),
+             "b": rng.integers(-3, 3, m).astype(np.int32), "x": Column(rng.normal(size=m), rng.random(m) < 0.2),
+             "i": rng.integers(-2**40, 2**40, m).astype(np.int64)}
+    tables += [extra, extra, extra]
+    queries += [QueryDescriptor(filters=[FilterOp("b", "gte", 0)],
+                                aggregates=[AggregateOp("sum", "x"), AggregateOp("count", "*"), AggregateOp("max", "i")]),
+                QueryDescriptor(group_by=["a", "b"], aggregates=[AggregateOp("sum", "i"), AggregateOp("avg", "x"),
+                                                                  AggregateOp("count", "x")]),
+                QueryDescriptor(filters=[FilterOp("x", "gt", 5.0)], group_by=["a"],
+                                aggregates=[AggregateOp("sum", "x"), AggregateOp("count", "*")])]
+    return tables, queries
+
+
+def test_batch_matches_oracle(ctx):
+    tables, queries = mixed_batch()
+    handles = [ctx.table(t) for t in tables]
+    refs = [oracle.run(t, q) for t, q in zip(tables, queries)]
+    b = ctx.batch(handles, queries)
+    try:
+        for run in range(2):  # capture, then replay
+            res = b.run()
+            for i, (g, r) in enumerate(zip(res, refs)):
+                assert_same(g, r, ctx_msg=f"run {run} query {i}")
+        b.set_tuning(chunk_tiles=64, local_kb=0, blocks_per_sm=1)
+        res = b.run()
+        for i, (g, r) in enumerate(zip(res, refs)):
+            assert_same(g, r, ctx_msg=f"retuned query {i}")
+        st = b.stats()
+        assert st["rows"] == sum(len(next(iter(t.values())).values if hasattr(next(iter(t.values())), "values")
+                                     else next(iter(t.values()))) for t in tables)
+    finally:
+        b.close()
+
+
+def test_batch_equals_single_queries(ctx):
+    specs = datagen.batch_specs(16, seed=9, rows_lo=1e4, rows_hi=2e6, card_lo=4, card_hi=2e5)
+    tables = [ctx.table(datagen.batch_table(s)) for s in specs]
+    queries = [datagen.batch_query(s) for s in specs]
+    singles = [t.run(q) for t, q in zip(tables, queries)]
+    b = ctx.batch(tables, queries)
+    try:
+        for g, r in zip(b.run(), singles):
+            assert_same(g, r)
+    finally:
+        b.close()
