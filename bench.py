@@ -71,13 +71,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per scan launch from the committed ncu summary, if any."""
+def profiled_traffic(rows: int):
+    """DRAM bytes per scan launch over `rows` rows, from the per-row traffic
+    in the committed ncu summary (traffic grows in proportion to rows)."""
     path = os.path.join(ROOT, "profiles", "qm_scan_kernel_events_100m.md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
+    m = re.search(r"traffic_bytes_per_row:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) * rows if m else None
 
 
 class ClockSampler:
@@ -367,7 +368,7 @@ def main():
     peak, peak_kind = load_peaks()
     scan_avg = float(np.mean(scan_ms))
     achieved = bytes_per_query / (scan_avg / 1e3) / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(n)
 
     # end to end through the C ABI with host inputs in pinned memory
     e2e = None
@@ -411,7 +412,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "i64/f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "rows_per_gpu": n, "bytes_per_row": BYTES_PER_ROW,
                        "groups": int(res.n_rows), "rows_selected": int(res.stats.rows_selected),
-                       "l2": "inputs 2.8 GB per GPU > 126 MB L2 (no flush needed)",
+                       "l2": f"inputs {n * BYTES_PER_ROW / 1e9:.2f} GB per GPU > 126 MB L2 (no flush needed)",
                        "parallelism": f"dp{world} (independent shards)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
