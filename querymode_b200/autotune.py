@@ -17,7 +17,7 @@ import time
 DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 DEFAULT_GRID = {
     "chunk_tiles": [128, 512, 2048],
-    "local_kb": [0, 24, 40],
+    "local_kb": [0, 24, 40, 96, 160],
     "blocks_per_sm": [0, 1],
 }
 

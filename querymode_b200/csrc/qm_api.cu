@@ -803,7 +803,11 @@ int ilog2_ceil(int64_t x) {
   return l;
 }
 
-constexpr size_t LOCAL_BUDGET = 40 * 1024;  // bytes of the block-local table
+constexpr size_t LOCAL_BUDGET = 40 * 1024;  // bytes of the block-local hash table
+// A dense (direct) key range whose table fits this many bytes is aggregated
+// entirely in shared memory, even at one block per SM: every row then stays
+// on the shared-memory path instead of the L2 atomics of the global table.
+constexpr size_t DIRECT_LOCAL_BUDGET = 180 * 1024;
 
 void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning &tu) {
   const int words = pl.agg.n_words;
@@ -817,7 +821,7 @@ void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning
     ex.strategy = 0;
     return;
   }
-  if (pl.key.mode == QK_DIRECT && tu.local_slots >= 0 && (ex.n_slots + 1) * per_slot <= (int64_t)LOCAL_BUDGET) {
+  if (pl.key.mode == QK_DIRECT && tu.local_slots >= 0 && (ex.n_slots + 1) * per_slot <= (int64_t)DIRECT_LOCAL_BUDGET) {
     ex.local_slots = (int)(ex.n_slots + 1);
     ex.local_hash = 0;
     ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : (ex.n_slots <= 256 ? 1 : 0);

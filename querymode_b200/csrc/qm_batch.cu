@@ -122,6 +122,8 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
       uint32_t m;
       const int64_t r0 = e0 + (int64_t)lane * QM_R;
       if (P.vec_ok && e0 + QM_TILE_ROWS <= P.n) {
+        const int64_t nxt = tile + warps;
+        if (nxt < ch.tile1 && (nxt + 1) * QM_TILE_ROWS <= P.n) prefetch_tile_l2(P.pred, nxt * QM_TILE_ROWS, lane);
         m = eval_pred_contig(P.pred, r0, (1u << QM_R) - 1);
       } else {
         int64_t rowv[QM_R];

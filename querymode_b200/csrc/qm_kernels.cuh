@@ -592,6 +592,31 @@ __device__ __forceinline__ void min_i64(uint64_t *p, int64_t v) {
 __device__ __forceinline__ void max_i64(uint64_t *p, int64_t v) {
   if (v > (int64_t)*reinterpret_cast<volatile uint64_t *>(p)) atomicMax(reinterpret_cast<long long *>(p), (long long)v);
 }
+// In the global table the read test costs an L2 round trip that the warp
+// waits for; there the atomics go out unconditionally (no returned value, so
+// they are fire-and-forget reductions).
+__device__ __forceinline__ void upd_min_u64(uint64_t *p, uint64_t v, bool local) {
+  if (local) min_u64(p, v);
+  else atomicMin(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
+}
+__device__ __forceinline__ void upd_min_i64(uint64_t *p, int64_t v, bool local) {
+  if (local) min_i64(p, v);
+  else atomicMin(reinterpret_cast<long long *>(p), (long long)v);
+}
+__device__ __forceinline__ void upd_max_i64(uint64_t *p, int64_t v, bool local) {
+  if (local) max_i64(p, v);
+  else atomicMax(reinterpret_cast<long long *>(p), (long long)v);
+}
+
+// Butterfly reductions over all 32 lanes (every lane gets the result): the
+// peer loops below are O(peers), this is O(log 32) for the common case of a
+// whole warp in one group (no GROUP BY, or a dominant key).
+template <class T, class OP>
+__device__ __forceinline__ T warp_allreduce(T v, OP op) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = op(v, __shfl_xor_sync(QM_FULL, v, o));
+  return v;
+}
 
 // Apply one compacted row (merged with its equal-key peers) to a slot whose
 // accumulator word w lives at tp[w * ws].  Every peer executes this (the
@@ -600,6 +625,7 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
                                           unsigned peers, int lane, uint64_t grow,
                                           const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
   const bool solo = (peers & (peers - 1)) == 0;
+  const bool full = peers == QM_FULL;
   for (int i = 0; i < A.n_accs; ++i) {
     const qm_acc ac = A.acc[i];
     uint64_t *w0 = tp ? tp + (int64_t)ac.word * ws : nullptr;
@@ -610,12 +636,14 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
     }
     if (ac.kind == QA_FIRST) {
       uint64_t first = grow;
-      if (!solo)
+      if (full)
+        first = warp_allreduce(first, [](uint64_t x, uint64_t y) { return min(x, y); });
+      else if (!solo)
         for (unsigned m = peers; m; m &= m - 1) {
           const uint64_t x = __shfl_sync(peers, grow, __ffs(m) - 1);
           first = min(first, x);
         }
-      if (tp) min_u64(w0, first);
+      if (tp) upd_min_u64(w0, first, local);
       continue;
     }
     const bool valid = !((vnull >> ac.vcol) & 1);
@@ -630,7 +658,9 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
         int64_t v = valid ? (int64_t)raw : 0;
         if (!ac.wide) {
           int64_t s = v;
-          if (!solo)
+          if (full)
+            s = warp_allreduce(s, [](int64_t x, int64_t y) { return x + y; });
+          else if (!solo)
             for (unsigned m = peers; m; m &= m - 1) {
               int src = __ffs(m) - 1;
               int64_t x = __shfl_sync(peers, v, src);
@@ -644,7 +674,16 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
           // 128-bit sum of up to 32 int64 cells
           uint64_t lo = (uint64_t)v;
           int64_t hi = v < 0 ? -1 : 0;
-          if (!solo)
+          if (full) {
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+              const uint64_t xl = __shfl_xor_sync(QM_FULL, lo, o);
+              const int64_t xh = __shfl_xor_sync(QM_FULL, hi, o);
+              const uint64_t nlo = lo + xl;
+              hi += xh + (nlo < lo ? 1 : 0);
+              lo = nlo;
+            }
+          } else if (!solo)
             for (unsigned m = peers; m; m &= m - 1) {
               int src = __ffs(m) - 1;
               int64_t x = __shfl_sync(peers, v, src);
@@ -665,7 +704,10 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
           double vh, vl;
           split_parts(v, split, vh, vl);
           double h = vh, l = vl;
-          if (!solo)
+          if (full) {
+            h = warp_allreduce(h, [](double x, double y) { return x + y; });  // exact (grid multiples)
+            l = warp_allreduce(l, [](double x, double y) { return x + y; });
+          } else if (!solo)
             for (unsigned m = peers; m; m &= m - 1) {
               int src = __ffs(m) - 1;
               double xh = __shfl_sync(peers, vh, src), xl = __shfl_sync(peers, vl, src);
@@ -681,7 +723,16 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
           break;
         }
         double s = v, c = 0.0;
-        if (!solo)
+        if (full) {
+#pragma unroll
+          for (int o = 16; o; o >>= 1) {
+            const double xs = __shfl_xor_sync(QM_FULL, s, o);
+            const double xc = __shfl_xor_sync(QM_FULL, c, o);
+            double cc = c + xc;
+            two_sum_acc(s, cc, xs);
+            c = cc;
+          }
+        } else if (!solo)
           for (unsigned m = peers; m; m &= m - 1) {
             int src = __ffs(m) - 1;
             double x = __shfl_sync(peers, v, src);
@@ -694,7 +745,10 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
       case QA_IMAX: {
         const bool mx = ac.kind == QA_IMAX;
         int64_t v = valid ? (int64_t)raw : (mx ? INT64_MIN : INT64_MAX);
-        if (!solo)
+        if (full)
+          v = mx ? warp_allreduce(v, [](int64_t x, int64_t y) { return max(x, y); })
+                 : warp_allreduce(v, [](int64_t x, int64_t y) { return min(x, y); });
+        else if (!solo)
           for (unsigned m = peers; m; m &= m - 1) {
             int src = __ffs(m) - 1;
             int64_t x = __shfl_sync(peers, v, src);
@@ -712,7 +766,10 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
         double d = __longlong_as_double((long long)raw);
         bool ok = valid && !isnan(d); // NaN never wins '<' / '>' (src/partial-agg.ts:80-81)
         int64_t o = ok ? f2ord(d == 0.0 ? 0.0 : d) : (mx ? INT64_MIN : INT64_MAX);
-        if (!solo)
+        if (full)
+          o = mx ? warp_allreduce(o, [](int64_t x, int64_t y) { return max(x, y); })
+                 : warp_allreduce(o, [](int64_t x, int64_t y) { return min(x, y); });
+        else if (!solo)
           for (unsigned m = peers; m; m &= m - 1) {
             int src = __ffs(m) - 1;
             int64_t x = __shfl_sync(peers, o, src);
@@ -728,7 +785,9 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
         double d = __longlong_as_double((long long)raw);
         bool z = valid && d == 0.0;
         uint64_t code = z ? ((grow << 1) | (raw >> 63)) : ~0ULL;
-        if (!solo) {
+        if (full) {
+          if (__any_sync(QM_FULL, z)) code = warp_allreduce(code, [](uint64_t x, uint64_t y) { return min(x, y); });
+        } else if (!solo) {
           if (__any_sync(peers, z))
             for (unsigned m = peers; m; m &= m - 1) {
               int src = __ffs(m) - 1;
@@ -749,7 +808,7 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
 __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
                                         uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
   atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)A.w_count * ws), 1ULL);
-  if (A.w_first >= 0) min_u64(tp + (int64_t)A.w_first * ws, grow);
+  if (A.w_first >= 0) upd_min_u64(tp + (int64_t)A.w_first * ws, grow, local);
 #pragma unroll
   for (int c = 0; c < QM_MAX_VCOLS; ++c) {
     if (c >= A.n_vcols) break;
@@ -764,8 +823,8 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
         if (local && !(f & VF_WIDE)) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)v);
         else add128(w0, w0 + ws, (uint64_t)v, v < 0 ? -1 : 0);
       }
-      if (f & VF_MIN) min_i64(tp + (int64_t)vc.w_min * ws, v);
-      if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * ws, v);
+      if (f & VF_MIN) upd_min_i64(tp + (int64_t)vc.w_min * ws, v, local);
+      if (f & VF_MAX) upd_max_i64(tp + (int64_t)vc.w_max * ws, v, local);
     } else {
       const double d = __longlong_as_double((long long)vb[c]);
       if (f & VF_SUM) {
@@ -775,10 +834,10 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
       }
       if ((f & (VF_MIN | VF_MAX)) && !isnan(d)) {  // NaN never wins '<' / '>'
         const int64_t o = f2ord(d == 0.0 ? 0.0 : d);
-        if (f & VF_MIN) min_i64(tp + (int64_t)vc.w_min * ws, o);
-        if (f & VF_MAX) max_i64(tp + (int64_t)vc.w_max * ws, o);
+        if (f & VF_MIN) upd_min_i64(tp + (int64_t)vc.w_min * ws, o, local);
+        if (f & VF_MAX) upd_max_i64(tp + (int64_t)vc.w_max * ws, o, local);
       }
-      if ((f & VF_ZERO) && d == 0.0) min_u64(tp + (int64_t)vc.w_zero * ws, (grow << 1) | (vb[c] >> 63));
+      if ((f & VF_ZERO) && d == 0.0) upd_min_u64(tp + (int64_t)vc.w_zero * ws, (grow << 1) | (vb[c] >> 63), local);
     }
   }
 }
