@@ -644,6 +644,8 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
     a.vcol = vcol;
     a.word = A.n_words;
     a.wide = wide;
+    a.narrow = 0;
+    a.pad = 0;
     uint64_t init = 0;
     switch (kind) {
       case QA_FIRST: case QA_FZERO: init = ~0ULL; break;
@@ -793,6 +795,7 @@ struct Exec {
   int local_hash = 0;
   int dedupe = 1;
   int strategy = 0;
+  int priv = 0;  // direct block-local table copied per warp (no atomics)
 };
 
 int64_t special_slots(int mode) { return mode == QK_HASH ? 2 : (mode == QK_DIRECT ? 1 : 0); }
@@ -808,16 +811,21 @@ constexpr size_t LOCAL_BUDGET = 40 * 1024;  // bytes of the block-local hash tab
 // entirely in shared memory, even at one block per SM: every row then stays
 // on the shared-memory path instead of the L2 atomics of the global table.
 constexpr size_t DIRECT_LOCAL_BUDGET = 180 * 1024;
+// Bytes of all per-warp copies of a small direct table.
+constexpr size_t PRIV_BUDGET = 64 * 1024;
+constexpr int64_t PRIV_MIN_ROWS = (int64_t)8 << 20;
 
 void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning &tu) {
   const int words = pl.agg.n_words;
   ex.stride = 1 + words;
   ex.total_slots = ex.n_slots + special_slots(pl.key.mode);
   const int64_t per_slot = (int64_t)words * 8;
+  ex.priv = 0;
   if (pl.key.mode == QK_NONE) {
     ex.local_slots = 1;
     ex.local_hash = 0;
     ex.dedupe = 1;
+    ex.priv = 1;
     ex.strategy = 0;
     return;
   }
@@ -825,6 +833,10 @@ void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning
     ex.local_slots = (int)(ex.n_slots + 1);
     ex.local_hash = 0;
     ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : (ex.n_slots <= 256 ? 1 : 0);
+    // few groups: every warp of a block hits the same words, so the table is
+    // copied per warp and updated without atomics (deduplicated rows have
+    // distinct slots within a warp)
+    ex.priv = ex.dedupe && (ex.n_slots + 1) * per_slot * (QM_SCAN_THREADS / 32) <= (int64_t)PRIV_BUDGET;
     ex.strategy = 0;
     return;
   }
@@ -1115,6 +1127,7 @@ void fill_args(const GroupTable &gt, qm_scan_args &a, qm_status *st) {
   a.local_slots = gt.ex.local_slots;
   a.local_hash = gt.ex.local_hash;
   a.dedupe = gt.ex.dedupe;
+  a.priv = gt.ex.priv;
   a.max_probe = 1 << 12;
   a.status = st;
   a.vec_ok = 1;
@@ -1259,11 +1272,15 @@ int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel) {
   int depth = ctx->tuning.stage_depth <= 0 ? 0 : ctx->tuning.stage_depth;
   if (depth > QM_STAGE_MAX_DEPTH) depth = QM_STAGE_MAX_DEPTH;
   bool staged = false;
-  size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, 0, 0);
+  // per-warp copies pay for their set-up and fold only when every warp has
+  // many tiles to aggregate
+  if (a.priv && n < PRIV_MIN_ROWS) a.priv = 0;
+  size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, 0, 0, a.priv);
   if (!sel && depth >= 2 && n >= (int64_t)QM_TILE_ROWS * 256) {
     for (; depth >= 2 && !staged; depth--) {
       if (!setup_staging(a.pred, a.stage, depth)) break;
-      size_t sm = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, a.stage.tile_bytes, depth);
+      size_t sm = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, a.stage.tile_bytes, depth,
+                                     a.priv);
       if (sm <= SMEM_LIMIT) {
         smem = sm;
         staged = true;
@@ -1304,6 +1321,25 @@ int plan_query(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl) {
 
 namespace {
 
+// Integer sums of int32 cells over a table of fewer than 2^32 rows stay
+// within a signed 64-bit word (|sum| < 2^32 * 2^31), so the global table
+// takes them with plain 64-bit atomic adds, which need no returned value.
+void plan_narrow_sums(Plan &pl, int64_t n_rows) {
+  if (n_rows >= ((int64_t)1 << 32)) return;
+  qm_aggspec &A = pl.agg;
+  for (int i = 0; i < A.n_accs; i++) {
+    qm_acc &ac = A.acc[i];
+    if (ac.kind != QA_ISUM || ac.wide) continue;
+    ac.narrow = 1;
+    for (int c = 0; c < A.n_vcols; c++)
+      if ((A.vcol[c].flags & VF_SUM) && A.vcol[c].w_sum == ac.word) A.vcol[c].flags |= VF_NARROW;
+    for (int k = 0; k < pl.outs.n_out; k++) {
+      qm_out &o = pl.outs.o[k];
+      if ((o.kind == QO_SUM_I2F || o.kind == QO_AVG_I2F) && o.word == ac.word) o.narrow = 1;
+    }
+  }
+}
+
 // Plan `q` over registered table `t`: lower it, pack its keys, pick the
 // key mode (direct when the key range from column statistics is dense, else
 // hash) and estimate the group count (HyperLogLog, cached per column).
@@ -1319,6 +1355,7 @@ int plan_table_query(qm_ctx *ctx, qm_table *t, const qm_query *q, GroupTable &gt
   uint64_t space = 0;
   if ((rc = plan_key_packing(ctx, pl, t->n_rows, true, &space))) return rc;
   if ((rc = plan_split_sums(ctx, pl, t->n_rows))) return rc;
+  plan_narrow_sums(pl, t->n_rows);
   if (pl.key.n_cols == 0) {
     pl.key.mode = QK_NONE;
   } else {
@@ -2221,7 +2258,7 @@ extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
     a.n = n_rows;
     a.sel = nullptr;
     a.row_offset = 0;
-    const size_t smem = qm_scan_smem_bytes(ex.local_slots, ex.local_hash, pl.agg.n_words, 0, 0);
+    const size_t smem = qm_scan_smem_bytes(ex.local_slots, ex.local_hash, pl.agg.n_words, 0, 0, ex.priv);
     const int blocks = scan_blocks(ctx, smem, n_rows, false);
     CK(qm_launch_scan(a, blocks, smem, ctx->stream));
   }
@@ -2379,6 +2416,7 @@ int batch_layout(qm_batch *b) {
     gt.table = (uint64_t *)b->arena.p + table_off[i];
     qm_bq &q = b->bq[i];
     fill_args(gt, q.a, (qm_status *)b->d_status.p + i);
+    q.a.priv = 0;  // the batched kernel keeps one block-local copy
     q.a.n = b->rows[i];
     q.a.sel = nullptr;
     q.a.row_offset = 0;

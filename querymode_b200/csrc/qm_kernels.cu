@@ -26,13 +26,13 @@ struct smem_layout {
 // Per warp staging region: QM_STAGE_MAX_DEPTH mbarriers (32 bytes), then
 // `depth` tile buffers of tile_bytes each.
 __host__ __device__ inline smem_layout make_smem_layout(int local_slots, int local_hash, int n_words, int warps,
-                                                        int stage_tile_bytes = 0, int stage_depth = 0) {
+                                                        int stage_tile_bytes = 0, int stage_depth = 0, int priv = 0) {
   smem_layout s;
   s.L = local_slots;
   s.keys_off = 0;
   size_t kb = (local_slots > 0 && local_hash) ? (size_t)local_slots * 8 : 0;
   s.words_off = kb;
-  size_t wb = (size_t)local_slots * n_words * 8;
+  size_t wb = (size_t)local_slots * n_words * 8 * (priv ? warps : 1);  // priv: one copy per warp
   s.queue_off = (s.words_off + wb + 15) & ~(size_t)15;
   s.scratch_off = (s.queue_off + (size_t)warps * QM_WQ * sizeof(uint32_t) + 15) & ~(size_t)15;
   s.stage_off = (s.scratch_off + (size_t)warps * 64 * sizeof(uint64_t) + 127) & ~(size_t)127;
@@ -41,10 +41,10 @@ __host__ __device__ inline smem_layout make_smem_layout(int local_slots, int loc
   return s;
 }
 
-template <bool SEL>
+template <bool SEL, int DD>
 __device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
                                             int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
-  drain_round_any(a, lkeys, lw, L, l_used, lane, active, row, scr);
+  drain_round_any<DD>(a, lkeys, lw, L, l_used, lane, active, row, scr);
 }
 
 // The fused scan.  Each warp takes tiles of QM_TILE_ROWS rows round robin,
@@ -55,7 +55,7 @@ __device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lke
 // columns of the warp's next tiles stream into its shared-memory buffers by
 // bulk async copies (lane 0 issues, an mbarrier per buffer counts the bytes)
 // while the current tile is evaluated.
-template <bool SEL, bool STAGED>
+template <bool SEL, bool STAGED, int DD>
 __global__ void __launch_bounds__(QM_SCAN_THREADS)
     qm_scan_kernel(const __grid_constant__ qm_scan_args a) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -65,10 +65,13 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
   const qm_aggspec &A = a.agg;
   const qm_staging &S = a.stage;
   const smem_layout lay =
-      make_smem_layout(a.local_slots, a.local_hash, A.n_words, warps, STAGED ? S.tile_bytes : 0, STAGED ? S.depth : 0);
+      make_smem_layout(a.local_slots, a.local_hash, A.n_words, warps, STAGED ? S.tile_bytes : 0, STAGED ? S.depth : 0,
+                       a.priv);
   const int L = lay.L;
   uint64_t *lkeys = reinterpret_cast<uint64_t *>(smem + lay.keys_off);
   uint64_t *lw = reinterpret_cast<uint64_t *>(smem + lay.words_off);
+  // a private (per-warp) table: this warp's copy
+  uint64_t *lwm = a.priv ? lw + (int64_t)warp * L * A.n_words : lw;
   uint32_t *queue = reinterpret_cast<uint32_t *>(smem + lay.queue_off) + warp * QM_WQ;
   uint64_t *scr = reinterpret_cast<uint64_t *>(smem + lay.scratch_off) + warp * 64;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + lay.stage_off + warp * lay.stage_warp_bytes);
@@ -83,7 +86,8 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
   if (L > 0) {
     if (a.local_hash)
       for (int s = threadIdx.x; s < L; s += blockDim.x) lkeys[s] = QM_EMPTY_KEY;
-    for (int i = threadIdx.x; i < L * A.n_words; i += blockDim.x) lw[i] = A.init[i / L];
+    const int per = L * A.n_words;
+    for (int i = threadIdx.x; i < per * (a.priv ? warps : 1); i += blockDim.x) lw[i] = A.init[(i % per) / L];
   }
   if (STAGED && lane == 0) {
     for (int d = 0; d < S.depth; ++d) mbar_init(&mbar[d], 1);
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
       const int64_t row = queue[qn - 32 + lane];
       __syncwarp();
       qn -= 32;
-      drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, true, row, scr);
+      drain_round<SEL, DD>(a, lkeys, lwm, L, &l_used, lane, true, row, scr);
     }
   }
   if (STAGED && failed) {
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
     const bool active = lane < qn;
     const int64_t row = active ? (int64_t)queue[lane] : 0;
     __syncwarp();
-    drain_round<SEL>(a, lkeys, lw, L, &l_used, lane, active, row, scr);
+    drain_round<SEL, DD>(a, lkeys, lwm, L, &l_used, lane, active, row, scr);
   }
 
   if (lane == 0 && selected) atomicAdd(&blk_selected, selected);
@@ -224,13 +228,22 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
   // merge the block-local table into the global table
   if (L > 0) {
     const int cw = A.w_count;
+    if (a.priv) {  // fold the per-warp copies into copy 0
+      for (int s = threadIdx.x; s < L; s += blockDim.x)
+        for (int w = 1; w < warps; ++w) {
+          const uint64_t *src = lw + (int64_t)w * L * A.n_words + s;
+          if (src[(int64_t)cw * L] != 0) merge_plain(A, lw + s, src, L);
+        }
+      __syncthreads();
+    }
     for (int s = threadIdx.x; s < L; s += blockDim.x) {
-      if (lw[(int64_t)cw * L + s] == 0) continue;
+      const uint64_t *lp = lw + s;
+      if (lp[(int64_t)cw * L] == 0) continue;
       int64_t gs;
       if (a.local_hash) gs = global_slot(a, lkeys[s], 0);
       else gs = s;
       if (gs < 0) continue;
-      merge_local(A, lw + s, L, a.table + gs * a.stride + 1);
+      merge_local(A, lp, L, a.table + gs * a.stride + 1);
     }
   }
 }
@@ -426,31 +439,47 @@ __global__ void qm_minmax_init(long long *out) {
 // ---------------------------------------------------------------- launchers
 using namespace qm;
 
-size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth) {
-  return make_smem_layout(local_slots, local_hash, n_words, QM_SCAN_THREADS / 32, stage_tile_bytes, stage_depth).bytes;
+size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth,
+                          int priv) {
+  return make_smem_layout(local_slots, local_hash, n_words, QM_SCAN_THREADS / 32, stage_tile_bytes, stage_depth, priv)
+      .bytes;
 }
 
 cudaError_t qm_scan_configure(size_t smem_bytes, bool staged, int *blocks_per_sm) {
   cudaError_t e;
+#define QM_SMEM_ATTR(K)                                                                          \
+  do {                                                                                           \
+    e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes); \
+    if (e != cudaSuccess) return e;                                                              \
+  } while (0)
   if (staged) {
-    e = cudaFuncSetAttribute(qm_scan_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false, true>, QM_SCAN_THREADS,
-                                                         smem_bytes);
+    QM_SMEM_ATTR((qm_scan_kernel<false, true, 0>));
+    QM_SMEM_ATTR((qm_scan_kernel<false, true, 1>));
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false, true, 0>,
+                                                         QM_SCAN_THREADS, smem_bytes);
   }
-  e = cudaFuncSetAttribute(qm_scan_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(qm_scan_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-  if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false, false>, QM_SCAN_THREADS,
-                                                       smem_bytes);
+  QM_SMEM_ATTR((qm_scan_kernel<false, false, 0>));
+  QM_SMEM_ATTR((qm_scan_kernel<false, false, 1>));
+  QM_SMEM_ATTR((qm_scan_kernel<true, false, 0>));
+  QM_SMEM_ATTR((qm_scan_kernel<true, false, 1>));
+#undef QM_SMEM_ATTR
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_scan_kernel<false, false, 0>,
+                                                       QM_SCAN_THREADS, smem_bytes);
 }
 
 cudaError_t qm_launch_scan(const qm_scan_args &a, int blocks, size_t smem_bytes, cudaStream_t st) {
   if (a.n <= 0) return cudaSuccess;
-  if (a.sel) qm_scan_kernel<true, false><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
-  else if (a.stage.n > 0) qm_scan_kernel<false, true><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
-  else qm_scan_kernel<false, false><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  const bool dd = a.dedupe != 0;
+  if (a.sel) {
+    if (dd) qm_scan_kernel<true, false, 1><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+    else qm_scan_kernel<true, false, 0><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  } else if (a.stage.n > 0) {
+    if (dd) qm_scan_kernel<false, true, 1><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+    else qm_scan_kernel<false, true, 0><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  } else {
+    if (dd) qm_scan_kernel<false, false, 1><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+    else qm_scan_kernel<false, false, 0><<<blocks, QM_SCAN_THREADS, smem_bytes, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -608,6 +608,52 @@ __device__ __forceinline__ void upd_max_i64(uint64_t *p, int64_t v, bool local) 
   else atomicMax(reinterpret_cast<long long *>(p), (long long)v);
 }
 
+// Accumulator word updates, atomic or (plain = the slot is private to the
+// calling lane's warp and only one lane writes it) a plain read-modify-write.
+__device__ __forceinline__ void acc_add_u64(uint64_t *p, uint64_t v, bool plain) {
+  if (plain) *p += v;
+  else atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
+}
+__device__ __forceinline__ void acc_add_f64(uint64_t *p, double v, bool plain) {
+  if (plain) *reinterpret_cast<double *>(p) += v;
+  else atomicAdd(reinterpret_cast<double *>(p), v);
+}
+__device__ __forceinline__ void acc_min_u64(uint64_t *p, uint64_t v, bool plain, bool local) {
+  if (plain) *p = min(*p, v);
+  else upd_min_u64(p, v, local);
+}
+__device__ __forceinline__ void acc_min_i64(uint64_t *p, int64_t v, bool plain) {
+  if (plain) *p = (uint64_t)min((int64_t)*p, v);
+  else atomicMin(reinterpret_cast<long long *>(p), (long long)v);
+}
+__device__ __forceinline__ void acc_max_i64(uint64_t *p, int64_t v, bool plain) {
+  if (plain) *p = (uint64_t)max((int64_t)*p, v);
+  else atomicMax(reinterpret_cast<long long *>(p), (long long)v);
+}
+__device__ __forceinline__ void acc_add128(uint64_t *lo, uint64_t *hi, uint64_t vlo, int64_t vhi, bool plain) {
+  if (!plain) {
+    add128(lo, hi, vlo, vhi);
+    return;
+  }
+  const uint64_t o = *lo, n = o + vlo;
+  *lo = n;
+  *hi = (uint64_t)((int64_t)*hi + vhi + (n < o ? 1 : 0));
+}
+__device__ __forceinline__ void acc_fsum(uint64_t *hp, uint64_t *lp, double x, double xc, bool plain) {
+  if (!plain) {
+    fsum_add(hp, lp, x, xc);
+    return;
+  }
+  if (x == 0.0 && xc == 0.0) return;
+  const double old = __longlong_as_double((long long)*hp);
+  const double s = old + x;
+  *hp = (uint64_t)__double_as_longlong(s);
+  if (!isfinite(s)) return;
+  const double bb = s - old;
+  const double add = xc + ((old - (s - bb)) + (x - bb));
+  if (add != 0.0) *reinterpret_cast<double *>(lp) += add;
+}
+
 // Butterfly reductions over all 32 lanes (every lane gets the result): the
 // peer loops below are O(peers), this is O(log 32) for the common case of a
 // whole warp in one group (no GROUP BY, or a dominant key).
@@ -618,56 +664,67 @@ __device__ __forceinline__ T warp_allreduce(T v, OP op) {
   return v;
 }
 
+// Reduction of `v` over the calling lane's peer group, for every lane of
+// `act` (the lanes executing this; peers is a subset of act).  One loop of
+// `iters` steps (the largest group's size - 1) runs in lockstep for all
+// groups, so groups do not serialise on divergent loops; a whole-warp group
+// takes the butterfly.
+template <class T, class OP>
+__device__ __forceinline__ T group_reduce(T v, unsigned act, unsigned peers, int lane, int iters, OP op) {
+  if (peers == QM_FULL) return warp_allreduce(v, op);
+  T r = v;
+  unsigned rem = peers & ~(1u << lane);
+  for (int it = 0; it < iters; ++it) {
+    const int src = rem ? __ffs(rem) - 1 : lane;
+    const T x = __shfl_sync(act, v, src);
+    if (rem) {
+      r = op(r, x);
+      rem &= rem - 1;
+    }
+  }
+  return r;
+}
+
 // Apply one compacted row (merged with its equal-key peers) to a slot whose
-// accumulator word w lives at tp[w * ws].  Every peer executes this (the
-// shuffles need them); only the leader, with tp != nullptr, writes.
-__device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
-                                          unsigned peers, int lane, uint64_t grow,
-                                          const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
-  const bool solo = (peers & (peers - 1)) == 0;
+// accumulator word w lives at tp[w * ws].  Every lane of `act` executes this
+// (the shuffles need them); only group leaders, with tp != nullptr, write.
+// iters = (largest peer group in act) - 1.
+__device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local, unsigned act,
+                                          unsigned peers, int iters, int lane, uint64_t grow,
+                                          const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull, bool plain = false) {
   const bool full = peers == QM_FULL;
+  auto umin = [](uint64_t x, uint64_t y) { return min(x, y); };
+  auto imin = [](int64_t x, int64_t y) { return min(x, y); };
+  auto imax = [](int64_t x, int64_t y) { return max(x, y); };
+  auto iadd = [](int64_t x, int64_t y) { return x + y; };
+  auto fadd = [](double x, double y) { return x + y; };
   for (int i = 0; i < A.n_accs; ++i) {
     const qm_acc ac = A.acc[i];
     uint64_t *w0 = tp ? tp + (int64_t)ac.word * ws : nullptr;
     uint64_t *w1 = tp ? tp + (int64_t)(ac.word + 1) * ws : nullptr;
     if (ac.kind == QA_COUNT) {
-      if (tp) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)__popc(peers));
+      if (tp) acc_add_u64(w0, (uint64_t)__popc(peers), plain);
       continue;
     }
     if (ac.kind == QA_FIRST) {
-      uint64_t first = grow;
-      if (full)
-        first = warp_allreduce(first, [](uint64_t x, uint64_t y) { return min(x, y); });
-      else if (!solo)
-        for (unsigned m = peers; m; m &= m - 1) {
-          const uint64_t x = __shfl_sync(peers, grow, __ffs(m) - 1);
-          first = min(first, x);
-        }
-      if (tp) upd_min_u64(w0, first, local);
+      const uint64_t first = iters > 0 ? group_reduce(grow, act, peers, lane, iters, umin) : grow;
+      if (tp) acc_min_u64(w0, first, plain, local);
       continue;
     }
     const bool valid = !((vnull >> ac.vcol) & 1);
     const uint64_t raw = pick(vb, ac.vcol);
     switch (ac.kind) {
       case QA_NN: {
-        unsigned nn = solo ? (unsigned)valid : __popc(__ballot_sync(peers, valid));
-        if (tp && nn) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)nn);
+        const unsigned nn = __popc(__ballot_sync(act, valid) & peers);
+        if (tp && nn) acc_add_u64(w0, (uint64_t)nn, plain);
         break;
       }
       case QA_ISUM: {
-        int64_t v = valid ? (int64_t)raw : 0;
+        const int64_t v = valid ? (int64_t)raw : 0;
         if (!ac.wide) {
-          int64_t s = v;
-          if (full)
-            s = warp_allreduce(s, [](int64_t x, int64_t y) { return x + y; });
-          else if (!solo)
-            for (unsigned m = peers; m; m &= m - 1) {
-              int src = __ffs(m) - 1;
-              int64_t x = __shfl_sync(peers, v, src);
-              if (src != lane) s += x;
-            }
+          const int64_t s = iters > 0 ? group_reduce(v, act, peers, lane, iters, iadd) : v;
           if (tp && s != 0) {
-            if (local) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)s);
+            if (local || ac.narrow) acc_add_u64(w0, (uint64_t)s, plain);
             else add128(w0, w1, (uint64_t)s, s < 0 ? -1 : 0);
           }
         } else {
@@ -683,42 +740,36 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
               hi += xh + (nlo < lo ? 1 : 0);
               lo = nlo;
             }
-          } else if (!solo)
-            for (unsigned m = peers; m; m &= m - 1) {
-              int src = __ffs(m) - 1;
-              int64_t x = __shfl_sync(peers, v, src);
-              if (src != lane) {
-                uint64_t nlo = lo + (uint64_t)x;
+          } else {
+            unsigned rem = peers & ~(1u << lane);
+            for (int it = 0; it < iters; ++it) {
+              const int src = rem ? __ffs(rem) - 1 : lane;
+              const int64_t x = __shfl_sync(act, v, src);
+              if (rem) {
+                const uint64_t nlo = lo + (uint64_t)x;
                 hi += (x < 0 ? -1 : 0) + (nlo < lo ? 1 : 0);
                 lo = nlo;
+                rem &= rem - 1;
               }
             }
-          if (tp && (lo != 0 || hi != 0)) add128(w0, w1, lo, hi);
+          }
+          if (tp && (lo != 0 || hi != 0)) acc_add128(w0, w1, lo, hi, plain);
         }
         break;
       }
       case QA_FSUM: {
-        double v = valid ? __longlong_as_double((long long)raw) : 0.0;
+        const double v = valid ? __longlong_as_double((long long)raw) : 0.0;
         const double split = A.vcol[ac.vcol].split;
         if (split != 0.0) {
-          double vh, vl;
-          split_parts(v, split, vh, vl);
-          double h = vh, l = vl;
-          if (full) {
-            h = warp_allreduce(h, [](double x, double y) { return x + y; });  // exact (grid multiples)
-            l = warp_allreduce(l, [](double x, double y) { return x + y; });
-          } else if (!solo)
-            for (unsigned m = peers; m; m &= m - 1) {
-              int src = __ffs(m) - 1;
-              double xh = __shfl_sync(peers, vh, src), xl = __shfl_sync(peers, vl, src);
-              if (src != lane) {
-                h += xh;  // exact: multiples of ulp(split) below split
-                l += xl;
-              }
-            }
+          double h, l;
+          split_parts(v, split, h, l);
+          if (iters > 0) {
+            h = group_reduce(h, act, peers, lane, iters, fadd);  // exact: multiples of ulp(split) below split
+            l = group_reduce(l, act, peers, lane, iters, fadd);
+          }
           if (tp) {
-            if (h != 0.0 || isnan(h)) atomicAdd(reinterpret_cast<double *>(w0), h);
-            if (l != 0.0) atomicAdd(reinterpret_cast<double *>(w1), l);
+            if (h != 0.0 || isnan(h)) acc_add_f64(w0, h, plain);
+            if (l != 0.0) acc_add_f64(w1, l, plain);
           }
           break;
         }
@@ -732,70 +783,50 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
             two_sum_acc(s, cc, xs);
             c = cc;
           }
-        } else if (!solo)
-          for (unsigned m = peers; m; m &= m - 1) {
-            int src = __ffs(m) - 1;
-            double x = __shfl_sync(peers, v, src);
-            if (src != lane) two_sum_acc(s, c, x);
+        } else {
+          unsigned rem = peers & ~(1u << lane);
+          for (int it = 0; it < iters; ++it) {
+            const int src = rem ? __ffs(rem) - 1 : lane;
+            const double x = __shfl_sync(act, v, src);
+            if (rem) {
+              two_sum_acc(s, c, x);
+              rem &= rem - 1;
+            }
           }
-        if (tp) fsum_add(w0, w1, s, c);
+        }
+        if (tp) acc_fsum(w0, w1, s, c, plain);
         break;
       }
       case QA_IMIN:
       case QA_IMAX: {
         const bool mx = ac.kind == QA_IMAX;
         int64_t v = valid ? (int64_t)raw : (mx ? INT64_MIN : INT64_MAX);
-        if (full)
-          v = mx ? warp_allreduce(v, [](int64_t x, int64_t y) { return max(x, y); })
-                 : warp_allreduce(v, [](int64_t x, int64_t y) { return min(x, y); });
-        else if (!solo)
-          for (unsigned m = peers; m; m &= m - 1) {
-            int src = __ffs(m) - 1;
-            int64_t x = __shfl_sync(peers, v, src);
-            v = mx ? max(v, x) : min(v, x);
-          }
+        if (iters > 0) v = mx ? group_reduce(v, act, peers, lane, iters, imax) : group_reduce(v, act, peers, lane, iters, imin);
         if (tp && v != (mx ? INT64_MIN : INT64_MAX)) {
-          if (mx) atomicMax(reinterpret_cast<long long *>(w0), (long long)v);
-          else atomicMin(reinterpret_cast<long long *>(w0), (long long)v);
+          if (mx) acc_max_i64(w0, v, plain);
+          else acc_min_i64(w0, v, plain);
         }
         break;
       }
       case QA_FMIN:
       case QA_FMAX: {
         const bool mx = ac.kind == QA_FMAX;
-        double d = __longlong_as_double((long long)raw);
-        bool ok = valid && !isnan(d); // NaN never wins '<' / '>' (src/partial-agg.ts:80-81)
+        const double d = __longlong_as_double((long long)raw);
+        const bool ok = valid && !isnan(d);  // NaN never wins '<' / '>' (src/partial-agg.ts:80-81)
         int64_t o = ok ? f2ord(d == 0.0 ? 0.0 : d) : (mx ? INT64_MIN : INT64_MAX);
-        if (full)
-          o = mx ? warp_allreduce(o, [](int64_t x, int64_t y) { return max(x, y); })
-                 : warp_allreduce(o, [](int64_t x, int64_t y) { return min(x, y); });
-        else if (!solo)
-          for (unsigned m = peers; m; m &= m - 1) {
-            int src = __ffs(m) - 1;
-            int64_t x = __shfl_sync(peers, o, src);
-            o = mx ? max(o, x) : min(o, x);
-          }
+        if (iters > 0) o = mx ? group_reduce(o, act, peers, lane, iters, imax) : group_reduce(o, act, peers, lane, iters, imin);
         if (tp && o != (mx ? INT64_MIN : INT64_MAX)) {
-          if (mx) atomicMax(reinterpret_cast<long long *>(w0), (long long)o);
-          else atomicMin(reinterpret_cast<long long *>(w0), (long long)o);
+          if (mx) acc_max_i64(w0, o, plain);
+          else acc_min_i64(w0, o, plain);
         }
         break;
       }
       case QA_FZERO: {
-        double d = __longlong_as_double((long long)raw);
-        bool z = valid && d == 0.0;
+        const double d = __longlong_as_double((long long)raw);
+        const bool z = valid && d == 0.0;
         uint64_t code = z ? ((grow << 1) | (raw >> 63)) : ~0ULL;
-        if (full) {
-          if (__any_sync(QM_FULL, z)) code = warp_allreduce(code, [](uint64_t x, uint64_t y) { return min(x, y); });
-        } else if (!solo) {
-          if (__any_sync(peers, z))
-            for (unsigned m = peers; m; m &= m - 1) {
-              int src = __ffs(m) - 1;
-              uint64_t x = __shfl_sync(peers, code, src);
-              code = min(code, x);
-            }
-        }
-        if (tp && code != ~0ULL) atomicMin(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)code);
+        if (__any_sync(act, z) && iters > 0) code = group_reduce(code, act, peers, lane, iters, umin);
+        if (tp && code != ~0ULL) acc_min_u64(w0, code, plain, false);
         break;
       }
     }
@@ -805,10 +836,48 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
 // One row's update of the slot whose word w lives at tp[w * ws]: straight
 // line per value column, values already gathered into vb (NULL bits in
 // vnull) so the cell loads overlap the key lookup.
+#ifndef QM_GLOBAL_READ_TEST
+#define QM_GLOBAL_READ_TEST 0
+#endif
 __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
                                         uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
+  // In the global table, the FIRST word and the MIN / MAX words of the first
+  // two value columns are read up front, in one L2 round trip; the atomics
+  // then go out only where the row beats the word read.  A word only moves
+  // one way, so a stale read can cause an unneeded atomic, never skip one.
+  uint64_t g_first = 0;
+  int64_t g_mn[2] = {0, 0}, g_mx[2] = {0, 0};
+  const bool gtest = QM_GLOBAL_READ_TEST && !local;
+  if (gtest) {
+    if (A.w_first >= 0) g_first = __ldcg(reinterpret_cast<const unsigned long long *>(tp + (int64_t)A.w_first * ws));
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      if (c >= A.n_vcols) break;
+      const int f = A.vcol[c].flags;
+      if (f & VF_MIN) g_mn[c] = __ldcg(reinterpret_cast<const long long *>(tp + (int64_t)A.vcol[c].w_min * ws));
+      if (f & VF_MAX) g_mx[c] = __ldcg(reinterpret_cast<const long long *>(tp + (int64_t)A.vcol[c].w_max * ws));
+    }
+  }
   atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)A.w_count * ws), 1ULL);
-  if (A.w_first >= 0) upd_min_u64(tp + (int64_t)A.w_first * ws, grow, local);
+  if (A.w_first >= 0) {
+    uint64_t *p = tp + (int64_t)A.w_first * ws;
+    if (!gtest) upd_min_u64(p, grow, local);
+    else if (grow < g_first) atomicMin(reinterpret_cast<unsigned long long *>(p), (unsigned long long)grow);
+  }
+  auto gmin = [&](int c, uint64_t *p, int64_t v) {
+    if (gtest && c < 2) {
+      if (v < g_mn[c]) atomicMin(reinterpret_cast<long long *>(p), (long long)v);
+    } else {
+      upd_min_i64(p, v, local);
+    }
+  };
+  auto gmax = [&](int c, uint64_t *p, int64_t v) {
+    if (gtest && c < 2) {
+      if (v > g_mx[c]) atomicMax(reinterpret_cast<long long *>(p), (long long)v);
+    } else {
+      upd_max_i64(p, v, local);
+    }
+  };
 #pragma unroll
   for (int c = 0; c < QM_MAX_VCOLS; ++c) {
     if (c >= A.n_vcols) break;
@@ -820,11 +889,12 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
       const int64_t v = (int64_t)vb[c];
       if ((f & VF_SUM) && v != 0) {
         uint64_t *w0 = tp + (int64_t)vc.w_sum * ws;
-        if (local && !(f & VF_WIDE)) atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)v);
+        if ((local && !(f & VF_WIDE)) || (f & VF_NARROW))
+          atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)v);
         else add128(w0, w0 + ws, (uint64_t)v, v < 0 ? -1 : 0);
       }
-      if (f & VF_MIN) upd_min_i64(tp + (int64_t)vc.w_min * ws, v, local);
-      if (f & VF_MAX) upd_max_i64(tp + (int64_t)vc.w_max * ws, v, local);
+      if (f & VF_MIN) gmin(c, tp + (int64_t)vc.w_min * ws, v);
+      if (f & VF_MAX) gmax(c, tp + (int64_t)vc.w_max * ws, v);
     } else {
       const double d = __longlong_as_double((long long)vb[c]);
       if (f & VF_SUM) {
@@ -834,8 +904,8 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
       }
       if ((f & (VF_MIN | VF_MAX)) && !isnan(d)) {  // NaN never wins '<' / '>'
         const int64_t o = f2ord(d == 0.0 ? 0.0 : d);
-        if (f & VF_MIN) upd_min_i64(tp + (int64_t)vc.w_min * ws, o, local);
-        if (f & VF_MAX) upd_max_i64(tp + (int64_t)vc.w_max * ws, o, local);
+        if (f & VF_MIN) gmin(c, tp + (int64_t)vc.w_min * ws, o);
+        if (f & VF_MAX) gmax(c, tp + (int64_t)vc.w_max * ws, o);
       }
       if ((f & VF_ZERO) && d == 0.0) upd_min_u64(tp + (int64_t)vc.w_zero * ws, (grow << 1) | (vb[c] >> 63), local);
     }
@@ -965,6 +1035,7 @@ __device__ __forceinline__ void merge_local(const qm_aggspec &A, const uint64_t 
         break;
       case QA_ISUM:
         if (ac.wide) add128(g0, g1, v0, (int64_t)lp[(int64_t)(ac.word + 1) * L]);
+        else if (v0 && ac.narrow) atomicAdd(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
         else if (v0) add128(g0, g1, v0, (int64_t)v0 < 0 ? -1 : 0);
         break;
       case QA_FSUM:
@@ -990,11 +1061,47 @@ __device__ __forceinline__ void merge_local(const qm_aggspec &A, const uint64_t 
   }
 }
 
+// Fold block-local slot words src[w * L] into dst[w * L] (both in this
+// block's shared memory, no other writer): the per-warp copies of a private
+// table collapse into one before the global merge.
+__device__ __forceinline__ void merge_plain(const qm_aggspec &A, uint64_t *dst, const uint64_t *src, int L) {
+  for (int i = 0; i < A.n_accs; ++i) {
+    const qm_acc ac = A.acc[i];
+    const int64_t w0 = (int64_t)ac.word * L, w1 = (int64_t)(ac.word + 1) * L;
+    switch (ac.kind) {
+      case QA_COUNT:
+      case QA_NN: dst[w0] += src[w0]; break;
+      case QA_FIRST:
+      case QA_FZERO: dst[w0] = min(dst[w0], src[w0]); break;
+      case QA_ISUM:
+        if (ac.wide) acc_add128(dst + w0, dst + w1, src[w0], (int64_t)src[w1], true);
+        else dst[w0] += src[w0];
+        break;
+      case QA_FSUM:
+        if (A.vcol[ac.vcol].split != 0.0) {
+          acc_add_f64(dst + w0, __longlong_as_double((long long)src[w0]), true);
+          acc_add_f64(dst + w1, __longlong_as_double((long long)src[w1]), true);
+        } else {
+          acc_fsum(dst + w0, dst + w1, __longlong_as_double((long long)src[w0]),
+                   __longlong_as_double((long long)src[w1]), true);
+        }
+        break;
+      case QA_IMIN:
+      case QA_FMIN: acc_min_i64(dst + w0, (int64_t)src[w0], true); break;
+      case QA_IMAX:
+      case QA_FMAX: acc_max_i64(dst + w0, (int64_t)src[w0], true); break;
+    }
+  }
+}
+
 // Aggregates one survivor per lane (lanes with active = false sit out).
+// DD: 0 / 1 = the plan's dedupe flag fixed at compile time (separate kernels
+// keep each path's registers and code apart), 2 = read it from the plan.
+template <int DD = 2>
 __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
                                             int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
   const qm_aggspec &A = a.agg;
-  if (a.dedupe) {
+  if (DD == 2 ? a.dedupe != 0 : DD == 1) {
     const unsigned act = __ballot_sync(QM_FULL, active);
     if (!active) return;
     const uint64_t grow = (uint64_t)(a.row_offset + row);
@@ -1024,7 +1131,8 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
         if (gs >= 0) tp = a.table + gs * a.stride + 1;
       }
     }
-    apply_row(A, tp, ws, local, peers, lane, grow, vb, vnull);
+    const int iters = (int)__reduce_max_sync(act, (unsigned)__popc(peers)) - 1;
+    apply_row(A, tp, ws, local, act, peers, iters, lane, grow, vb, vnull, local && a.priv);
     return;
   }
   uint64_t grow = 0, key = 0;
@@ -1157,7 +1265,8 @@ __device__ __forceinline__ void emit_group(const uint64_t *t, int stride, uint64
       }
       case QO_SUM_I2F:
       case QO_AVG_I2F: {
-        double s2 = i128_to_f64(w[o.word], (int64_t)w[o.word + 1]);
+        const int64_t hi = o.narrow ? ((int64_t)w[o.word] >> 63) : (int64_t)w[o.word + 1];
+        double s2 = i128_to_f64(w[o.word], hi);
         reinterpret_cast<double *>(col)[i] = o.kind == QO_SUM_I2F ? s2 : s2 / (double)nn;
         break;
       }

@@ -9,7 +9,8 @@
 #define QM_SCAN_THREADS 512
 #define QM_HLL_P 12
 
-size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth);
+size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth,
+                          int priv);
 cudaError_t qm_scan_configure(size_t smem_bytes, bool staged, int *blocks_per_sm);
 cudaError_t qm_launch_scan(const qm_scan_args &a, int blocks, size_t smem_bytes, cudaStream_t st);
 cudaError_t qm_launch_init_table(uint64_t *t, int64_t n_slots_total, int stride, int hash_keys,

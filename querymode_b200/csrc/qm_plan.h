@@ -111,6 +111,10 @@ struct qm_acc {
   int32_t vcol;  // value column index, -1 for COUNT / FIRST
   int32_t word;  // first word of the accumulator within a slot (after key)
   int32_t wide;  // QA_ISUM over int64 cells (128-bit even block-locally)
+  int32_t narrow;  // QA_ISUM over int32 cells of a table below 2^32 rows:
+                   // the sum fits a signed 64-bit word everywhere (the high
+                   // word stays 0 and is the low word's sign at finalize)
+  int32_t pad;
 };
 
 // Per value column: which accumulators read it (VF_* bits) and where their
@@ -121,6 +125,7 @@ struct qm_acc {
 #define VF_MAX 8
 #define VF_ZERO 16  // QA_FZERO (float MIN / MAX)
 #define VF_WIDE 32  // 128-bit integer sum even block-locally (int64 cells)
+#define VF_NARROW 64  // signed 64-bit integer sum in the global table too
 
 struct qm_vcol {
   const void *data;
@@ -172,6 +177,8 @@ struct qm_out {
   int32_t nn_word;  // count word deciding NULL (and the AVG divisor)
   int32_t zero_word;// QA_FZERO word for float MIN/MAX, else -1
   int32_t src;      // key column index for QO_KEY
+  int32_t narrow;   // QO_SUM_I2F / QO_AVG_I2F over a narrow (64-bit) sum
+  int32_t pad;
   int64_t offset;   // byte offset of the column in the output buffer
   int64_t null_offset; // byte offset of its 32-bit-word null bitmap, or -1
 };
@@ -226,6 +233,8 @@ struct qm_scan_args {
   int32_t dedupe;        // warp-level pre-aggregation of equal keys
   int32_t vec_ok;          // every term column is 16-byte aligned: vector loads
   int32_t max_probe;     // bound on linear probing in the global table
+  int32_t priv;          // direct block-local table copied per warp: its
+                         // (deduplicated) updates need no atomics
   qm_status *status;
   qm_staging stage;
 };

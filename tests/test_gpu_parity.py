@@ -322,3 +322,28 @@ def test_staged_filter_columns(ctx, depth):
     finally:
         ctx.set_tuning()
     assert_same(g2, oracle.run(c2, q2))
+
+
+def test_per_warp_tables_large(ctx):
+    # past the size where small direct tables (and the single no-GROUP-BY
+    # slot) are copied per warp and updated without atomics
+    rng = np.random.default_rng(21)
+    n = 9_000_000
+    x = rng.normal(size=n) * 100
+    x[rng.random(n) < 0.001] = 0.0
+    x[rng.random(n) < 0.001] = -0.0
+    x[rng.random(n) < 1e-5] = math.nan
+    cols = {"k": Column(rng.integers(0, 12, n).astype(np.int32), rng.random(n) < 0.02),
+            "x": Column(x, rng.random(n) < 0.05),
+            "i": rng.integers(-2**62, 2**62, n).astype(np.int64),
+            "j": rng.integers(-2**31, 2**31 - 1, n).astype(np.int32),
+            "f": rng.integers(0, 100, n).astype(np.int32)}
+    aggs = [AggregateOp("sum", "x"), AggregateOp("min", "x"), AggregateOp("max", "x"), AggregateOp("avg", "x"),
+            AggregateOp("count", "x"), AggregateOp("sum", "i"), AggregateOp("avg", "i"), AggregateOp("min", "i"),
+            AggregateOp("sum", "j"), AggregateOp("max", "j"), AggregateOp("count", "*")]
+    t = ctx.table(cols)
+    for q in (QueryDescriptor(filters=[FilterOp("f", "lt", 70)], group_by=["k"], aggregates=aggs),
+              QueryDescriptor(filters=[FilterOp("f", "gte", 10)], aggregates=aggs)):
+        g = t.run(q)
+        r = oracle.run(cols, q, threads=8)
+        assert_same(g, r)
