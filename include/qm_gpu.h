@@ -327,6 +327,72 @@ int qm_batch_stats(const qm_batch *batch, double *device_ms, int64_t *rows,
                    int64_t *bytes, int32_t *chunks);
 int qm_batch_destroy(qm_batch *batch);
 
+/* ---- serving loop -----------------------------------------------------------
+ * Continuous batching of single requests over resident tables.  The reference
+ * serves each query in its own durable object (src/query-do.ts fan-out, one
+ * single-threaded engine per object, src/wasm-engine.ts:181-186); here one
+ * worker thread per server drains a request queue into batched persistent
+ * launches (qm_batch_*) back to back: requests that arrive while a batch runs
+ * form the next one.
+ *
+ * HBM budget admission: the server counts the device bytes of every table
+ * it has been given (resident) plus each queued request's working memory
+ * (group table, bitmaps, packed result).  A batch takes queued requests in
+ * arrival order while resident + working bytes stay within hbm_budget_bytes;
+ * the rest wait for the next batch.  A request that cannot fit even alone
+ * completes with QM_ERR_OOM.
+ *
+ * The server drives the context it is created on from its worker thread:
+ * register tables first, and make no other call on that context (or its
+ * tables) until qm_server_destroy returns.  submit / cancel / wait / stats
+ * may be called from any thread. */
+typedef struct qm_server qm_server;
+
+typedef struct {
+  int64_t hbm_budget_bytes; /* resident tables + working memory, bytes     */
+  int32_t max_batch;        /* requests per batched launch (1..4096)       */
+  int32_t max_wait_us;      /* the oldest queued request waits at most this
+                               long for others before a launch (0: none)   */
+  int32_t reserved[4];
+} qm_server_config;
+
+typedef struct {
+  int64_t queued_us;  /* submit -> launch of its batch                     */
+  int64_t run_us;     /* launch -> result in host memory                   */
+  int64_t total_us;   /* submit -> result in host memory                   */
+  int32_t batch_size; /* requests in its batch                             */
+  int32_t reserved;
+} qm_server_timing;
+
+typedef struct {
+  int64_t submitted, completed, failed, cancelled, refused, batches;
+  int64_t resident_bytes;     /* device bytes of the tables seen           */
+  int64_t peak_working_bytes; /* largest admitted batch's working memory   */
+  int64_t queued;             /* requests waiting now                      */
+} qm_server_counters;
+
+int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out);
+/* Queue one request (the query is copied; the table must stay alive).
+ * *ticket identifies it for cancel / wait.  Planning errors surface from
+ * qm_server_wait with the request's own code and message. */
+int qm_server_submit(qm_server *srv, const qm_table *table, const qm_query *query,
+                     uint64_t *ticket);
+/* Cancel a request that has not been launched yet: its wait returns
+ * QM_ERR_CANCELLED.  QM_ERR_INVALID if it is unknown, running or done. */
+int qm_server_cancel(qm_server *srv, uint64_t ticket);
+/* Wait for a request (timeout_us < 0: no limit; QM_ERR_TIMEOUT when it runs
+ * out, the request stays pending) and take its result (destroy it) and
+ * timing (may be null).  Returns the request's status; a ticket is
+ * consumed by the wait that returns anything but QM_ERR_TIMEOUT.  The
+ * message of a failed request is copied to msg (msg_len bytes) if given. */
+int qm_server_wait(qm_server *srv, uint64_t ticket, int64_t timeout_us, qm_result **out,
+                   qm_server_timing *timing, char *msg, size_t msg_len);
+int qm_server_stats(qm_server *srv, qm_server_counters *out);
+/* Stop the worker after the batch in flight and free the server.  Requests
+ * not yet taken by a wait are dropped with their results; no wait may be in
+ * progress. */
+int qm_server_destroy(qm_server *srv);
+
 /* ---- results ------------------------------------------------------------- */
 int qm_result_num_rows(const qm_result *res, int64_t *out);
 int qm_result_num_columns(const qm_result *res, int32_t *out);

@@ -108,6 +108,22 @@ class QmStats(C.Structure):
                 ("launches", C.c_int32), ("scan_ms", C.c_double)]
 
 
+class QmServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_batch", C.c_int32), ("max_wait_us", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
+
+
+class QmServerTiming(C.Structure):
+    _fields_ = [("queued_us", C.c_int64), ("run_us", C.c_int64), ("total_us", C.c_int64),
+                ("batch_size", C.c_int32), ("reserved", C.c_int32)]
+
+
+class QmServerCounters(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("cancelled", C.c_int64), ("refused", C.c_int64), ("batches", C.c_int64),
+                ("resident_bytes", C.c_int64), ("peak_working_bytes", C.c_int64), ("queued", C.c_int64)]
+
+
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libqm_gpu.so")
 
@@ -144,6 +160,13 @@ SIGNATURES = [
     ("qm_batch_stats", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                  C.POINTER(C.c_int32)]),
     ("qm_batch_destroy", C.c_int, [_P]),
+    ("qm_server_create", C.c_int, [_P, C.POINTER(QmServerConfig), _PP]),
+    ("qm_server_submit", C.c_int, [_P, _P, C.POINTER(QmQuery), C.POINTER(C.c_uint64)]),
+    ("qm_server_cancel", C.c_int, [_P, C.c_uint64]),
+    ("qm_server_wait", C.c_int, [_P, C.c_uint64, C.c_int64, _PP, C.POINTER(QmServerTiming), C.c_char_p,
+                                 C.c_size_t]),
+    ("qm_server_stats", C.c_int, [_P, C.POINTER(QmServerCounters)]),
+    ("qm_server_destroy", C.c_int, [_P]),
     ("qm_result_num_rows", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("qm_result_num_columns", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("qm_result_column", C.c_int, [_P, C.c_int32, C.POINTER(QmResultCol)]),

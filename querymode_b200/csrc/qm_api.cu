@@ -2497,88 +2497,76 @@ int batch_layout(qm_batch *b) {
   return QM_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int qm_batch_create(qm_ctx *ctx, int32_t n, const qm_table *const *tables, const qm_query *const *queries,
-                    qm_batch **out) {
-  if (!ctx || !out || n <= 0 || !tables || !queries) return set_err(ctx, QM_ERR_INVALID, "qm_batch_create: bad arguments");
-  if (n > QM_BATCH_MAX) return set_err(ctx, QM_ERR_UNSUPPORTED, "at most %d queries per batch", QM_BATCH_MAX);
-  *out = nullptr;
-  cudaSetDevice(ctx->device);
-  qm_batch *b = new qm_batch();
-  b->ctx = ctx;
+void batch_reset(qm_batch *b, int n) {
   b->n = n;
-  b->gts.resize(n);
-  b->bq.resize(n);
-  b->rows.resize(n);
-  b->est.resize(n);
-  for (int i = 0; i < n; i++) {
-    if (!tables[i] || !queries[i]) {
-      delete b;
-      return set_err(ctx, QM_ERR_INVALID, "query %d: null table or query", i);
-    }
-    qm_query q = *queries[i];
-    q.flags &= ~QM_FLAG_UNORDERED;  // the batched finalize always orders by first row
-    qm_table *t = const_cast<qm_table *>(tables[i]);
-    GroupTable &gt = b->gts[i];
-    int64_t est = 1, direct_size = 0;
-    int rc = plan_table_query(ctx, t, &q, gt, est, direct_size);
-    if (rc) {
-      delete b;
-      return rc;
-    }
-    // sizes as setup_table, without allocating
-    Exec &ex = gt.ex;
-    if (gt.pl.key.mode == QK_NONE) {
-      ex.n_slots = 1;
-    } else if (gt.pl.key.mode == QK_DIRECT) {
-      ex.n_slots = direct_size;
-    } else {
-      int64_t want = std::max<int64_t>(1024, est * 2 + est / 8);
-      ex.log2cap = ilog2_ceil(want);
-      ex.n_slots = (int64_t)1 << ex.log2cap;
-    }
-    choose_layout(gt.pl, est, ex, ctx->tuning);
-    b->est[i] = est;
-    qm_bq &qb = b->bq[i];
-    memset(&qb, 0, sizeof qb);
-    qb.outs = gt.pl.outs;
-    qb.none = gt.pl.key.mode == QK_NONE;
-    for (int k = 0; k < qb.outs.n_out; k++) {
-      qb.width[k] = (int32_t)dtype_size(qb.outs.o[k].dtype);
-      qb.nullable[k] = gt.pl.meta[k].nullable ? 1 : 0;
-    }
-    b->rows[i] = t->n_rows;
-    b->total_rows += t->n_rows;
-    b->bytes_scanned += gt.pl.bytes_per_row * t->n_rows;
+  b->gts.assign(n, GroupTable());
+  b->bq.assign(n, qm_bq());
+  b->rows.assign(n, 0);
+  b->est.assign(n, 1);
+  b->total_rows = 0;
+  b->bytes_scanned = 0;
+  drop_graph(b);
+}
+
+// Plan query i of the batch over table t and size its group table (the
+// batch's arena is laid out later by batch_layout).
+int batch_plan_one(qm_batch *b, int i, const qm_table *table, const qm_query *query) {
+  qm_ctx *ctx = b->ctx;
+  if (!table || !query) return set_err(ctx, QM_ERR_INVALID, "query %d: null table or query", i);
+  qm_query q = *query;
+  q.flags &= ~QM_FLAG_UNORDERED;  // the batched finalize always orders by first row
+  qm_table *t = const_cast<qm_table *>(table);
+  GroupTable &gt = b->gts[i];
+  int64_t est = 1, direct_size = 0;
+  int rc = plan_table_query(ctx, t, &q, gt, est, direct_size);
+  if (rc) return rc;
+  // sizes as setup_table, without allocating
+  Exec &ex = gt.ex;
+  if (gt.pl.key.mode == QK_NONE) {
+    ex.n_slots = 1;
+  } else if (gt.pl.key.mode == QK_DIRECT) {
+    ex.n_slots = direct_size;
+  } else {
+    int64_t want = std::max<int64_t>(1024, est * 2 + est / 8);
+    ex.log2cap = ilog2_ceil(want);
+    ex.n_slots = (int64_t)1 << ex.log2cap;
   }
-  int rc = batch_layout(b);
-  if (rc) {
-    delete b;
-    return rc;
+  choose_layout(gt.pl, est, ex, ctx->tuning);
+  b->est[i] = est;
+  qm_bq &qb = b->bq[i];
+  memset(&qb, 0, sizeof qb);
+  qb.outs = gt.pl.outs;
+  qb.none = gt.pl.key.mode == QK_NONE;
+  for (int k = 0; k < qb.outs.n_out; k++) {
+    qb.width[k] = (int32_t)dtype_size(qb.outs.o[k].dtype);
+    qb.nullable[k] = gt.pl.meta[k].nullable ? 1 : 0;
   }
-  *out = b;
+  b->rows[i] = t->n_rows;
+  b->total_rows += t->n_rows;
+  b->bytes_scanned += gt.pl.bytes_per_row * t->n_rows;
   return QM_OK;
 }
 
-int qm_batch_set_tuning(qm_batch *b, int32_t chunk_tiles, int32_t local_kb, int32_t blocks_per_sm) {
-  if (!b) return QM_ERR_INVALID;
-  if (chunk_tiles > 0) b->chunk_tiles = chunk_tiles;
-  if (local_kb >= 0) b->local_kb = std::min(local_kb, 160);
-  if (blocks_per_sm >= 0) b->bps = blocks_per_sm;
-  cudaSetDevice(b->ctx->device);
-  // rebuild block-local table choices from the planner's, then re-lay out
-  for (int i = 0; i < b->n; i++) choose_layout(b->gts[i].pl, b->est[i], b->gts[i].ex, b->ctx->tuning);
-  return batch_layout(b);
+// Device bytes the batch's group tables, bitmaps and packed results take
+// (what batch_layout sizes its buffers to).
+int64_t batch_query_bytes(const qm_batch *b, int i) {
+  const GroupTable &gt = b->gts[i];
+  const qm_bq &q = b->bq[i];
+  const int64_t total_slots = gt.ex.n_slots + special_slots(gt.pl.key.mode);
+  const int64_t table = total_slots * (1 + gt.pl.agg.n_words) * 8;
+  const int64_t gmax = q.none ? 1 : std::min<int64_t>(total_slots, std::max<int64_t>(b->rows[i], 1));
+  int64_t res = 0;
+  for (int k = 0; k < q.outs.n_out; k++) res += (gmax * q.width[k] + 15) / 16 * 16 + (q.nullable[k] ? 2 * gmax + 64 : 0);
+  return table + res + b->rows[i] / 8 * 3 + 4096;
 }
 
-int qm_batch_run(qm_batch *b, qm_result **results) {
-  if (!b || !results) return QM_ERR_INVALID;
+// Run the laid-out batch (through its captured graph, or with plain
+// launches when use_graph is false) and build one result per query.
+// codes[i] receives each query's status; results[i] is null where it failed.
+int batch_execute(qm_batch *b, qm_result **results, int *codes, bool use_graph) {
   qm_ctx *ctx = b->ctx;
   cudaSetDevice(ctx->device);
-  if (!b->gexec) {
+  if (use_graph && !b->gexec) {
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = qm_batch_launch_all(b->dev, ctx->stream);
     cudaError_t e2 = cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n, cudaMemcpyDeviceToHost,
@@ -2595,16 +2583,22 @@ int qm_batch_run(qm_batch *b, qm_result **results) {
     CK(cudaGraphInstantiate(&b->gexec, g, 0));
   }
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  CK(cudaGraphLaunch(b->gexec, ctx->stream));
+  if (use_graph) {
+    CK(cudaGraphLaunch(b->gexec, ctx->stream));
+  } else {
+    CK(qm_batch_launch_all(b->dev, ctx->stream));
+    CK(cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  }
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   const qm_status *st = (const qm_status *)b->h_status.p;
-  for (int i = 0; i < b->n; i++)
-    if (st[i].error)
-      return set_err(ctx, st[i].error == QM_DEV_OVERFLOW ? QM_ERR_CAPACITY : QM_ERR_CUDA,
-                     "query %d of the batch: device status %d (group estimate too small)", i, st[i].error);
+  for (int i = 0; i < b->n; i++) {
+    results[i] = nullptr;
+    codes[i] = st[i].error == 0 ? QM_OK : (st[i].error == QM_DEV_OVERFLOW ? QM_ERR_CAPACITY : QM_ERR_CUDA);
+  }
   const qm_batch_meta *meta = (const qm_batch_meta *)b->h_meta.p;
   auto holder = std::make_shared<SharedPinned>();
   holder->pool = ctx->pool;
@@ -2618,6 +2612,7 @@ int qm_batch_run(qm_batch *b, qm_result **results) {
   b->last_ms = ms2;
   const uint8_t *h = (const uint8_t *)holder->buf.p;
   for (int i = 0; i < b->n; i++) {
+    if (codes[i] != QM_OK) continue;
     const qm_bq &qb = b->bq[i];
     const Plan &pl = b->gts[i].pl;
     const int64_t G = meta->groups[i];
@@ -2654,6 +2649,63 @@ int qm_batch_run(qm_batch *b, qm_result **results) {
   return QM_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int qm_batch_create(qm_ctx *ctx, int32_t n, const qm_table *const *tables, const qm_query *const *queries,
+                    qm_batch **out) {
+  if (!ctx || !out || n <= 0 || !tables || !queries) return set_err(ctx, QM_ERR_INVALID, "qm_batch_create: bad arguments");
+  if (n > QM_BATCH_MAX) return set_err(ctx, QM_ERR_UNSUPPORTED, "at most %d queries per batch", QM_BATCH_MAX);
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  qm_batch *b = new qm_batch();
+  b->ctx = ctx;
+  batch_reset(b, n);
+  for (int i = 0; i < n; i++) {
+    int rc = batch_plan_one(b, i, tables[i], queries[i]);
+    if (rc) {
+      delete b;
+      return rc;
+    }
+  }
+  int rc = batch_layout(b);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return QM_OK;
+}
+
+int qm_batch_set_tuning(qm_batch *b, int32_t chunk_tiles, int32_t local_kb, int32_t blocks_per_sm) {
+  if (!b) return QM_ERR_INVALID;
+  if (chunk_tiles > 0) b->chunk_tiles = chunk_tiles;
+  if (local_kb >= 0) b->local_kb = std::min(local_kb, 160);
+  if (blocks_per_sm >= 0) b->bps = blocks_per_sm;
+  cudaSetDevice(b->ctx->device);
+  // rebuild block-local table choices from the planner's, then re-lay out
+  for (int i = 0; i < b->n; i++) choose_layout(b->gts[i].pl, b->est[i], b->gts[i].ex, b->ctx->tuning);
+  return batch_layout(b);
+}
+
+int qm_batch_run(qm_batch *b, qm_result **results) {
+  if (!b || !results) return QM_ERR_INVALID;
+  std::vector<int> codes(b->n, QM_OK);
+  int rc = batch_execute(b, results, codes.data(), true);
+  if (rc) return rc;
+  for (int i = 0; i < b->n; i++)
+    if (codes[i] != QM_OK) {
+      for (int k = 0; k < b->n; k++) {
+        delete results[k];
+        results[k] = nullptr;
+      }
+      return set_err(b->ctx, codes[i], "query %d of the batch: device status %d (group estimate too small)", i,
+                     ((const qm_status *)b->h_status.p)[i].error);
+    }
+  return QM_OK;
+}
+
 int qm_batch_stats(const qm_batch *b, double *device_ms, int64_t *rows, int64_t *bytes, int32_t *chunks) {
   if (!b) return QM_ERR_INVALID;
   if (device_ms) *device_ms = b->last_ms;
@@ -2672,3 +2724,5 @@ int qm_batch_destroy(qm_batch *b) {
 }
 
 }  // extern "C"
+
+#include "qm_server.cuh"

@@ -8,6 +8,7 @@ optional boolean NULL mask, or torch CUDA tensors already resident in HBM
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 from typing import Any, Mapping
 
@@ -275,9 +276,18 @@ class Context:
             raise A.QmError(st, f"qm_ctx_create(device={device})")
         self.h = h
         self.device = device
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, child) -> None:
+        """Track a table / batch / stream / server made on this context: the
+        context closes them before itself, whatever order they are collected
+        in."""
+        self._children.add(child)
 
     def close(self) -> None:
         if getattr(self, "h", None):
+            for child in sorted(list(self._children), key=lambda c: c._close_order):
+                child.close()
             self.lib.qm_ctx_destroy(self.h)
             self.h = None
 
@@ -358,6 +368,9 @@ class Context:
     def batch(self, tables: list["Table"], queries: list[QueryDescriptor]) -> "Batch":
         return Batch(self, tables, queries)
 
+    def server(self, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0) -> "Server":
+        return Server(self, hbm_budget_bytes, max_batch, max_wait_us)
+
 
 class Table:
     """A qm_table: numeric columns resident in HBM."""
@@ -368,10 +381,14 @@ class Table:
         self.n_rows = n_rows
         self.names = names
         self._keep = keep  # device-resident inputs are read in place
+        ctx._adopt(self)
+
+    _close_order = 2
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.ctx.lib.qm_table_destroy(self.h)
+            if self.ctx.h:
+                self.ctx.lib.qm_table_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -399,6 +416,7 @@ class AggStream:
         h = C.c_void_p()
         ctx.check(ctx.lib.qm_agg_begin(ctx.h, self.cq.ref, C.byref(h)))
         self.h = h
+        ctx._adopt(self)
 
     def push(self, columns: Mapping[str, Any], selection: np.ndarray | None = None) -> None:
         cs = _ColumnSet(columns)
@@ -419,9 +437,12 @@ class AggStream:
         finally:
             self.ctx.lib.qm_result_destroy(r)
 
+    _close_order = 1
+
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.ctx.lib.qm_agg_destroy(self.h)
+            if self.ctx.h:
+                self.ctx.lib.qm_agg_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -448,6 +469,7 @@ class Batch:
         ctx.check(ctx.lib.qm_batch_create(ctx.h, n, th, qs, C.byref(h)))
         self.h = h
         self.n = n
+        ctx._adopt(self)
 
     def set_tuning(self, chunk_tiles: int = -1, local_kb: int = -1, blocks_per_sm: int = -1) -> None:
         self.ctx.check(self.ctx.lib.qm_batch_set_tuning(self.h, chunk_tiles, local_kb, blocks_per_sm))
@@ -466,9 +488,12 @@ class Batch:
                                                    C.byref(chunks)))
         return {"device_ms": ms.value, "rows": rows.value, "bytes": nbytes.value, "chunks": chunks.value}
 
+    _close_order = 1
+
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.ctx.lib.qm_batch_destroy(self.h)
+            if self.ctx.h:
+                self.ctx.lib.qm_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -504,5 +529,65 @@ class BatchResults:
             for i, h in enumerate(self.handles):
                 if i not in self.cache and h:
                     self.lib.qm_result_destroy(C.c_void_p(h))
+        except Exception:
+            pass
+
+
+class Server:
+    """A qm_server: a native worker thread that batches submitted requests
+    over resident tables into persistent launches, within an HBM budget.
+    While it runs, the context is the worker's: register tables first."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us)
+        h = C.c_void_p()
+        ctx.check(self.lib.qm_server_create(ctx.h, C.byref(cfg), C.byref(h)))
+        self.h = h
+        ctx._adopt(self)
+        self._queries: dict[int, CQuery] = {}
+
+    def submit(self, table: Table, query) -> int:
+        cq = query if isinstance(query, CQuery) else CQuery(query)
+        t = C.c_uint64()
+        status = self.lib.qm_server_submit(self.h, table.h, C.byref(cq.struct), C.byref(t))
+        if status != A.QM_OK:
+            raise A.QmError(status, "submit")
+        return t.value
+
+    def cancel(self, ticket: int) -> bool:
+        return self.lib.qm_server_cancel(self.h, ticket) == A.QM_OK
+
+    def wait(self, ticket: int, timeout_s: float | None = None) -> tuple["Result", dict]:
+        """The request's Result and timing (µs); raises QmError with the
+        request's own status and message if it failed or was cancelled."""
+        out = C.c_void_p()
+        tm = A.QmServerTiming()
+        msg = C.create_string_buffer(512)
+        tmo = -1 if timeout_s is None else int(timeout_s * 1e6)
+        status = self.lib.qm_server_wait(self.h, ticket, tmo, C.byref(out), C.byref(tm), msg, len(msg))
+        timing = {"queued_us": tm.queued_us, "run_us": tm.run_us, "total_us": tm.total_us,
+                  "batch_size": tm.batch_size}
+        if status != A.QM_OK:
+            raise A.QmError(status, msg.value.decode(errors="replace"))
+        return Result.from_handle(self.lib, out, owned=True), timing
+
+    def stats(self) -> dict:
+        c = A.QmServerCounters()
+        _check(self.lib, None, self.lib.qm_server_stats(self.h, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in A.QmServerCounters._fields_}
+
+    _close_order = 0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            if self.ctx.h:
+                self.lib.qm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
