@@ -57,6 +57,9 @@ def parse_args():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serve-queries", type=int, default=1500, help="requests per offered load")
+    p.add_argument("--serve-loads", default="0.25,0.5,0.75,0.95", help="offered loads as fractions of capacity")
     p.add_argument("--batch-queries", type=int, default=256)
     p.add_argument("--batch-reps", type=int, default=3)
     return p.parse_args()
@@ -285,6 +288,162 @@ def run_batched(ctx, stream, local: int, args) -> dict:
     return out
 
 
+def serving_tables(device: int) -> dict:
+    """The serving mix's resident tables, generated on the device (seeded):
+    the orders / events / wide-keys shapes at 1M-200M rows."""
+    import torch
+    dev = f"cuda:{device}"
+    g = torch.Generator(device=dev)
+
+    def orders(n, seed):
+        g.manual_seed(seed)
+        return {"status": torch.randint(0, 3, (n,), dtype=torch.int32, device=dev, generator=g),
+                "region": torch.randint(0, 16, (n,), dtype=torch.int32, device=dev, generator=g),
+                "amount": torch.empty(n, dtype=torch.float64, device=dev).log_normal_(3.0, 1.0, generator=g)}
+
+    def events(n, seed, n_keys=65_536):
+        g.manual_seed(seed)
+        w = torch.arange(1, n_keys + 1, dtype=torch.float64, device=dev) ** -1.1
+        cdf = torch.cumsum(w, 0)
+        cdf /= cdf[-1].clone()
+        perm = torch.randperm(n_keys, device=dev, generator=g)
+        key = torch.empty(n, dtype=torch.int64, device=dev)
+        for i in range(0, n, 1 << 25):
+            u = torch.rand(min(1 << 25, n - i), dtype=torch.float64, device=dev, generator=g)
+            key[i:i + len(u)] = perm[torch.searchsorted(cdf, u, right=True).clamp_(max=n_keys - 1)]
+        return {"key": key,
+                "qty": torch.randint(1, 101, (n,), dtype=torch.int32, device=dev, generator=g),
+                "price": torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 1000.0,
+                "ts": torch.randint(datagen_year_start(), datagen_year_start() + 365 * 86_400_000, (n,),
+                                    dtype=torch.int64, device=dev, generator=g)}
+
+    def wide(n, seed, n_keys=1 << 24):
+        g.manual_seed(seed)
+        return {"key": torch.randint(0, n_keys, (n,), dtype=torch.int64, device=dev, generator=g),
+                "val": torch.randn(n, dtype=torch.float64, device=dev, generator=g) * 1e3,
+                "flag": (torch.rand(n, device=dev, generator=g) < 0.01).to(torch.int32)}
+
+    return {"orders_1m": ("orders", orders(1_000_000, 40)), "orders_200m": ("orders", orders(200_000_000, 41)),
+            "events_100m": ("events", events(100_000_000, 42)), "events_200m_a": ("events", events(200_000_000, 43)),
+            "events_200m_b": ("events", events(200_000_000, 44)), "wide_50m": ("wide", wide(50_000_000, 45)),
+            "wide_200m_a": ("wide", wide(200_000_000, 46)), "wide_200m_b": ("wide", wide(200_000_000, 47))}
+
+
+def datagen_year_start() -> int:
+    from querymode_b200 import datagen
+    return datagen.YEAR_START_MS
+
+
+def run_serving(local: int, args) -> dict:
+    """Poisson arrivals of single requests mixing the orders / events /
+    wide-keys queries over 8 resident tables, served by the native
+    continuous-batching loop under a 150 GB HBM budget; latency = submit ->
+    result in host memory, per offered load."""
+    import threading
+
+    import torch
+
+    from querymode_b200 import datagen
+    from querymode_b200.engine import Context
+    from querymode_b200.query import AggregateOp, CQuery, FilterOp, QueryDescriptor
+
+    rng = np.random.default_rng(4)
+    tabs = serving_tables(local)
+    torch.cuda.synchronize()
+    table_bytes = sum(t.numel() * t.element_size() for _, cols in tabs.values() for t in cols.values())
+    sctx = Context(local)
+    handles = {name: (kind, sctx.table(cols)) for name, (kind, cols) in tabs.items()}
+
+    # request templates per table kind (query objects built once)
+    events_q = [CQuery(datagen.events_query(window_start_day=int(d))) for d in rng.integers(0, 330, 48)]
+    orders_q = [CQuery(QueryDescriptor(filters=[FilterOp("status", "eq", s)], group_by=["region"],
+                                       aggregates=[AggregateOp("sum", "amount"), AggregateOp("count", "*")]))
+                for s in range(3)]
+    wide_q = [CQuery(datagen.wide_keys_query(True)),
+              CQuery(QueryDescriptor(filters=[FilterOp("flag", "eq", 1)], group_by=["key"],
+                                     aggregates=[AggregateOp("max", "val"), AggregateOp("count", "*")]))]
+    wide_full = CQuery(datagen.wide_keys_query(False))
+    names = list(handles)
+
+    def draw(r):
+        name = names[int(r.integers(len(names)))]
+        kind, t = handles[name]
+        if kind == "orders":
+            return t, orders_q[int(r.integers(3))]
+        if kind == "events":
+            return t, events_q[int(r.integers(len(events_q)))]
+        if r.random() < 0.01:  # the unfiltered 16M-group aggregate, rarely
+            return t, wide_full
+        return t, wide_q[int(r.integers(2))]
+
+    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0)
+    try:
+        # warm-up: every table and query kind once (column statistics are cached)
+        warm = []
+        for name, (kind, t) in handles.items():
+            qs = orders_q if kind == "orders" else (events_q[:2] if kind == "events" else wide_q + [wide_full])
+            warm += [srv.submit(t, q) for q in qs]
+        for tk in warm:
+            srv.wait(tk)
+
+        def serve(reqs, rate):
+            """Submit reqs at Poisson arrivals of `rate` per second (all at
+            once if rate is None); returns (latencies us, batch sizes, span s)."""
+            tickets = [None] * len(reqs)
+            lat, bs = [0.0] * len(reqs), [0] * len(reqs)
+            gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+            done_at = [0.0]
+
+            def collect():
+                for i in range(len(reqs)):
+                    while tickets[i] is None:
+                        time.sleep(0)
+                    _, tm = srv.wait(tickets[i])
+                    lat[i], bs[i] = tm["total_us"], tm["batch_size"]
+                done_at[0] = time.perf_counter()
+
+            th = threading.Thread(target=collect)
+            th.start()
+            t0 = time.perf_counter()
+            due = t0
+            for i, (t, q) in enumerate(reqs):
+                due += gaps[i]
+                rem = due - time.perf_counter()
+                if rem > 0.002:
+                    time.sleep(rem - 0.001)
+                while time.perf_counter() < due:
+                    pass
+                tickets[i] = srv.submit(t, q)
+            th.join()
+            return np.array(lat), np.array(bs), done_at[0] - t0
+
+        # capacity: a closed burst of requests
+        burst = [draw(rng) for _ in range(max(200, args.serve_queries // 4))]
+        _, bsz, span = serve(burst, None)
+        capacity = len(burst) / span
+        loads = []
+        for frac in [float(x) for x in args.serve_loads.split(",")]:
+            reqs = [draw(rng) for _ in range(args.serve_queries)]
+            lat, bsz, span = serve(reqs, capacity * frac)
+            loads.append({"offered_qps": round(capacity * frac, 1), "achieved_qps": round(len(reqs) / span, 1),
+                          "p50_ms": round(float(np.percentile(lat, 50)) / 1e3, 3),
+                          "p95_ms": round(float(np.percentile(lat, 95)) / 1e3, 3),
+                          "p99_ms": round(float(np.percentile(lat, 99)) / 1e3, 3),
+                          "mean_batch": round(float(bsz.mean()), 2)})
+        st = srv.stats()
+    finally:
+        srv.close()
+        sctx.close()
+        del tabs, handles
+        torch.cuda.empty_cache()
+    return {"tables": 8, "table_gb": round(table_bytes / 1e9, 2), "hbm_budget_gb": 150,
+            "capacity_qps": round(capacity, 1), "queries_per_load": args.serve_queries, "loads": loads,
+            "server": {k: st[k] for k in ("completed", "failed", "refused", "batches", "peak_working_bytes")},
+            "mix": "uniform over 8 tables (orders 1M/200M, events 100M/200M/200M, wide 50M/200M/200M); "
+                   "orders: status filter by region; events: 30-day window + qty, 48 windows; wide: flag (+val) "
+                   "filters, 1% unfiltered 16M-group; Poisson arrivals (seed 4)"}
+
+
 def run_reference(args, world, rank):
     """Reference arm: the reference's algorithm (oracle port) on the host cores."""
     if rank != 0:
@@ -404,6 +563,9 @@ def main():
         table.close()
         table = None
         batched = run_batched(ctx, stream, local, args)
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = run_serving(local, args)
 
     if rank == 0:
         line = {
@@ -420,6 +582,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "batched": batched,
+            "serving": serving,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "rows_per_s": n * world * args.steps / (elapsed_max / 1e3),
