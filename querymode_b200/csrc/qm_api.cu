@@ -22,6 +22,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <deque>
 #include <vector>
 
 #include "../../include/qm_gpu.h"
@@ -939,6 +940,31 @@ int estimate_groups(qm_ctx *ctx, const qm_keyspec &K, int64_t n, double *out) {
   return QM_OK;
 }
 
+// Upper bound on the rows a filtered query selects, from a strided sample
+// of the predicate (6 standard deviations above the sampled fraction).
+constexpr int SEL_SAMPLES = 1 << 16;
+
+bool has_filter(const qm_pred &P) {
+  const int nt = P.n_groups > 0 ? P.group_end[P.n_groups - 1] : P.n_and;
+  for (int i = 0; i < nt; i++)
+    if (P.t[i].kind != QT_TRUE) return true;
+  return false;
+}
+
+int selected_rows_bound(qm_ctx *ctx, const qm_pred &P, int64_t n, int64_t *out) {
+  int rc = ensure(ctx, ctx->counter, 64);
+  if (rc) return rc;
+  rc = ensure_host(ctx, ctx->hstatus, 64);
+  if (rc) return rc;
+  CK(qm_launch_sample_pred(P, n, SEL_SAMPLES, (unsigned long long *)ctx->counter.p, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->counter.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const double p = (double)*(const uint64_t *)ctx->hstatus.p / SEL_SAMPLES;
+  const double up = std::min(1.0, p + 6.0 * std::sqrt(p * (1.0 - p) / SEL_SAMPLES) + 8.0 / SEL_SAMPLES);
+  *out = std::min<int64_t>(n, (int64_t)(up * (double)n) + 4096);
+  return QM_OK;
+}
+
 int column_maxabs(qm_ctx *ctx, DevCol &c, int64_t n) {
   if (c.has_maxabs) return QM_OK;
   int rc = ensure(ctx, ctx->counter, 64);
@@ -1384,6 +1410,13 @@ int plan_table_query(qm_ctx *ctx, qm_table *t, const qm_query *q, GroupTable &gt
       }
     }
     const bool single = pl.key.n_cols == 1;
+    // a wide dense range that a selective filter leaves mostly empty: a hash
+    // table sized by the selected rows is smaller to clear and to compact
+    int64_t sel_bound = -1;  // sampled bound on selected rows, when taken
+    if (direct && direct_size > (1 << 20) && t->n_rows >= 4 * (int64_t)SEL_SAMPLES && has_filter(pl.pred)) {
+      if ((rc = selected_rows_bound(ctx, pl.pred, t->n_rows, &sel_bound))) return rc;
+      if (sel_bound * 4 < direct_size) direct = false;
+    }
     if (direct) {
       pl.key.mode = QK_DIRECT;
       est = direct_size;
@@ -1417,6 +1450,11 @@ int plan_table_query(qm_ctx *ctx, qm_table *t, const qm_query *q, GroupTable &gt
         }
       }
       est = std::min<int64_t>(est, std::max<int64_t>(t->n_rows, 1));
+      // a filtered query has at most as many groups as selected rows
+      if (est > 65536 && t->n_rows >= 4 * (int64_t)SEL_SAMPLES && has_filter(pl.pred)) {
+        if (sel_bound < 0 && (rc = selected_rows_bound(ctx, pl.pred, t->n_rows, &sel_bound))) return rc;
+        est = std::min(est, sel_bound);
+      }
     }
   }
   return QM_OK;
@@ -2331,6 +2369,56 @@ int64_t region_bytes(int64_t G, const qm_bq &b) {
   return off;
 }
 
+// A deep copy of a qm_query (the caller's strings and arrays may go away
+// once submit returns).
+struct OwnedQuery {  // holds pointers into itself: never copied or moved
+  OwnedQuery() = default;
+  OwnedQuery(const OwnedQuery &) = delete;
+  OwnedQuery &operator=(const OwnedQuery &) = delete;
+  std::deque<std::string> strs;  // deque: stable addresses
+  std::vector<qm_filter> filters, or_filters;
+  std::vector<int32_t> or_sizes;
+  std::vector<const char *> group_by;
+  std::vector<qm_aggregate> aggs;
+  qm_query q{};
+
+  const char *keep(const char *p) {
+    if (!p) return nullptr;
+    strs.emplace_back(p);
+    return strs.back().c_str();
+  }
+  void copy(const qm_query &src) {
+    q = src;
+    for (int i = 0; i < src.n_filters; i++) {
+      qm_filter f = src.filters[i];
+      f.column = keep(f.column);
+      filters.push_back(f);
+    }
+    int64_t n_or = 0;
+    for (int g = 0; g < src.n_or_groups; g++) {
+      or_sizes.push_back(src.or_group_sizes[g]);
+      n_or += src.or_group_sizes[g];
+    }
+    for (int64_t i = 0; i < n_or; i++) {
+      qm_filter f = src.or_filters[i];
+      f.column = keep(f.column);
+      or_filters.push_back(f);
+    }
+    for (int i = 0; i < src.n_group_by; i++) group_by.push_back(keep(src.group_by[i]));
+    for (int i = 0; i < src.n_aggregates; i++) {
+      qm_aggregate a = src.aggregates[i];
+      a.column = keep(a.column);
+      a.alias = keep(a.alias);
+      aggs.push_back(a);
+    }
+    q.filters = filters.empty() ? nullptr : filters.data();
+    q.or_group_sizes = or_sizes.empty() ? nullptr : or_sizes.data();
+    q.or_filters = or_filters.empty() ? nullptr : or_filters.data();
+    q.group_by = group_by.empty() ? nullptr : group_by.data();
+    q.aggregates = aggs.empty() ? nullptr : aggs.data();
+  }
+};
+
 }  // namespace
 
 struct qm_batch {
@@ -2340,6 +2428,8 @@ struct qm_batch {
   std::vector<qm_bq> bq;
   std::vector<int64_t> rows;
   std::vector<int64_t> est;  // planner's group estimate per query
+  std::vector<const qm_table *> tabs;  // query i's table and a copy of the
+  std::vector<std::unique_ptr<OwnedQuery>> queries;  // query, to rerun it alone
   DevBuf arena, d_bq, d_slot0, d_chunks, d_counter, d_status, d_bitmap, d_popc, d_ranks, d_temp, d_meta,
       d_packed, d_nullbytes;
   HostBuf h_meta, h_status;
@@ -2503,6 +2593,9 @@ void batch_reset(qm_batch *b, int n) {
   b->bq.assign(n, qm_bq());
   b->rows.assign(n, 0);
   b->est.assign(n, 1);
+  b->tabs.assign(n, nullptr);
+  b->queries.clear();
+  b->queries.resize(n);  // null until planned
   b->total_rows = 0;
   b->bytes_scanned = 0;
   drop_graph(b);
@@ -2513,6 +2606,9 @@ void batch_reset(qm_batch *b, int n) {
 int batch_plan_one(qm_batch *b, int i, const qm_table *table, const qm_query *query) {
   qm_ctx *ctx = b->ctx;
   if (!table || !query) return set_err(ctx, QM_ERR_INVALID, "query %d: null table or query", i);
+  b->tabs[i] = table;
+  b->queries[i].reset(new OwnedQuery());
+  b->queries[i]->copy(*query);
   qm_query q = *query;
   q.flags &= ~QM_FLAG_UNORDERED;  // the batched finalize always orders by first row
   qm_table *t = const_cast<qm_table *>(table);
@@ -2694,6 +2790,12 @@ int qm_batch_run(qm_batch *b, qm_result **results) {
   std::vector<int> codes(b->n, QM_OK);
   int rc = batch_execute(b, results, codes.data(), true);
   if (rc) return rc;
+  for (int i = 0; i < b->n; i++)
+    if (codes[i] == QM_ERR_CAPACITY) {
+      // more groups than the batched table was sized for: this query alone,
+      // where its table regrows
+      codes[i] = qm_query_run(b->ctx, b->tabs[i], &b->queries[i]->q, &results[i]);
+    }
   for (int i = 0; i < b->n; i++)
     if (codes[i] != QM_OK) {
       for (int k = 0; k < b->n; k++) {

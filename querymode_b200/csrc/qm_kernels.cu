@@ -248,6 +248,20 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
   }
 }
 
+// Filter pass count over a strided sample of rows (row i*n/n_samples):
+// planning sizes a filtered query's group table by min(distinct keys,
+// selected rows), and the sample bounds the selected rows.
+__global__ void qm_sample_pred(const __grid_constant__ qm_pred P, int64_t n, int n_samples,
+                               unsigned long long *count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t r = i < n_samples ? (int64_t)i * n / n_samples : 0;
+  uint32_t m = i < n_samples ? 1u : 0u;
+  auto rowf = [&](int) { return r; };
+  m = eval_pred(P, rowf, m);
+  const unsigned b = __ballot_sync(QM_FULL, m & 1u);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, (unsigned long long)__popc(b));
+}
+
 __global__ void qm_init_table(uint64_t *t, int64_t n_slots_total, int stride, int hash_keys,
                               const __grid_constant__ qm_aggspec A) {
   const int64_t n = n_slots_total * stride;
@@ -547,6 +561,14 @@ cudaError_t qm_launch_check_selection(const uint32_t *sel, int64_t n_sel, int64_
   if (n_sel <= 0) return cudaSuccess;
   int blocks = (int)std::min<int64_t>((n_sel + 255) / 256, (int64_t)sm_count * 4);
   qm_check_selection<<<blocks, 256, 0, stream>>>(sel, n_sel, n_rows, st);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_sample_pred(const qm_pred &P, int64_t n, int n_samples, unsigned long long *count,
+                                  cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess || n <= 0 || n_samples <= 0) return e;
+  qm_sample_pred<<<(n_samples + 255) / 256, 256, 0, st>>>(P, n, n_samples, count);
   return cudaGetLastError();
 }
 

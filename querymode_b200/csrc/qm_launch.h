@@ -32,6 +32,8 @@ cudaError_t qm_launch_select_write(int64_t n_tiles, const uint32_t *sel, const u
                                    cudaStream_t st);
 cudaError_t qm_launch_minmax(const void *p, int dtype, const uint32_t *nulls, int64_t n, long long *out,
                              int sm_count, cudaStream_t st);
+cudaError_t qm_launch_sample_pred(const qm_pred &P, int64_t n, int n_samples, unsigned long long *count,
+                                  cudaStream_t st);
 cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st);
 cudaError_t qm_launch_rehash(const uint64_t *old_t, int64_t old_cap, int stride, int count_word, uint64_t *new_t,
                              int log2cap, qm_status *st, int sm_count, cudaStream_t stream);

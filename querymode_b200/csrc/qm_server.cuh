@@ -4,60 +4,12 @@
 // that file's internal planning / layout / execution steps.
 #include <chrono>
 #include <condition_variable>
-#include <deque>
 #include <thread>
 #include <unordered_map>
 
 namespace {
 
 using srv_clock = std::chrono::steady_clock;
-
-// A deep copy of a qm_query (the caller's strings and arrays may go away
-// once submit returns).
-struct OwnedQuery {
-  std::deque<std::string> strs;  // deque: stable addresses
-  std::vector<qm_filter> filters, or_filters;
-  std::vector<int32_t> or_sizes;
-  std::vector<const char *> group_by;
-  std::vector<qm_aggregate> aggs;
-  qm_query q{};
-
-  const char *keep(const char *p) {
-    if (!p) return nullptr;
-    strs.emplace_back(p);
-    return strs.back().c_str();
-  }
-  void copy(const qm_query &src) {
-    q = src;
-    for (int i = 0; i < src.n_filters; i++) {
-      qm_filter f = src.filters[i];
-      f.column = keep(f.column);
-      filters.push_back(f);
-    }
-    int64_t n_or = 0;
-    for (int g = 0; g < src.n_or_groups; g++) {
-      or_sizes.push_back(src.or_group_sizes[g]);
-      n_or += src.or_group_sizes[g];
-    }
-    for (int64_t i = 0; i < n_or; i++) {
-      qm_filter f = src.or_filters[i];
-      f.column = keep(f.column);
-      or_filters.push_back(f);
-    }
-    for (int i = 0; i < src.n_group_by; i++) group_by.push_back(keep(src.group_by[i]));
-    for (int i = 0; i < src.n_aggregates; i++) {
-      qm_aggregate a = src.aggregates[i];
-      a.column = keep(a.column);
-      a.alias = keep(a.alias);
-      aggs.push_back(a);
-    }
-    q.filters = filters.empty() ? nullptr : filters.data();
-    q.or_group_sizes = or_sizes.empty() ? nullptr : or_sizes.data();
-    q.or_filters = or_filters.empty() ? nullptr : or_filters.data();
-    q.group_by = group_by.empty() ? nullptr : group_by.data();
-    q.aggregates = aggs.empty() ? nullptr : aggs.data();
-  }
-};
 
 enum ReqState { RQ_QUEUED, RQ_RUNNING, RQ_DONE };
 

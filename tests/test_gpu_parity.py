@@ -347,3 +347,27 @@ def test_per_warp_tables_large(ctx):
         g = t.run(q)
         r = oracle.run(cols, q, threads=8)
         assert_same(g, r)
+
+
+def test_selective_filter_sampled_estimate(ctx):
+    # a selective filter over a wide key range: the group table is sized from
+    # a strided sample of the predicate (and a sparse dense range turns into
+    # a hash table); sorted and clustered filter columns included
+    rng = np.random.default_rng(33)
+    n = 3_000_000
+    cols = {"key": rng.integers(0, 1 << 22, n).astype(np.int64),
+            "flag": (rng.random(n) < 0.01).astype(np.int32),
+            "ts": np.sort(rng.integers(0, 1 << 40, n)).astype(np.int64),
+            "v": rng.normal(size=n)}
+    t = ctx.table(cols)
+    qs = [QueryDescriptor(filters=[FilterOp("flag", "eq", 1)], group_by=["key"],
+                          aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")]),
+          QueryDescriptor(filters=[FilterOp("ts", "lt", int(cols["ts"][n // 50]))], group_by=["key"],
+                          aggregates=[AggregateOp("max", "v"), AggregateOp("count", "*")]),
+          QueryDescriptor(filters=[FilterOp("ts", "gte", int(cols["ts"][n - n // 30]))], group_by=["key"],
+                          aggregates=[AggregateOp("min", "v"), AggregateOp("avg", "v")])]
+    for q in qs:
+        g = t.run(q)
+        assert_same(g, oracle.run(cols, q, threads=8))
+        assert g.stats.retries == 0
+        assert g.stats.table_capacity <= 18  # a hash table of at most 2^18 slots
