@@ -12,13 +12,14 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libqm_gpu.so")
-SOURCES = ["qm_api.cu", "qm_kernels.cu", "qm_batch.cu"]
-HEADERS = ["qm_plan.h", "qm_launch.h", "qm_kernels.cuh", "qm_batch.h",
-           os.path.join("..", "..", "include", "qm_gpu.h")]
+SOURCES = ["qm_api.cu", "qm_kernels.cu", "qm_batch.cu"] + [f"qm_scan_nv{n}.cu" for n in range(5)]
+HEADERS = ["qm_plan.h", "qm_launch.h", "qm_kernels.cuh", "qm_batch.h", "qm_scan.cuh", "qm_scan_spec.cuh",
+           "qm_server.cuh", os.path.join("..", "..", "include", "qm_gpu.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -51,15 +52,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
     vers = os.path.join(build_dir, "exports.map")
     with open(vers, "w") as f:
         f.write("{ global: qm_*; local: *; };\n")
-    objs = []
     nvcc = _nvcc()
+    cmds = []
     for s in SOURCES:
         obj = os.path.join(build_dir, s.replace(".cu", ".o"))
-        cmd = [nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, s), "-o", obj]
+        cmds.append((obj, [nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, s), "-o", obj]))
+    objs = [o for o, _ in cmds]
+
+    def compile_one(cmd):
         if verbose:
-            print(" ".join(cmd))
+            print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    # translation units compile in parallel (the scan kernel's specialised
+    # instantiations are spread over several of them)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(compile_one, c) for _, c in cmds]:
+            f.result()
     tmp = OUT + ".tmp"
     cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static",
            "-Xlinker", f"--version-script={vers}", "-o", tmp, *objs]

@@ -419,8 +419,27 @@ __device__ __forceinline__ uint32_t eval_pred(const qm_pred &P, const ROWS &row,
 // ---- group keys -------------------------------------------------------------
 // Key word of one row.  special: 0 ordinary, 1 the key equals the empty-slot
 // sentinel (hash mode), 2 NULL key.
+// Key kinds a scan kernel can be specialised for (KK): 0 any plan; 1 one
+// int64 column without NULLs; 2 one int32 column without NULLs; 3 no GROUP BY.
+#define QM_KK_ANY 0
+#define QM_KK_I64 1
+#define QM_KK_I32 2
+#define QM_KK_NONE 3
+// Value-column counts (NV): 0..QM_MAX_VCOLS exactly, or QM_NV_ANY (read the
+// plan's n_vcols at run time).
+#define QM_NV_ANY (QM_MAX_VCOLS + 1)
+#define QM_NV_BOUND(NV) ((NV) > QM_MAX_VCOLS ? QM_MAX_VCOLS : (NV))
+
+template <int KK = QM_KK_ANY>
 __device__ __forceinline__ uint64_t row_key(const qm_keyspec &K, int64_t r, int &special) {
   special = 0;
+  if (KK == QM_KK_NONE) return 0;
+  if (KK == QM_KK_I64 || KK == QM_KK_I32) {
+    const uint64_t k = KK == QM_KK_I64 ? (uint64_t)ldcs<long long>(K.data[0], r)
+                                       : (uint64_t)(int64_t)ldcs<int>(K.data[0], r);
+    if (K.mode == QK_HASH && k == QM_EMPTY_KEY) special = 1;
+    return k;
+  }
   if (K.n_cols == 0) return 0;
   uint64_t k;
   if (K.pack == QP_CONCAT) {
@@ -579,6 +598,14 @@ __device__ __forceinline__ uint64_t pick(const uint64_t (&v)[QM_MAX_VCOLS], int 
   for (int c = 0; c < QM_MAX_VCOLS; ++c)
     if (c == i) r = v[c];
   return r;
+}
+
+// Value cell c of a row: a plain register when the kernel knows the column
+// count (c is then a compile-time index), else a select over the array.
+template <int NV>
+__device__ __forceinline__ uint64_t vget(const uint64_t (&vb)[QM_MAX_VCOLS], int c) {
+  if constexpr (NV > QM_MAX_VCOLS) return pick(vb, c);
+  else return vb[c];
 }
 
 // Monotone updates: the word only ever decreases (min) or increases (max),
@@ -839,6 +866,7 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
 #ifndef QM_GLOBAL_READ_TEST
 #define QM_GLOBAL_READ_TEST 0
 #endif
+template <int NV = QM_NV_ANY>
 __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
                                         uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
   // In the global table, the FIRST word and the MIN / MAX words of the first
@@ -879,8 +907,8 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
     }
   };
 #pragma unroll
-  for (int c = 0; c < QM_MAX_VCOLS; ++c) {
-    if (c >= A.n_vcols) break;
+  for (int c = 0; c < QM_NV_BOUND(NV); ++c) {
+    if (NV > QM_MAX_VCOLS && c >= A.n_vcols) break;
     if ((vnull >> c) & 1) continue;
     const qm_vcol &vc = A.vcol[c];
     const int f = vc.flags;
@@ -917,13 +945,16 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
 // contributions through the warp's shared scratch, and the group leader adds
 // them once; MIN / MAX / FIRST stay per lane (64-bit min/max atomics resolve
 // conflicts in hardware, and most are skipped by the read test).
+template <int NV = QM_NV_ANY>
 __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp, int L, unsigned lmask, unsigned peers,
                                                int lane, uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS],
                                                uint32_t vnull, uint64_t *scr) {
   const bool leader = lane == __ffs(peers) - 1;
   if (leader) atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)A.w_count * L), (unsigned long long)__popc(peers));
   if (A.w_first >= 0) min_u64(tp + (int64_t)A.w_first * L, grow);
-  for (int c = 0; c < A.n_vcols; ++c) {
+  const int nv = NV > QM_MAX_VCOLS ? A.n_vcols : NV;
+#pragma unroll
+  for (int c = 0; c < nv; ++c) {
     const qm_vcol &vc = A.vcol[c];
     const int f = vc.flags;
     const bool valid = !((vnull >> c) & 1);
@@ -932,7 +963,7 @@ __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp
       if (leader && nn) atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)vc.w_nn * L), (unsigned long long)nn);
     }
     const bool isint = vc.dtype == QM_I32 || vc.dtype == QM_I64;
-    const uint64_t raw = pick(vb, c);
+    const uint64_t raw = vget<NV>(vb, c);
     if (f & VF_SUM) {
       uint64_t *w0 = tp + (int64_t)vc.w_sum * L;
       if (isint) {
@@ -1003,13 +1034,14 @@ __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp
 }
 
 // Gather a row's value cells (float32 widened to double, as JS numbers).
+template <int NV = QM_NV_ANY>
 __device__ __forceinline__ void gather_values(const qm_aggspec &A, int64_t row, uint64_t (&vb)[QM_MAX_VCOLS],
                                               uint32_t &vnull) {
   vnull = 0;
 #pragma unroll
   for (int c = 0; c < QM_MAX_VCOLS; ++c) {
     vb[c] = 0;
-    if (c < A.n_vcols) {
+    if (c < QM_NV_BOUND(NV) && (NV <= QM_MAX_VCOLS || c < A.n_vcols)) {
       const qm_vcol &vc = A.vcol[c];
       if (cell_null(vc.nulls, row)) vnull |= 1u << c;
       else if (vc.dtype == QM_I32 || vc.dtype == QM_I64) vb[c] = (uint64_t)ld_int(vc.data, vc.dtype, row);
@@ -1097,7 +1129,7 @@ __device__ __forceinline__ void merge_plain(const qm_aggspec &A, uint64_t *dst, 
 // Aggregates one survivor per lane (lanes with active = false sit out).
 // DD: 0 / 1 = the plan's dedupe flag fixed at compile time (separate kernels
 // keep each path's registers and code apart), 2 = read it from the plan.
-template <int DD = 2>
+template <int DD = 2, int NV = QM_NV_ANY, int KK = QM_KK_ANY>
 __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
                                             int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
   const qm_aggspec &A = a.agg;
@@ -1106,10 +1138,10 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
     if (!active) return;
     const uint64_t grow = (uint64_t)(a.row_offset + row);
     int special;
-    const uint64_t key = row_key(a.key, row, special);
+    const uint64_t key = row_key<KK>(a.key, row, special);
     uint64_t vb[QM_MAX_VCOLS];
     uint32_t vnull;
-    gather_values(A, row, vb, vnull);
+    gather_values<NV>(A, row, vb, vnull);
     unsigned peers = __match_any_sync(act, key);
     if (__any_sync(act, special != 0)) peers &= __match_any_sync(act, special);
     const bool leader = lane == __ffs(peers) - 1;
@@ -1142,8 +1174,8 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
   int ls = -1;
   if (active) {
     grow = (uint64_t)(a.row_offset + row);
-    key = row_key(a.key, row, special);
-    gather_values(A, row, vb, vnull);
+    key = row_key<KK>(a.key, row, special);
+    gather_values<NV>(A, row, vb, vnull);
     if (L > 0) {
       if (!a.local_hash) ls = (int)global_slot(a, key, special);
       else if (special == 0) ls = local_find(lkeys, L, key, l_used);
@@ -1155,11 +1187,11 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
   if (loc) peers = __match_any_sync(lmask, ls);
   const bool merge = __any_sync(QM_FULL, (peers & (peers - 1)) != 0);
   if (loc) {
-    if (merge) agg_row_merged(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr);
-    else agg_row(A, lw + ls, L, true, grow, vb, vnull);
+    if (merge) agg_row_merged<NV>(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr);
+    else agg_row<NV>(A, lw + ls, L, true, grow, vb, vnull);
   } else if (active && !(L > 0 && !a.local_hash)) {
     const int64_t gs = global_slot(a, key, special);
-    if (gs >= 0) agg_row(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull);
+    if (gs >= 0) agg_row<NV>(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull);
   }
 }
 

@@ -9,6 +9,21 @@
 #define QM_SCAN_THREADS 512
 #define QM_HLL_P 12
 
+// Scan kernels specialised for N = 0..QM_SPEC_NV_MAX value columns
+// (qm_scan_nvN.cu): dynamic shared memory limit of each, and the launch of
+// the one for (dedupe flag, key kind QM_KK_*).
+#define QM_SPEC_NV_MAX 4
+#define QM_DECL_SPEC(N)                                                                        \
+  cudaError_t qm_scan_nv##N##_attr(int max_smem);                                           \
+  cudaError_t qm_scan_nv##N##_launch(const qm_scan_args &a, int dd, int kk, int blocks, size_t smem, \
+                                     cudaStream_t st);
+QM_DECL_SPEC(0)
+QM_DECL_SPEC(1)
+QM_DECL_SPEC(2)
+QM_DECL_SPEC(3)
+QM_DECL_SPEC(4)
+#undef QM_DECL_SPEC
+
 size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth,
                           int priv);
 cudaError_t qm_scan_configure(size_t smem_bytes, bool staged, int *blocks_per_sm);
