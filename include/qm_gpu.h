@@ -255,6 +255,32 @@ int qm_agg_push(qm_agg *agg, int64_t n_rows, int32_t n_cols,
 int qm_agg_finish(qm_agg *agg, qm_result **out);
 int qm_agg_destroy(qm_agg *agg);
 
+/* Push every row of a registered table as one batch (its columns are read
+ * in place and its cached column statistics are used).  Same semantics as
+ * qm_agg_push of those columns without a selection. */
+int qm_agg_push_table(qm_agg *agg, const qm_table *table);
+
+/* Partial group states across shards (multi-GPU).  The reference fans a
+ * query out to fragment DOs and merges their partial aggregates
+ * (src/query-do.ts:1747-1887, mergePartialAggs src/partial-agg.ts:277-304);
+ * here each GPU streams its shard through its own qm_agg, exports the
+ * occupied group slots as partial rows in device memory, and one GPU merges
+ * the others' rows into its aggregation before qm_agg_finish.
+ *
+ * A partial row is *row_words 64-bit words: the group's key word, its
+ * special flag (0; 1 key equal to the empty-slot sentinel; 2 NULL key) and
+ * the aggregation's accumulator words.  Shards of one query over one schema
+ * produce the same layout.  row_offset = the shard's first global row: FIRST
+ * (first-seen order) moves by it.  With dst null only *n_groups and
+ * *row_words are returned.  dst / src are device memory of this context's
+ * GPU (copy other GPUs' rows in first: NCCL all-gather, peer copy). */
+int qm_agg_partial_export(qm_agg *agg, int64_t row_offset, uint64_t *dst, int64_t capacity_rows,
+                          int64_t *n_groups, int32_t *row_words);
+/* rows_end: one past the last global row the partial covers (bounds the
+ * first-seen sort). */
+int qm_agg_partial_merge(qm_agg *agg, const uint64_t *src, int64_t n_groups, int32_t row_words,
+                         int64_t rows_end);
+
 /* ---- filter-only selection (FilterOperator / WASM filter drop-in) ------- */
 /* Evaluate the filters of `query` (aggregates and group_by ignored) over one
  * batch — over the rows listed by `selection` (ascending, n_selected) when it

@@ -148,6 +148,10 @@ SIGNATURES = [
                               C.POINTER(C.c_uint32), C.c_int64]),
     ("qm_agg_finish", C.c_int, [_P, _PP]),
     ("qm_agg_destroy", C.c_int, [_P]),
+    ("qm_agg_push_table", C.c_int, [_P, _P]),
+    ("qm_agg_partial_export", C.c_int, [_P, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_int32)]),
+    ("qm_agg_partial_merge", C.c_int, [_P, C.c_void_p, C.c_int64, C.c_int32, C.c_int64]),
     ("qm_filter_select", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn),
                                    C.POINTER(QmQuery), C.POINTER(C.c_uint32), C.c_int64,
                                    C.POINTER(C.c_uint32), C.c_int64, C.POINTER(C.c_int64)]),

@@ -100,6 +100,7 @@ struct qm_ctx {
   // grow-only scratch reused across runs of this context
   DevBuf table, status, keys, slots, keys2, slots2, sort_temp, counter, out, hll;
   DevBuf masks, counts, offsets, sel_out, sel_in;
+  DevBuf agg_spare;  // group table of a destroyed qm_agg, reused by the next one
   std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
   HostBuf hout, hstatus;
   std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
@@ -1281,6 +1282,7 @@ int setup_table(qm_ctx *ctx, GroupTable &gt, int64_t est_groups, int64_t direct_
   choose_layout(pl, est_groups, ex, ctx->tuning);
   size_t bytes = (size_t)ex.total_slots * ex.stride * 8;
   DevBuf &buf = owned ? gt.own : ctx->table;
+  if (owned && !buf.p && ctx->agg_spare.bytes >= bytes) std::swap(buf, ctx->agg_spare);
   int rc = ensure(ctx, buf, bytes);
   if (rc) return rc;
   gt.table = (uint64_t *)buf.p;
@@ -1510,7 +1512,7 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   DevBuf *bufs[] = {&ctx->table, &ctx->status, &ctx->keys, &ctx->slots, &ctx->keys2, &ctx->slots2,
                     &ctx->sort_temp, &ctx->counter, &ctx->out, &ctx->hll, &ctx->masks, &ctx->counts,
-                    &ctx->offsets, &ctx->sel_out, &ctx->sel_in};
+                    &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare};
   for (DevBuf *b : bufs) release(*b);
   for (auto &b : ctx->staged) release(b);
   if (ctx->hout.p) cudaFreeHost(ctx->hout.p);
@@ -1845,6 +1847,86 @@ int grow_table(qm_ctx *ctx, GroupTable &gt, int64_t upper) {
   return QM_OK;
 }
 
+// Distinct-key estimate of a streamed batch: the key column's cached
+// HyperLogLog when it has one (a registered table's column), else a sketch
+// of this batch.
+int key_estimate(qm_ctx *ctx, const Plan &pl, int64_t n_rows, double *e) {
+  if (pl.key.n_cols == 1 && pl.keycols[0]) {
+    DevCol &kc = *const_cast<DevCol *>(pl.keycols[0]);
+    if (kc.has_hll) {
+      *e = kc.hll;
+      return QM_OK;
+    }
+    int rc = estimate_groups(ctx, pl.key, n_rows, e);
+    if (!rc) {
+      kc.hll = *e;
+      kc.has_hll = true;
+    }
+    return rc;
+  }
+  return estimate_groups(ctx, pl.key, n_rows, e);
+}
+
+// One pushed batch (columns in env) through the aggregation's table.
+int agg_push_env(qm_agg *a, const ColEnv &env, int64_t n_rows, const uint32_t *dsel, int64_t n_elems) {
+  qm_ctx *ctx = a->ctx;
+  int rc;
+  GroupTable &gt = a->gt;
+  Plan pl;
+  if ((rc = plan_query(ctx, &a->q, env, pl))) return rc;
+  uint64_t space = 0;
+  if ((rc = plan_key_packing(ctx, pl, n_rows, false, &space))) return rc;
+  pl.key.mode = pl.key.n_cols == 0 ? QK_NONE : QK_HASH;
+  if (!a->planned) {
+    gt.pl = pl;
+    int64_t est = 1;
+    if (pl.key.mode == QK_HASH) {
+      est = n_elems;
+      if (n_elems > (1 << 16)) {
+        double e;
+        if ((rc = key_estimate(ctx, pl, n_rows, &e))) return rc;
+        est = std::min<int64_t>(est, (int64_t)(e * 1.1) + 1024);
+      }
+    }
+    if ((rc = setup_table(ctx, gt, std::max<int64_t>(est, 1), 0, true))) return rc;
+    a->planned = true;
+  } else {
+    // same structure, this batch's column pointers
+    pl.key.base = gt.pl.key.base;
+    gt.pl.pred = pl.pred;
+    gt.pl.agg = pl.agg;
+    memcpy(gt.pl.key.data, pl.key.data, sizeof pl.key.data);
+    memcpy(gt.pl.key.nulls, pl.key.nulls, sizeof pl.key.nulls);
+    if (gt.pl.key.mode == QK_HASH) {
+      int64_t add = n_elems;
+      if (n_elems > (1 << 16)) {
+        double e;
+        if ((rc = key_estimate(ctx, pl, n_rows, &e))) return rc;
+        add = std::min<int64_t>(add, (int64_t)(e * 1.1) + 1024);
+      }
+      if ((rc = grow_table(ctx, gt, gt.groups_upper + add))) return rc;
+    }
+  }
+  CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  if ((rc = run_scan(ctx, gt, n_elems, dsel))) return rc;
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  qm_status st;
+  if ((rc = read_status(ctx, &st))) return rc;
+  take_scan_time(ctx, gt, true);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  a->device_ms += ms;
+  if (st.error) {
+    a->failed = true;
+    return set_err(ctx, QM_ERR_CUDA, "group table overflow in a streamed batch (device status %d)", st.error);
+  }
+  gt.groups_upper += (int64_t)st.groups_inserted;
+  gt.selected += st.rows_selected;
+  gt.rows_done += n_rows;
+  return QM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1929,60 +2011,21 @@ int qm_agg_push(qm_agg *a, int64_t n_rows, int32_t n_cols, const qm_column *cols
   const int64_t n_elems = selection ? n_selected : n_rows;
   ColEnv env;
   for (auto &c : dcols) env.views.push_back({&c, n_rows});
-  GroupTable &gt = a->gt;
-  Plan pl;
-  if ((rc = plan_query(ctx, &a->q, env, pl))) return rc;
-  uint64_t space = 0;
-  if ((rc = plan_key_packing(ctx, pl, n_rows, false, &space))) return rc;
-  pl.key.mode = pl.key.n_cols == 0 ? QK_NONE : QK_HASH;
-  if (!a->planned) {
-    gt.pl = pl;
-    int64_t est = 1;
-    if (pl.key.mode == QK_HASH) {
-      est = n_elems;
-      if (n_elems > (1 << 16)) {
-        double e;
-        if ((rc = estimate_groups(ctx, pl.key, n_rows, &e))) return rc;
-        est = std::min<int64_t>(est, (int64_t)(e * 1.1) + 1024);
-      }
-    }
-    if ((rc = setup_table(ctx, gt, std::max<int64_t>(est, 1), 0, true))) return rc;
-    a->planned = true;
-  } else {
-    // same structure, this batch's column pointers
-    pl.key.base = gt.pl.key.base;
-    gt.pl.pred = pl.pred;
-    gt.pl.agg = pl.agg;
-    memcpy(gt.pl.key.data, pl.key.data, sizeof pl.key.data);
-    memcpy(gt.pl.key.nulls, pl.key.nulls, sizeof pl.key.nulls);
-    if (gt.pl.key.mode == QK_HASH) {
-      int64_t add = n_elems;
-      if (n_elems > (1 << 16)) {
-        double e;
-        if ((rc = estimate_groups(ctx, gt.pl.key, n_rows, &e))) return rc;
-        add = std::min<int64_t>(add, (int64_t)(e * 1.1) + 1024);
-      }
-      if ((rc = grow_table(ctx, gt, gt.groups_upper + add))) return rc;
-    }
-  }
-  CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
-  CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  if ((rc = run_scan(ctx, gt, n_elems, dsel))) return rc;
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  qm_status st;
-  if ((rc = read_status(ctx, &st))) return rc;
-  take_scan_time(ctx, gt, true);
-  float ms = 0;
-  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  a->device_ms += ms;
-  if (st.error) {
-    a->failed = true;
-    return set_err(ctx, QM_ERR_CUDA, "group table overflow in a streamed batch (device status %d)", st.error);
-  }
-  gt.groups_upper += (int64_t)st.groups_inserted;
-  gt.selected += st.rows_selected;
-  gt.rows_done += n_rows;
-  return QM_OK;
+  return agg_push_env(a, env, n_rows, dsel, n_elems);
+}
+
+int qm_agg_push_table(qm_agg *a, const qm_table *table) {
+  if (!a || !table) return QM_ERR_INVALID;
+  qm_ctx *ctx = a->ctx;
+  if (a->failed) return set_err(ctx, QM_ERR_INVALID, "aggregation already failed");
+  if (table->ctx != ctx) return set_err(ctx, QM_ERR_INVALID, "table of another context");
+  if (table->n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
+  cudaSetDevice(ctx->device);
+  if (!a->planned)
+    for (auto &c : table->cols) a->schema.push_back({c.name, c.dtype});
+  ColEnv env;
+  for (auto &c : table->cols) env.views.push_back({&c, table->n_rows});
+  return agg_push_env(a, env, table->n_rows, nullptr, table->n_rows);
 }
 
 int qm_agg_finish(qm_agg *a, qm_result **out) {
@@ -2016,8 +2059,73 @@ int qm_agg_destroy(qm_agg *a) {
   if (!a) return QM_OK;
   cudaSetDevice(a->ctx->device);
   cudaStreamSynchronize(a->ctx->stream);
+  // keep the larger of this table and the spare for the next aggregation
+  if (a->gt.own.bytes > a->ctx->agg_spare.bytes) std::swap(a->gt.own, a->ctx->agg_spare);
   release(a->gt.own);
   delete a;
+  return QM_OK;
+}
+
+int qm_agg_partial_export(qm_agg *a, int64_t row_offset, uint64_t *dst, int64_t capacity_rows, int64_t *n_groups,
+                          int32_t *row_words) {
+  if (!a || !n_groups || !row_words || row_offset < 0 || (dst && capacity_rows < 0)) return QM_ERR_INVALID;
+  qm_ctx *ctx = a->ctx;
+  if (a->failed) return set_err(ctx, QM_ERR_INVALID, "aggregation failed earlier");
+  if (!a->planned) return set_err(ctx, QM_ERR_INVALID, "partial export before the first push");
+  cudaSetDevice(ctx->device);
+  GroupTable &gt = a->gt;
+  const Exec &ex = gt.ex;
+  *row_words = ex.stride + 1;
+  int64_t G = 1;
+  const uint32_t *slots = nullptr;
+  if (gt.pl.key.mode != QK_NONE) {
+    int rc;
+    if ((rc = ensure(ctx, ctx->keys, ex.total_slots * 8)) || (rc = ensure(ctx, ctx->slots, ex.total_slots * 4)) ||
+        (rc = ensure(ctx, ctx->counter, 64)) || (rc = ensure_host(ctx, ctx->hstatus, 64)))
+      return rc;
+    CK(cudaMemsetAsync(ctx->counter.p, 0, 8, ctx->stream));
+    CK(qm_launch_compact(gt.table, ex.total_slots, ex.stride, gt.pl.agg.acc[gt.pl.agg.acc_count].word, -1,
+                         (uint64_t *)ctx->keys.p, (uint32_t *)ctx->slots.p, (unsigned long long *)ctx->counter.p,
+                         ctx->sm_count, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->counter.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    G = (int64_t)*(unsigned long long *)ctx->hstatus.p;
+    slots = (const uint32_t *)ctx->slots.p;
+  }
+  *n_groups = G;
+  if (!dst) return QM_OK;
+  if (G > capacity_rows) return set_err(ctx, QM_ERR_CAPACITY, "partial has %lld groups, room for %lld", (long long)G,
+                                        (long long)capacity_rows);
+  CK(qm_launch_export_partial(gt.table, ex.stride, slots, G, ex.n_slots, gt.pl.key.mode, gt.pl.agg, row_offset, dst,
+                              ctx->sm_count, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return QM_OK;
+}
+
+int qm_agg_partial_merge(qm_agg *a, const uint64_t *src, int64_t n_groups, int32_t row_words, int64_t rows_end) {
+  if (!a || (n_groups > 0 && !src) || n_groups < 0 || rows_end < 0) return QM_ERR_INVALID;
+  qm_ctx *ctx = a->ctx;
+  if (a->failed) return set_err(ctx, QM_ERR_INVALID, "aggregation failed earlier");
+  if (!a->planned) return set_err(ctx, QM_ERR_INVALID, "partial merge before the first push");
+  GroupTable &gt = a->gt;
+  if (row_words != gt.ex.stride + 1)
+    return set_err(ctx, QM_ERR_INVALID, "partial rows of %d words; this aggregation's are %d", row_words,
+                   gt.ex.stride + 1);
+  cudaSetDevice(ctx->device);
+  int rc;
+  if (gt.pl.key.mode == QK_HASH && (rc = grow_table(ctx, gt, gt.groups_upper + n_groups))) return rc;
+  qm_scan_args args;
+  fill_args(gt, args, (qm_status *)ctx->status.p);
+  CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
+  CK(qm_launch_merge_partial(args, src, n_groups, ctx->sm_count, ctx->stream));
+  qm_status st;
+  if ((rc = read_status(ctx, &st))) return rc;
+  if (st.error) {
+    a->failed = true;
+    return set_err(ctx, QM_ERR_CUDA, "group table overflow while merging a partial (device status %d)", st.error);
+  }
+  gt.groups_upper += (int64_t)st.groups_inserted;
+  gt.rows_done = std::max(gt.rows_done, rows_end);
   return QM_OK;
 }
 

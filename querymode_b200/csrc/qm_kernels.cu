@@ -15,6 +15,79 @@
 
 namespace qm {
 
+// ---- partial group states across shards (multi-GPU) --------------------------
+// A partial row is [key word, special (0, 1 = sentinel-valued key, 2 = NULL
+// key), accumulator words].  Export moves FIRST / FZERO by the shard's first
+// global row, so merged tables keep the global first-seen order.
+__global__ void qm_export_partial(const uint64_t *t, int stride, const uint32_t *slots, int64_t G, int64_t n_slots,
+                                  int key_mode, const __grid_constant__ qm_aggspec A, int64_t row_offset,
+                                  uint64_t *dst) {
+  const int rw = stride + 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = slots ? (int64_t)slots[i] : 0;
+    const uint64_t *w = t + s * stride;
+    uint64_t *o = dst + i * rw;
+    int special = 0;
+    if (key_mode == QK_HASH) special = s == n_slots ? 1 : (s == n_slots + 1 ? 2 : 0);
+    o[0] = key_mode == QK_NONE ? 0 : (special == 1 ? QM_EMPTY_KEY : (special == 2 ? 0 : w[0]));
+    o[1] = (uint64_t)special;
+    for (int k = 0; k < A.n_words; ++k) o[2 + k] = w[1 + k];
+    for (int k = 0; k < A.n_accs; ++k) {
+      const qm_acc ac = A.acc[k];
+      uint64_t &v = o[2 + ac.word];
+      if (ac.kind == QA_FIRST && v != ~0ULL) v += (uint64_t)row_offset;
+      if (ac.kind == QA_FZERO && v != ~0ULL) v += (uint64_t)row_offset << 1;
+    }
+  }
+}
+
+// Fold partial rows into the group table (slots found / claimed as in the
+// scan); integer sums are 128-bit, float sums compensated (TwoSum).
+__global__ void qm_merge_partial(const __grid_constant__ qm_scan_args a, const uint64_t *src, int64_t n) {
+  const qm_aggspec &A = a.agg;
+  const int rw = a.stride + 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t *row = src + i * rw;
+    const int64_t gs = global_slot(a, row[0], (int)row[1]);
+    if (gs < 0) continue;
+    uint64_t *gp = a.table + gs * a.stride + 1;
+    const uint64_t *v = row + 2;
+    for (int k = 0; k < A.n_accs; ++k) {
+      const qm_acc ac = A.acc[k];
+      const uint64_t v0 = v[ac.word];
+      uint64_t *g0 = gp + ac.word, *g1 = gp + ac.word + 1;
+      switch (ac.kind) {
+        case QA_COUNT:
+        case QA_NN:
+          if (v0) atomicAdd(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
+          break;
+        case QA_FIRST:
+        case QA_FZERO:
+          if (v0 != ~0ULL) atomicMin(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
+          break;
+        case QA_ISUM:
+          if (ac.narrow) {
+            if (v0) atomicAdd(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
+          } else if (v0 || v[ac.word + 1]) {
+            add128(g0, g1, v0, (int64_t)v[ac.word + 1]);
+          }
+          break;
+        case QA_FSUM:
+          fsum_add(g0, g1, __longlong_as_double((long long)v0), __longlong_as_double((long long)v[ac.word + 1]));
+          break;
+        case QA_IMIN:
+        case QA_FMIN:
+          if ((int64_t)v0 != (int64_t)A.init[ac.word]) atomicMin(reinterpret_cast<long long *>(g0), (long long)v0);
+          break;
+        case QA_IMAX:
+        case QA_FMAX:
+          if ((int64_t)v0 != (int64_t)A.init[ac.word]) atomicMax(reinterpret_cast<long long *>(g0), (long long)v0);
+          break;
+      }
+    }
+  }
+}
+
 // Filter pass count over a strided sample of rows (row i*n/n_samples):
 // planning sizes a filtered query's group table by min(distinct keys,
 // selected rows), and the sample bounds the selected rows.
@@ -372,6 +445,23 @@ cudaError_t qm_launch_check_selection(const uint32_t *sel, int64_t n_sel, int64_
   if (n_sel <= 0) return cudaSuccess;
   int blocks = (int)std::min<int64_t>((n_sel + 255) / 256, (int64_t)sm_count * 4);
   qm_check_selection<<<blocks, 256, 0, stream>>>(sel, n_sel, n_rows, st);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_export_partial(const uint64_t *t, int stride, const uint32_t *slots, int64_t G, int64_t n_slots,
+                                     int key_mode, const qm_aggspec &A, int64_t row_offset, uint64_t *dst, int sm_count,
+                                     cudaStream_t st) {
+  if (G <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((G + 255) / 256, (int64_t)sm_count * 8);
+  qm_export_partial<<<blocks, 256, 0, st>>>(t, stride, slots, G, n_slots, key_mode, A, row_offset, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_merge_partial(const qm_scan_args &a, const uint64_t *src, int64_t n, int sm_count,
+                                    cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 8);
+  qm_merge_partial<<<blocks, 256, 0, st>>>(a, src, n);
   return cudaGetLastError();
 }
 

@@ -47,6 +47,11 @@ cudaError_t qm_launch_select_write(int64_t n_tiles, const uint32_t *sel, const u
                                    cudaStream_t st);
 cudaError_t qm_launch_minmax(const void *p, int dtype, const uint32_t *nulls, int64_t n, long long *out,
                              int sm_count, cudaStream_t st);
+cudaError_t qm_launch_export_partial(const uint64_t *t, int stride, const uint32_t *slots, int64_t G, int64_t n_slots,
+                                     int key_mode, const qm_aggspec &A, int64_t row_offset, uint64_t *dst, int sm_count,
+                                     cudaStream_t st);
+cudaError_t qm_launch_merge_partial(const qm_scan_args &a, const uint64_t *src, int64_t n, int sm_count,
+                                    cudaStream_t st);
 cudaError_t qm_launch_sample_pred(const qm_pred &P, int64_t n, int n_samples, unsigned long long *count,
                                   cudaStream_t st);
 cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st);

@@ -429,6 +429,37 @@ class AggStream:
             n_sel = sel.size
         self.ctx.check(self.ctx.lib.qm_agg_push(self.h, cs.n_rows, cs.count, cs.array, sel_ptr, n_sel))
 
+    def push_table(self, table: "Table") -> None:
+        """Push a registered table's rows as one batch (read in place)."""
+        self.ctx.check(self.ctx.lib.qm_agg_push_table(self.h, table.h))
+
+    def export_partial(self, row_offset: int = 0):
+        """This shard's occupied group slots as partial rows: an int64 CUDA
+        tensor [groups, row_words] on the context's device (key word,
+        special flag, accumulator words; FIRST moved by row_offset, the
+        shard's first global row)."""
+        import torch
+        n = C.c_int64()
+        w = C.c_int32()
+        self.ctx.check(self.ctx.lib.qm_agg_partial_export(self.h, row_offset, None, 0, C.byref(n), C.byref(w)))
+        out = torch.empty((n.value, w.value), dtype=torch.int64, device=f"cuda:{self.ctx.device}")
+        torch.cuda.current_stream(self.ctx.device).synchronize()
+        self.ctx.check(self.ctx.lib.qm_agg_partial_export(self.h, row_offset, C.c_void_p(out.data_ptr()),
+                                                          n.value, C.byref(n), C.byref(w)))
+        return out
+
+    def merge_partial(self, rows, rows_end: int) -> None:
+        """Fold another shard's partial rows (a CUDA tensor on this context's
+        device, from export_partial) into this aggregation; rows_end bounds
+        the global rows they cover."""
+        import torch
+        rows = rows.contiguous()
+        if rows.dtype != torch.int64 or rows.dim() != 2:
+            raise ValueError("partial rows are an int64 [groups, row_words] tensor")
+        torch.cuda.current_stream(rows.device).synchronize()
+        self.ctx.check(self.ctx.lib.qm_agg_partial_merge(self.h, C.c_void_p(rows.data_ptr()) if rows.numel() else None,
+                                                         rows.shape[0], rows.shape[1], rows_end))
+
     def finish(self, with_qmcb: bool = False) -> Result:
         r = C.c_void_p()
         self.ctx.check(self.ctx.lib.qm_agg_finish(self.h, C.byref(r)))

@@ -371,3 +371,55 @@ def test_selective_filter_sampled_estimate(ctx):
         assert_same(g, oracle.run(cols, q, threads=8))
         assert g.stats.retries == 0
         assert g.stats.table_capacity <= 18  # a hash table of at most 2^18 slots
+
+
+@pytest.mark.parametrize("shards", [2, 3])
+def test_sharded_partials_merge_to_whole_table(ctx, shards):
+    # the multi-GPU exchange on one GPU: each shard through its own
+    # aggregation, partial rows exported with global row offsets and merged
+    # into the first shard's aggregation, against the whole table
+    import torch
+    from querymode_b200.distributed import shard_range
+    rng = np.random.default_rng(50 + shards)
+    n = 600_000
+    cols = {"k": Column(rng.integers(-5000, 5000, n).astype(np.int64), rng.random(n) < 0.01),
+            "x": Column(rng.normal(size=n) * 10, rng.random(n) < 0.05),
+            "i": rng.integers(-2**62, 2**62, n).astype(np.int64),
+            "j": rng.integers(-1000, 1000, n).astype(np.int32)}
+    cols["x"].values[rng.random(n) < 0.001] = -0.0
+    qs = [QueryDescriptor(filters=[FilterOp("j", "gt", -500)], group_by=["k"],
+                          aggregates=[AggregateOp("sum", "x"), AggregateOp("min", "x"), AggregateOp("max", "x"),
+                                      AggregateOp("avg", "i"), AggregateOp("sum", "i"), AggregateOp("count", "*"),
+                                      AggregateOp("count", "x"), AggregateOp("max", "j")]),
+          QueryDescriptor(filters=[FilterOp("j", "lt", 100)],
+                          aggregates=[AggregateOp("sum", "i"), AggregateOp("min", "x"), AggregateOp("count", "*")])]
+    for q in qs:
+        streams = []
+        parts = []
+        for r in range(shards):
+            a, b = shard_range(n, r, shards)
+            shard = {k: (Column(v.values[a:b], v.nulls[a:b]) if isinstance(v, Column) else v[a:b])
+                     for k, v in cols.items()}
+            s = ctx.aggregate(q)
+            s.push(shard)
+            parts.append(s.export_partial(a))
+            streams.append(s)
+        for p in parts[1:]:
+            streams[0].merge_partial(p, n)
+        g = streams[0].finish()
+        ref = oracle.run(cols, q)
+        assert_same(g, ref)
+        # the same through registered shard tables (push_table)
+        tables = []
+        for r in range(shards):
+            a, b = shard_range(n, r, shards)
+            tables.append(ctx.table({k: (Column(v.values[a:b], v.nulls[a:b]) if isinstance(v, Column) else v[a:b])
+                                     for k, v in cols.items()}))
+        aggs = [ctx.aggregate(q) for _ in range(shards)]
+        for t, s in zip(tables, aggs):
+            s.push_table(t)
+        rows = [s.export_partial(shard_range(n, r, shards)[0]) for r, s in enumerate(aggs)]
+        for p in rows[1:]:
+            aggs[0].merge_partial(p, n)
+        assert_same(aggs[0].finish(), ref)
+        torch.cuda.synchronize()
