@@ -348,6 +348,13 @@ int qm_batch_run(qm_batch *batch, qm_result **results);
  * value keeps the current setting.  Re-captures the graph on the next run. */
 int qm_batch_set_tuning(qm_batch *batch, int32_t chunk_tiles, int32_t local_kb,
                         int32_t blocks_per_sm);
+/* How the batch scans: 1 (default) one scan launch per query, each
+ * specialised for its plan (value-column count, key kind) with the
+ * planner's block-local table, spread over parallel stream branches of the
+ * graph, largest query first; 0 one persistent kernel whose blocks claim
+ * (query, chunk of tiles) work items and read each query's plan at run
+ * time (the chunk / local-table knobs below apply to it). */
+int qm_batch_set_mode(qm_batch *batch, int32_t mode);
 /* Device time of the last run, total rows and algorithmic bytes, chunks. */
 int qm_batch_stats(const qm_batch *batch, double *device_ms, int64_t *rows,
                    int64_t *bytes, int32_t *chunks);

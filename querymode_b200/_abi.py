@@ -161,6 +161,7 @@ SIGNATURES = [
     ("qm_batch_create", C.c_int, [_P, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.POINTER(QmQuery)), _PP]),
     ("qm_batch_run", C.c_int, [_P, C.POINTER(C.c_void_p)]),
     ("qm_batch_set_tuning", C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    ("qm_batch_set_mode", C.c_int, [_P, C.c_int32]),
     ("qm_batch_stats", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                  C.POINTER(C.c_int32)]),
     ("qm_batch_destroy", C.c_int, [_P]),

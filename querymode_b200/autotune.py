@@ -1,9 +1,10 @@
 """Autotuner for the batched launch.
 
-Times a batch under a grid of launch shapes — tiles of 256 rows per work
-chunk, block-local table budget (KiB of shared memory; 0 places every group
-table in global memory only) and resident blocks per SM — and keeps the
-fastest.  Choices persist in a JSON tuning table keyed by a workload
+Times a batch run as per-query specialised launches (mode 1) and as one
+persistent kernel (mode 0) under a grid of launch shapes — tiles of 256 rows
+per work chunk, block-local table budget (KiB of shared memory; 0 places
+every group table in global memory only) and resident blocks per SM — and
+keeps the fastest.  Choices persist in a JSON tuning table keyed by a workload
 signature (GPU, query count, total-row bucket), so a later batch of the same
 shape starts from the stored choice.
 """
@@ -44,19 +45,30 @@ def tune_batch(batch, grid: dict | None = None, reps: int = 2, table_path: str |
     grid = grid or DEFAULT_GRID
     trials = []
     t0 = time.perf_counter()
+    # per-query launches (the chunk / local-table knobs do not apply)
+    batch.set_mode(1)
+    trials.append({"mode": 1, "chunk_tiles": 0, "local_kb": 0, "blocks_per_sm": 0, "ms": _time(batch, reps)})
+    batch.set_mode(0)
     for ct in grid["chunk_tiles"]:
         for lk in grid["local_kb"]:
             for bps in grid["blocks_per_sm"]:
                 batch.set_tuning(ct, lk, bps)
                 ms = _time(batch, reps)
-                trials.append({"chunk_tiles": ct, "local_kb": lk, "blocks_per_sm": bps, "ms": ms})
+                trials.append({"mode": 0, "chunk_tiles": ct, "local_kb": lk, "blocks_per_sm": bps, "ms": ms})
     best = min(trials, key=lambda t: t["ms"])
-    batch.set_tuning(best["chunk_tiles"], best["local_kb"], best["blocks_per_sm"])
-    out = {"choice": {k: best[k] for k in ("chunk_tiles", "local_kb", "blocks_per_sm")}, "ms": best["ms"],
+    apply_choice(batch, best)
+    out = {"choice": {k: best[k] for k in ("mode", "chunk_tiles", "local_kb", "blocks_per_sm")}, "ms": best["ms"],
            "trials": trials, "search_s": time.perf_counter() - t0}
     if table_path:
         save_choice(table_path, signature(batch, device_name), out["choice"], best["ms"])
     return out
+
+
+def apply_choice(batch, choice: dict) -> None:
+    mode = choice.get("mode", 0)
+    batch.set_mode(mode)
+    if mode == 0:
+        batch.set_tuning(choice["chunk_tiles"], choice["local_kb"], choice["blocks_per_sm"])
 
 
 def load_table(path: str = DEFAULT_TABLE) -> dict:
@@ -79,5 +91,5 @@ def apply_stored(batch, path: str = DEFAULT_TABLE, device_name: str = "") -> dic
     """Apply the stored choice for this batch's signature, if any."""
     entry = load_table(path).get(signature(batch, device_name))
     if entry:
-        batch.set_tuning(entry["chunk_tiles"], entry["local_kb"], entry["blocks_per_sm"])
+        apply_choice(batch, entry)
     return entry

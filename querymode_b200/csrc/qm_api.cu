@@ -2536,6 +2536,18 @@ struct qm_batch {
   std::vector<qm_bq> bq;
   std::vector<int64_t> rows;
   std::vector<int64_t> est;  // planner's group estimate per query
+  std::vector<Exec> ex_plan;  // the planner's block-local layout per query (mode 1)
+  struct Launch {
+    qm_scan_args a;
+    int blocks;
+    size_t smem;
+  };
+  std::vector<Launch> launches;       // mode 1: one specialised scan per query
+  std::vector<int> launch_order;      // largest first
+  std::vector<cudaStream_t> side;     // mode 1: branches the launches spread over
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
+  int mode = 1;  // 0: one persistent kernel over (query, chunk) work items; 1: per-query launches
   std::vector<const qm_table *> tabs;  // query i's table and a copy of the
   std::vector<std::unique_ptr<OwnedQuery>> queries;  // query, to rerun it alone
   DevBuf arena, d_bq, d_slot0, d_chunks, d_counter, d_status, d_bitmap, d_popc, d_ranks, d_temp, d_meta,
@@ -2553,6 +2565,9 @@ struct qm_batch {
   ~qm_batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
+    for (cudaStream_t st : side) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : side_ev) cudaEventDestroy(ev);
+    if (fork_ev) cudaEventDestroy(fork_ev);
     DevBuf *bufs[] = {&arena, &d_bq, &d_slot0, &d_chunks, &d_counter, &d_status, &d_bitmap, &d_popc, &d_ranks,
                       &d_temp, &d_meta, &d_packed, &d_nullbytes};
     for (DevBuf *b : bufs) release(*b);
@@ -2691,7 +2706,64 @@ int batch_layout(qm_batch *b) {
   if (bps < 1) bps = 1;
   if (b->bps > 0 && b->bps < bps) bps = b->bps;
   d.scan_blocks = std::max(1, std::min(ctx->sm_count * bps, d.n_chunks));
+  // mode 1: each query's own specialised scan, with the planner's block-local
+  // layout, on one of several stream branches
+  b->launches.resize(n);
+  b->launch_order.resize(n);
+  for (int i = 0; i < n; i++) {
+    GroupTable g;
+    g.pl = b->gts[i].pl;
+    g.ex = b->ex_plan[i];
+    g.table = b->gts[i].table;
+    qm_batch::Launch &L = b->launches[i];
+    fill_args(g, L.a, (qm_status *)b->d_status.p + i);
+    L.a.n = b->rows[i];
+    L.a.sel = nullptr;
+    L.a.row_offset = 0;
+    memset(&L.a.stage, 0, sizeof L.a.stage);
+    if (L.a.priv && L.a.n < PRIV_MIN_ROWS) L.a.priv = 0;
+    L.smem = qm_scan_smem_bytes(g.ex.local_slots, g.ex.local_hash, g.pl.agg.n_words, 0, 0, L.a.priv);
+    L.blocks = scan_blocks(ctx, L.smem, L.a.n, false);
+    b->launch_order[i] = i;
+  }
+  std::sort(b->launch_order.begin(), b->launch_order.end(),
+            [&](int x, int y) { return b->rows[x] > b->rows[y]; });
+  const int k = std::min(n, 16);
+  while ((int)b->side.size() < k) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->side.push_back(st);
+    b->side_ev.push_back(ev);
+  }
+  if (!b->fork_ev) CK(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
   drop_graph(b);
+  return QM_OK;
+}
+
+// Issue the whole batched run on the context's stream (captured into the
+// batch's graph, or launched directly).
+int batch_launch(qm_batch *b) {
+  qm_ctx *ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  if (b->mode == 0) {
+    CK(qm_batch_launch_all(b->dev, st));
+    return QM_OK;
+  }
+  CK(qm_batch_launch_init(b->dev, st));
+  const int k = std::min<int>(b->n, (int)b->side.size());
+  CK(cudaEventRecord(b->fork_ev, st));
+  for (int j = 0; j < k; j++) CK(cudaStreamWaitEvent(b->side[j], b->fork_ev, 0));
+  for (int j = 0; j < b->n; j++) {
+    const qm_batch::Launch &L = b->launches[b->launch_order[j]];
+    CK(qm_launch_scan(L.a, L.blocks, L.smem, b->side[j % k]));
+  }
+  for (int j = 0; j < k; j++) {
+    CK(cudaEventRecord(b->side_ev[j], b->side[j]));
+    CK(cudaStreamWaitEvent(st, b->side_ev[j], 0));
+  }
+  CK(qm_batch_launch_finalize(b->dev, st));
   return QM_OK;
 }
 
@@ -2702,6 +2774,7 @@ void batch_reset(qm_batch *b, int n) {
   b->rows.assign(n, 0);
   b->est.assign(n, 1);
   b->tabs.assign(n, nullptr);
+  b->ex_plan.assign(n, Exec());
   b->queries.clear();
   b->queries.resize(n);  // null until planned
   b->total_rows = 0;
@@ -2737,6 +2810,7 @@ int batch_plan_one(qm_batch *b, int i, const qm_table *table, const qm_query *qu
   }
   choose_layout(gt.pl, est, ex, ctx->tuning);
   b->est[i] = est;
+  b->ex_plan[i] = ex;
   qm_bq &qb = b->bq[i];
   memset(&qb, 0, sizeof qb);
   qb.outs = gt.pl.outs;
@@ -2772,16 +2846,17 @@ int batch_execute(qm_batch *b, qm_result **results, int *codes, bool use_graph) 
   cudaSetDevice(ctx->device);
   if (use_graph && !b->gexec) {
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = qm_batch_launch_all(b->dev, ctx->stream);
-    cudaError_t e2 = cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n, cudaMemcpyDeviceToHost,
-                                     ctx->stream);
+    const int rc = batch_launch(b);
+    cudaError_t e2 = rc ? cudaSuccess
+                        : cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n,
+                                          cudaMemcpyDeviceToHost, ctx->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e3 = cudaStreamEndCapture(ctx->stream, &g);
-    if (e != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+    if (rc || e2 != cudaSuccess || e3 != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       cudaGetLastError();
       return set_err(ctx, QM_ERR_CUDA, "capturing the batched launch: %s",
-                     cudaGetErrorString(e != cudaSuccess ? e : (e2 != cudaSuccess ? e2 : e3)));
+                     cudaGetErrorString(e2 != cudaSuccess ? e2 : e3));
     }
     b->graph = g;
     CK(cudaGraphInstantiate(&b->gexec, g, 0));
@@ -2790,7 +2865,8 @@ int batch_execute(qm_batch *b, qm_result **results, int *codes, bool use_graph) 
   if (use_graph) {
     CK(cudaGraphLaunch(b->gexec, ctx->stream));
   } else {
-    CK(qm_batch_launch_all(b->dev, ctx->stream));
+    int rc = batch_launch(b);
+    if (rc) return rc;
     CK(cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n, cudaMemcpyDeviceToHost,
                        ctx->stream));
   }
@@ -2879,6 +2955,15 @@ int qm_batch_create(qm_ctx *ctx, int32_t n, const qm_table *const *tables, const
     return rc;
   }
   *out = b;
+  return QM_OK;
+}
+
+int qm_batch_set_mode(qm_batch *b, int32_t mode) {
+  if (!b || (mode != 0 && mode != 1)) return QM_ERR_INVALID;
+  if (b->mode != mode) {
+    b->mode = mode;
+    drop_graph(b);
+  }
   return QM_OK;
 }
 

@@ -286,14 +286,30 @@ static int grid_for(int64_t n, int sm_count, int per_sm) {
   return (int)std::max<int64_t>(b, 1);
 }
 
-cudaError_t qm_batch_launch_all(const qm_batch_dev &d, cudaStream_t st) {
+cudaError_t qm_batch_launch_init(const qm_batch_dev &d, cudaStream_t st) {
   cudaError_t e;
   if ((e = cudaMemsetAsync(d.statuses, 0, sizeof(qm_status) * d.n, st))) return e;
   if ((e = cudaMemsetAsync(d.counter, 0, sizeof(int), st))) return e;
   if ((e = cudaMemsetAsync(d.bitmap, 0, sizeof(uint32_t) * (d.bm_words + 1), st))) return e;
   qm_batch_init<<<grid_for(d.total_slots, d.sm_count, 16), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_batch_launch_persistent(const qm_batch_dev &d, cudaStream_t st) {
   qm_batch_scan<<<d.scan_blocks, QM_SCAN_THREADS, d.scan_smem, st>>>(d.bq, d.chunks, d.n_chunks, d.counter,
                                                                      d.local_bytes);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_batch_launch_all(const qm_batch_dev &d, cudaStream_t st) {
+  cudaError_t e;
+  if ((e = qm_batch_launch_init(d, st))) return e;
+  if ((e = qm_batch_launch_persistent(d, st))) return e;
+  return qm_batch_launch_finalize(d, st);
+}
+
+cudaError_t qm_batch_launch_finalize(const qm_batch_dev &d, cudaStream_t st) {
+  cudaError_t e;
   qm_batch_mark<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap);
   qm_batch_popc<<<grid_for(d.bm_words + 1, d.sm_count, 8), 256, 0, st>>>(d.bitmap, d.bm_words, d.popc);
   size_t tb = d.scan_temp_bytes;

@@ -63,5 +63,12 @@ struct qm_batch_dev {
 
 size_t qm_batch_smem_bytes(int local_bytes);
 cudaError_t qm_batch_configure(size_t smem, int *blocks_per_sm);
+// The three phases of a batched run: clear statuses, bitmaps and group
+// tables; the persistent scan over every query's chunks (or, instead, one
+// specialised scan launch per query issued by the host); rank, lay out,
+// emit and pack the results.
+cudaError_t qm_batch_launch_init(const qm_batch_dev &d, cudaStream_t st);
+cudaError_t qm_batch_launch_persistent(const qm_batch_dev &d, cudaStream_t st);
+cudaError_t qm_batch_launch_finalize(const qm_batch_dev &d, cudaStream_t st);
 cudaError_t qm_batch_launch_all(const qm_batch_dev &d, cudaStream_t st);
 cudaError_t qm_batch_scan_temp_bytes(int64_t words, size_t *bytes);

@@ -505,6 +505,11 @@ class Batch:
     def set_tuning(self, chunk_tiles: int = -1, local_kb: int = -1, blocks_per_sm: int = -1) -> None:
         self.ctx.check(self.ctx.lib.qm_batch_set_tuning(self.h, chunk_tiles, local_kb, blocks_per_sm))
 
+    def set_mode(self, mode: int) -> None:
+        """1: one specialised scan launch per query on parallel graph
+        branches (default); 0: one persistent kernel over all queries."""
+        self.ctx.check(self.ctx.lib.qm_batch_set_mode(self.h, mode))
+
     def run(self) -> "BatchResults":
         out = (C.c_void_p * self.n)()
         self.ctx.check(self.ctx.lib.qm_batch_run(self.h, out))

@@ -42,10 +42,13 @@ def test_batch_matches_oracle(ctx):
             res = b.run()
             for i, (g, r) in enumerate(zip(res, refs)):
                 assert_same(g, r, ctx_msg=f"run {run} query {i}")
-        b.set_tuning(chunk_tiles=64, local_kb=0, blocks_per_sm=1)
-        res = b.run()
-        for i, (g, r) in enumerate(zip(res, refs)):
-            assert_same(g, r, ctx_msg=f"retuned query {i}")
+        # the persistent kernel, default and retuned
+        b.set_mode(0)
+        for tuning in ({}, {"chunk_tiles": 64, "local_kb": 0, "blocks_per_sm": 1}):
+            b.set_tuning(**tuning)
+            res = b.run()
+            for i, (g, r) in enumerate(zip(res, refs)):
+                assert_same(g, r, ctx_msg=f"persistent {tuning} query {i}")
         st = b.stats()
         assert st["rows"] == sum(len(next(iter(t.values())).values if hasattr(next(iter(t.values())), "values")
                                      else next(iter(t.values()))) for t in tables)
