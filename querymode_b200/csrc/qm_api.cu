@@ -1112,6 +1112,7 @@ struct GroupTable {
   unsigned long long selected = 0;
   bool scan_pending = false;  // evs0/evs1 bracket a scan not yet timed
   double scan_ms = 0;         // accumulated scan-kernel time
+  int64_t sel_bound = -1;     // planner's sampled bound on selected rows, if taken
 };
 
 int read_status(qm_ctx *ctx, qm_status *out) {
@@ -1289,7 +1290,7 @@ int setup_table(qm_ctx *ctx, GroupTable &gt, int64_t est_groups, int64_t direct_
   return init_table(ctx, gt);
 }
 
-int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel) {
+int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel, bool timed = true) {
   qm_scan_args a;
   fill_args(gt, a, (qm_status *)ctx->status.p);
   a.n = n;
@@ -1317,9 +1318,9 @@ int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel) {
   }
   if (!staged) memset(&a.stage, 0, sizeof a.stage);
   int blocks = scan_blocks(ctx, smem, n, staged);
-  CK(cudaEventRecord(ctx->evs0, ctx->stream));
+  if (timed) CK(cudaEventRecord(ctx->evs0, ctx->stream));
   CK(qm_launch_scan(a, blocks, smem, ctx->stream));
-  CK(cudaEventRecord(ctx->evs1, ctx->stream));
+  if (timed) CK(cudaEventRecord(ctx->evs1, ctx->stream));
   if (n > 0) ctx->launches++;
   gt.scan_pending = true;
   return QM_OK;
@@ -1366,6 +1367,51 @@ void plan_narrow_sums(Plan &pl, int64_t n_rows) {
       if ((o.kind == QO_SUM_I2F || o.kind == QO_AVG_I2F) && o.word == ac.word) o.narrow = 1;
     }
   }
+}
+
+// A dense (direct) group table larger than this is updated in key-range
+// passes, each pass's slots staying in L2: the scan re-reads the key column
+// once per pass, but every atomic update then hits L2 instead of DRAM.
+#ifndef QM_L2_TABLE_MB
+#define QM_L2_TABLE_MB 64
+#endif
+constexpr int64_t L2_TABLE_BUDGET = (int64_t)QM_L2_TABLE_MB << 20;
+
+// Key-range passes for a direct-indexed table query (1: a single scan).
+int key_range_passes(const GroupTable &gt, int64_t n_rows, int64_t sel_bound) {
+  const Plan &pl = gt.pl;
+  if (pl.key.mode != QK_DIRECT || pl.key.n_cols != 1 || pl.key.pack != QP_RAW) return 1;
+  if (pl.pred.n_and + (pl.pred.n_groups > 0 ? pl.pred.group_end[pl.pred.n_groups - 1] - pl.pred.n_and : 0) >=
+      QM_MAX_TERMS)
+    return 1;
+  const int64_t bytes = gt.ex.total_slots * gt.ex.stride * 8;
+  if (bytes <= L2_TABLE_BUDGET) return 1;
+  // worth it when rows outnumber slots (dense updates); a selective filter
+  // leaves few atomics to save
+  const int64_t rows = sel_bound >= 0 ? sel_bound : n_rows;
+  if (rows < gt.ex.n_slots) return 1;
+  return (int)std::min<int64_t>(64, (bytes + L2_TABLE_BUDGET - 1) / L2_TABLE_BUDGET);
+}
+
+// The predicate with an extra AND term: key in [lo, hi] (NULL keys pass in
+// one chosen pass only, so each row is aggregated exactly once).
+qm_pred with_key_range(const qm_pred &P, const qm_keyspec &K, int64_t lo, int64_t hi, bool nulls_pass) {
+  qm_pred q = P;
+  const int nt = P.n_groups > 0 ? P.group_end[P.n_groups - 1] : P.n_and;
+  for (int i = nt; i > P.n_and; i--) q.t[i] = P.t[i - 1];
+  for (int g = 0; g < P.n_groups; g++) q.group_end[g] = P.group_end[g] + 1;
+  qm_term &t = q.t[P.n_and];
+  memset(&t, 0, sizeof t);
+  t.data = K.data[0];
+  t.nulls = K.nulls[0];
+  t.dtype = K.dtype[0];
+  t.kind = QT_IRANGE;
+  t.null_pass = nulls_pass ? 1 : 0;
+  t.sidx = -1;
+  t.lo = lo;
+  t.hi = hi;
+  q.n_and = P.n_and + 1;
+  return q;
 }
 
 // Plan `q` over registered table `t`: lower it, pack its keys, pick the
@@ -1458,6 +1504,7 @@ int plan_table_query(qm_ctx *ctx, qm_table *t, const qm_query *q, GroupTable &gt
         est = std::min(est, sel_bound);
       }
     }
+    gt.sel_bound = sel_bound;
   }
   return QM_OK;
 }
@@ -1699,7 +1746,24 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if ((rc = setup_table(ctx, gt, est, direct_size, false))) return rc;
-    if ((rc = run_scan(ctx, gt, t->n_rows, nullptr))) return rc;
+    const int passes = key_range_passes(gt, t->n_rows, gt.sel_bound);
+    if (passes <= 1) {
+      if ((rc = run_scan(ctx, gt, t->n_rows, nullptr))) return rc;
+    } else {
+      const qm_pred base = pl.pred;
+      const int64_t span = (gt.ex.n_slots + passes - 1) / passes;
+      CK(cudaEventRecord(ctx->evs0, ctx->stream));
+      for (int p = 0; p < passes; p++) {
+        const int64_t lo = pl.key.base + p * span;
+        const int64_t hi = std::min<int64_t>(pl.key.base + gt.ex.n_slots - 1, lo + span - 1);
+        pl.pred = with_key_range(base, pl.key, lo, hi, p == 0);
+        rc = run_scan(ctx, gt, t->n_rows, nullptr, false);
+        pl.pred = base;
+        if (rc) return rc;
+      }
+      CK(cudaEventRecord(ctx->evs1, ctx->stream));
+      gt.scan_pending = true;
+    }
     qm_status st;
     if ((rc = read_status(ctx, &st))) return rc;
     take_scan_time(ctx, gt, st.error == QM_DEV_OK);

@@ -423,3 +423,20 @@ def test_sharded_partials_merge_to_whole_table(ctx, shards):
             aggs[0].merge_partial(p, n)
         assert_same(aggs[0].finish(), ref)
         torch.cuda.synchronize()
+
+
+def test_large_dense_table_key_range_passes(ctx):
+    # a dense key range whose group table exceeds the L2 budget is updated in
+    # key-range passes (each row once; NULL keys in the first pass only)
+    rng = np.random.default_rng(61)
+    n = 5_000_000
+    cols = {"k": Column(rng.integers(0, 2_500_000, n).astype(np.int64), rng.random(n) < 0.001),
+            "x": rng.normal(size=n), "f": rng.integers(0, 10, n).astype(np.int32)}
+    t = ctx.table(cols)
+    for q in (QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("sum", "x"), AggregateOp("count", "*"),
+                                                          AggregateOp("max", "x")]),
+              QueryDescriptor(filters=[FilterOp("f", "lt", 9)], group_by=["k"],
+                              aggregates=[AggregateOp("avg", "x"), AggregateOp("count", "*")])):
+        g = t.run(q)
+        assert g.stats.strategy in (0, 1, 2)
+        assert_same(g, oracle.run(cols, q, threads=8))
