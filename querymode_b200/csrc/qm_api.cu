@@ -101,6 +101,7 @@ struct qm_ctx {
   DevBuf table, status, keys, slots, keys2, slots2, sort_temp, counter, out, hll;
   DevBuf masks, counts, offsets, sel_out, sel_in;
   DevBuf agg_spare;  // group table of a destroyed qm_agg, reused by the next one
+  DevBuf fbits, fcounts, franks;  // first-row bitmap, its popcounts and prefix sums
   std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
   HostBuf hout, hstatus;
   std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
@@ -834,10 +835,12 @@ void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning
   if (pl.key.mode == QK_DIRECT && tu.local_slots >= 0 && (ex.n_slots + 1) * per_slot <= (int64_t)DIRECT_LOCAL_BUDGET) {
     ex.local_slots = (int)(ex.n_slots + 1);
     ex.local_hash = 0;
-    ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : (ex.n_slots <= 256 ? 1 : 0);
-    // few groups: every warp of a block hits the same words, so the table is
-    // copied per warp and updated without atomics (deduplicated rows have
-    // distinct slots within a warp)
+    // warp deduplication is off by default for dense keys: the scan's own
+    // equal-slot merge costs fewer instructions (measured 2.5x faster at 11
+    // groups, 1.5x at 16)
+    ex.dedupe = tu.dedupe >= 0 ? tu.dedupe : 0;
+    // deduplicated rows have distinct slots within a warp, so a small table
+    // copied per warp is then updated without atomics
     ex.priv = ex.dedupe && (ex.n_slots + 1) * per_slot * (QM_SCAN_THREADS / 32) <= (int64_t)PRIV_BUDGET;
     ex.strategy = 0;
     return;
@@ -1171,8 +1174,27 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   const Exec &ex = gt.ex;
   int64_t G = 0;
   const uint32_t *slots = nullptr;
+  const int first_word_o = pl.agg.acc_first >= 0 ? pl.agg.acc[pl.agg.acc_first].word : -1;
+  const bool ranked = pl.key.mode != QK_NONE && first_word_o >= 0;
+  const int64_t bm_words = std::max<int64_t>(gt.rows_done, 1) / 32 + 1;
   if (pl.key.mode == QK_NONE) {
     G = 1;  // ungrouped: exactly one row (src/partial-agg.ts:313-320)
+  } else if (ranked) {
+    // first-seen order: a bit per first row, prefix popcounts give the ranks
+    int rc;
+    size_t tb = 0;
+    CK(qm_rank_temp_bytes(bm_words, &tb));
+    if ((rc = ensure(ctx, ctx->fbits, (bm_words + 1) * 4)) || (rc = ensure(ctx, ctx->fcounts, (bm_words + 1) * 4)) ||
+        (rc = ensure(ctx, ctx->franks, (bm_words + 1) * 8)) || (rc = ensure(ctx, ctx->sort_temp, tb + 16)) ||
+        (rc = ensure_host(ctx, ctx->hstatus, 64)))
+      return rc;
+    CK(qm_launch_rank_first(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
+                            (uint32_t *)ctx->fbits.p, bm_words, (uint32_t *)ctx->fcounts.p, (uint64_t *)ctx->franks.p,
+                            ctx->sort_temp.p, ctx->sort_temp.bytes, ctx->sm_count, ctx->stream));
+    ctx->launches += 3;
+    CK(cudaMemcpyAsync(ctx->hstatus.p, (uint64_t *)ctx->franks.p + bm_words, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    G = (int64_t)*(uint64_t *)ctx->hstatus.p;
   } else {
     int rc;
     if ((rc = ensure(ctx, ctx->keys, ex.total_slots * 8)) || (rc = ensure(ctx, ctx->slots, ex.total_slots * 4)) ||
@@ -1224,8 +1246,15 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   R->pool = ctx->pool;
   R->buf = hbuf;
   CK(cudaMemsetAsync(ctx->out.p, 0, off + 16, ctx->stream));
-  CK(qm_launch_emit(gt.table, ex.stride, slots, G, pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p,
-                    ctx->sm_count, ctx->stream));
+  if (ranked) {
+    if (G > 0)
+      CK(qm_launch_emit_ranked(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
+                               (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, pl.key, ex.n_slots, O,
+                               (unsigned char *)ctx->out.p, ctx->sm_count, ctx->stream));
+  } else {
+    CK(qm_launch_emit(gt.table, ex.stride, slots, G, pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p,
+                      ctx->sm_count, ctx->stream));
+  }
   if (G > 0) ctx->launches++;
   CK(cudaMemcpyAsync(R->buf.p, ctx->out.p, off, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -1559,7 +1588,8 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   DevBuf *bufs[] = {&ctx->table, &ctx->status, &ctx->keys, &ctx->slots, &ctx->keys2, &ctx->slots2,
                     &ctx->sort_temp, &ctx->counter, &ctx->out, &ctx->hll, &ctx->masks, &ctx->counts,
-                    &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare};
+                    &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare, &ctx->fbits, &ctx->fcounts,
+                    &ctx->franks};
   for (DevBuf *b : bufs) release(*b);
   for (auto &b : ctx->staged) release(b);
   if (ctx->hout.p) cudaFreeHost(ctx->hout.p);

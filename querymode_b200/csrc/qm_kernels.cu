@@ -160,6 +160,38 @@ __global__ void qm_emit_groups(const uint64_t *t, int stride, const uint32_t *sl
     emit_group<false>(t, stride, slots ? slots[i] : (uint64_t)i, i, K, n_slots, O, out, nullptr, nullptr);
 }
 
+// First-seen ranking without a sort: bit `first row` of every occupied slot
+// in a row bitmap (each row belongs to one group, so bits are distinct);
+// the prefix popcount of the bitmap then gives each group's output row.
+__global__ void qm_mark_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                              uint32_t *bitmap) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots_total;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t *w = t + s * stride + 1;
+    if (w[count_word] == 0) continue;
+    const uint64_t f = w[first_word];
+    atomicOr(bitmap + (f >> 5), 1u << (f & 31));
+  }
+}
+
+__global__ void qm_popc_words(const uint32_t *bitmap, int64_t words, uint32_t *counts) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= words; i += (int64_t)gridDim.x * blockDim.x)
+    counts[i] = i < words ? __popc(bitmap[i]) : 0;
+}
+
+__global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                               const uint32_t *bitmap, const uint64_t *ranks, const __grid_constant__ qm_keyspec K,
+                               int64_t n_slots, const __grid_constant__ qm_outspec O, unsigned char *out) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots_total;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t *w = t + s * stride + 1;
+    if (w[count_word] == 0) continue;
+    const uint64_t f = w[first_word];
+    const int64_t i = (int64_t)ranks[f >> 5] + __popc(bitmap[f >> 5] & ((1u << (f & 31)) - 1u));
+    emit_group<false>(t, stride, (uint64_t)s, i, K, n_slots, O, out, nullptr, nullptr);
+  }
+}
+
 // Filter-only pass 1: per warp tile, the 32-bit survivor masks and counts.
 template <bool SEL>
 __global__ void __launch_bounds__(QM_SCAN_THREADS)
@@ -422,6 +454,33 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
   if (blocks < 1) return cudaSuccess;
   if (sel) qm_select_masks<true><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
   else qm_select_masks<false><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                                 uint32_t *bitmap, int64_t words, uint32_t *counts, uint64_t *ranks, void *temp,
+                                 size_t temp_bytes, int sm_count, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(bitmap, 0, sizeof(uint32_t) * (size_t)(words + 1), st);
+  if (e != cudaSuccess) return e;
+  int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
+  qm_mark_first<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap);
+  blocks = (int)std::min<int64_t>((words + 256) / 256, (int64_t)sm_count * 8);
+  qm_popc_words<<<std::max(blocks, 1), 256, 0, st>>>(bitmap, words, counts);
+  return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, ranks, (int)(words + 1), st);
+}
+
+cudaError_t qm_rank_temp_bytes(int64_t words, size_t *bytes) {
+  return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
+                                       (int)(words + 1));
+}
+
+cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
+                                  int first_word, const uint32_t *bitmap, const uint64_t *ranks, const qm_keyspec &K,
+                                  int64_t n_slots, const qm_outspec &O, unsigned char *out, int sm_count,
+                                  cudaStream_t st) {
+  const int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
+  qm_emit_ranked<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap, ranks,
+                                                      K, n_slots, O, out);
   return cudaGetLastError();
 }
 

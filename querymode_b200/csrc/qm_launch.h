@@ -52,6 +52,16 @@ cudaError_t qm_launch_export_partial(const uint64_t *t, int stride, const uint32
                                      cudaStream_t st);
 cudaError_t qm_launch_merge_partial(const qm_scan_args &a, const uint64_t *src, int64_t n, int sm_count,
                                     cudaStream_t st);
+// First-seen ranking of the occupied slots through a row bitmap and its
+// prefix popcount (ranks[words] = number of groups), then the emit by rank.
+cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                                 uint32_t *bitmap, int64_t words, uint32_t *counts, uint64_t *ranks, void *temp,
+                                 size_t temp_bytes, int sm_count, cudaStream_t st);
+cudaError_t qm_rank_temp_bytes(int64_t words, size_t *bytes);
+cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
+                                  int first_word, const uint32_t *bitmap, const uint64_t *ranks, const qm_keyspec &K,
+                                  int64_t n_slots, const qm_outspec &O, unsigned char *out, int sm_count,
+                                  cudaStream_t st);
 cudaError_t qm_launch_sample_pred(const qm_pred &P, int64_t n, int n_samples, unsigned long long *count,
                                   cudaStream_t st);
 cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st);

@@ -342,11 +342,16 @@ def test_per_warp_tables_large(ctx):
             AggregateOp("count", "x"), AggregateOp("sum", "i"), AggregateOp("avg", "i"), AggregateOp("min", "i"),
             AggregateOp("sum", "j"), AggregateOp("max", "j"), AggregateOp("count", "*")]
     t = ctx.table(cols)
-    for q in (QueryDescriptor(filters=[FilterOp("f", "lt", 70)], group_by=["k"], aggregates=aggs),
-              QueryDescriptor(filters=[FilterOp("f", "gte", 10)], aggregates=aggs)):
-        g = t.run(q)
-        r = oracle.run(cols, q, threads=8)
-        assert_same(g, r)
+    try:
+        for dedupe in (-1, 1):  # planner's choice; warp deduplication (per-warp copies) forced
+            ctx.set_tuning(dedupe=dedupe)
+            for q in (QueryDescriptor(filters=[FilterOp("f", "lt", 70)], group_by=["k"], aggregates=aggs),
+                      QueryDescriptor(filters=[FilterOp("f", "gte", 10)], aggregates=aggs)):
+                g = t.run(q)
+                r = oracle.run(cols, q, threads=8)
+                assert_same(g, r, ctx_msg=f"dedupe={dedupe}")
+    finally:
+        ctx.set_tuning()
 
 
 def test_selective_filter_sampled_estimate(ctx):
