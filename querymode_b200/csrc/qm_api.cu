@@ -1169,32 +1169,55 @@ void fill_args(const GroupTable &gt, qm_scan_args &a, qm_status *st) {
 
 // Finalize the group table into a qm_result (compaction, first-seen order,
 // per-group finalize on the device, one copy back).
-int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far) {
+bool ranked_finish(const GroupTable &gt) {
+  return gt.pl.key.mode != QK_NONE && gt.pl.agg.acc_first >= 0;
+}
+
+int64_t rank_words(const GroupTable &gt) { return std::max<int64_t>(gt.rows_done, 1) / 32 + 1; }
+
+// First-seen order: a bit per first row, prefix popcounts give the ranks.
+// Queues the ranking and a copy of the group count to ctx->hstatus + 32
+// (read after the caller's next synchronize).
+int launch_rank(qm_ctx *ctx, const GroupTable &gt) {
+  const Plan &pl = gt.pl;
+  const Exec &ex = gt.ex;
+  const int64_t bm_words = rank_words(gt);
+  int rc;
+  size_t tb = 0;
+  CK(qm_rank_temp_bytes(bm_words, &tb));
+  if ((rc = ensure(ctx, ctx->fbits, (bm_words + 1) * 4)) || (rc = ensure(ctx, ctx->fcounts, (bm_words + 1) * 4)) ||
+      (rc = ensure(ctx, ctx->franks, (bm_words + 1) * 8)) || (rc = ensure(ctx, ctx->sort_temp, tb + 16)) ||
+      (rc = ensure_host(ctx, ctx->hstatus, 64)))
+    return rc;
+  CK(qm_launch_rank_first(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word,
+                          pl.agg.acc[pl.agg.acc_first].word, (uint32_t *)ctx->fbits.p, bm_words,
+                          (uint32_t *)ctx->fcounts.p, (uint64_t *)ctx->franks.p, ctx->sort_temp.p, ctx->sort_temp.bytes,
+                          ctx->sm_count, ctx->stream));
+  ctx->launches += 3;
+  CK(cudaMemcpyAsync((char *)ctx->hstatus.p + 32, (uint64_t *)ctx->franks.p + bm_words, 8, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  return QM_OK;
+}
+
+// groups_known >= 0: launch_rank already ran and its count was read.
+int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1) {
   const Plan &pl = gt.pl;
   const Exec &ex = gt.ex;
   int64_t G = 0;
   const uint32_t *slots = nullptr;
   const int first_word_o = pl.agg.acc_first >= 0 ? pl.agg.acc[pl.agg.acc_first].word : -1;
-  const bool ranked = pl.key.mode != QK_NONE && first_word_o >= 0;
-  const int64_t bm_words = std::max<int64_t>(gt.rows_done, 1) / 32 + 1;
+  const bool ranked = ranked_finish(gt);
   if (pl.key.mode == QK_NONE) {
     G = 1;  // ungrouped: exactly one row (src/partial-agg.ts:313-320)
   } else if (ranked) {
-    // first-seen order: a bit per first row, prefix popcounts give the ranks
-    int rc;
-    size_t tb = 0;
-    CK(qm_rank_temp_bytes(bm_words, &tb));
-    if ((rc = ensure(ctx, ctx->fbits, (bm_words + 1) * 4)) || (rc = ensure(ctx, ctx->fcounts, (bm_words + 1) * 4)) ||
-        (rc = ensure(ctx, ctx->franks, (bm_words + 1) * 8)) || (rc = ensure(ctx, ctx->sort_temp, tb + 16)) ||
-        (rc = ensure_host(ctx, ctx->hstatus, 64)))
-      return rc;
-    CK(qm_launch_rank_first(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
-                            (uint32_t *)ctx->fbits.p, bm_words, (uint32_t *)ctx->fcounts.p, (uint64_t *)ctx->franks.p,
-                            ctx->sort_temp.p, ctx->sort_temp.bytes, ctx->sm_count, ctx->stream));
-    ctx->launches += 3;
-    CK(cudaMemcpyAsync(ctx->hstatus.p, (uint64_t *)ctx->franks.p + bm_words, 8, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    G = (int64_t)*(uint64_t *)ctx->hstatus.p;
+    if (groups_known >= 0) {
+      G = groups_known;
+    } else {
+      int rc = launch_rank(ctx, gt);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(ctx->stream));
+      G = (int64_t)*(uint64_t *)((char *)ctx->hstatus.p + 32);
+    }
   } else {
     int rc;
     if ((rc = ensure(ctx, ctx->keys, ex.total_slots * 8)) || (rc = ensure(ctx, ctx->slots, ex.total_slots * 4)) ||
@@ -1772,6 +1795,7 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
   if (rc) return rc;
   Plan &pl = gt.pl;
   gt.rows_done = 0;
+  int64_t groups = -1;
   for (int attempt = 0;; attempt++) {
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -1794,11 +1818,17 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
       CK(cudaEventRecord(ctx->evs1, ctx->stream));
       gt.scan_pending = true;
     }
+    // rank the groups before reading the status: one synchronize for both
+    // (an overflowed table's ranking is discarded with it)
+    gt.rows_done = t->n_rows;
+    const bool ranked = ranked_finish(gt);
+    if (ranked && (rc = launch_rank(ctx, gt))) return rc;
     qm_status st;
     if ((rc = read_status(ctx, &st))) return rc;
     take_scan_time(ctx, gt, st.error == QM_DEV_OK);
     if (st.error == QM_DEV_OK) {
       gt.selected = st.rows_selected;
+      if (ranked) groups = (int64_t)*(uint64_t *)((char *)ctx->hstatus.p + 32);
       break;
     }
     if (attempt >= 4) return set_err(ctx, QM_ERR_CUDA, "group table overflow after %d regrowths", attempt);
@@ -1809,7 +1839,7 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
     est = std::max<int64_t>(est * 4, (int64_t)st.groups_inserted * 2);
   }
   gt.rows_done = t->n_rows;
-  rc = finish_table(ctx, gt, out, 0.f);
+  rc = finish_table(ctx, gt, out, 0.f, groups);
   if (rc) return rc;
   (*out)->stats.rows_scanned = t->n_rows;
   (*out)->stats.bytes_scanned = pl.bytes_per_row * t->n_rows;
