@@ -376,7 +376,9 @@ def run_serving(local: int, args) -> dict:
             return t, wide_full
         return t, wide_q[int(r.integers(2))]
 
-    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0)
+    # batches of small requests; a 200M-row request is scanned alone (it
+    # fills the GPU by itself, and batching it would hold back the others)
+    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0, max_batch_rows=1 << 27)
     try:
         # warm-up: every table and query kind once (column statistics are cached)
         warm = []
@@ -417,7 +419,9 @@ def run_serving(local: int, args) -> dict:
             th.join()
             return np.array(lat), np.array(bs), done_at[0] - t0
 
-        # capacity: a closed burst of requests
+        # capacity: a closed burst of requests (after one untimed burst, which
+        # grows the server's buffers to the mix's working set)
+        serve([draw(rng) for _ in range(100)], None)
         burst = [draw(rng) for _ in range(max(200, args.serve_queries // 4))]
         _, bsz, span = serve(burst, None)
         capacity = len(burst) / span

@@ -386,7 +386,11 @@ typedef struct {
   int32_t max_batch;        /* requests per batched launch (1..4096)       */
   int32_t max_wait_us;      /* the oldest queued request waits at most this
                                long for others before a launch (0: none)   */
-  int32_t reserved[4];
+  int64_t max_batch_rows;   /* rows a batch may scan (0: no limit); a batch
+                               always takes its first request.  Bounds the
+                               latency a large request adds to small ones
+                               sharing its batch                            */
+  int32_t reserved[2];
 } qm_server_config;
 
 typedef struct {

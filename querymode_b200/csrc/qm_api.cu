@@ -52,6 +52,10 @@ struct PinnedPool {
   ~PinnedPool() {
     for (auto &b : free) cudaFreeHost(b.p);
   }
+  // Buffers are power-of-two sized (results of similar size share them) and
+  // kept up to a byte cap: allocating or freeing pinned memory costs far
+  // more than a query (and freeing synchronises the device).
+  static constexpr size_t CACHE_CAP = (size_t)8 << 30;
   bool acquire(size_t bytes, HostBuf &out) {
     {
       std::lock_guard<std::mutex> lk(mu);
@@ -64,7 +68,8 @@ struct PinnedPool {
         return true;
       }
     }
-    size_t want = std::max<size_t>(bytes, 64 * 1024);
+    size_t want = 64 * 1024;
+    while (want < bytes) want <<= 1;
     if (cudaMallocHost(&out.p, want) != cudaSuccess) {
       cudaGetLastError();
       out = HostBuf();
@@ -76,7 +81,9 @@ struct PinnedPool {
   void release(HostBuf &b) {
     if (!b.p) return;
     std::lock_guard<std::mutex> lk(mu);
-    if (free.size() < 8) {
+    size_t cached = b.bytes;
+    for (auto &f : free) cached += f.bytes;
+    if (cached <= CACHE_CAP && free.size() < 64) {
       free.push_back(b);
     } else {
       cudaFreeHost(b.p);
@@ -129,12 +136,18 @@ int set_err(qm_ctx *ctx, int code, const char *fmt, ...) {
 
 int ensure(qm_ctx *ctx, DevBuf &b, size_t bytes) {
   if (b.bytes >= bytes && b.p) return QM_OK;
+  const size_t old_bytes = b.p ? b.bytes : 0;
   if (b.p) {
     cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
   }
+  // grow by at least half again (and to a 2 MiB multiple), so buffers that
+  // track a changing working set are reallocated rarely: cudaFree
+  // synchronises the device
   size_t want = std::max<size_t>(bytes, 256);
+  if (old_bytes) want = std::max(want, old_bytes + old_bytes / 2);
+  if (want > ((size_t)1 << 21)) want = (want + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
   cudaError_t e = cudaMalloc(&b.p, want);
   if (e != cudaSuccess) {
     cudaGetLastError();

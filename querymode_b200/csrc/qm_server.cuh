@@ -78,13 +78,17 @@ struct qm_server {
     }
     batch_reset(b, (int)take.size());
     std::vector<std::shared_ptr<Request>> admitted, deferred;
-    int64_t working = 0;
+    int64_t working = 0, rows = 0;
     for (auto &r : take) {
       if (!deferred.empty()) {  // keep arrival order behind a deferred request
         deferred.push_back(r);
         continue;
       }
       const int k = (int)admitted.size();
+      if (k > 0 && cfg.max_batch_rows > 0 && rows + r->table->n_rows > cfg.max_batch_rows) {
+        deferred.push_back(r);
+        continue;
+      }
       int rc = batch_plan_one(b, k, r->table, &r->query.q);
       if (rc) {
         complete(r, rc, ctx->err, nullptr);
@@ -103,6 +107,7 @@ struct qm_server {
         continue;
       }
       working += need;
+      rows += r->table->n_rows;
       admitted.push_back(r);
     }
     if (!deferred.empty()) {

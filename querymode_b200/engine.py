@@ -368,8 +368,9 @@ class Context:
     def batch(self, tables: list["Table"], queries: list[QueryDescriptor]) -> "Batch":
         return Batch(self, tables, queries)
 
-    def server(self, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0) -> "Server":
-        return Server(self, hbm_budget_bytes, max_batch, max_wait_us)
+    def server(self, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0,
+               max_batch_rows: int = 0) -> "Server":
+        return Server(self, hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows)
 
 
 class Table:
@@ -574,10 +575,11 @@ class Server:
     over resident tables into persistent launches, within an HBM budget.
     While it runs, the context is the worker's: register tables first."""
 
-    def __init__(self, ctx: Context, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0):
+    def __init__(self, ctx: Context, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0,
+                 max_batch_rows: int = 0):
         self.ctx = ctx
         self.lib = ctx.lib
-        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us)
+        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows)
         h = C.c_void_p()
         ctx.check(self.lib.qm_server_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h

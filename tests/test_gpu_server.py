@@ -131,3 +131,25 @@ def test_cancel_bad_descriptor_and_timeout():
         assert st["cancelled"] == 2 and st["failed"] == 1
     finally:
         srv.close()
+
+
+def test_batch_row_cap_keeps_results():
+    # a batch stops taking requests once their rows would pass max_batch_rows
+    # (a request larger than the cap runs alone); results are unchanged
+    ctx = Context(0)
+    tables, queries = workload(11)
+    handles = {k: ctx.table(v) for k, v in tables.items()}
+    alone = [handles[name].run(q) for name, q in queries]
+    cap = 700_000
+    srv = ctx.server(hbm_budget_bytes=8 << 30, max_batch=64, max_wait_us=50_000, max_batch_rows=cap)
+    try:
+        order = [i % len(queries) for i in range(24)]
+        tickets = [srv.submit(handles[queries[i][0]], queries[i][1]) for i in order]
+        for i, t in zip(order, tickets):
+            res, timing = srv.wait(t)
+            assert_same(res, alone[i])
+            rows = handles[queries[i][0]].n_rows
+            assert timing["batch_size"] == 1 or rows <= cap
+        assert srv.stats()["batches"] > 24 * 400_000 // cap // 4
+    finally:
+        srv.close()
