@@ -153,6 +153,20 @@ typedef struct {
   const qm_aggregate *aggregates;
   int32_t flags;
   int32_t reserved;
+  /* Post-aggregate ORDER BY / LIMIT / OFFSET on the result rows, as the
+   * reference's pipeline applies them after AggregateOperator
+   * (src/operators.ts:3116-3128): with order_by and has_limit, TopKOperator's
+   * heap (src/operators.ts:1716-1841, ties resolved as its heap does);
+   * order_by alone, InMemorySortOperator's stable sort by rowComparator
+   * (src/types.ts:26-38: NULL and NaN last); has_limit or offset alone, the
+   * first-seen rows [offset, offset + limit).  order_by names an output
+   * column (a group key or an aggregate's alias).  Supported by
+   * qm_query_run and qm_agg_finish. */
+  const char *order_by;
+  int32_t order_desc;
+  int32_t has_limit;
+  int64_t limit;
+  int64_t offset;
 } qm_query;
 
 /* One output column.  `data` is host memory owned by the result; dtype is

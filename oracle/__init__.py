@@ -75,6 +75,11 @@ class OracleResult(Result):
         super().__init__(columns, n_rows)
         self.diag = diag  # name -> (exact_sum float64 pair summed, abs_sum)
 
+    def take(self, order) -> "OracleResult":
+        idx = np.asarray(order, dtype=np.int64)
+        base = Result.take(self, idx)
+        return OracleResult(base.columns, base.n_rows, {k: tuple(a[idx] for a in v) for k, v in self.diag.items()})
+
 
 def _collect(L, h) -> OracleResult:
     n = L.oracle_result_num_rows(h)

@@ -87,7 +87,8 @@ class QmQuery(C.Structure):
                 ("or_filters", C.POINTER(QmFilter)), ("group_by", C.POINTER(C.c_char_p)),
                 ("n_group_by", C.c_int32), ("n_aggregates", C.c_int32),
                 ("aggregates", C.POINTER(QmAggregate)), ("flags", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("reserved", C.c_int32), ("order_by", C.c_char_p), ("order_desc", C.c_int32),
+                ("has_limit", C.c_int32), ("limit", C.c_int64), ("offset", C.c_int64)]
 
 
 class QmTuning(C.Structure):

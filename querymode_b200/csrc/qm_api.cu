@@ -109,6 +109,8 @@ struct qm_ctx {
   DevBuf masks, counts, offsets, sel_out, sel_in;
   DevBuf agg_spare;  // group table of a destroyed qm_agg, reused by the next one
   DevBuf fbits, fcounts, franks;  // first-row bitmap, its popcounts and prefix sums
+  // post-aggregate ORDER BY / LIMIT: sort keys, row orders, scratch, result
+  DevBuf post_last, post_hi, post_lo, post_idx, post_idx2, post_k1, post_k2, post_l1, post_l2, post_temp, out2;
   std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
   HostBuf hout, hstatus;
   std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
@@ -304,6 +306,13 @@ struct Plan {
   int key_col_dtype = 0;
   const DevCol *keycols[QM_MAX_KEYS] = {nullptr, nullptr, nullptr, nullptr};
   const DevCol *vcolsrc[QM_MAX_VCOLS] = {};
+  // post-aggregate ORDER BY / LIMIT / OFFSET: 0 none, 1 first-seen slice,
+  // 2 stable sort (then OFFSET), 3 TopK heap (LIMIT + OFFSET rows, then OFFSET)
+  int post = 0;
+  int post_col = -1;  // output column sorted by; -1: a name no output has
+  int post_desc = 0;
+  int post_has_limit = 0;
+  int64_t post_limit = 0, post_offset = 0;
 };
 
 const i128 BIG = (i128)1 << 100;
@@ -1212,6 +1221,99 @@ int launch_rank(qm_ctx *ctx, const GroupTable &gt) {
   return QM_OK;
 }
 
+// Column offsets of a result buffer of G rows (values, then a word bitmap
+// of NULLs for a nullable column, each 16-byte aligned); returns its bytes.
+size_t result_layout(const Plan &pl, qm_outspec &O, int64_t G) {
+  size_t off = 0;
+  const size_t null_words_bytes = (size_t)((G + 31) / 32) * 4;
+  for (int k = 0; k < O.n_out; k++) {
+    O.o[k].offset = (int64_t)off;
+    off += ((size_t)G * dtype_size(O.o[k].dtype) + 15) & ~(size_t)15;
+    if (pl.meta[k].nullable) {
+      O.o[k].null_offset = (int64_t)off;
+      off += (null_words_bytes + 15) & ~(size_t)15;
+    } else {
+      O.o[k].null_offset = -1;
+    }
+  }
+  return off;
+}
+
+// ORDER BY / LIMIT / OFFSET over the G emitted rows in ctx->out (layout O):
+// the selected rows in output order into ctx->out2 (layout O2, *G2 rows).
+int post_aggregate(qm_ctx *ctx, const Plan &pl, const qm_outspec &O, int64_t G, qm_outspec &O2, int64_t *G2,
+                   size_t *bytes2) {
+  const int64_t off0 = std::min(pl.post_offset, G);
+  const uint32_t *idx = nullptr;
+  int64_t first = 0, n = 0;
+  int rc;
+  if (pl.post == 1) {  // LimitOperator: first-seen rows [OFFSET, OFFSET + LIMIT)
+    first = off0;
+    n = pl.post_has_limit ? std::min<int64_t>(G - off0, pl.post_limit) : G - off0;
+  } else if (G > 0) {
+    const bool wide = pl.post_col >= 0 && O.o[pl.post_col].dtype == QM_I128;
+    if ((rc = ensure(ctx, ctx->post_last, G * 4)) || (rc = ensure(ctx, ctx->post_hi, G * 8)) ||
+        (rc = ensure(ctx, ctx->post_lo, G * 8)) || (rc = ensure(ctx, ctx->post_idx, G * 4)))
+      return rc;
+    if (pl.post_col >= 0) {
+      const qm_out &c = O.o[pl.post_col];
+      CK(qm_launch_sort_keys((const unsigned char *)ctx->out.p + c.offset,
+                             c.null_offset >= 0 ? (const uint32_t *)((const unsigned char *)ctx->out.p + c.null_offset)
+                                                : nullptr,
+                             c.dtype, pl.post_desc, G, (uint32_t *)ctx->post_last.p, (uint64_t *)ctx->post_hi.p,
+                             (uint64_t *)ctx->post_lo.p, (uint32_t *)ctx->post_idx.p, ctx->sm_count, ctx->stream));
+    } else {  // no output of that name: every row's value is undefined (compares equal, sorts last)
+      CK(cudaMemsetAsync(ctx->post_last.p, 1, G * 4, ctx->stream));
+      CK(cudaMemsetAsync(ctx->post_hi.p, 0, G * 8, ctx->stream));
+      CK(cudaMemsetAsync(ctx->post_lo.p, 0, G * 8, ctx->stream));
+    }
+    ctx->launches++;
+    if (pl.post == 2) {  // InMemorySortOperator: stable sort, then OFFSET
+      if (pl.post_col >= 0) {
+        size_t tb = 0;
+        CK(qm_stable_sort_rows(nullptr, nullptr, nullptr, wide, G, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                               nullptr, &tb, ctx->sm_count, ctx->stream));
+        if ((rc = ensure(ctx, ctx->post_idx2, G * 4)) || (rc = ensure(ctx, ctx->post_k1, G * 8)) ||
+            (rc = ensure(ctx, ctx->post_k2, G * 8)) || (rc = ensure(ctx, ctx->post_l1, G * 4)) ||
+            (rc = ensure(ctx, ctx->post_l2, G * 4)) || (rc = ensure(ctx, ctx->post_temp, tb + 16)))
+          return rc;
+        size_t tbytes = ctx->post_temp.bytes;
+        CK(qm_stable_sort_rows((const uint32_t *)ctx->post_last.p, (const uint64_t *)ctx->post_hi.p,
+                               (const uint64_t *)ctx->post_lo.p, wide, G, (uint32_t *)ctx->post_idx.p,
+                               (uint32_t *)ctx->post_idx2.p, (uint64_t *)ctx->post_k1.p, (uint64_t *)ctx->post_k2.p,
+                               (uint32_t *)ctx->post_l1.p, (uint32_t *)ctx->post_l2.p, ctx->post_temp.p, &tbytes,
+                               ctx->sm_count, ctx->stream));
+        ctx->launches += wide ? 7 : 5;
+        idx = (const uint32_t *)ctx->post_idx.p;
+      }
+      first = off0;
+      n = G - off0;
+    } else {  // TopKOperator: heap of LIMIT + OFFSET rows, then OFFSET
+      const int64_t k = pl.post_limit + pl.post_offset;
+      const int64_t held = std::min(k, G);
+      if ((rc = ensure(ctx, ctx->post_idx2, std::max<int64_t>(held, 1) * 4))) return rc;
+      if (G > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "ORDER BY over more than 2^32 groups");
+      CK(qm_launch_topk((const uint32_t *)ctx->post_last.p, (const uint64_t *)ctx->post_hi.p,
+                        (const uint64_t *)ctx->post_lo.p, G, k, (uint32_t *)ctx->post_idx.p,
+                        (uint32_t *)ctx->post_idx2.p, ctx->stream));
+      ctx->launches++;
+      idx = (const uint32_t *)ctx->post_idx2.p;
+      first = std::min(pl.post_offset, held);
+      n = held - first;
+    }
+  }
+  if (n < 0) n = 0;
+  O2 = O;
+  *bytes2 = result_layout(pl, O2, n);
+  if ((rc = ensure(ctx, ctx->out2, *bytes2 + 16))) return rc;
+  CK(cudaMemsetAsync(ctx->out2.p, 0, *bytes2 + 16, ctx->stream));
+  CK(qm_launch_gather_rows((const unsigned char *)ctx->out.p, O, O2, idx, first, n, (unsigned char *)ctx->out2.p,
+                           ctx->sm_count, ctx->stream));
+  if (n > 0) ctx->launches++;
+  *G2 = n;
+  return QM_OK;
+}
+
 // groups_known >= 0: launch_rank already ran and its count was read.
 int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1) {
   const Plan &pl = gt.pl;
@@ -1292,7 +1394,23 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
                       ctx->sm_count, ctx->stream));
   }
   if (G > 0) ctx->launches++;
-  CK(cudaMemcpyAsync(R->buf.p, ctx->out.p, off, cudaMemcpyDeviceToHost, ctx->stream));
+  // post-aggregate ORDER BY / LIMIT / OFFSET: only the selected rows come back
+  const void *res_dev = ctx->out.p;
+  size_t res_bytes = off;
+  if (pl.post) {
+    qm_outspec O2;
+    int64_t G2 = 0;
+    size_t b2 = 0;
+    if ((rc = post_aggregate(ctx, pl, O, G, O2, &G2, &b2))) {
+      delete R;
+      return rc;
+    }
+    O = O2;
+    G = G2;
+    res_dev = ctx->out2.p;
+    res_bytes = b2;
+  }
+  CK(cudaMemcpyAsync(R->buf.p, res_dev, res_bytes, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   cudaError_t se = cudaStreamSynchronize(ctx->stream);
   if (se != cudaSuccess) {
@@ -1405,6 +1523,22 @@ int plan_query(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl) {
   if (rc) return rc;
   pl.bytes_per_row = 0;
   for (auto *c : touched) pl.bytes_per_row += (int64_t)dtype_size(c->dtype);
+  // post-aggregate ordering (src/operators.ts:3116-3128)
+  pl.post = 0;
+  pl.post_col = -1;
+  if (q->offset < 0 || (q->has_limit && q->limit < 0))
+    return set_err(ctx, QM_ERR_INVALID, "LIMIT and OFFSET are non-negative");
+  pl.post_has_limit = q->has_limit ? 1 : 0;
+  pl.post_limit = q->has_limit ? q->limit : 0;
+  pl.post_offset = q->offset;
+  pl.post_desc = q->order_desc ? 1 : 0;
+  if (q->order_by) {
+    for (int k = 0; k < (int)pl.meta.size(); k++)
+      if (pl.meta[k].name == q->order_by) pl.post_col = k;
+    pl.post = q->has_limit ? 3 : 2;
+  } else if (q->has_limit || q->offset) {
+    pl.post = 1;
+  }
   return QM_OK;
 }
 
@@ -1625,7 +1759,9 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   DevBuf *bufs[] = {&ctx->table, &ctx->status, &ctx->keys, &ctx->slots, &ctx->keys2, &ctx->slots2,
                     &ctx->sort_temp, &ctx->counter, &ctx->out, &ctx->hll, &ctx->masks, &ctx->counts,
                     &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare, &ctx->fbits, &ctx->fcounts,
-                    &ctx->franks};
+                    &ctx->franks, &ctx->post_last, &ctx->post_hi, &ctx->post_lo, &ctx->post_idx,
+                    &ctx->post_idx2, &ctx->post_k1, &ctx->post_k2, &ctx->post_l1, &ctx->post_l2,
+                    &ctx->post_temp, &ctx->out2};
   for (DevBuf *b : bufs) release(*b);
   for (auto &b : ctx->staged) release(b);
   if (ctx->hout.p) cudaFreeHost(ctx->hout.p);
@@ -2076,7 +2212,7 @@ int qm_agg_begin(qm_ctx *ctx, const qm_query *q, qm_agg **out) {
   // deep copy (names live in a->strs; reserve so c_str() stays valid)
   int n_or = 0;
   for (int g = 0; g < q->n_or_groups; g++) n_or += q->or_group_sizes[g];
-  a->strs.reserve(2 + q->n_filters + n_or + q->n_group_by + 2 * q->n_aggregates);
+  a->strs.reserve(3 + q->n_filters + n_or + q->n_group_by + 2 * q->n_aggregates);
   auto dup = [&](const char *s) -> const char * {
     if (!s) return nullptr;
     a->strs.emplace_back(s);
@@ -2101,6 +2237,7 @@ int qm_agg_begin(qm_ctx *ctx, const qm_query *q, qm_agg **out) {
     a->aggs.push_back(ag);
   }
   a->q = *q;
+  a->q.order_by = dup(q->order_by);
   a->q.filters = a->filters.data();
   a->q.or_filters = a->or_filters.data();
   a->q.or_group_sizes = a->or_sizes.data();
@@ -2463,6 +2600,8 @@ extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
       max_groups <= 0)
     return set_err(ctx, QM_ERR_INVALID, "qm_query_run_noalloc: bad arguments");
   if (n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
+  if (q->order_by || q->has_limit || q->offset)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "ORDER BY / LIMIT / OFFSET run through qm_query_run");
   *out_groups = 0;
   cudaSetDevice(ctx->device);
   unsigned char *scratch = nullptr;
@@ -2661,6 +2800,7 @@ struct OwnedQuery {  // holds pointers into itself: never copied or moved
     q.or_filters = or_filters.empty() ? nullptr : or_filters.data();
     q.group_by = group_by.empty() ? nullptr : group_by.data();
     q.aggregates = aggs.empty() ? nullptr : aggs.data();
+    q.order_by = keep(src.order_by);
   }
 };
 
@@ -2924,6 +3064,8 @@ void batch_reset(qm_batch *b, int n) {
 int batch_plan_one(qm_batch *b, int i, const qm_table *table, const qm_query *query) {
   qm_ctx *ctx = b->ctx;
   if (!table || !query) return set_err(ctx, QM_ERR_INVALID, "query %d: null table or query", i);
+  if (query->order_by || query->has_limit || query->offset)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "query %d: ORDER BY / LIMIT / OFFSET run through qm_query_run", i);
   b->tabs[i] = table;
   b->queries[i].reset(new OwnedQuery());
   b->queries[i]->copy(*query);

@@ -192,6 +192,203 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
   }
 }
 
+// ---- post-aggregate ORDER BY / LIMIT on the emitted result rows ------------
+// A row's sort value under rowComparator (src/types.ts:26-38): NULL and NaN
+// are "last" in either direction; other values compare as JS numbers /
+// bigints (exactly: int32 / int64 / 128-bit integers, IEEE doubles with -0
+// equal to 0).  key = an unsigned 128-bit image ordered like the value,
+// bit-inverted for descending order, so ascending key order is output order.
+__device__ __forceinline__ void sort_key(const unsigned char *data, const uint32_t *nulls, int dtype, int desc,
+                                         int64_t i, uint32_t &last, uint64_t &hi, uint64_t &lo) {
+  last = (nulls && ((nulls[i >> 5] >> (i & 31)) & 1u)) ? 1u : 0u;
+  hi = 0;
+  lo = 0;
+  if (!last) {
+    switch (dtype) {
+      case QM_I32: lo = (uint64_t)(int64_t)reinterpret_cast<const int32_t *>(data)[i] ^ (1ULL << 63); break;
+      case QM_I64: lo = (uint64_t)reinterpret_cast<const int64_t *>(data)[i] ^ (1ULL << 63); break;
+      case QM_I128:
+        lo = reinterpret_cast<const uint64_t *>(data)[2 * i];
+        hi = reinterpret_cast<const uint64_t *>(data)[2 * i + 1] ^ (1ULL << 63);
+        break;
+      default: {
+        double d = reinterpret_cast<const double *>(data)[i];
+        if (isnan(d)) {
+          last = 1u;
+        } else {
+          if (d == 0.0) d = 0.0;
+          lo = (uint64_t)f2ord(d) ^ (1ULL << 63);
+        }
+      }
+    }
+  }
+  if (last) {
+    hi = 0;
+    lo = 0;
+  } else if (desc) {
+    hi = ~hi;
+    lo = ~lo;
+  }
+}
+
+__global__ void qm_sort_keys(const unsigned char *data, const uint32_t *nulls, int dtype, int desc, int64_t G,
+                             uint32_t *last, uint64_t *hi, uint64_t *lo, uint32_t *idx) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t l;
+    uint64_t h, w;
+    sort_key(data, nulls, dtype, desc, i, l, h, w);
+    last[i] = l;
+    hi[i] = h;
+    lo[i] = w;
+    idx[i] = (uint32_t)i;
+  }
+}
+
+// x[i] = src[idx[i]] (the next key of an LSD radix sort, in the order so far)
+__global__ void qm_gather_u64(const uint64_t *src, const uint32_t *idx, int64_t n, uint64_t *x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = src[idx[i]];
+}
+__global__ void qm_gather_u32(const uint32_t *src, const uint32_t *idx, int64_t n, uint32_t *x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = src[idx[i]];
+}
+
+// TopKOperator (src/operators.ts:1716-1841) over result rows 0..G-1 in
+// order, exactly: a max-heap of k row indices under the reference's cmp
+// (worse rows toward the root), a row replacing the root only when strictly
+// better, extraction by repeated root removal, reversed.  The heap itself is
+// sequential (one thread, as in the reference); rows are screened against
+// the root in parallel first: the root only improves, so a row that does not
+// beat the root at the start of its chunk cannot enter later in the chunk.
+__device__ __forceinline__ int topk_cmp(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, uint32_t a,
+                                        uint32_t b) {
+  const uint32_t la = last[a], lb = last[b];
+  if (la && lb) return 0;
+  if (la) return 1;
+  if (lb) return -1;
+  if (hi[a] != hi[b]) return hi[a] < hi[b] ? -1 : 1;
+  if (lo[a] != lo[b]) return lo[a] < lo[b] ? -1 : 1;
+  return 0;
+}
+
+__device__ __forceinline__ bool topk_better(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, uint32_t r,
+                                            uint32_t root) {
+  if (last[r]) return false;
+  if (last[root]) return true;
+  if (hi[r] != hi[root]) return hi[r] < hi[root];
+  return lo[r] < lo[root];
+}
+
+__device__ void topk_sift_down(uint32_t *h, int64_t n, int64_t i, const uint32_t *last, const uint64_t *hi,
+                               const uint64_t *lo) {
+  for (;;) {
+    int64_t t = i;
+    const int64_t l = 2 * i + 1, r = 2 * i + 2;
+    if (l < n && topk_cmp(last, hi, lo, h[l], h[t]) > 0) t = l;
+    if (r < n && topk_cmp(last, hi, lo, h[r], h[t]) > 0) t = r;
+    if (t == i) break;
+    const uint32_t x = h[i];
+    h[i] = h[t];
+    h[t] = x;
+    i = t;
+  }
+}
+
+#define QM_TOPK_THREADS 1024
+__global__ void __launch_bounds__(QM_TOPK_THREADS)
+    qm_topk_heap(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, int64_t G, int64_t k, uint32_t *heap,
+                 uint32_t *out) {
+  __shared__ uint32_t cand[QM_TOPK_THREADS];
+  __shared__ int n_cand;
+  __shared__ long long hlen;
+  if (threadIdx.x == 0) hlen = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < G; base += QM_TOPK_THREADS) {
+    const int64_t i = base + threadIdx.x;
+    const long long len = hlen;
+    bool c = i < G && k > 0;
+    if (c && len >= k) c = topk_better(last, hi, lo, (uint32_t)i, heap[0]);
+    if (threadIdx.x == 0) n_cand = 0;
+    __syncthreads();
+    // keep the candidates in row order: warp ballots, warps in turn
+    const unsigned bal = __ballot_sync(QM_FULL, c);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int wcount[QM_TOPK_THREADS / 32];
+    if (lane == 0) wcount[warp] = __popc(bal);
+    __syncthreads();
+    if (c) {
+      int off = 0;
+      for (int w = 0; w < warp; ++w) off += wcount[w];
+      cand[off + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)i;
+    }
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int w = 0; w < QM_TOPK_THREADS / 32; ++w) tot += wcount[w];
+      n_cand = tot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long n = hlen;
+      for (int j = 0; j < n_cand; ++j) {
+        const uint32_t r = cand[j];
+        if (n < k) {  // push + sift up
+          int64_t x = n++;
+          heap[x] = r;
+          while (x > 0) {
+            const int64_t p = (x - 1) >> 1;
+            if (topk_cmp(last, hi, lo, heap[x], heap[p]) > 0) {
+              const uint32_t y = heap[x];
+              heap[x] = heap[p];
+              heap[p] = y;
+              x = p;
+            } else {
+              break;
+            }
+          }
+        } else if (n > 0 && topk_better(last, hi, lo, r, heap[0])) {
+          heap[0] = r;
+          topk_sift_down(heap, n, 0, last, hi, lo);
+        }
+      }
+      hlen = n;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    // extraction: root first (the worst kept), then reversed
+    long long n = hlen;
+    const long long total = n;
+    for (long long e = 0; n > 0; ++e) {
+      out[total - 1 - e] = heap[0];
+      heap[0] = heap[n - 1];
+      --n;
+      if (n > 0) topk_sift_down(heap, n, 0, last, hi, lo);
+    }
+  }
+}
+
+// Copy the selected result rows (idx[0..n)) of every output column, with
+// their NULL bits, into a second result buffer laid out for n rows.
+__global__ void qm_gather_rows(const unsigned char *src, const __grid_constant__ qm_outspec O,
+                               const __grid_constant__ qm_outspec O2, const uint32_t *idx, int64_t first, int64_t n,
+                               unsigned char *dst) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx ? (int64_t)idx[first + j] : first + j;
+    for (int k = 0; k < O.n_out; ++k) {
+      const int w = O.o[k].dtype == QM_I128 ? 16 : (O.o[k].dtype == QM_I32 ? 4 : 8);
+      const unsigned char *s = src + O.o[k].offset + i * w;
+      unsigned char *d = dst + O2.o[k].offset + j * w;
+      for (int b = 0; b < w; b += 4) *reinterpret_cast<uint32_t *>(d + b) = *reinterpret_cast<const uint32_t *>(s + b);
+      if (O.o[k].null_offset >= 0) {
+        const uint32_t *sn = reinterpret_cast<const uint32_t *>(src + O.o[k].null_offset);
+        if ((sn[i >> 5] >> (i & 31)) & 1u)
+          atomicOr(reinterpret_cast<uint32_t *>(dst + O2.o[k].null_offset) + (j >> 5), 1u << (j & 31));
+      }
+    }
+  }
+}
+
 // Filter-only pass 1: per warp tile, the 32-bit survivor masks and counts.
 template <bool SEL>
 __global__ void __launch_bounds__(QM_SCAN_THREADS)
@@ -454,6 +651,62 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
   if (blocks < 1) return cudaSuccess;
   if (sel) qm_select_masks<true><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
   else qm_select_masks<false><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_sort_keys(const unsigned char *data, const uint32_t *nulls, int dtype, int desc, int64_t G,
+                                uint32_t *last, uint64_t *hi, uint64_t *lo, uint32_t *idx, int sm_count, cudaStream_t st) {
+  if (G <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((G + 255) / 256, (int64_t)sm_count * 8);
+  qm_sort_keys<<<blocks, 256, 0, st>>>(data, nulls, dtype, desc, G, last, hi, lo, idx);
+  return cudaGetLastError();
+}
+
+// Stable sort of result rows by (last, hi, lo): LSD passes of stable radix
+// sorts, each keyed by the next more significant word in the current order.
+// idx holds 0..G-1 on entry and the sorted order on exit; tmp* are scratch of
+// G elements.
+cudaError_t qm_stable_sort_rows(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, bool wide, int64_t G,
+                                uint32_t *idx, uint32_t *idx2, uint64_t *k1, uint64_t *k2, uint32_t *l1, uint32_t *l2,
+                                void *temp, size_t *temp_bytes, int sm_count, cudaStream_t st) {
+  size_t need = 0, t2 = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, need, k1, k2, idx, idx2, (int)G, 0, 64, st);
+  if (e != cudaSuccess) return e;
+  e = cub::DeviceRadixSort::SortPairs(nullptr, t2, l1, l2, idx, idx2, (int)G, 0, 1, st);
+  if (e != cudaSuccess) return e;
+  need = std::max(need, t2);
+  if (!temp) {
+    *temp_bytes = need;
+    return cudaSuccess;
+  }
+  if (G <= 1) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((G + 255) / 256, (int64_t)sm_count * 8);
+  const uint64_t *words[2] = {lo, wide ? hi : nullptr};
+  for (int p = 0; p < 2; ++p) {
+    if (!words[p]) continue;
+    qm_gather_u64<<<blocks, 256, 0, st>>>(words[p], idx, G, k1);
+    size_t tb = *temp_bytes;
+    if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, idx, idx2, (int)G, 0, 64, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(idx, idx2, sizeof(uint32_t) * G, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+  }
+  qm_gather_u32<<<blocks, 256, 0, st>>>(last, idx, G, l1);
+  size_t tb = *temp_bytes;
+  if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, l1, l2, idx, idx2, (int)G, 0, 1, st)) != cudaSuccess) return e;
+  return cudaMemcpyAsync(idx, idx2, sizeof(uint32_t) * G, cudaMemcpyDeviceToDevice, st);
+}
+
+cudaError_t qm_launch_topk(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, int64_t G, int64_t k,
+                           uint32_t *heap, uint32_t *out, cudaStream_t st) {
+  qm_topk_heap<<<1, QM_TOPK_THREADS, 0, st>>>(last, hi, lo, G, k, heap, out);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O, const qm_outspec &O2,
+                                  const uint32_t *idx, int64_t first, int64_t n, unsigned char *dst, int sm_count,
+                                  cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 8);
+  qm_gather_rows<<<blocks, 256, 0, st>>>(src, O, O2, idx, first, n, dst);
   return cudaGetLastError();
 }
 

@@ -62,6 +62,18 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
                                   int first_word, const uint32_t *bitmap, const uint64_t *ranks, const qm_keyspec &K,
                                   int64_t n_slots, const qm_outspec &O, unsigned char *out, int sm_count,
                                   cudaStream_t st);
+// Post-aggregate ORDER BY / LIMIT over emitted result rows (see qm_kernels.cu).
+cudaError_t qm_launch_sort_keys(const unsigned char *data, const uint32_t *nulls, int dtype, int desc, int64_t G,
+                                uint32_t *last, uint64_t *hi, uint64_t *lo, uint32_t *idx, int sm_count, cudaStream_t st);
+cudaError_t qm_stable_sort_rows(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, bool wide, int64_t G,
+                                uint32_t *idx, uint32_t *idx2, uint64_t *k1, uint64_t *k2, uint32_t *l1, uint32_t *l2,
+                                void *temp, size_t *temp_bytes, int sm_count, cudaStream_t st);
+cudaError_t qm_launch_topk(const uint32_t *last, const uint64_t *hi, const uint64_t *lo, int64_t G, int64_t k,
+                           uint32_t *heap, uint32_t *out, cudaStream_t st);
+// rows idx[first + j] (or first + j when idx is null), j < n
+cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O, const qm_outspec &O2,
+                                  const uint32_t *idx, int64_t first, int64_t n, unsigned char *dst, int sm_count,
+                                  cudaStream_t st);
 cudaError_t qm_launch_sample_pred(const qm_pred &P, int64_t n, int n_samples, unsigned long long *count,
                                   cudaStream_t st);
 cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st);

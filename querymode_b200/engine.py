@@ -169,6 +169,13 @@ class Result:
         self.stats = stats
         self.qmcb = qmcb
 
+    def take(self, order) -> "Result":
+        """The rows at `order` (a list of row indices), as a new Result."""
+        idx = np.asarray(order, dtype=np.int64)
+        cols = [ResultColumn(c.name, c.dtype, c.is_key, c.values[idx],
+                             None if c.nulls is None else c.nulls[idx]) for c in self.columns]
+        return Result(cols, len(idx), self.stats)
+
     def column(self, name: str) -> ResultColumn:
         for c in self.columns:
             if c.name == name:

@@ -51,6 +51,12 @@ class QueryDescriptor:
     group_by: list[str] | None = None
     aggregates: list[AggregateOp] | None = None
     flags: int = 0
+    # post-aggregate ORDER BY / LIMIT / OFFSET (QueryDescriptor.sortColumn,
+    # sortDirection, limit, offset)
+    sort_column: str | None = None
+    sort_desc: bool = False
+    limit: int | None = None
+    offset: int = 0
 
 
 def _value(v: Any) -> A.QmValue:
@@ -129,6 +135,15 @@ class CQuery:
         s.n_aggregates = len(aggs)
         s.aggregates = self.aggregates
         s.flags = q.flags
+        if q.sort_column is not None:
+            oc = q.sort_column.encode()
+            keep.append(oc)
+            s.order_by = oc
+            s.order_desc = 1 if q.sort_desc else 0
+        if q.limit is not None:
+            s.has_limit = 1
+            s.limit = int(q.limit)
+        s.offset = int(q.offset or 0)
         self.struct = s
 
     @property
