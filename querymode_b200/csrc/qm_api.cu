@@ -109,6 +109,7 @@ struct qm_ctx {
   DevBuf masks, counts, offsets, sel_out, sel_in;
   DevBuf agg_spare;  // group table of a destroyed qm_agg, reused by the next one
   DevBuf fbits, fcounts, franks;  // first-row bitmap, its popcounts and prefix sums
+  DevBuf zstat, zones;           // zone-map statistics pass; the kept zones of a query
   // post-aggregate ORDER BY / LIMIT: sort keys, row orders, scratch, result
   DevBuf post_last, post_hi, post_lo, post_idx, post_idx2, post_k1, post_k2, post_l1, post_l2, post_temp, out2;
   std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
@@ -203,6 +204,8 @@ struct DevCol {
   double hll = 0;
   bool has_maxabs = false;
   double maxabs = 0;  // max |x| over finite non-NULL cells (float columns)
+  bool has_zones = false;  // zone maps (QM_ZONE_ROWS rows per zone)
+  std::vector<int64_t> zmin, zmax, zcount;  // float columns: double bits
 };
 
 }  // namespace
@@ -1138,6 +1141,8 @@ struct GroupTable {
   bool scan_pending = false;  // evs0/evs1 bracket a scan not yet timed
   double scan_ms = 0;         // accumulated scan-kernel time
   int64_t sel_bound = -1;     // planner's sampled bound on selected rows, if taken
+  const uint32_t *zones = nullptr;  // kept zones (device), or null: scan every tile
+  int64_t n_zone_tiles = 0;
 };
 
 int read_status(qm_ctx *ctx, qm_status *out) {
@@ -1181,6 +1186,8 @@ void fill_args(const GroupTable &gt, qm_scan_args &a, qm_status *st) {
   a.local_hash = gt.ex.local_hash;
   a.dedupe = gt.ex.dedupe;
   a.priv = gt.ex.priv;
+  a.zones = gt.zones;
+  a.n_zone_tiles = gt.n_zone_tiles;
   a.max_probe = 1 << 12;
   a.status = st;
   a.vec_ok = 1;
@@ -1488,7 +1495,7 @@ int run_scan(qm_ctx *ctx, GroupTable &gt, int64_t n, const uint32_t *sel, bool t
   // many tiles to aggregate
   if (a.priv && n < PRIV_MIN_ROWS) a.priv = 0;
   size_t smem = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, 0, 0, a.priv);
-  if (!sel && depth >= 2 && n >= (int64_t)QM_TILE_ROWS * 256) {
+  if (!sel && !gt.zones && depth >= 2 && n >= (int64_t)QM_TILE_ROWS * 256) {
     for (; depth >= 2 && !staged; depth--) {
       if (!setup_staging(a.pred, a.stage, depth)) break;
       size_t sm = qm_scan_smem_bytes(gt.ex.local_slots, gt.ex.local_hash, gt.pl.agg.n_words, a.stage.tile_bytes, depth,
@@ -1548,6 +1555,111 @@ int plan_query(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl) {
 // ================================================================== C ABI
 
 namespace {
+
+// Zone maps of one column, computed on first use and kept on the column
+// (like its min / max): per zone of QM_ZONE_ROWS rows the non-NULL (non-NaN)
+// cells' min, max and count.
+int column_zones(qm_ctx *ctx, DevCol &c, int64_t n) {
+  if (c.has_zones) return QM_OK;
+  const int64_t zones = (n + QM_ZONE_ROWS - 1) / QM_ZONE_ROWS;
+  int rc = ensure(ctx, ctx->zstat, (size_t)std::max<int64_t>(zones, 1) * 24);
+  if (rc) return rc;
+  int64_t *d = (int64_t *)ctx->zstat.p;
+  CK(qm_launch_zone_stats(c.data, c.dtype, c.nulls, n, d, d + zones, d + 2 * zones, ctx->stream));
+  std::vector<int64_t> h((size_t)zones * 3);
+  if (zones) CK(cudaMemcpyAsync(h.data(), d, (size_t)zones * 24, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  c.zmin.assign(h.begin(), h.begin() + zones);
+  c.zmax.assign(h.begin() + zones, h.begin() + 2 * zones);
+  c.zcount.assign(h.begin() + 2 * zones, h.end());
+  c.has_zones = true;
+  return QM_OK;
+}
+
+// Can term t reject every row of zone z?  A row passes t when its cell is
+// NULL and t.null_pass, or when its value passes the test; the zone map
+// bounds the values (NaN cells, which pass no range test, are outside it).
+bool zone_rejects(const qm_term &t, const DevCol &c, int64_t z, int64_t zone_rows) {
+  const bool isf = c.dtype == QM_F64 || c.dtype == QM_F32;
+  if (t.kind == QT_TRUE)  // passes every non-NULL cell: rejects a zone of NULLs only
+    return !t.null_pass && !isf && c.zcount[z] == 0;
+  const int64_t cnt = c.zcount[z];
+  const bool all_present = cnt == zone_rows;  // no NULL (nor NaN) cell
+  if (t.null_pass && !all_present) return false;
+  bool value_may_pass = cnt > 0;
+  if (value_may_pass) {
+    if (t.kind == QT_IRANGE && !isf) {
+      value_may_pass = !(c.zmax[z] < t.lo || c.zmin[z] > t.hi);
+    } else if (t.kind == QT_INRANGE && !isf) {
+      value_may_pass = !(t.lo <= c.zmin[z] && c.zmax[z] <= t.hi);
+    } else if (t.kind == QT_FRANGE && isf) {
+      double mn, mx;
+      memcpy(&mn, &c.zmin[z], 8);
+      memcpy(&mx, &c.zmax[z], 8);
+      value_may_pass = !(mx < t.f0 || mn > t.f1);
+    } else if (t.kind == QT_FALSE) {
+      value_may_pass = false;
+    } else {
+      return false;  // other tests: no bound from the zone map
+    }
+  }
+  return !value_may_pass;
+}
+
+// Zones of table t that the plan's predicate may match (AND terms: one
+// rejecting term rejects the zone; OR groups: every group must reject).
+// Leaves gt.zones null when every zone stays.
+int plan_zones(qm_ctx *ctx, qm_table *t, GroupTable &gt) {
+  gt.zones = nullptr;
+  gt.n_zone_tiles = 0;
+  const qm_pred &P = gt.pl.pred;
+  const int64_t n = t->n_rows;
+  const int64_t nz = (n + QM_ZONE_ROWS - 1) / QM_ZONE_ROWS;
+  const int nt = P.n_groups > 0 ? P.group_end[P.n_groups - 1] : P.n_and;
+  if (nz < 4 || nt == 0) return QM_OK;
+  std::vector<DevCol *> tc(nt, nullptr);
+  bool any = false;
+  for (int i = 0; i < nt; i++) {
+    const qm_term &term = P.t[i];
+    if (term.kind == QT_TRUE && term.null_pass) continue;
+    for (auto &c : t->cols)
+      if (c.data == term.data) tc[i] = &c;
+    if (!tc[i]) continue;
+    int rc = column_zones(ctx, *tc[i], n);
+    if (rc) return rc;
+    any = true;
+  }
+  if (!any) return QM_OK;
+  std::vector<uint32_t> kept;
+  kept.reserve(nz);
+  for (int64_t z = 0; z < nz; z++) {
+    const int64_t rows = std::min<int64_t>(QM_ZONE_ROWS, n - z * QM_ZONE_ROWS);
+    auto rej = [&](int i) { return tc[i] && zone_rejects(P.t[i], *tc[i], z, rows); };
+    bool skip = false;
+    for (int i = 0; i < P.n_and && !skip; i++) skip = rej(i);
+    if (!skip && P.n_groups > 0) {
+      bool all = true;
+      int b = P.n_and;
+      for (int g = 0; g < P.n_groups && all; g++) {
+        bool grp = false;
+        for (int i = b; i < P.group_end[g] && !grp; i++) grp = rej(i);
+        all = grp;
+        b = P.group_end[g];
+      }
+      skip = all;
+    }
+    if (!skip) kept.push_back((uint32_t)z);
+  }
+  if ((int64_t)kept.size() == nz) return QM_OK;
+  int rc = ensure(ctx, ctx->zones, std::max<size_t>(kept.size(), 1) * 4);
+  if (rc) return rc;
+  if (!kept.empty())
+    CK(cudaMemcpyAsync(ctx->zones.p, kept.data(), kept.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  gt.zones = (const uint32_t *)ctx->zones.p;
+  gt.n_zone_tiles = (int64_t)kept.size() * QM_ZONE_TILES;
+  return QM_OK;
+}
 
 // Integer sums of int32 cells over a table of fewer than 2^32 rows stay
 // within a signed 64-bit word (|sum| < 2^32 * 2^31), so the global table
@@ -1761,7 +1873,7 @@ int qm_ctx_destroy(qm_ctx *ctx) {
                     &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare, &ctx->fbits, &ctx->fcounts,
                     &ctx->franks, &ctx->post_last, &ctx->post_hi, &ctx->post_lo, &ctx->post_idx,
                     &ctx->post_idx2, &ctx->post_k1, &ctx->post_k2, &ctx->post_l1, &ctx->post_l2,
-                    &ctx->post_temp, &ctx->out2};
+                    &ctx->post_temp, &ctx->out2, &ctx->zstat, &ctx->zones};
   for (DevBuf *b : bufs) release(*b);
   for (auto &b : ctx->staged) release(b);
   if (ctx->hout.p) cudaFreeHost(ctx->hout.p);
@@ -1942,6 +2054,7 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
   int64_t est = 1, direct_size = 0;
   int rc = plan_table_query(ctx, t, q, gt, est, direct_size);
   if (rc) return rc;
+  if ((rc = plan_zones(ctx, t, gt))) return rc;
   Plan &pl = gt.pl;
   gt.rows_done = 0;
   int64_t groups = -1;

@@ -9,6 +9,8 @@
 //   qm_minmax_kernel    integer column min / max (planning statistics)
 #include <cub/cub.cuh>
 
+#include <climits>
+
 #include <mutex>
 
 #include "qm_scan.cuh"
@@ -189,6 +191,68 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
     const uint64_t f = w[first_word];
     const int64_t i = (int64_t)ranks[f >> 5] + __popc(bitmap[f >> 5] & ((1u << (f & 31)) - 1u));
     emit_group<false>(t, stride, (uint64_t)s, i, K, n_slots, O, out, nullptr, nullptr);
+  }
+}
+
+// ---- zone maps -----------------------------------------------------------------
+// Per zone of QM_ZONE_ROWS rows: min and max of the non-NULL cells (integer
+// columns as int64; float columns as doubles, NaN excluded) and how many
+// such cells there are.  One block per zone.
+__global__ void qm_zone_stats(const void *p, int dtype, const uint32_t *nulls, int64_t n, int64_t *zmin,
+                              int64_t *zmax, int64_t *zcount) {
+  const int64_t z = blockIdx.x;
+  const int64_t r0 = z * QM_ZONE_ROWS, r1 = min(n, r0 + (int64_t)QM_ZONE_ROWS);
+  const bool isf = dtype == QM_F64 || dtype == QM_F32;
+  long long mn = LLONG_MAX, mx = LLONG_MIN, cnt = 0;
+  double fmn = INFINITY, fmx = -INFINITY;
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    if (cell_null(nulls, r)) continue;
+    if (isf) {
+      const double d = ld_flt(p, dtype, r);
+      if (isnan(d)) continue;
+      fmn = fmin(fmn, d);
+      fmx = fmax(fmx, d);
+    } else {
+      const long long v = ld_int(p, dtype, r);
+      mn = min(mn, v);
+      mx = max(mx, v);
+    }
+    ++cnt;
+  }
+  for (int o = 16; o; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(QM_FULL, mn, o));
+    mx = max(mx, __shfl_xor_sync(QM_FULL, mx, o));
+    fmn = fmin(fmn, __shfl_xor_sync(QM_FULL, fmn, o));
+    fmx = fmax(fmx, __shfl_xor_sync(QM_FULL, fmx, o));
+    cnt += __shfl_xor_sync(QM_FULL, cnt, o);
+  }
+  __shared__ long long smn[32], smx[32], scnt[32];
+  __shared__ double sfmn[32], sfmx[32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    smn[w] = mn;
+    smx[w] = mx;
+    scnt[w] = cnt;
+    sfmn[w] = fmn;
+    sfmx[w] = fmx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+      mn = min(mn, smn[i]);
+      mx = max(mx, smx[i]);
+      cnt += scnt[i];
+      fmn = fmin(fmn, sfmn[i]);
+      fmx = fmax(fmx, sfmx[i]);
+    }
+    if (isf) {
+      zmin[z] = __double_as_longlong(fmn);
+      zmax[z] = __double_as_longlong(fmx);
+    } else {
+      zmin[z] = mn;
+      zmax[z] = mx;
+    }
+    zcount[z] = cnt;
   }
 }
 
@@ -651,6 +715,14 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
   if (blocks < 1) return cudaSuccess;
   if (sel) qm_select_masks<true><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
   else qm_select_masks<false><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_zone_stats(const void *p, int dtype, const uint32_t *nulls, int64_t n, int64_t *zmin,
+                                 int64_t *zmax, int64_t *zcount, cudaStream_t st) {
+  const int64_t zones = (n + QM_ZONE_ROWS - 1) / QM_ZONE_ROWS;
+  if (zones <= 0) return cudaSuccess;
+  qm_zone_stats<<<(unsigned)zones, 512, 0, st>>>(p, dtype, nulls, n, zmin, zmax, zcount);
   return cudaGetLastError();
 }
 

@@ -74,6 +74,8 @@ cudaError_t qm_launch_topk(const uint32_t *last, const uint64_t *hi, const uint6
 cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O, const qm_outspec &O2,
                                   const uint32_t *idx, int64_t first, int64_t n, unsigned char *dst, int sm_count,
                                   cudaStream_t st);
+cudaError_t qm_launch_zone_stats(const void *p, int dtype, const uint32_t *nulls, int64_t n, int64_t *zmin,
+                                 int64_t *zmax, int64_t *zcount, cudaStream_t st);
 cudaError_t qm_launch_sample_pred(const qm_pred &P, int64_t n, int n_samples, unsigned long long *count,
                                   cudaStream_t st);
 cudaError_t qm_launch_hll(const qm_keyspec &K, int64_t n, uint32_t *regs, int sm_count, cudaStream_t st);

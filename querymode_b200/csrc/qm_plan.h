@@ -18,7 +18,11 @@
 #define QM_MAX_ACCS 16
 #define QM_MAX_WORDS 24
 #define QM_MAX_OUT 24
-#define QM_R 8                   // rows per lane per warp tile
+#define QM_R 8
+// Zone maps: per column min / max over zones of QM_ZONE_TILES tiles
+// (65,536 rows); zones the predicate cannot match are not scanned.
+#define QM_ZONE_TILES 256
+#define QM_ZONE_ROWS (QM_ZONE_TILES * 256)                   // rows per lane per warp tile
 #define QM_TILE_ROWS (QM_R * 32) // rows per warp tile
 
 // ---- predicate terms -------------------------------------------------------
@@ -235,6 +239,8 @@ struct qm_scan_args {
   int32_t max_probe;     // bound on linear probing in the global table
   int32_t priv;          // direct block-local table copied per warp: its
                          // (deduplicated) updates need no atomics
+  const uint32_t *zones; // zones (QM_ZONE_TILES tiles each) to scan, ascending, or null: every tile
+  int64_t n_zone_tiles;  // zones: tiles covered (count of zones x QM_ZONE_TILES)
   qm_status *status;
   qm_staging stage;
 };

@@ -120,8 +120,15 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
   if (STAGED)
     for (int64_t k = 0; k < S.depth - 1; ++k) issue(k);
 
+  // with zone maps, virtual tile v walks the kept zones' tiles
+  const int64_t n_virtual = a.zones ? a.n_zone_tiles : n_tiles;
+  auto tile_of = [&](int64_t v) -> int64_t {
+    return a.zones ? ((int64_t)a.zones[v / QM_ZONE_TILES] * QM_ZONE_TILES + v % QM_ZONE_TILES) : v;
+  };
   int64_t k = 0;
-  for (int64_t tile = first; tile < n_tiles; tile += gwarps, ++k) {
+  for (int64_t v = first; v < n_virtual; v += gwarps, ++k) {
+    const int64_t tile = tile_of(v);
+    if (tile >= n_tiles) continue;  // the table's last zone is partial
     const int64_t e0 = tile * QM_TILE_ROWS;
     uint32_t m = 0;
     if (STAGED && tile < full_tiles) {
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
     } else if (!SEL && a.vec_ok && e0 + QM_TILE_ROWS <= a.n) {
       // full dense tile: the lane's rows are r0 .. r0+7
       const int64_t r0 = e0 + (int64_t)lane * QM_R;
-      const int64_t nxt = (tile + gwarps) * QM_TILE_ROWS;
+      const int64_t nxt = v + gwarps < n_virtual ? tile_of(v + gwarps) * QM_TILE_ROWS : a.n;
       if (nxt + QM_TILE_ROWS <= a.n) prefetch_tile_l2(a.pred, nxt, lane);
       m = eval_pred_contig(a.pred, r0, (1u << QM_R) - 1);
       const uint32_t cnt = __popc(m);

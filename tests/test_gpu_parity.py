@@ -445,3 +445,29 @@ def test_large_dense_table_key_range_passes(ctx):
         g = t.run(q)
         assert g.stats.strategy in (0, 1, 2)
         assert_same(g, oracle.run(cols, q, threads=8))
+
+
+def test_zone_maps_skip_zones_exactly(ctx):
+    # sorted / clustered filter columns let whole 65,536-row zones be skipped;
+    # the result must equal a scan of every row
+    rng = np.random.default_rng(71)
+    n = 3_000_000
+    ts = np.sort(rng.integers(0, 10**12, n)).astype(np.int64)
+    f = np.repeat(rng.normal(size=n // 1000), 1000)[:n] * 100
+    f = np.concatenate([f, np.zeros(n - len(f))])
+    cols = {"ts": Column(ts, rng.random(n) < 0.001), "f": f,
+            "c": (np.arange(n) // 70_000).astype(np.int32),
+            "k": rng.integers(0, 5000, n).astype(np.int64), "v": rng.normal(size=n)}
+    t = ctx.table(cols)
+    cut = int(ts[n // 3]), int(ts[n // 3 + 200_000])
+    qs = [QueryDescriptor(filters=[FilterOp("ts", "gte", cut[0]), FilterOp("ts", "lt", cut[1])], group_by=["k"],
+                          aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")]),
+          QueryDescriptor(filters=[FilterOp("c", "eq", 7)], aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")]),
+          QueryDescriptor(filters=[FilterOp("c", "neq", 7)], group_by=["c"], aggregates=[AggregateOp("count", "*")]),
+          QueryDescriptor(filters=[FilterOp("f", "gt", 250.0)], group_by=["k"], aggregates=[AggregateOp("max", "v")]),
+          QueryDescriptor(filter_groups=[[FilterOp("c", "eq", 3)], [FilterOp("c", "between", [30, 31])]],
+                          group_by=["c"], aggregates=[AggregateOp("count", "*"), AggregateOp("min", "ts")]),
+          QueryDescriptor(filters=[FilterOp("ts", "is_null")], aggregates=[AggregateOp("count", "*")]),
+          QueryDescriptor(filters=[FilterOp("ts", "gt", 10**13)], aggregates=[AggregateOp("count", "*")])]
+    for q in qs:
+        assert_same(t.run(q), oracle.run(cols, q, threads=8))
