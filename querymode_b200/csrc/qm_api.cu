@@ -2128,12 +2128,6 @@ struct qm_agg {
 
 namespace {
 
-const char *keep_str(qm_agg *a, const char *s) {
-  if (!s) return nullptr;
-  a->strs.emplace_back(s);
-  return nullptr;
-}
-
 // Stage one batch's columns on the device: host columns are copied into
 // grow-only per-column buffers of the context, null bitmaps into word-padded
 // buffers.  Views point at the staged copies.
@@ -2356,7 +2350,6 @@ int qm_agg_begin(qm_ctx *ctx, const qm_query *q, qm_agg **out) {
   a->q.or_group_sizes = a->or_sizes.data();
   a->q.group_by = a->group_by.data();
   a->q.aggregates = a->aggs.data();
-  (void)keep_str;
   *out = a;
   return QM_OK;
 }
