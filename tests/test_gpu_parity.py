@@ -471,3 +471,23 @@ def test_zone_maps_skip_zones_exactly(ctx):
           QueryDescriptor(filters=[FilterOp("ts", "gt", 10**13)], aggregates=[AggregateOp("count", "*")])]
     for q in qs:
         assert_same(t.run(q), oracle.run(cols, q, threads=8))
+
+
+def test_large_hash_table_update_passes(ctx):
+    # a hash table far beyond L2 (4M slots), with a NULL key and a key equal
+    # to the empty-slot sentinel (both in reserved slots)
+    rng = np.random.default_rng(81)
+    n = 20_000_000
+    universe = rng.integers(-2**62, 2**62, 1_000_000).astype(np.int64)
+    universe[7] = np.iinfo(np.int64).min
+    key = universe[rng.integers(0, len(universe), n)]
+    cols = {"k": Column(key, rng.random(n) < 0.001), "x": rng.normal(size=n),
+            "f": rng.integers(0, 10, n).astype(np.int32)}
+    t = ctx.table(cols)
+    for q in (QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("sum", "x"), AggregateOp("count", "*")]),
+              QueryDescriptor(filters=[FilterOp("f", "lt", 8)], group_by=["k"],
+                              aggregates=[AggregateOp("max", "x"), AggregateOp("count", "*")])):
+        g = t.run(q)
+        assert g.stats.retries == 0
+        assert_same(g, oracle.run(cols, q, threads=16))
+        assert g.stats.rows_selected == (n if not q.filters else int((cols["f"] < 8).sum()))
