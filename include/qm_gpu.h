@@ -374,6 +374,32 @@ int qm_batch_stats(const qm_batch *batch, double *device_ms, int64_t *rows,
                    int64_t *bytes, int32_t *chunks);
 int qm_batch_destroy(qm_batch *batch);
 
+/* ---- Parquet column chunks ------------------------------------------------
+ * Build a table from Parquet column chunks whose pages are PLAIN-encoded and
+ * uncompressed (data page v1 or v2, definition levels for optional columns):
+ * the bytes the reference's decodeParquetColumnChunk reads
+ * (src/parquet-decode.ts:390-618), decoded into HBM with the same results —
+ * rows per page, NULLs from definition level 0, the v1 level section
+ * recognised as the reference recognises it.  The chunk is the bytes from
+ * the chunk's first page header (ColumnMetaData.data_page_offset) for
+ * total_compressed_size bytes; num_values is ColumnMetaData.num_values.
+ * Dictionary pages, other encodings and compressed pages give
+ * QM_ERR_UNSUPPORTED.  Every column must decode to the same row count. */
+typedef struct {
+  const char *name;
+  int32_t dtype;         /* QM_I32 / QM_I64 / QM_F32 / QM_F64: INT32 / INT64 / FLOAT / DOUBLE */
+  int32_t reserved;
+  const uint8_t *chunk;  /* host memory */
+  int64_t chunk_bytes;
+  int64_t num_values;
+} qm_parquet_column;
+
+int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *cols, qm_table **out);
+/* Copy a table column back to the host: values (n_rows cells of its dtype,
+ * 0 where NULL) and/or one byte per row, 1 = NULL.  No counterpart in the
+ * reference (inspection and tests). */
+int qm_table_read_column(const qm_table *table, int32_t column, void *values, uint8_t *null_bytes);
+
 /* ---- serving loop -----------------------------------------------------------
  * Continuous batching of single requests over resident tables.  The reference
  * serves each query in its own durable object (src/query-do.ts fan-out, one

@@ -1,0 +1,204 @@
+"""Test infrastructure: the reference's Parquet column-chunk decode restated
+for PLAIN numeric pages, to check the device decoder against.
+
+Follows src/parquet-decode.ts: decodeParquetColumnChunk (:390-618, the
+DATA_PAGE v1 and v2 PLAIN paths, the v1 level-section heuristic),
+parsePageHeader / parseDataPageHeader(V2) (:204-276, Thrift compact
+protocol), readV1DefLevels (:108-116), decodeRleBitPacked (:119-188) and
+decodePlainValues (:280-386).  Values come back as Python numbers (int64 as
+int, like the reference's bigint) with None for NULL.
+"""
+from __future__ import annotations
+
+import struct
+
+
+class _Thrift:
+    def __init__(self, b: bytes, pos: int):
+        self.b, self.pos, self.last, self.stack = b, pos, 0, []
+
+    def varint(self) -> int:
+        v = shift = 0
+        while True:
+            c = self.b[self.pos]
+            self.pos += 1
+            v |= (c & 0x7F) << shift
+            if not c & 0x80:
+                return v
+            shift += 7
+
+    def zigzag(self) -> int:
+        v = self.varint()
+        return (v >> 1) ^ -(v & 1)
+
+    def field(self):
+        h = self.b[self.pos]
+        self.pos += 1
+        if h == 0:
+            return None
+        t, d = h & 0x0F, h >> 4
+        fid = self.last + d if d else self.zigzag()
+        self.last = fid
+        return fid, t
+
+    def skip(self, t: int):
+        if t in (1, 2):
+            return
+        if t == 3:
+            self.pos += 1
+        elif t in (4, 5, 6):
+            self.varint()
+        elif t == 7:
+            self.pos += 8
+        elif t == 8:
+            n = self.varint()
+            self.pos += n
+        elif t in (9, 10):
+            h = self.b[self.pos]
+            self.pos += 1
+            size = h >> 4
+            if size == 15:
+                size = self.varint()
+            for _ in range(size):
+                self.skip(h & 0x0F)
+        elif t == 11:
+            size = self.varint()
+            if size:
+                kv = self.b[self.pos]
+                self.pos += 1
+                for _ in range(size):
+                    self.skip(kv >> 4)
+                    self.skip(kv & 0x0F)
+        elif t == 12:
+            self.stack.append(self.last)
+            self.last = 0
+            while (f := self.field()) is not None:
+                self.skip(f[1])
+            self.last = self.stack.pop()
+
+
+def parse_page_header(b: bytes, offset: int) -> dict:
+    r = _Thrift(b, offset)
+    h = dict(type=0, uncompressed=0, compressed=0, num_values=0, encoding=0, def_len=0, rep_len=0)
+    while (f := r.field()) is not None:
+        fid, t = f
+        if fid == 1:
+            h["type"] = r.zigzag()
+        elif fid == 2:
+            h["uncompressed"] = r.zigzag()
+        elif fid == 3:
+            h["compressed"] = r.zigzag()
+        elif fid in (5, 7, 8):
+            r.stack.append(r.last)
+            r.last = 0
+            while (g := r.field()) is not None:
+                gid, gt = g
+                if gid == 1:
+                    h["num_values"] = r.zigzag()
+                elif fid != 8 and gid == 2:
+                    h["encoding"] = r.zigzag()
+                elif fid == 8 and gid == 4:
+                    h["encoding"] = r.zigzag()
+                elif fid == 8 and gid == 5:
+                    h["def_len"] = r.zigzag()
+                elif fid == 8 and gid == 6:
+                    h["rep_len"] = r.zigzag()
+                else:
+                    r.skip(gt)
+            r.last = r.stack.pop()
+        else:
+            r.skip(t)
+    h["header_size"] = r.pos - offset
+    return h
+
+
+def decode_rle_bit_packed(b: bytes, bit_width: int, max_values: int) -> list[int]:
+    values: list[int] = []
+    pos = 0
+    mask = (1 << bit_width) - 1
+    while pos < len(b) and len(values) < max_values:
+        r = _Thrift(b, pos)
+        header = r.varint()
+        pos = r.pos
+        if header & 1 == 0:
+            count = header >> 1
+            val = 0
+            for i in range((bit_width + 7) // 8):
+                if pos < len(b):
+                    val |= b[pos] << (8 * i)
+                    pos += 1
+            values += [val & mask] * min(count, max_values - len(values))
+        else:
+            groups = header >> 1
+            n = min(groups * 8, max_values - len(values))
+            bitpos = pos * 8
+            for _ in range(n):
+                v = 0
+                for k in range(bit_width):
+                    byte = bitpos >> 3
+                    bit = (b[byte] >> (bitpos & 7)) & 1 if byte < len(b) else 0
+                    v |= bit << k
+                    bitpos += 1
+                values.append(v)
+            pos += (groups * 8 * bit_width + 7) // 8
+    return values
+
+
+_FMT = {"int32": ("<i", 4), "int64": ("<q", 8), "float32": ("<f", 4), "float64": ("<d", 8)}
+
+
+def decode_plain(b: bytes, dtype: str, n: int) -> list:
+    fmt, w = _FMT[dtype]
+    n = min(n, len(b) // w)
+    return [struct.unpack_from(fmt, b, i * w)[0] for i in range(n)]
+
+
+def decode_column_chunk(b: bytes, dtype: str, num_values: int) -> list:
+    values: list = []
+    w = _FMT[dtype][1]
+    pos = 0
+    while pos < len(b) and len(values) < num_values:
+        h = parse_page_header(b, pos)
+        if h["compressed"] <= 0:
+            break
+        pos += h["header_size"]
+        page = b[pos:pos + h["compressed"]]
+        pos += h["compressed"]
+        if h["type"] not in (0, 3):
+            continue
+        if h["encoding"] != 0:
+            raise NotImplementedError("only PLAIN pages")
+        defs = None
+        off = 0
+        if h["type"] == 0:
+            if 8 <= len(page):
+                plen = struct.unpack_from("<i", page, 0)[0]
+                max_def = max(64, -(-h["num_values"] // 4) + 8)
+                if 0 < plen <= max_def and plen < len(page) - 4:
+                    rem = len(page) - 4 - plen
+                    if 0 <= rem <= h["num_values"] * w:
+                        defs = decode_rle_bit_packed(page[4:4 + plen], 1, h["num_values"])
+                        off = 4 + plen
+        else:
+            d0 = h["rep_len"]
+            if h["def_len"] > 0:
+                defs = decode_rle_bit_packed(page[d0:d0 + h["def_len"]], 1, h["num_values"])
+            off = d0 + h["def_len"]
+        nonnull = h["num_values"] if defs is None else sum(1 for d in defs if d > 0)
+        decoded = decode_plain(page[off:], dtype, nonnull)
+        if defs is not None:
+            dp = 0
+            for i in range(h["num_values"]):
+                if len(values) >= num_values:
+                    break
+                if i < len(defs) and defs[i] == 0:
+                    values.append(None)
+                else:
+                    values.append(decoded[dp] if dp < len(decoded) else None)
+                    dp += 1
+        else:
+            for v in decoded:
+                if len(values) >= num_values:
+                    break
+                values.append(v)
+    return values

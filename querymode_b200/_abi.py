@@ -125,6 +125,11 @@ class QmServerCounters(C.Structure):
                 ("resident_bytes", C.c_int64), ("peak_working_bytes", C.c_int64), ("queued", C.c_int64)]
 
 
+class QmParquetColumn(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("reserved", C.c_int32),
+                ("chunk", C.c_void_p), ("chunk_bytes", C.c_int64), ("num_values", C.c_int64)]
+
+
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libqm_gpu.so")
 
@@ -166,6 +171,8 @@ SIGNATURES = [
     ("qm_batch_stats", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                  C.POINTER(C.c_int32)]),
     ("qm_batch_destroy", C.c_int, [_P]),
+    ("qm_table_from_parquet", C.c_int, [_P, C.c_int32, C.POINTER(QmParquetColumn), _PP]),
+    ("qm_table_read_column", C.c_int, [_P, C.c_int32, C.c_void_p, C.c_void_p]),
     ("qm_server_create", C.c_int, [_P, C.POINTER(QmServerConfig), _PP]),
     ("qm_server_submit", C.c_int, [_P, _P, C.POINTER(QmQuery), C.POINTER(C.c_uint64)]),
     ("qm_server_cancel", C.c_int, [_P, C.c_uint64]),

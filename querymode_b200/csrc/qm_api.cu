@@ -3406,3 +3406,4 @@ int qm_batch_destroy(qm_batch *b) {
 }  // extern "C"
 
 #include "qm_server.cuh"
+#include "qm_parquet.cuh"

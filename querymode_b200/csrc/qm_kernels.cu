@@ -194,6 +194,100 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
   }
 }
 
+// ---- Parquet PLAIN pages -> a column ----------------------------------------
+// (src/parquet-decode.ts:390-618: decodeParquetColumnChunk's PLAIN path)
+// One thread per 32-row word: the word's presence bits from the pages'
+// definition-level runs (level 1 = a value, 0 = NULL; pages without levels
+// are all present).
+__device__ __forceinline__ int64_t pq_find_page(const qm_pq_page *pages, int n, int64_t r) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pages[mid].row0 <= r) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void qm_pq_present(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
+                              int64_t n_rows, uint32_t *present) {
+  const int64_t words = (n_rows + 31) / 32;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = 0;
+    int p = (int)pq_find_page(pages, n_pages, w * 32);
+    int ri = -1;
+    for (int b = 0; b < 32; ++b) {
+      const int64_t r = w * 32 + b;
+      if (r >= n_rows) break;
+      while (p + 1 < n_pages && pages[p + 1].row0 <= r) {
+        ++p;
+        ri = -1;
+      }
+      const qm_pq_page &pg = pages[p];
+      bool on;
+      if (pg.run0 >= pg.run1) {
+        on = true;
+      } else {
+        if (ri < 0) {  // the run holding r: binary search within the page
+          int lo = pg.run0, hi = pg.run1 - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (runs[mid].row0 <= r) lo = mid;
+            else hi = mid - 1;
+          }
+          ri = lo;
+        }
+        while (ri + 1 < pg.run1 && runs[ri + 1].row0 <= r) ++ri;
+        const qm_pq_run &run = runs[ri];
+        const int64_t k = r - run.row0;
+        if (k < 0 || k >= run.count) on = true;  // past the levels decoded: present (undefined !== 0)
+        else if (run.packed) on = (k >> 3) < run.value && ((chunk[run.byte_off + (k >> 3)] >> (k & 7)) & 1);
+        else on = run.value & 1;
+      }
+      bits |= (uint32_t)on << b;
+    }
+    present[w] = bits;
+  }
+}
+
+// Values by rank: row r of page p, present, is that page's j-th value with
+// j = rank(r) - rank(first row of p); j past the values present gives NULL
+// (as the reference's decoded[dPtr++] running out does).
+__global__ void qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, int width, int64_t n_rows,
+                              const uint32_t *present, const uint64_t *ranks, unsigned char *out, uint32_t *nulls) {
+  const int64_t words = (n_rows + 31) / 32;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t nb = 0;
+    int p = (int)pq_find_page(pages, n_pages, w * 32);
+    const uint32_t pw = present[w];
+    for (int b = 0; b < 32; ++b) {
+      const int64_t r = w * 32 + b;
+      if (r >= n_rows) break;
+      while (p + 1 < n_pages && pages[p + 1].row0 <= r) ++p;
+      const qm_pq_page &pg = pages[p];
+      unsigned char *dst = out + r * width;
+      bool null = !((pw >> b) & 1);
+      if (!null) {
+        const int64_t f = pg.row0;
+        const int64_t rank_f = (int64_t)ranks[f >> 5] + __popc(present[f >> 5] & ((1u << (f & 31)) - 1u));
+        const int64_t rank_r = (int64_t)ranks[w] + __popc(pw & ((1u << b) - 1u));
+        const int64_t j = rank_r - rank_f;
+        if (j >= pg.avail) {
+          null = true;
+        } else {
+          const uint8_t *src = chunk + pg.val_off + j * width;
+          for (int i = 0; i < width; ++i) dst[i] = src[i];
+        }
+      }
+      if (null) {
+        for (int i = 0; i < width; ++i) dst[i] = 0;
+        nb |= 1u << b;
+      }
+    }
+    if (nulls) nulls[w] = nb;
+  }
+}
+
 // ---- zone maps -----------------------------------------------------------------
 // Per zone of QM_ZONE_ROWS rows: min and max of the non-NULL cells (integer
 // columns as int64; float columns as doubles, NaN excluded) and how many
@@ -715,6 +809,23 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
   if (blocks < 1) return cudaSuccess;
   if (sel) qm_select_masks<true><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
   else qm_select_masks<false><<<blocks, QM_SCAN_THREADS, 0, st>>>(P, n, sel, masks, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
+                                int width, int64_t n_rows, uint32_t *present, uint32_t *counts, uint64_t *ranks,
+                                void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls, int sm_count,
+                                cudaStream_t st) {
+  const int64_t words = (n_rows + 31) / 32;
+  if (!temp) return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
+                                                  (int)(words + 1));
+  if (n_rows <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
+  qm_pq_present<<<blocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
+  qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
+  if (e != cudaSuccess) return e;
+  qm_pq_scatter<<<blocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, present, ranks, out, nulls);
   return cudaGetLastError();
 }
 

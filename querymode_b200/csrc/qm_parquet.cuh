@@ -1,0 +1,348 @@
+// Parquet column chunks -> a table: PLAIN-encoded numeric pages (data page
+// v1 and v2) with optional definition levels, uncompressed.  Included at the
+// end of qm_api.cu.  The page headers (Thrift compact protocol) and the run
+// headers of the RLE / bit-packed hybrid definition levels are parsed on the
+// host (a few bytes per page / run); presence bits, ranks and the values are
+// expanded on the device.  Follows decodeParquetColumnChunk's PLAIN path
+// (src/parquet-decode.ts:390-618), parsePageHeader (:239-276),
+// decodeRleBitPacked (:119-188) and decodePlainValues (:280-386).
+
+namespace {
+
+// Thrift compact protocol reader (enough for PageHeader and to skip the rest).
+struct ThriftIn {
+  const uint8_t *b;
+  int64_t n, pos;
+  bool bad = false;
+  int16_t last = 0;
+  std::vector<int16_t> stack;
+
+  uint64_t varint() {
+    uint64_t v = 0;
+    int shift = 0;
+    while (pos < n && shift < 64) {
+      const uint8_t c = b[pos++];
+      v |= (uint64_t)(c & 0x7f) << shift;
+      if (!(c & 0x80)) return v;
+      shift += 7;
+    }
+    bad = true;
+    return v;
+  }
+  int64_t zigzag() {
+    const uint64_t v = varint();
+    return (int64_t)(v >> 1) ^ -(int64_t)(v & 1);
+  }
+  // next field of the current struct: false at STOP
+  bool field(int &id, int &type) {
+    if (pos >= n) {
+      bad = true;
+      return false;
+    }
+    const uint8_t h = b[pos++];
+    if (h == 0) return false;
+    type = h & 0x0f;
+    const int delta = h >> 4;
+    id = delta ? last + delta : (int)zigzag();
+    last = (int16_t)id;
+    return true;
+  }
+  void begin() {
+    stack.push_back(last);
+    last = 0;
+  }
+  void end() {
+    last = stack.empty() ? 0 : stack.back();
+    if (!stack.empty()) stack.pop_back();
+  }
+  void skip(int type, int depth = 0) {
+    if (depth > 32) {
+      bad = true;
+      return;
+    }
+    switch (type) {
+      case 1: case 2: break;  // bool in the type nibble
+      case 3: pos += 1; break;
+      case 4: case 5: case 6: varint(); break;
+      case 7: pos += 8; break;
+      case 8: {
+        const int64_t len = (int64_t)varint();
+        pos += len;
+        break;
+      }
+      case 9: case 10: {
+        if (pos >= n) { bad = true; return; }
+        const uint8_t h = b[pos++];
+        int64_t size = h >> 4;
+        if (size == 15) size = (int64_t)varint();
+        for (int64_t i = 0; i < size && !bad; i++) skip(h & 0x0f, depth + 1);
+        break;
+      }
+      case 11: {
+        const int64_t size = (int64_t)varint();
+        if (size > 0) {
+          if (pos >= n) { bad = true; return; }
+          const uint8_t kv = b[pos++];
+          for (int64_t i = 0; i < size && !bad; i++) {
+            skip(kv >> 4, depth + 1);
+            skip(kv & 0x0f, depth + 1);
+          }
+        }
+        break;
+      }
+      case 12: {
+        begin();
+        int id, t;
+        while (!bad && field(id, t)) skip(t, depth + 1);
+        end();
+        break;
+      }
+      default: bad = true;
+    }
+    if (pos > n) bad = true;
+  }
+};
+
+struct PqHeader {
+  int type = 0;
+  int64_t uncompressed = 0, compressed = 0, num_values = 0;
+  int encoding = 0;
+  int64_t def_len = 0, rep_len = 0;
+  int64_t header_size = 0;
+};
+
+// parsePageHeader: fields 1-3, data page (5), dictionary page (7), v2 (8).
+bool pq_page_header(const uint8_t *b, int64_t n, int64_t off, PqHeader &h) {
+  ThriftIn r{b, n, off};
+  int id, t;
+  while (!r.bad && r.field(id, t)) {
+    if (id == 1 && t == 5) h.type = (int)r.zigzag();
+    else if (id == 2 && t == 5) h.uncompressed = r.zigzag();
+    else if (id == 3 && t == 5) h.compressed = r.zigzag();
+    else if ((id == 5 || id == 7 || id == 8) && t == 12) {
+      r.begin();
+      int fid, ft;
+      while (!r.bad && r.field(fid, ft)) {
+        if (fid == 1 && ft == 5) h.num_values = r.zigzag();
+        else if (id == 8 && fid == 4 && ft == 5) h.encoding = (int)r.zigzag();
+        else if (id != 8 && fid == 2 && ft == 5) h.encoding = (int)r.zigzag();
+        else if (id == 8 && fid == 5 && ft == 5) h.def_len = r.zigzag();
+        else if (id == 8 && fid == 6 && ft == 5) h.rep_len = r.zigzag();
+        else r.skip(ft);
+      }
+      r.end();
+    } else {
+      r.skip(t);
+    }
+  }
+  if (r.bad) return false;
+  h.header_size = r.pos - off;
+  return true;
+}
+
+// Run headers of an RLE / bit-packed hybrid stream of bit width 1 holding at
+// most max_values levels (decodeRleBitPacked): appended to runs with rows
+// from row0.  Returns the levels the stream yields.
+int64_t pq_def_runs(const uint8_t *b, int64_t start, int64_t end, int64_t max_values, int64_t row0,
+                    std::vector<qm_pq_run> &runs, int64_t &present) {
+  int64_t pos = start, got = 0;
+  present = 0;
+  while (pos < end && got < max_values) {
+    ThriftIn r{b, end, pos};
+    const uint64_t header = r.varint();
+    if (r.bad) break;
+    pos = r.pos;
+    qm_pq_run run{};
+    run.row0 = row0 + got;
+    if ((header & 1) == 0) {
+      const int64_t count = (int64_t)(header >> 1);
+      run.value = pos < end ? (b[pos] & 1) : 0;
+      pos += 1;
+      run.count = std::min(count, max_values - got);
+      present += run.value ? run.count : 0;
+    } else {
+      const int64_t groups = (int64_t)(header >> 1);
+      run.packed = 1;
+      run.byte_off = pos;
+      run.count = std::min(groups * 8, max_values - got);
+      run.value = (int32_t)std::max<int64_t>(0, std::min<int64_t>(end - pos, groups));
+      for (int64_t k = 0; k < run.count; k++)
+        if ((k >> 3) < run.value && ((b[pos + (k >> 3)] >> (k & 7)) & 1)) present++;
+      pos += groups;
+    }
+    if (run.count > 0) runs.push_back(run);
+    got += run.count;
+  }
+  return got;
+}
+
+int pq_width(int dtype) { return dtype == QM_I64 || dtype == QM_F64 ? 8 : 4; }
+
+// Host parse of one column chunk into pages and definition-level runs.
+int pq_parse_chunk(qm_ctx *ctx, const qm_parquet_column &c, std::vector<qm_pq_page> &pages,
+                   std::vector<qm_pq_run> &runs, int64_t &rows) {
+  const uint8_t *b = c.chunk;
+  const int64_t n = c.chunk_bytes;
+  const int w = pq_width(c.dtype);
+  int64_t pos = 0;
+  rows = 0;
+  while (pos < n && rows < c.num_values) {
+    PqHeader h;
+    if (!pq_page_header(b, n, pos, h) || h.compressed <= 0) break;
+    pos += h.header_size;
+    const int64_t data = pos, data_end = std::min(n, pos + h.compressed);
+    pos += h.compressed;
+    if (h.type == 2)
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dictionary-encoded pages are not decoded on the GPU", c.name);
+    if (h.type != 0 && h.type != 3) continue;  // other page types are skipped
+    if (h.encoding != 0)
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: page encoding %d (only PLAIN)", c.name, h.encoding);
+    if (h.compressed != h.uncompressed)
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: compressed pages (pass an uncompressed chunk)", c.name);
+    const int64_t len = data_end - data;
+    qm_pq_page pg{};
+    pg.row0 = rows;
+    pg.run0 = pg.run1 = (int32_t)runs.size();
+    int64_t plain = data;
+    bool has_def = false;
+    int64_t nonnull = 0;
+    if (h.type == 0) {
+      // v1: levels behind a 4-byte length, recognised as the reference does
+      if (8 <= len) {
+        int32_t plen;
+        memcpy(&plen, b + data, 4);
+        const int64_t max_def = std::max<int64_t>(64, (h.num_values + 3) / 4 + 8);
+        if (plen > 0 && plen <= max_def && plen < len - 4) {
+          const int64_t rem = len - 4 - plen;
+          if (rem >= 0 && rem <= h.num_values * w) {
+            pq_def_runs(b, data + 4, data + 4 + plen, h.num_values, rows, runs, nonnull);
+            plain = data + 4 + plen;
+            has_def = true;
+          }
+        }
+      }
+    } else {
+      const int64_t def0 = data + h.rep_len;
+      if (h.def_len > 0) {
+        pq_def_runs(b, def0, std::min(data_end, def0 + h.def_len), h.num_values, rows, runs, nonnull);
+        has_def = true;
+      }
+      plain = def0 + h.def_len;
+    }
+    pg.run1 = (int32_t)runs.size();
+    pg.val_off = plain;
+    pg.avail = std::max<int64_t>(0, (data_end - plain) / w);
+    if (has_def) {
+      pg.rows = h.num_values;
+      pg.avail = std::min(pg.avail, nonnull);  // decodePlainValues(plain, dtype, nonNullCount)
+    } else {
+      pg.rows = std::min(h.num_values, pg.avail);
+      pg.run1 = pg.run0;
+    }
+    pg.rows = std::min(pg.rows, c.num_values - rows);
+    if (pg.rows <= 0) continue;
+    pages.push_back(pg);
+    rows += pg.rows;
+  }
+  return QM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *cols, qm_table **out) {
+  if (!ctx || !out || n_cols <= 0 || !cols) return set_err(ctx, QM_ERR_INVALID, "qm_table_from_parquet: bad arguments");
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  qm_table *t = new qm_table();
+  t->ctx = ctx;
+  DevBuf chunk, pgs, rns, present, counts, ranks, temp;
+  auto fail = [&](int rc) {
+    DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};
+    for (DevBuf *x : bufs) release(*x);
+    qm_table_destroy(t);
+    return rc;
+  };
+  for (int i = 0; i < n_cols; i++) {
+    const qm_parquet_column &c = cols[i];
+    if (!c.name || (!c.chunk && c.chunk_bytes > 0) || c.chunk_bytes < 0 || c.num_values < 0 ||
+        (c.dtype != QM_I32 && c.dtype != QM_I64 && c.dtype != QM_F32 && c.dtype != QM_F64))
+      return fail(set_err(ctx, QM_ERR_INVALID, "parquet column %d: bad descriptor", i));
+    std::vector<qm_pq_page> pages;
+    std::vector<qm_pq_run> runs;
+    int64_t rows = 0;
+    int rc = pq_parse_chunk(ctx, c, pages, runs, rows);
+    if (rc) return fail(rc);
+    if (i == 0) {
+      if (rows > 0xffffffffLL) return fail(set_err(ctx, QM_ERR_UNSUPPORTED, "tables are limited to 2^32-1 rows"));
+      t->n_rows = rows;
+    } else if (rows != t->n_rows) {
+      return fail(set_err(ctx, QM_ERR_INVALID, "column %s decodes to %lld rows, column %s to %lld", c.name,
+                          (long long)rows, cols[0].name, (long long)t->n_rows));
+    }
+    for (auto &e : t->cols)
+      if (e.name == c.name) return fail(set_err(ctx, QM_ERR_INVALID, "duplicate column %s", c.name));
+    const int w = pq_width(c.dtype);
+    const int64_t words = (rows + 31) / 32;
+    size_t tb = 0;
+    CK(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb, nullptr,
+                           nullptr, ctx->sm_count, ctx->stream));
+    if ((rc = ensure(ctx, chunk, (size_t)c.chunk_bytes + 16)) ||
+        (rc = ensure(ctx, pgs, std::max<size_t>(pages.size(), 1) * sizeof(qm_pq_page))) ||
+        (rc = ensure(ctx, rns, std::max<size_t>(runs.size(), 1) * sizeof(qm_pq_run))) ||
+        (rc = ensure(ctx, present, (size_t)(words + 1) * 4)) || (rc = ensure(ctx, counts, (size_t)(words + 1) * 4)) ||
+        (rc = ensure(ctx, ranks, (size_t)(words + 1) * 8)) || (rc = ensure(ctx, temp, tb + 16)))
+      return fail(rc);
+    DevCol col;
+    col.name = c.name;
+    col.dtype = c.dtype;
+    const bool nullable = !runs.empty();
+    if (cudaMalloc(&col.data, std::max<size_t>((size_t)rows * w, 16)) != cudaSuccess ||
+        (nullable && cudaMalloc((void **)&col.nulls, (size_t)std::max<int64_t>(words, 1) * 4) != cudaSuccess)) {
+      cudaGetLastError();
+      free_col(col);
+      return fail(set_err(ctx, QM_ERR_OOM, "column %s: device memory", c.name));
+    }
+    col.own_data = true;
+    col.own_nulls = nullable;
+    if (c.chunk_bytes)
+      CK(cudaMemcpyAsync(chunk.p, c.chunk, (size_t)c.chunk_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (!pages.empty())
+      CK(cudaMemcpyAsync(pgs.p, pages.data(), pages.size() * sizeof(qm_pq_page), cudaMemcpyHostToDevice, ctx->stream));
+    if (!runs.empty())
+      CK(cudaMemcpyAsync(rns.p, runs.data(), runs.size() * sizeof(qm_pq_run), cudaMemcpyHostToDevice, ctx->stream));
+    size_t tbytes = temp.bytes;
+    CK(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pages.size(),
+                           (const qm_pq_run *)rns.p, w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
+                           (uint64_t *)ranks.p, temp.p, &tbytes, (unsigned char *)col.data, col.nulls,
+                           ctx->sm_count, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // the host vectors above go out of scope
+    t->cols.push_back(col);
+  }
+  DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};
+  for (DevBuf *x : bufs) release(*x);
+  *out = t;
+  return QM_OK;
+}
+
+int qm_table_read_column(const qm_table *t, int32_t col, void *values, uint8_t *null_bytes) {
+  if (!t || col < 0 || col >= (int32_t)t->cols.size() || (!values && !null_bytes)) return QM_ERR_INVALID;
+  qm_ctx *ctx = t->ctx;
+  cudaSetDevice(ctx->device);
+  const DevCol &c = t->cols[col];
+  const int64_t n = t->n_rows;
+  if (values && n)
+    CK(cudaMemcpyAsync(values, c.data, (size_t)n * dtype_size(c.dtype), cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<uint32_t> nb;
+  if (null_bytes && c.nulls) {
+    nb.resize((size_t)(n + 31) / 32);
+    if (n) CK(cudaMemcpyAsync(nb.data(), c.nulls, nb.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (null_bytes)
+    for (int64_t r = 0; r < n; r++) null_bytes[r] = c.nulls ? (uint8_t)((nb[r >> 5] >> (r & 31)) & 1) : 0;
+  return QM_OK;
+}
+
+}  // extern "C"

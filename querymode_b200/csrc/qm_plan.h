@@ -244,3 +244,23 @@ struct qm_scan_args {
   qm_status *status;
   qm_staging stage;
 };
+
+// ---- Parquet column chunk decode (PLAIN pages) --------------------------------
+// A page of a column chunk after its header was parsed on the host.
+struct qm_pq_page {
+  int64_t row0;     // first row of the page in the column
+  int64_t rows;     // rows the page yields
+  int64_t val_off;  // byte offset of its PLAIN values in the chunk
+  int64_t avail;    // PLAIN values present (value bytes / width)
+  int32_t run0;     // its definition-level runs: [run0, run1); none: every row present
+  int32_t run1;
+};
+// A run of the RLE / bit-packed hybrid definition levels (bit width 1).
+struct qm_pq_run {
+  int64_t row0;      // first row it covers (column-wide)
+  int64_t count;     // rows it covers
+  int64_t byte_off;  // bit-packed: its first data byte in the chunk
+  int32_t packed;    // 1 bit-packed, 0 RLE
+  int32_t value;     // RLE: the repeated level; bit-packed: data bytes present
+                     // (levels past them read as 0)
+};

@@ -340,6 +340,54 @@ class Context:
         self.check(self.lib.qm_table_create(self.h, cs.n_rows, cs.count, cs.array, C.byref(h)))
         return Table(self, h, cs.n_rows, list(columns.keys()), keep=cs.keep)
 
+    def table_from_parquet_chunks(self, chunks: list[tuple[str, int, bytes, int]]) -> "Table":
+        """A table from Parquet column chunks (name, QM dtype, chunk bytes
+        from the first page header, ColumnMetaData.num_values), PLAIN pages
+        decoded on the device."""
+        n = len(chunks)
+        arr = (A.QmParquetColumn * n)()
+        keep = []
+        for i, (name, dtype, data, num_values) in enumerate(chunks):
+            nb = name.encode()
+            buf = C.create_string_buffer(bytes(data), len(data))
+            keep += [nb, buf]
+            arr[i].name = nb
+            arr[i].dtype = dtype
+            arr[i].chunk = C.cast(buf, C.c_void_p)
+            arr[i].chunk_bytes = len(data)
+            arr[i].num_values = num_values
+        h = C.c_void_p()
+        self.check(self.lib.qm_table_from_parquet(self.h, n, arr, C.byref(h)))
+        rows = C.c_int64()
+        self.check(self.lib.qm_table_num_rows(h, C.byref(rows)))
+        t = Table(self, h, rows.value, [c[0] for c in chunks])
+        t._dtypes = [c[1] for c in chunks]
+        return t
+
+    def table_from_parquet(self, path: str, row_group: int = 0, columns: list[str] | None = None) -> "Table":
+        """One row group of a Parquet file: its INT32 / INT64 / FLOAT / DOUBLE
+        columns (or `columns`), located through the file's footer (pyarrow
+        reads the footer only; the pages are decoded on the device)."""
+        import pyarrow.parquet as pq
+        types = {"INT32": A.QM_I32, "INT64": A.QM_I64, "FLOAT": A.QM_F32, "DOUBLE": A.QM_F64}
+        md = pq.ParquetFile(path).metadata.row_group(row_group)
+        with open(path, "rb") as f:
+            raw = f.read()
+        chunks = []
+        for c in range(md.num_columns):
+            cc = md.column(c)
+            name = cc.path_in_schema
+            if columns is not None and name not in columns:
+                continue
+            if cc.physical_type not in types:
+                if columns is not None:
+                    raise ValueError(f"column {name}: {cc.physical_type} is not a numeric column")
+                continue
+            start = cc.dictionary_page_offset if cc.dictionary_page_offset is not None else cc.data_page_offset
+            chunks.append((name, types[cc.physical_type], raw[start:start + cc.total_compressed_size],
+                           cc.num_values))
+        return self.table_from_parquet_chunks(chunks)
+
     def table_from_qmcb(self, buf: bytes) -> "Table":
         b = bytes(buf)
         h = C.c_void_p()
@@ -392,6 +440,19 @@ class Table:
         ctx._adopt(self)
 
     _close_order = 2
+
+    def read_column(self, name: str) -> tuple[np.ndarray, np.ndarray]:
+        """A column copied back to the host: (values, NULL mask)."""
+        idx = self.names.index(name)
+        dtypes = {A.QM_I32: np.int32, A.QM_I64: np.int64, A.QM_F32: np.float32, A.QM_F64: np.float64}
+        raw_types = getattr(self, "_dtypes", None)
+        if not raw_types:
+            raise ValueError("read_column needs a table whose column dtypes are known (table_from_parquet)")
+        vals = np.empty(self.n_rows, dtype=dtypes[raw_types[idx]])
+        nulls = np.empty(self.n_rows, dtype=np.uint8)
+        self.ctx.check(self.ctx.lib.qm_table_read_column(self.h, idx, vals.ctypes.data_as(C.c_void_p),
+                                                         nulls.ctypes.data_as(C.c_void_p)))
+        return vals, nulls.astype(bool)
 
     def close(self) -> None:
         if getattr(self, "h", None):

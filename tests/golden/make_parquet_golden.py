@@ -1,0 +1,39 @@
+"""Writes tests/golden/parquet_plain.json from the reference's own Parquet
+test fixture wasm/tests/fixtures/simple_plain.parquet (PLAIN pages, optional
+INT64 and DOUBLE columns): each numeric column chunk's bytes (from its first
+page header) with ColumnMetaData.num_values and the values the reference's
+test expects (tests/test_parquet.zig reads this file; pyarrow decodes it
+here as the expected values).  Run where the reference is mounted:
+
+    python tests/golden/make_parquet_golden.py /root/reference
+"""
+import base64
+import json
+import os
+import sys
+
+import pyarrow.parquet as pq
+
+
+def main(ref_root: str) -> None:
+    path = os.path.join(ref_root, "wasm", "tests", "fixtures", "simple_plain.parquet")
+    raw = open(path, "rb").read()
+    md = pq.ParquetFile(path).metadata.row_group(0)
+    table = pq.read_table(path)
+    cols = []
+    for c in range(md.num_columns):
+        cc = md.column(c)
+        if cc.physical_type not in ("INT32", "INT64", "FLOAT", "DOUBLE"):
+            continue
+        start = cc.dictionary_page_offset if cc.dictionary_page_offset is not None else cc.data_page_offset
+        cols.append({"name": cc.path_in_schema, "physical_type": cc.physical_type,
+                     "num_values": cc.num_values,
+                     "chunk": base64.b64encode(raw[start:start + cc.total_compressed_size]).decode(),
+                     "values": table.column(cc.path_in_schema).to_pylist()})
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "parquet_plain.json")
+    with open(out, "w") as f:
+        json.dump({"source": "wasm/tests/fixtures/simple_plain.parquet", "columns": cols}, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,77 @@
+"""Parquet PLAIN column chunks decoded on the device (qm_table_from_parquet)
+against the reference's decode restated (oracle/parquet.py): the same rows,
+values and NULLs; then a query over the decoded table against the oracle."""
+import base64
+import io
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle.parquet import decode_column_chunk
+from querymode_b200 import _abi as A
+from querymode_b200.engine import Column
+from querymode_b200.query import AggregateOp, FilterOp, QueryDescriptor
+from tests.helpers import assert_same
+from tests.parquet_util import PHYS, chunks_of, sample_columns, write_plain
+
+pytestmark = pytest.mark.gpu
+
+QM = {"INT32": A.QM_I32, "INT64": A.QM_I64, "FLOAT": A.QM_F32, "DOUBLE": A.QM_F64}
+NP = {"INT32": np.int32, "INT64": np.int64, "FLOAT": np.float32, "DOUBLE": np.float64}
+
+
+def check_decoded(t, name, phys, chunk, nv):
+    vals, nulls = t.read_column(name)
+    want = decode_column_chunk(chunk, PHYS[phys], nv)
+    assert len(vals) == len(want)
+    wn = np.array([w is None for w in want])
+    assert np.array_equal(nulls, wn), name
+    wv = np.array([0 if w is None else w for w in want], dtype=NP[phys])
+    assert np.array_equal(vals.view(np.uint8), wv.view(np.uint8)), name  # bit-exact, zeros where NULL
+
+
+def test_reference_fixture(ctx):
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "parquet_plain.json")))
+    chunks = [(c["name"], QM[c["physical_type"]], base64.b64decode(c["chunk"]), c["num_values"]) for c in g["columns"]]
+    t = ctx.table_from_parquet_chunks(chunks)
+    for c in g["columns"]:
+        vals, nulls = t.read_column(c["name"])
+        assert vals.tolist() == c["values"] and not nulls.any()
+
+
+@pytest.mark.parametrize("version", ["1.0", "2.0"])
+@pytest.mark.parametrize("n,page", [(50_000, 4096), (1_000_003, 1 << 20), (7, 64)])
+def test_written_files(ctx, tmp_path, version, n, page):
+    raw = write_plain(sample_columns(n, 5), version, page_size=page)
+    chunks = chunks_of(raw)
+    t = ctx.table_from_parquet_chunks([(nm, QM[ph], ch, nv) for nm, ph, ch, nv in chunks])
+    assert t.n_rows == n
+    for nm, ph, ch, nv in chunks:
+        check_decoded(t, nm, ph, ch, nv)
+    # and a query over the decoded table, against the oracle over the same data
+    path = tmp_path / "t.parquet"
+    path.write_bytes(raw)
+    t2 = ctx.table_from_parquet(str(path))
+    cols = {}
+    for nm, ph, ch, nv in chunks:
+        vals, nulls = t2.read_column(nm)
+        cols[nm] = Column(vals, nulls if nulls.any() else None)
+    q = QueryDescriptor(filters=[FilterOp("i32", "gt", 0)], group_by=["key"],
+                        aggregates=[AggregateOp("sum", "f64"), AggregateOp("count", "i64"), AggregateOp("max", "f32"),
+                                    AggregateOp("sum", "i64")])
+    assert_same(t2.run(q), oracle.run(cols, q))
+
+
+def test_unsupported_pages(ctx, tmp_path):
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+    tab = pa.table({"x": pa.array(np.arange(1000, dtype=np.int64) % 10)})
+    for kw in ({"use_dictionary": True, "compression": "NONE"}, {"use_dictionary": False, "compression": "SNAPPY"}):
+        p = tmp_path / "u.parquet"
+        pq.write_table(tab, p, **kw)
+        with pytest.raises(A.QmError) as e:
+            ctx.table_from_parquet(str(p))
+        assert e.value.status == A.QM_ERR_UNSUPPORTED
