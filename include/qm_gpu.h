@@ -395,6 +395,40 @@ typedef struct {
 } qm_parquet_column;
 
 int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *cols, qm_table **out);
+/* ---- Scan pages (Lance and Parquet) ----------------------------------------
+ * Build a table from the page buffers a scan fetches: per column its pages in
+ * order, decoded and concatenated as the reference's decodeAllColumns
+ * (src/decode.ts:201-229) does.  A page with `parquet` set (PageInfo.encoding
+ * present) is a Parquet column chunk of row_count values, decoded as
+ * qm_table_from_parquet decodes it.  Any other page is decoded as decodePage
+ * (src/decode.ts:251-331): PLAIN little-endian values; when null_count > 0
+ * and row_count > 0 the page starts with a validity bitmap of
+ * ceil(row_count / 8) bytes (bit set = a value), followed by either the
+ * non-NULL values packed (data_offset < 0) or, from byte data_offset, one
+ * slot per row (Lance v2 nullable pages, PageInfo.dataOffsetInPage).  Short
+ * pages yield what the reference's decode yields (fewer rows, or NULLs where
+ * the values run out).  Every column must decode to the same row count.
+ * Pages are staged through pinned host buffers: many small pages become a few
+ * DMA copies. */
+typedef struct {
+  const uint8_t *buf;   /* host memory */
+  int64_t bytes;
+  int64_t row_count;    /* PageInfo.rowCount (0: as many values as the bytes hold) */
+  int64_t null_count;   /* PageInfo.nullCount */
+  int64_t data_offset;  /* PageInfo.dataOffsetInPage, -1 when absent */
+  int32_t parquet;      /* 1: PageInfo.encoding present, buf is a Parquet column chunk */
+  int32_t reserved;
+} qm_page;
+
+typedef struct {
+  const char *name;
+  int32_t dtype;        /* QM_I32 / QM_I64 / QM_F32 / QM_F64 */
+  int32_t n_pages;
+  const qm_page *pages;
+} qm_page_column;
+
+int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols, qm_table **out);
+
 /* Copy a table column back to the host: values (n_rows cells of its dtype,
  * 0 where NULL) and/or one byte per row, 1 = NULL.  No counterpart in the
  * reference (inspection and tests). */

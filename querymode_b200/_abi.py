@@ -130,6 +130,15 @@ class QmParquetColumn(C.Structure):
                 ("chunk", C.c_void_p), ("chunk_bytes", C.c_int64), ("num_values", C.c_int64)]
 
 
+class QmPage(C.Structure):
+    _fields_ = [("buf", C.c_void_p), ("bytes", C.c_int64), ("row_count", C.c_int64), ("null_count", C.c_int64),
+                ("data_offset", C.c_int64), ("parquet", C.c_int32), ("reserved", C.c_int32)]
+
+
+class QmPageColumn(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("n_pages", C.c_int32), ("pages", C.POINTER(QmPage))]
+
+
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libqm_gpu.so")
 
@@ -172,6 +181,7 @@ SIGNATURES = [
                                  C.POINTER(C.c_int32)]),
     ("qm_batch_destroy", C.c_int, [_P]),
     ("qm_table_from_parquet", C.c_int, [_P, C.c_int32, C.POINTER(QmParquetColumn), _PP]),
+    ("qm_table_from_pages", C.c_int, [_P, C.c_int32, C.POINTER(QmPageColumn), _PP]),
     ("qm_table_read_column", C.c_int, [_P, C.c_int32, C.c_void_p, C.c_void_p]),
     ("qm_server_create", C.c_int, [_P, C.POINTER(QmServerConfig), _PP]),
     ("qm_server_submit", C.c_int, [_P, _P, C.POINTER(QmQuery), C.POINTER(C.c_uint64)]),

@@ -250,41 +250,51 @@ __global__ void qm_pq_present(const uint8_t *chunk, const qm_pq_page *pages, int
   }
 }
 
-// Values by rank: row r of page p, present, is that page's j-th value with
-// j = rank(r) - rank(first row of p); j past the values present gives NULL
-// (as the reference's decoded[dPtr++] running out does).
+// Values into rows, one thread per row and one warp per 32-row word (stores
+// coalesced).  A present row r of page p takes that page's value j: in a
+// packed page j = rank(r) - rank(first row of p), in a slotted page
+// j = r - row0.  j past the values present gives NULL (as the reference's
+// decoded[dPtr++] / values[vi++] running out does).
 __global__ void qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, int width, int64_t n_rows,
                               const uint32_t *present, const uint64_t *ranks, unsigned char *out, uint32_t *nulls) {
+  const int lane = threadIdx.x & 31;
   const int64_t words = (n_rows + 31) / 32;
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t nb = 0;
-    int p = (int)pq_find_page(pages, n_pages, w * 32);
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
+    const int64_t r = w * 32 + lane;
+    int p = 0;
+    if (lane == 0) p = (int)pq_find_page(pages, n_pages, w * 32);
+    p = __shfl_sync(QM_FULL, p, 0);
     const uint32_t pw = present[w];
-    for (int b = 0; b < 32; ++b) {
-      const int64_t r = w * 32 + b;
-      if (r >= n_rows) break;
+    bool null = true;
+    if (r < n_rows) {
       while (p + 1 < n_pages && pages[p + 1].row0 <= r) ++p;
       const qm_pq_page &pg = pages[p];
-      unsigned char *dst = out + r * width;
-      bool null = !((pw >> b) & 1);
-      if (!null) {
-        const int64_t f = pg.row0;
-        const int64_t rank_f = (int64_t)ranks[f >> 5] + __popc(present[f >> 5] & ((1u << (f & 31)) - 1u));
-        const int64_t rank_r = (int64_t)ranks[w] + __popc(pw & ((1u << b) - 1u));
-        const int64_t j = rank_r - rank_f;
-        if (j >= pg.avail) {
-          null = true;
+      uint64_t v = 0;
+      if ((pw >> lane) & 1) {
+        int64_t j;
+        if (pg.slotted) {
+          j = r - pg.row0;
         } else {
+          const int64_t f = pg.row0;
+          const int64_t rank_f = (int64_t)ranks[f >> 5] + __popc(present[f >> 5] & ((1u << (f & 31)) - 1u));
+          j = (int64_t)ranks[w] + __popc(pw & ((1u << lane) - 1u)) - rank_f;
+        }
+        if (j < pg.avail) {
+          null = false;
           const uint8_t *src = chunk + pg.val_off + j * width;
-          for (int i = 0; i < width; ++i) dst[i] = src[i];
+          if (((uintptr_t)src & (width - 1)) == 0) {
+            v = width == 8 ? *(const uint64_t *)src : *(const uint32_t *)src;
+          } else {
+            for (int i = width - 1; i >= 0; --i) v = (v << 8) | src[i];
+          }
         }
       }
-      if (null) {
-        for (int i = 0; i < width; ++i) dst[i] = 0;
-        nb |= 1u << b;
-      }
+      if (width == 8) ((uint64_t *)out)[r] = v;
+      else ((uint32_t *)out)[r] = (uint32_t)v;
     }
-    if (nulls) nulls[w] = nb;
+    const uint32_t nb = __ballot_sync(QM_FULL, null && r < n_rows);
+    if (nulls && lane == 0) nulls[w] = nb;
   }
 }
 
@@ -825,7 +835,8 @@ cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, i
   qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
   cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
   if (e != cudaSuccess) return e;
-  qm_pq_scatter<<<blocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, present, ranks, out, nulls);
+  const int sblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * 8);
+  qm_pq_scatter<<<sblocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, present, ranks, out, nulls);
   return cudaGetLastError();
 }
 

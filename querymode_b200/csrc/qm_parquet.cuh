@@ -178,30 +178,52 @@ int64_t pq_def_runs(const uint8_t *b, int64_t start, int64_t end, int64_t max_va
 
 int pq_width(int dtype) { return dtype == QM_I64 || dtype == QM_F64 ? 8 : 4; }
 
-// Host parse of one column chunk into pages and definition-level runs.
-int pq_parse_chunk(qm_ctx *ctx, const qm_parquet_column &c, std::vector<qm_pq_page> &pages,
-                   std::vector<qm_pq_run> &runs, int64_t &rows) {
-  const uint8_t *b = c.chunk;
-  const int64_t n = c.chunk_bytes;
-  const int w = pq_width(c.dtype);
-  int64_t pos = 0;
-  rows = 0;
-  while (pos < n && rows < c.num_values) {
+// One column as the device decodes it: host byte segments laid end to end
+// (each at a 16-byte aligned offset) in one device buffer, the page
+// descriptors and level runs pointing into it.
+struct PqSeg {
+  const uint8_t *p;
+  int64_t bytes, off;
+};
+struct PqColumn {
+  std::vector<PqSeg> segs;
+  int64_t bytes = 0;  // device buffer size
+  std::vector<qm_pq_page> pages;
+  std::vector<qm_pq_run> runs;
+  int64_t rows = 0;
+  int64_t add_seg(const uint8_t *p, int64_t n) {
+    const int64_t off = (bytes + 15) & ~(int64_t)15;
+    segs.push_back({p, n, off});
+    bytes = off + n;
+    return off;
+  }
+};
+
+// Host parse of one Parquet column chunk (num_values values) into pages and
+// definition-level runs appended to col, its bytes at device offset base.
+int pq_parse_chunk(qm_ctx *ctx, const char *name, int dtype, const uint8_t *b, int64_t n, int64_t num_values,
+                   int64_t base, PqColumn &col) {
+  const int w = pq_width(dtype);
+  std::vector<qm_pq_run> &runs = col.runs;
+  const size_t run_first = runs.size();
+  int64_t pos = 0, rows = 0;
+  const int64_t row_base = col.rows;
+  while (pos < n && rows < num_values) {
     PqHeader h;
     if (!pq_page_header(b, n, pos, h) || h.compressed <= 0) break;
     pos += h.header_size;
     const int64_t data = pos, data_end = std::min(n, pos + h.compressed);
     pos += h.compressed;
     if (h.type == 2)
-      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dictionary-encoded pages are not decoded on the GPU", c.name);
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dictionary-encoded pages are not decoded on the GPU", name);
     if (h.type != 0 && h.type != 3) continue;  // other page types are skipped
     if (h.encoding != 0)
-      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: page encoding %d (only PLAIN)", c.name, h.encoding);
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: page encoding %d (only PLAIN)", name, h.encoding);
     if (h.compressed != h.uncompressed)
-      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: compressed pages (pass an uncompressed chunk)", c.name);
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: compressed pages (pass an uncompressed chunk)", name);
     const int64_t len = data_end - data;
     qm_pq_page pg{};
-    pg.row0 = rows;
+    pg.row0 = row_base + rows;
     pg.run0 = pg.run1 = (int32_t)runs.size();
     int64_t plain = data;
     bool has_def = false;
@@ -215,7 +237,7 @@ int pq_parse_chunk(qm_ctx *ctx, const qm_parquet_column &c, std::vector<qm_pq_pa
         if (plen > 0 && plen <= max_def && plen < len - 4) {
           const int64_t rem = len - 4 - plen;
           if (rem >= 0 && rem <= h.num_values * w) {
-            pq_def_runs(b, data + 4, data + 4 + plen, h.num_values, rows, runs, nonnull);
+            pq_def_runs(b, data + 4, data + 4 + plen, h.num_values, pg.row0, runs, nonnull);
             plain = data + 4 + plen;
             has_def = true;
           }
@@ -224,13 +246,13 @@ int pq_parse_chunk(qm_ctx *ctx, const qm_parquet_column &c, std::vector<qm_pq_pa
     } else {
       const int64_t def0 = data + h.rep_len;
       if (h.def_len > 0) {
-        pq_def_runs(b, def0, std::min(data_end, def0 + h.def_len), h.num_values, rows, runs, nonnull);
+        pq_def_runs(b, def0, std::min(data_end, def0 + h.def_len), h.num_values, pg.row0, runs, nonnull);
         has_def = true;
       }
       plain = def0 + h.def_len;
     }
     pg.run1 = (int32_t)runs.size();
-    pg.val_off = plain;
+    pg.val_off = base + plain;
     pg.avail = std::max<int64_t>(0, (data_end - plain) / w);
     if (has_def) {
       pg.rows = h.num_values;
@@ -239,20 +261,117 @@ int pq_parse_chunk(qm_ctx *ctx, const qm_parquet_column &c, std::vector<qm_pq_pa
       pg.rows = std::min(h.num_values, pg.avail);
       pg.run1 = pg.run0;
     }
-    pg.rows = std::min(pg.rows, c.num_values - rows);
-    if (pg.rows <= 0) continue;
-    pages.push_back(pg);
+    pg.rows = std::min(pg.rows, num_values - rows);
+    if (pg.rows <= 0) {
+      runs.resize(pg.run0);
+      continue;
+    }
+    col.pages.push_back(pg);
     rows += pg.rows;
   }
+  for (size_t i = run_first; i < runs.size(); i++) runs[i].byte_off += base;
+  col.rows += rows;
   return QM_OK;
+}
+
+// decodePage (src/decode.ts:251-331) for a numeric dtype: the rows a page
+// yields, its validity bitmap as one bit-packed level run, where its values
+// are.
+void lance_page(const qm_page &pa, int w, int64_t base, PqColumn &col) {
+  const int64_t rc = pa.row_count, nc = pa.null_count, n = pa.bytes;
+  qm_pq_page pg{};
+  pg.row0 = col.rows;
+  pg.run0 = pg.run1 = (int32_t)col.runs.size();
+  if (nc > 0 && rc > 0) {
+    const int64_t bm = (rc + 7) / 8;
+    if (n < bm) return;  // bitmap cut short: no rows
+    if (pa.data_offset >= 0) {  // Lance v2: every row has a slot
+      pg.slotted = 1;
+      pg.val_off = base + pa.data_offset;
+      pg.avail = std::max<int64_t>(0, n - pa.data_offset) / w;
+      pg.rows = std::min(rc, pg.avail);
+    } else {  // packed: rowCount - nullCount values after the bitmap
+      pg.val_off = base + bm;
+      pg.avail = std::max<int64_t>(0, std::min(rc - nc, (n - bm) / w));
+      pg.rows = rc;
+    }
+    if (pg.rows <= 0) return;
+    qm_pq_run run{};
+    run.row0 = pg.row0;
+    run.count = pg.rows;
+    run.byte_off = base;
+    run.packed = 1;
+    run.value = (int32_t)std::min<int64_t>(bm, INT32_MAX);
+    col.runs.push_back(run);
+    pg.run1 = pg.run0 + 1;
+  } else {
+    pg.val_off = base;
+    pg.avail = n / w;
+    pg.rows = rc > 0 ? std::min(rc, pg.avail) : pg.avail;
+    pg.avail = pg.rows;
+    if (pg.rows <= 0) return;
+  }
+  col.pages.push_back(pg);
+  col.rows += pg.rows;
+}
+
+// Host segments into the device buffer through two pinned staging buffers:
+// the column's byte image (segments at their offsets, zero between) goes
+// over in windows, the host filling one buffer while the other is copied.
+int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev) {
+  if (col.bytes <= 0) return QM_OK;
+  const int64_t win = std::min<int64_t>(col.bytes, (int64_t)64 << 20);
+  HostBuf hb[2];
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int rc = QM_OK;
+  for (int k = 0; k < 2 && rc == QM_OK; k++) {
+    if (!ctx->pool->acquire((size_t)win, hb[k])) rc = set_err(ctx, QM_ERR_OOM, "pinned staging (%lld bytes)", (long long)win);
+    else if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) rc = QM_ERR_CUDA;
+  }
+  size_t si = 0;
+  bool used[2] = {false, false};
+  for (int64_t a = 0, k = 0; rc == QM_OK && a < col.bytes; a += win, k ^= 1) {
+    const int64_t e = std::min(col.bytes, a + win);
+    if (used[k] && cudaEventSynchronize(ev[k]) != cudaSuccess) rc = QM_ERR_CUDA;
+    if (rc) break;
+    uint8_t *h = (uint8_t *)hb[k].p;
+    int64_t filled = a;
+    while (si < col.segs.size() && col.segs[si].off + col.segs[si].bytes <= a) si++;
+    for (size_t j = si; j < col.segs.size() && col.segs[j].off < e; j++) {
+      const PqSeg &g = col.segs[j];
+      const int64_t s0 = std::max(a, g.off), s1 = std::min(e, g.off + g.bytes);
+      if (s0 > filled) memset(h + (filled - a), 0, (size_t)(s0 - filled));
+      if (s1 > s0) memcpy(h + (s0 - a), g.p + (s0 - g.off), (size_t)(s1 - s0));
+      filled = std::max(filled, s1);
+    }
+    if (e > filled) memset(h + (filled - a), 0, (size_t)(e - filled));
+    if (cudaMemcpyAsync(dev + a, h, (size_t)(e - a), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaEventRecord(ev[k], ctx->stream) != cudaSuccess)
+      rc = QM_ERR_CUDA;
+    used[k] = true;
+  }
+  if (rc == QM_ERR_CUDA) set_err(ctx, QM_ERR_CUDA, "page upload: %s", cudaGetErrorString(cudaGetLastError()));
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == QM_OK)
+    rc = set_err(ctx, QM_ERR_CUDA, "page upload: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int k = 0; k < 2; k++) {
+    if (ev[k]) cudaEventDestroy(ev[k]);
+    ctx->pool->release(hb[k]);
+  }
+  return rc;
 }
 
 }  // namespace
 
 extern "C" {
 
-int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *cols, qm_table **out) {
-  if (!ctx || !out || n_cols <= 0 || !cols) return set_err(ctx, QM_ERR_INVALID, "qm_table_from_parquet: bad arguments");
+#define CKF(call)                                                                                   \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess) return fail(set_err(ctx, QM_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+  } while (0)
+
+int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols, qm_table **out) {
+  if (!ctx || !out || n_cols <= 0 || !cols) return set_err(ctx, QM_ERR_INVALID, "qm_table_from_pages: bad arguments");
   *out = nullptr;
   cudaSetDevice(ctx->device);
   qm_table *t = new qm_table();
@@ -265,39 +384,50 @@ int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *
     return rc;
   };
   for (int i = 0; i < n_cols; i++) {
-    const qm_parquet_column &c = cols[i];
-    if (!c.name || (!c.chunk && c.chunk_bytes > 0) || c.chunk_bytes < 0 || c.num_values < 0 ||
+    const qm_page_column &c = cols[i];
+    if (!c.name || c.n_pages < 0 || (c.n_pages > 0 && !c.pages) ||
         (c.dtype != QM_I32 && c.dtype != QM_I64 && c.dtype != QM_F32 && c.dtype != QM_F64))
-      return fail(set_err(ctx, QM_ERR_INVALID, "parquet column %d: bad descriptor", i));
-    std::vector<qm_pq_page> pages;
-    std::vector<qm_pq_run> runs;
-    int64_t rows = 0;
-    int rc = pq_parse_chunk(ctx, c, pages, runs, rows);
-    if (rc) return fail(rc);
+      return fail(set_err(ctx, QM_ERR_INVALID, "page column %d: bad descriptor", i));
+    for (auto &e : t->cols)
+      if (e.name == c.name) return fail(set_err(ctx, QM_ERR_INVALID, "duplicate column %s", c.name));
+    const int w = pq_width(c.dtype);
+    PqColumn pc;
+    for (int k = 0; k < c.n_pages; k++) {
+      const qm_page &pa = c.pages[k];
+      if ((!pa.buf && pa.bytes > 0) || pa.bytes < 0 || pa.row_count < 0 || pa.null_count < 0 || pa.data_offset < -1)
+        return fail(set_err(ctx, QM_ERR_INVALID, "column %s page %d: bad descriptor", c.name, k));
+      const int64_t base = pc.add_seg(pa.buf, pa.bytes);
+      if (pa.parquet) {
+        int rc = pq_parse_chunk(ctx, c.name, c.dtype, pa.buf, pa.bytes, pa.row_count, base, pc);
+        if (rc) return fail(rc);
+      } else {
+        lance_page(pa, w, base, pc);
+      }
+      if (pc.rows > 0xffffffffLL || pc.runs.size() > (size_t)INT32_MAX)
+        return fail(set_err(ctx, QM_ERR_UNSUPPORTED, "tables are limited to 2^32-1 rows"));
+    }
+    const int64_t rows = pc.rows;
     if (i == 0) {
-      if (rows > 0xffffffffLL) return fail(set_err(ctx, QM_ERR_UNSUPPORTED, "tables are limited to 2^32-1 rows"));
       t->n_rows = rows;
     } else if (rows != t->n_rows) {
       return fail(set_err(ctx, QM_ERR_INVALID, "column %s decodes to %lld rows, column %s to %lld", c.name,
                           (long long)rows, cols[0].name, (long long)t->n_rows));
     }
-    for (auto &e : t->cols)
-      if (e.name == c.name) return fail(set_err(ctx, QM_ERR_INVALID, "duplicate column %s", c.name));
-    const int w = pq_width(c.dtype);
     const int64_t words = (rows + 31) / 32;
     size_t tb = 0;
-    CK(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb, nullptr,
+    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb, nullptr,
                            nullptr, ctx->sm_count, ctx->stream));
-    if ((rc = ensure(ctx, chunk, (size_t)c.chunk_bytes + 16)) ||
-        (rc = ensure(ctx, pgs, std::max<size_t>(pages.size(), 1) * sizeof(qm_pq_page))) ||
-        (rc = ensure(ctx, rns, std::max<size_t>(runs.size(), 1) * sizeof(qm_pq_run))) ||
+    int rc;
+    if ((rc = ensure(ctx, chunk, (size_t)pc.bytes + 16)) ||
+        (rc = ensure(ctx, pgs, std::max<size_t>(pc.pages.size(), 1) * sizeof(qm_pq_page))) ||
+        (rc = ensure(ctx, rns, std::max<size_t>(pc.runs.size(), 1) * sizeof(qm_pq_run))) ||
         (rc = ensure(ctx, present, (size_t)(words + 1) * 4)) || (rc = ensure(ctx, counts, (size_t)(words + 1) * 4)) ||
         (rc = ensure(ctx, ranks, (size_t)(words + 1) * 8)) || (rc = ensure(ctx, temp, tb + 16)))
       return fail(rc);
     DevCol col;
     col.name = c.name;
     col.dtype = c.dtype;
-    const bool nullable = !runs.empty();
+    const bool nullable = !pc.runs.empty();
     if (cudaMalloc(&col.data, std::max<size_t>((size_t)rows * w, 16)) != cudaSuccess ||
         (nullable && cudaMalloc((void **)&col.nulls, (size_t)std::max<int64_t>(words, 1) * 4) != cudaSuccess)) {
       cudaGetLastError();
@@ -306,24 +436,41 @@ int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *
     }
     col.own_data = true;
     col.own_nulls = nullable;
-    if (c.chunk_bytes)
-      CK(cudaMemcpyAsync(chunk.p, c.chunk, (size_t)c.chunk_bytes, cudaMemcpyHostToDevice, ctx->stream));
-    if (!pages.empty())
-      CK(cudaMemcpyAsync(pgs.p, pages.data(), pages.size() * sizeof(qm_pq_page), cudaMemcpyHostToDevice, ctx->stream));
-    if (!runs.empty())
-      CK(cudaMemcpyAsync(rns.p, runs.data(), runs.size() * sizeof(qm_pq_run), cudaMemcpyHostToDevice, ctx->stream));
+    t->cols.push_back(col);
+    if ((rc = upload_segments(ctx, pc, (uint8_t *)chunk.p))) return fail(rc);
+    if (!pc.pages.empty())
+      CKF(cudaMemcpyAsync(pgs.p, pc.pages.data(), pc.pages.size() * sizeof(qm_pq_page), cudaMemcpyHostToDevice,
+                         ctx->stream));
+    if (!pc.runs.empty())
+      CKF(cudaMemcpyAsync(rns.p, pc.runs.data(), pc.runs.size() * sizeof(qm_pq_run), cudaMemcpyHostToDevice,
+                         ctx->stream));
     size_t tbytes = temp.bytes;
-    CK(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pages.size(),
+    CKF(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pc.pages.size(),
                            (const qm_pq_run *)rns.p, w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
                            (uint64_t *)ranks.p, temp.p, &tbytes, (unsigned char *)col.data, col.nulls,
                            ctx->sm_count, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));  // the host vectors above go out of scope
-    t->cols.push_back(col);
+    ctx->launches += 4;
+    CKF(cudaStreamSynchronize(ctx->stream));  // the host vectors above go out of scope
   }
   DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};
   for (DevBuf *x : bufs) release(*x);
   *out = t;
   return QM_OK;
+}
+#undef CKF
+
+int qm_table_from_parquet(qm_ctx *ctx, int32_t n_cols, const qm_parquet_column *cols, qm_table **out) {
+  if (!ctx || !out || n_cols <= 0 || !cols) return set_err(ctx, QM_ERR_INVALID, "qm_table_from_parquet: bad arguments");
+  std::vector<qm_page> pages((size_t)n_cols);
+  std::vector<qm_page_column> pc((size_t)n_cols);
+  for (int i = 0; i < n_cols; i++) {
+    const qm_parquet_column &c = cols[i];
+    if (c.num_values < 0 || c.chunk_bytes < 0 || (!c.chunk && c.chunk_bytes > 0))
+      return set_err(ctx, QM_ERR_INVALID, "parquet column %d: bad descriptor", i);
+    pages[i] = qm_page{c.chunk, c.chunk_bytes, c.num_values, 0, -1, 1, 0};
+    pc[i] = qm_page_column{c.name, c.dtype, 1, &pages[i]};
+  }
+  return qm_table_from_pages(ctx, n_cols, pc.data(), out);
 }
 
 int qm_table_read_column(const qm_table *t, int32_t col, void *values, uint8_t *null_bytes) {

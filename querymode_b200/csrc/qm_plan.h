@@ -254,6 +254,9 @@ struct qm_pq_page {
   int64_t avail;    // PLAIN values present (value bytes / width)
   int32_t run0;     // its definition-level runs: [run0, run1); none: every row present
   int32_t run1;
+  int32_t slotted;  // 1: one value slot per row (NULL rows too), value j = row - row0;
+                    // 0: present rows' values packed, value j = rank among present rows
+  int32_t reserved;
 };
 // A run of the RLE / bit-packed hybrid definition levels (bit width 1).
 struct qm_pq_run {

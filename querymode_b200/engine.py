@@ -53,6 +53,27 @@ class Column:
     nulls: np.ndarray | None = None
 
 
+@dataclass
+class Page:
+    """One page buffer of a scan (the reference's PageInfo beside its bytes):
+    `buf` any bytes-like object or uint8 array (read in place, not copied);
+    `parquet` marks a Parquet column chunk of `row_count` values (PageInfo
+    with an encoding); otherwise a PLAIN page with an optional validity
+    bitmap, `data_offset` = PageInfo.dataOffsetInPage."""
+    buf: Any
+    row_count: int = 0
+    null_count: int = 0
+    data_offset: int | None = None
+    parquet: bool = False
+
+
+def _host_bytes(obj) -> np.ndarray:
+    a = obj if isinstance(obj, np.ndarray) else np.frombuffer(obj, dtype=np.uint8)
+    if not a.flags.c_contiguous:
+        raise ValueError("page buffers must be contiguous")
+    return a
+
+
 class _ColumnSet:
     """Builds the qm_column array for a mapping of name -> array / Column and
     keeps every referenced buffer alive while the C side may read it."""
@@ -362,6 +383,37 @@ class Context:
         self.check(self.lib.qm_table_num_rows(h, C.byref(rows)))
         t = Table(self, h, rows.value, [c[0] for c in chunks])
         t._dtypes = [c[1] for c in chunks]
+        return t
+
+    def table_from_pages(self, columns: list[tuple[str, int, list[Page]]]) -> "Table":
+        """A table from scan pages: per column (name, QM dtype, its pages in
+        order), decoded on the device and concatenated page after page."""
+        n = len(columns)
+        arr = (A.QmPageColumn * n)()
+        keep = []
+        for i, (name, dtype, pages) in enumerate(columns):
+            nb = name.encode()
+            pa = (A.QmPage * max(len(pages), 1))()
+            keep += [nb, pa]
+            for k, pg in enumerate(pages):
+                b = _host_bytes(pg.buf)
+                keep.append(b)
+                pa[k].buf = b.ctypes.data if b.nbytes else None
+                pa[k].bytes = b.nbytes
+                pa[k].row_count = pg.row_count
+                pa[k].null_count = pg.null_count
+                pa[k].data_offset = -1 if pg.data_offset is None else pg.data_offset
+                pa[k].parquet = 1 if pg.parquet else 0
+            arr[i].name = nb
+            arr[i].dtype = dtype
+            arr[i].n_pages = len(pages)
+            arr[i].pages = pa
+        h = C.c_void_p()
+        self.check(self.lib.qm_table_from_pages(self.h, n, arr, C.byref(h)))
+        rows = C.c_int64()
+        self.check(self.lib.qm_table_num_rows(h, C.byref(rows)))
+        t = Table(self, h, rows.value, [c[0] for c in columns])
+        t._dtypes = [c[1] for c in columns]
         return t
 
     def table_from_parquet(self, path: str, row_group: int = 0, columns: list[str] | None = None) -> "Table":

@@ -52,3 +52,33 @@ def test_no_device_means_no_context():
 def test_version_string():
     lib = A.load_library()
     assert b"sm_100a" in lib.qm_version()
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes mirror of a qm_* struct has the header's size and field
+    offsets (a C program built against include/qm_gpu.h prints them)."""
+    import re
+    import subprocess
+
+    def c_name(cls):
+        return "qm_" + re.sub(r"(?<!^)([A-Z])", r"_\1", cls.__name__[2:]).lower()
+
+    mirrors = [getattr(A, n) for n in dir(A)
+               if n.startswith("Qm") and isinstance(getattr(A, n), type) and issubclass(getattr(A, n), C.Structure)]
+    assert len(mirrors) >= 14
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "qm_gpu.h"', "int main(void) {"]
+    for m in mirrors:
+        lines.append(f'  printf("{m.__name__} %zu\\n", sizeof({c_name(m)}));')
+        for f in m._fields_:
+            lines.append(f'  printf("{m.__name__}.{f[0]} %zu\\n", offsetof({c_name(m)}, {f[0]}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                          text=True).stdout.splitlines())
+    for m in mirrors:
+        assert int(got[m.__name__]) == C.sizeof(m), m.__name__
+        for f in m._fields_:
+            assert int(got[f"{m.__name__}.{f[0]}"]) == getattr(m, f[0]).offset, (m.__name__, f[0])

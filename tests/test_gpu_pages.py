@@ -1,0 +1,135 @@
+"""Scan pages decoded on the device (qm_table_from_pages) against the
+reference's decodePage / decodeAllColumns restated (oracle/pages.py): the
+reference's known answers, seeded pages of every layout including short and
+inconsistent ones, Parquet chunks among them, then a query over a table
+built from pages against the oracle."""
+import struct
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle.pages import decode_column_pages
+from querymode_b200 import _abi as A
+from querymode_b200.engine import Column, Page
+from querymode_b200.query import AggregateOp, FilterOp, QueryDescriptor
+from tests.helpers import assert_same
+from tests.page_util import as_tuples, encode_column, encode_page
+from tests.parquet_util import chunks_of, write_plain
+
+pytestmark = pytest.mark.gpu
+
+QM = {"int32": A.QM_I32, "int64": A.QM_I64, "float32": A.QM_F32, "float64": A.QM_F64}
+NP = {"int32": np.int32, "int64": np.int64, "float32": np.float32, "float64": np.float64}
+
+
+def check_column(t, name, dtype, pages):
+    vals, nulls = t.read_column(name)
+    want = decode_column_pages(as_tuples(pages), dtype)
+    assert len(vals) == len(want), name
+    wn = np.array([w is None for w in want], dtype=bool)
+    assert np.array_equal(nulls, wn), name
+    wv = np.array([0 if w is None else w for w in want], dtype=NP[dtype])
+    if dtype.startswith("float"):  # NaN payloads are not observable in the reference's numbers
+        nan = np.isnan(wv)
+        assert np.array_equal(np.isnan(vals), nan), name
+        vals, wv = vals[~nan], wv[~nan]
+    assert np.array_equal(vals.view(np.uint8), wv.view(np.uint8)), name  # bit-exact (+0 / -0 included)
+
+
+def test_reference_known_answers(ctx):  # src/decode.test.ts:11-99
+    cases = [("int32", [Page(struct.pack("<3i", 100, -50, 0))], [100, -50, 0]),
+             ("int64", [Page(struct.pack("<2q", 9007199254740993, -42))], [9007199254740993, -42]),
+             ("int32", [Page(bytes([0x05]) + struct.pack("<2i", 100, 300), 3, 1)], [100, None, 300])]
+    for dtype, pages, want in cases:
+        t = ctx.table_from_pages([("c", QM[dtype], pages)])
+        vals, nulls = t.read_column("c")
+        assert [None if z else v for v, z in zip(vals.tolist(), nulls.tolist())] == want
+    t = ctx.table_from_pages([("c", A.QM_F32, [Page(struct.pack("<2f", 3.14, -2.718))])])
+    vals, _ = t.read_column("c")
+    assert vals.tolist() == pytest.approx([3.14, -2.718], abs=5e-3)
+
+
+def random_pages(rng, dtype, n_pages):
+    w = np.dtype(NP[dtype]).itemsize
+    pages = []
+    for _ in range(n_pages):
+        n = int(rng.integers(0, 3000))
+        if dtype.startswith("int"):
+            vals = rng.integers(np.iinfo(NP[dtype]).min, np.iinfo(NP[dtype]).max, n, dtype=NP[dtype])
+        else:
+            vals = (rng.normal(size=n) * 1e6).astype(NP[dtype])
+        mask = rng.random(n) < rng.choice([0.0, 0.05, 0.5, 1.0])
+        kind = rng.integers(0, 9)
+        if kind == 7:  # a Parquet chunk among the pages
+            raw = write_plain({"c": (vals, mask if mask.any() else None)}, rng.choice(["1.0", "2.0"]),
+                              page_size=int(rng.choice([512, 4096])))
+            _, _, chunk, nv = chunks_of(raw)[0]
+            pages.append(Page(chunk, nv, 0, None, True))
+            continue
+        p = encode_page(vals, mask, ["plain", "packed", "slotted"][kind % 3], pad=int(rng.choice([1, 8, 64])))
+        buf = p.buf
+        if kind == 3:    # cut short at a random byte
+            buf = buf[:int(rng.integers(0, len(buf) + 1))]
+        elif kind == 4:  # rowCount 0: every value the bytes hold
+            p = Page(buf, 0, p.null_count, p.data_offset)
+        elif kind == 5:  # nullCount that disagrees with the bitmap
+            p = Page(buf, p.row_count, int(rng.integers(1, max(2, p.row_count + 3))), p.data_offset)
+        elif kind == 6 and p.data_offset is not None:  # slot offset past the end
+            p = Page(buf, p.row_count, p.null_count, len(buf) + int(rng.integers(0, 16)))
+        pages.append(Page(buf, p.row_count, p.null_count, p.data_offset))
+    return pages
+
+
+@pytest.mark.parametrize("dtype", ["int32", "int64", "float32", "float64"])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_random_pages(ctx, dtype, seed):
+    rng = np.random.default_rng(seed * 10 + len(dtype))
+    pages = random_pages(rng, dtype, 40)
+    t = ctx.table_from_pages([("c", QM[dtype], pages)])
+    check_column(t, "c", dtype, pages)
+
+
+def test_unaligned_values(ctx):
+    # packed values behind a 1-byte bitmap (odd offsets) and Parquet PLAIN values at any offset
+    rng = np.random.default_rng(7)
+    vals = rng.integers(-2**62, 2**62, 1001, dtype=np.int64)
+    mask = rng.random(1001) < 0.3
+    pages = [encode_page(vals[a:a + 7], mask[a:a + 7], "packed") for a in range(0, 1001, 7)]
+    t = ctx.table_from_pages([("c", A.QM_I64, pages)])
+    check_column(t, "c", "int64", pages)
+
+
+def test_query_over_pages(ctx):
+    rng = np.random.default_rng(11)
+    n = 300_000
+    key = (rng.zipf(1.3, n) % 1000).astype(np.int64)
+    qty = rng.integers(1, 100, n).astype(np.int32)
+    price = rng.random(n) * 1000
+    pmask = rng.random(n) < 0.05
+    qmask = rng.random(n) < 0.02
+    cols = [("key", A.QM_I64, encode_column(key, None, 10_000)),
+            ("qty", A.QM_I32, encode_column(qty, qmask, 10_000, ("packed", "slotted"), rng)),
+            ("price", A.QM_F64, encode_column(price, pmask, 10_000, ("packed", "slotted", "plain"), rng))]
+    t = ctx.table_from_pages(cols)
+    assert t.n_rows == n
+    ref_cols = {}
+    for name, qd, pages in cols:  # the oracle's decode of the same pages ("plain" pages drop the NULLs)
+        dt = {A.QM_I64: "int64", A.QM_I32: "int32", A.QM_F64: "float64"}[qd]
+        dec = decode_column_pages(as_tuples(pages), dt)
+        nulls = np.array([v is None for v in dec])
+        ref_cols[name] = Column(np.array([0 if v is None else v for v in dec], dtype=NP[dt]), nulls if nulls.any() else None)
+    assert ref_cols["price"].nulls.sum() < pmask.sum()
+    q = QueryDescriptor(filters=[FilterOp("qty", "gt", 10)], group_by=["key"],
+                        aggregates=[AggregateOp("sum", "price"), AggregateOp("sum", "qty"), AggregateOp("min", "price"),
+                                    AggregateOp("max", "price"), AggregateOp("count", "*"), AggregateOp("avg", "price")])
+    assert_same(t.run(q), oracle.run(ref_cols, q))
+
+
+def test_bad_descriptors(ctx):
+    with pytest.raises(A.QmError) as e:
+        ctx.table_from_pages([("a", A.QM_I32, [Page(bytes(8))]), ("b", A.QM_I32, [Page(bytes(12))])])
+    assert e.value.status == A.QM_ERR_INVALID
+    with pytest.raises(A.QmError) as e:
+        ctx.table_from_pages([("a", A.QM_I32, [Page(bytes(8), 2, 0, -5)])])
+    assert e.value.status == A.QM_ERR_INVALID
