@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--no-ingest", action="store_true")
+    p.add_argument("--ingest-reps", type=int, default=3)
     p.add_argument("--serve-queries", type=int, default=1500, help="requests per offered load")
     p.add_argument("--serve-loads", default="0.25,0.5,0.75,0.95", help="offered loads as fractions of capacity")
     p.add_argument("--batch-queries", type=int, default=256)
@@ -448,6 +450,58 @@ def run_serving(local: int, args) -> dict:
                    "filters, 1% unfiltered 16M-group; Poisson arrivals (seed 4)"}
 
 
+def run_ingest(ctx, cols: dict, args) -> dict:
+    """Scan pages in host memory -> a device table (qm_table_from_pages): the
+    events columns as 10,000-row pages (the page size of the reference's
+    benchmark data), each column's pages back to back in one host buffer
+    with a page table (offset, length, rowCount, nullCount), as a reader
+    holds a column's byte range; key, qty and ts plain, price with a
+    validity bitmap (1 % NULL) and its non-NULL values packed behind it.
+    Timed end to end (staging through pinned buffers, H2D, decode kernels)
+    by the host clock around the synchronous call."""
+    from querymode_b200 import _abi as A
+    from querymode_b200.engine import PageTable
+
+    rows_per_page = 10_000
+    n = len(next(iter(cols.values())))
+    rng = np.random.default_rng(5)
+    price_null = rng.random(n) < 0.01
+    types = {"key": A.QM_I64, "qty": A.QM_I32, "price": A.QM_F64, "ts": A.QM_I64}
+    starts = np.arange(0, n, rows_per_page, dtype=np.int64)
+    counts = np.minimum(rows_per_page, n - starts)
+    spec = []
+    page_bytes = 0
+    for name, qd in types.items():
+        v = cols[name]
+        if name == "price":
+            parts, lens, nulls = [], [], []
+            for a, c in zip(starts, counts):
+                m = price_null[a:a + c]
+                parts += [np.packbits(~m, bitorder="little"), v[a:a + c][~m].view(np.uint8)]
+                lens.append(parts[-2].nbytes + parts[-1].nbytes)
+                nulls.append(int(m.sum()))
+            buf = np.concatenate(parts)
+            lens = np.array(lens, dtype=np.int64)
+            pt = PageTable(buf, np.concatenate([[0], np.cumsum(lens)[:-1]]), lens, counts, np.array(nulls))
+        else:
+            buf = v.view(np.uint8)
+            pt = PageTable(buf, starts * v.itemsize, counts * v.itemsize, counts)
+        page_bytes += buf.nbytes
+        spec.append((name, qd, pt))
+    t = ctx.table_from_pages(spec)  # warm: pinned staging, device buffers
+    t.close()
+    times = []
+    for _ in range(args.ingest_reps):
+        t0 = time.perf_counter()
+        t = ctx.table_from_pages(spec)
+        times.append(time.perf_counter() - t0)
+        t.close()
+    med = float(np.median(times))
+    return {"workload": f"events {n} rows as {rows_per_page}-row pages, 4 columns ({len(starts)} pages each)",
+            "page_bytes": int(page_bytes), "ms": med * 1e3, "GB_per_s": page_bytes / med / 1e9,
+            "rows_per_s": n / med, "reps": args.ingest_reps, "clock": "host, around the synchronous call"}
+
+
 def run_reference(args, world, rank):
     """Reference arm: the reference's algorithm (oracle port) on the host cores."""
     if rank != 0:
@@ -579,6 +633,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cols, q, min(args.cpu_sample_rows, n))
 
+    ingest = None
+    if world == 1 and not args.no_ingest:
+        ingest = run_ingest(ctx, cols, args)
+
     batched = None
     if world == 1 and not args.no_batched:
         table.close()
@@ -604,6 +662,7 @@ def main():
             "e2e": e2e,
             "batched": batched,
             "serving": serving,
+            "ingest": ingest,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "rows_per_s": n * world * args.steps / (elapsed_max / 1e3),

@@ -195,11 +195,9 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
 }
 
 // ---- Parquet PLAIN pages -> a column ----------------------------------------
-// (src/parquet-decode.ts:390-618: decodeParquetColumnChunk's PLAIN path)
-// One thread per 32-row word: the word's presence bits from the pages'
-// definition-level runs (level 1 = a value, 0 = NULL; pages without levels
-// are all present).
-__device__ __forceinline__ int64_t pq_find_page(const qm_pq_page *pages, int n, int64_t r) {
+// (src/parquet-decode.ts:390-618: decodeParquetColumnChunk's PLAIN path, and
+// decodePage, src/decode.ts:251-331)
+__device__ __forceinline__ int pq_find_page(const qm_pq_page *pages, int n, int64_t r) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -209,92 +207,168 @@ __device__ __forceinline__ int64_t pq_find_page(const qm_pq_page *pages, int n, 
   return lo;
 }
 
-__global__ void qm_pq_present(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
-                              int64_t n_rows, uint32_t *present) {
+// The contiguous range of 32-row words this warp decodes: pages and runs
+// are then found once and followed forward.
+__device__ __forceinline__ void pq_warp_range(int64_t words, int64_t &w0, int64_t &w1) {
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t per = (words + warps - 1) / warps;
+  w0 = min(words, wid * per);
+  w1 = min(words, w0 + per);
+}
+
+// The page a lane is in, held in registers and followed forward.
+struct PqCur {
+  int p;
+  int64_t row0, next0, val_off, avail;
+  int32_t run0, run1, slotted;
+  __device__ __forceinline__ void load(const qm_pq_page *pages, int n_pages, int q) {
+    p = q;
+    const qm_pq_page &pg = pages[q];
+    row0 = pg.row0;
+    val_off = pg.val_off;
+    avail = pg.avail;
+    run0 = pg.run0;
+    run1 = pg.run1;
+    slotted = pg.slotted;
+    next0 = q + 1 < n_pages ? pages[q + 1].row0 : INT64_MAX;
+  }
+  __device__ __forceinline__ bool advance(const qm_pq_page *pages, int n_pages, int64_t r) {
+    if (r < next0) return false;
+    int q = p;
+    while (q + 1 < n_pages && pages[q + 1].row0 <= r) ++q;
+    load(pages, n_pages, q);
+    return true;
+  }
+};
+
+// Presence bits, one lane per row: definition level 1 (a value) or 0 (NULL)
+// from the page's level runs; pages without runs are all present, and so are
+// rows past the levels decoded (the reference's `undefined !== 0`).
+__global__ void __launch_bounds__(256) qm_pq_present(const uint8_t *chunk, const qm_pq_page *pages, int n_pages,
+                                                     const qm_pq_run *runs, int64_t n_rows, uint32_t *present) {
+  const int lane = threadIdx.x & 31;
   const int64_t words = (n_rows + 31) / 32;
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t bits = 0;
-    int p = (int)pq_find_page(pages, n_pages, w * 32);
-    int ri = -1;
-    for (int b = 0; b < 32; ++b) {
-      const int64_t r = w * 32 + b;
-      if (r >= n_rows) break;
-      while (p + 1 < n_pages && pages[p + 1].row0 <= r) {
-        ++p;
-        ri = -1;
-      }
-      const qm_pq_page &pg = pages[p];
-      bool on;
-      if (pg.run0 >= pg.run1) {
+  int64_t w0, w1;
+  pq_warp_range(words, w0, w1);
+  if (w0 >= w1) return;
+  PqCur c;
+  c.load(pages, n_pages, pq_find_page(pages, n_pages, min(w0 * 32 + lane, n_rows - 1)));
+  int ri = -1;
+  int64_t run_row0 = 0, run_end = -1, run_next = INT64_MAX, run_off = 0;
+  int32_t run_packed = 0, run_value = 0;
+  for (int64_t w = w0; w < w1; ++w) {
+    const int64_t r = w * 32 + lane;
+    bool on = false;
+    if (r < n_rows) {
+      if (c.advance(pages, n_pages, r)) ri = -1;
+      if (c.run0 >= c.run1) {
         on = true;
       } else {
-        if (ri < 0) {  // the run holding r: binary search within the page
-          int lo = pg.run0, hi = pg.run1 - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (runs[mid].row0 <= r) lo = mid;
-            else hi = mid - 1;
+        if (ri < 0 || r >= run_next) {
+          if (ri < 0) {  // the run holding r: binary search within the page
+            int lo = c.run0, hi = c.run1 - 1;
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (runs[mid].row0 <= r) lo = mid;
+              else hi = mid - 1;
+            }
+            ri = lo;
           }
-          ri = lo;
+          while (ri + 1 < c.run1 && runs[ri + 1].row0 <= r) ++ri;
+          const qm_pq_run &run = runs[ri];
+          run_row0 = run.row0;
+          run_end = run.row0 + run.count;
+          run_off = run.byte_off;
+          run_packed = run.packed;
+          run_value = run.value;
+          run_next = ri + 1 < c.run1 ? runs[ri + 1].row0 : INT64_MAX;
         }
-        while (ri + 1 < pg.run1 && runs[ri + 1].row0 <= r) ++ri;
-        const qm_pq_run &run = runs[ri];
-        const int64_t k = r - run.row0;
-        if (k < 0 || k >= run.count) on = true;  // past the levels decoded: present (undefined !== 0)
-        else if (run.packed) on = (k >> 3) < run.value && ((chunk[run.byte_off + (k >> 3)] >> (k & 7)) & 1);
-        else on = run.value & 1;
+        const int64_t k = r - run_row0;
+        if (k < 0 || r >= run_end) on = true;
+        else if (run_packed) on = (k >> 3) < run_value && ((chunk[run_off + (k >> 3)] >> (k & 7)) & 1);
+        else on = run_value & 1;
       }
-      bits |= (uint32_t)on << b;
     }
-    present[w] = bits;
+    const uint32_t bits = __ballot_sync(QM_FULL, on);
+    if (lane == 0) present[w] = bits;
   }
 }
 
-// Values into rows, one thread per row and one warp per 32-row word (stores
-// coalesced).  A present row r of page p takes that page's value j: in a
-// packed page j = rank(r) - rank(first row of p), in a slotted page
+// Values into rows, one lane per row, QM_PQ_UNROLL words per step with their
+// loads issued together (stores coalesced).  A present row r of page p
+// takes that page's value j: in a packed page j = rank(r) - rank(row0), in
+// a slotted page (or any page of a column without levels: present == null)
 // j = r - row0.  j past the values present gives NULL (as the reference's
 // decoded[dPtr++] / values[vi++] running out does).
-__global__ void qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, int width, int64_t n_rows,
-                              const uint32_t *present, const uint64_t *ranks, unsigned char *out, uint32_t *nulls) {
+#define QM_PQ_UNROLL 4
+__global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages,
+                                                     int width, int64_t n_rows, const uint32_t *present,
+                                                     const uint64_t *ranks, unsigned char *out, uint32_t *nulls) {
   const int lane = threadIdx.x & 31;
   const int64_t words = (n_rows + 31) / 32;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
-    const int64_t r = w * 32 + lane;
-    int p = 0;
-    if (lane == 0) p = (int)pq_find_page(pages, n_pages, w * 32);
-    p = __shfl_sync(QM_FULL, p, 0);
-    const uint32_t pw = present[w];
-    bool null = true;
-    if (r < n_rows) {
-      while (p + 1 < n_pages && pages[p + 1].row0 <= r) ++p;
-      const qm_pq_page &pg = pages[p];
-      uint64_t v = 0;
-      if ((pw >> lane) & 1) {
-        int64_t j;
-        if (pg.slotted) {
-          j = r - pg.row0;
-        } else {
-          const int64_t f = pg.row0;
-          const int64_t rank_f = (int64_t)ranks[f >> 5] + __popc(present[f >> 5] & ((1u << (f & 31)) - 1u));
-          j = (int64_t)ranks[w] + __popc(pw & ((1u << lane) - 1u)) - rank_f;
-        }
-        if (j < pg.avail) {
-          null = false;
-          const uint8_t *src = chunk + pg.val_off + j * width;
-          if (((uintptr_t)src & (width - 1)) == 0) {
-            v = width == 8 ? *(const uint64_t *)src : *(const uint32_t *)src;
+  int64_t w0, w1;
+  pq_warp_range(words, w0, w1);
+  if (w0 >= w1) return;
+  PqCur c;
+  c.load(pages, n_pages, pq_find_page(pages, n_pages, min(w0 * 32 + lane, n_rows - 1)));
+  int rank_p = -1;  // page whose first-row rank is in rank_f
+  int64_t rank_f = 0;
+  for (int64_t w = w0; w < w1; w += QM_PQ_UNROLL) {
+    const uint8_t *src[QM_PQ_UNROLL];
+    bool live[QM_PQ_UNROLL];
+#pragma unroll
+    for (int u = 0; u < QM_PQ_UNROLL; ++u) {
+      const int64_t r = (w + u) * 32 + lane;
+      live[u] = false;
+      src[u] = nullptr;
+      if (w + u < w1 && r < n_rows) {
+        c.advance(pages, n_pages, r);
+        const uint32_t pw = present ? present[w + u] : QM_FULL;
+        if ((pw >> lane) & 1) {
+          int64_t j;
+          if (c.slotted || !present) {
+            j = r - c.row0;
           } else {
-            for (int i = width - 1; i >= 0; --i) v = (v << 8) | src[i];
+            if (rank_p != c.p) {
+              const int64_t f = c.row0;
+              rank_f = (int64_t)ranks[f >> 5] + __popc(present[f >> 5] & ((1u << (f & 31)) - 1u));
+              rank_p = c.p;
+            }
+            j = (int64_t)ranks[w + u] + __popc(pw & ((1u << lane) - 1u)) - rank_f;
+          }
+          if (j < c.avail) {
+            live[u] = true;
+            src[u] = chunk + c.val_off + j * width;
           }
         }
       }
-      if (width == 8) ((uint64_t *)out)[r] = v;
-      else ((uint32_t *)out)[r] = (uint32_t)v;
     }
-    const uint32_t nb = __ballot_sync(QM_FULL, null && r < n_rows);
-    if (nulls && lane == 0) nulls[w] = nb;
+    uint64_t v[QM_PQ_UNROLL];
+#pragma unroll
+    for (int u = 0; u < QM_PQ_UNROLL; ++u) {
+      v[u] = 0;
+      if (live[u]) {
+        const uint8_t *s = src[u];
+        if (((uintptr_t)s & (width - 1)) == 0) {
+          v[u] = width == 8 ? *(const uint64_t *)s : *(const uint32_t *)s;
+        } else {
+          for (int i = width - 1; i >= 0; --i) v[u] = (v[u] << 8) | s[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < QM_PQ_UNROLL; ++u) {
+      const int64_t r = (w + u) * 32 + lane;
+      if (w + u < w1) {
+        if (r < n_rows) {
+          if (width == 8) ((uint64_t *)out)[r] = v[u];
+          else ((uint32_t *)out)[r] = (uint32_t)v[u];
+        }
+        const uint32_t nb = __ballot_sync(QM_FULL, !live[u] && r < n_rows);
+        if (nulls && lane == 0) nulls[w + u] = nb;
+      }
+    }
   }
 }
 
@@ -823,20 +897,33 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
 }
 
 cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
-                                int width, int64_t n_rows, uint32_t *present, uint32_t *counts, uint64_t *ranks,
-                                void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls, int sm_count,
-                                cudaStream_t st) {
+                                int n_runs, int width, int64_t n_rows, uint32_t *present, uint32_t *counts,
+                                uint64_t *ranks, void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls,
+                                int sm_count, cudaStream_t st) {
   const int64_t words = (n_rows + 31) / 32;
   if (!temp) return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
                                                   (int)(words + 1));
   if (n_rows <= 0) return cudaSuccess;
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
-  qm_pq_present<<<blocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
+  // one resident wave: every warp owns a fixed range of words
+  static int occ_present = 0, occ_scatter = 0;
+  if (!occ_present) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_present, qm_pq_present, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter, qm_pq_scatter, 256, 0);
+    occ_present = std::max(occ_present, 1);
+    occ_scatter = std::max(occ_scatter, 1);
+  }
+  const int pblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_present);
+  const int wblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_scatter);
+  if (n_runs == 0) {  // no levels: every row present, values by row
+    qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, nullptr, nullptr, out, nulls);
+    return cudaGetLastError();
+  }
+  qm_pq_present<<<pblocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
   qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
   cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
   if (e != cudaSuccess) return e;
-  const int sblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * 8);
-  qm_pq_scatter<<<sblocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, present, ranks, out, nulls);
+  qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, present, ranks, out, nulls);
   return cudaGetLastError();
 }
 

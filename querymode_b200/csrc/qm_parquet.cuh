@@ -7,6 +7,10 @@
 // (src/parquet-decode.ts:390-618), parsePageHeader (:239-276),
 // decodeRleBitPacked (:119-188) and decodePlainValues (:280-386).
 
+#include <condition_variable>
+#include <functional>
+#include <thread>
+
 namespace {
 
 // Thrift compact protocol reader (enough for PageHeader and to skip the rest).
@@ -315,10 +319,87 @@ void lance_page(const qm_page &pa, int w, int64_t base, PqColumn &col) {
   col.rows += pg.rows;
 }
 
+// A few host threads that run one function together (fn(part) for every
+// part), reused for every window of an upload.
+class HostTeam {
+ public:
+  explicit HostTeam(int n) : n_(n) {
+    for (int i = 1; i < n; i++) th_.emplace_back([this, i] { loop(i); });
+  }
+  ~HostTeam() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      quit_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+  int size() const { return n_; }
+  void run(const std::function<void(int)> &fn) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &fn;
+      pending_ = n_ - 1;
+      gen_++;
+    }
+    cv_.notify_all();
+    fn(0);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  void loop(int i) {
+    int64_t seen = 0;
+    for (;;) {
+      const std::function<void(int)> *fn;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return quit_ || gen_ != seen; });
+        if (quit_) return;
+        seen = gen_;
+        fn = fn_;
+      }
+      (*fn)(i);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (--pending_ == 0) done_.notify_one();
+      }
+    }
+  }
+  int n_;
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)> *fn_ = nullptr;
+  int pending_ = 0;
+  int64_t gen_ = 0;
+  bool quit_ = false;
+};
+
+// Bytes [a, e) of the column's image (segments at their offsets, zero
+// between) into h.
+void fill_window(const PqColumn &col, int64_t a, int64_t e, uint8_t *h, int64_t h0) {
+  size_t j = std::upper_bound(col.segs.begin(), col.segs.end(), a,
+                              [](int64_t x, const PqSeg &g) { return x < g.off; }) - col.segs.begin();
+  if (j > 0) j--;
+  int64_t filled = a;
+  for (; j < col.segs.size() && col.segs[j].off < e; j++) {
+    const PqSeg &g = col.segs[j];
+    const int64_t s0 = std::max(a, g.off), s1 = std::min(e, g.off + g.bytes);
+    if (s1 <= s0) continue;
+    if (s0 > filled) memset(h + (filled - h0), 0, (size_t)(s0 - filled));
+    memcpy(h + (s0 - h0), g.p + (s0 - g.off), (size_t)(s1 - s0));
+    filled = s1;
+  }
+  if (e > filled) memset(h + (filled - h0), 0, (size_t)(e - filled));
+}
+
 // Host segments into the device buffer through two pinned staging buffers:
-// the column's byte image (segments at their offsets, zero between) goes
-// over in windows, the host filling one buffer while the other is copied.
-int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev) {
+// the column's byte image goes over in windows, a team of host threads
+// filling one buffer while the other is copied.
+int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev, HostTeam *team) {
   if (col.bytes <= 0) return QM_OK;
   const int64_t win = std::min<int64_t>(col.bytes, (int64_t)64 << 20);
   HostBuf hb[2];
@@ -328,23 +409,21 @@ int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev) {
     if (!ctx->pool->acquire((size_t)win, hb[k])) rc = set_err(ctx, QM_ERR_OOM, "pinned staging (%lld bytes)", (long long)win);
     else if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) rc = QM_ERR_CUDA;
   }
-  size_t si = 0;
   bool used[2] = {false, false};
   for (int64_t a = 0, k = 0; rc == QM_OK && a < col.bytes; a += win, k ^= 1) {
     const int64_t e = std::min(col.bytes, a + win);
     if (used[k] && cudaEventSynchronize(ev[k]) != cudaSuccess) rc = QM_ERR_CUDA;
     if (rc) break;
     uint8_t *h = (uint8_t *)hb[k].p;
-    int64_t filled = a;
-    while (si < col.segs.size() && col.segs[si].off + col.segs[si].bytes <= a) si++;
-    for (size_t j = si; j < col.segs.size() && col.segs[j].off < e; j++) {
-      const PqSeg &g = col.segs[j];
-      const int64_t s0 = std::max(a, g.off), s1 = std::min(e, g.off + g.bytes);
-      if (s0 > filled) memset(h + (filled - a), 0, (size_t)(s0 - filled));
-      if (s1 > s0) memcpy(h + (s0 - a), g.p + (s0 - g.off), (size_t)(s1 - s0));
-      filled = std::max(filled, s1);
+    if (team && e - a >= ((int64_t)4 << 20)) {
+      const int parts = team->size();
+      team->run([&](int i) {
+        const int64_t s0 = a + (e - a) * i / parts, s1 = a + (e - a) * (i + 1) / parts;
+        if (s1 > s0) fill_window(col, s0, s1, h, a);
+      });
+    } else {
+      fill_window(col, a, e, h, a);
     }
-    if (e > filled) memset(h + (filled - a), 0, (size_t)(e - filled));
     if (cudaMemcpyAsync(dev + a, h, (size_t)(e - a), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
         cudaEventRecord(ev[k], ctx->stream) != cudaSuccess)
       rc = QM_ERR_CUDA;
@@ -377,6 +456,7 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
   qm_table *t = new qm_table();
   t->ctx = ctx;
   DevBuf chunk, pgs, rns, present, counts, ranks, temp;
+  std::unique_ptr<HostTeam> team;  // fills the staging buffers of large columns
   auto fail = [&](int rc) {
     DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};
     for (DevBuf *x : bufs) release(*x);
@@ -415,8 +495,8 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     }
     const int64_t words = (rows + 31) / 32;
     size_t tb = 0;
-    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb, nullptr,
-                           nullptr, ctx->sm_count, ctx->stream));
+    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, 0, w, rows, nullptr, nullptr, nullptr, nullptr, &tb,
+                            nullptr, nullptr, ctx->sm_count, ctx->stream));
     int rc;
     if ((rc = ensure(ctx, chunk, (size_t)pc.bytes + 16)) ||
         (rc = ensure(ctx, pgs, std::max<size_t>(pc.pages.size(), 1) * sizeof(qm_pq_page))) ||
@@ -437,7 +517,11 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     col.own_data = true;
     col.own_nulls = nullable;
     t->cols.push_back(col);
-    if ((rc = upload_segments(ctx, pc, (uint8_t *)chunk.p))) return fail(rc);
+    if (pc.bytes >= ((int64_t)16 << 20) && !team) {
+      const int hw = (int)std::thread::hardware_concurrency();
+      team.reset(new HostTeam(std::max(1, std::min(16, hw / 2))));
+    }
+    if ((rc = upload_segments(ctx, pc, (uint8_t *)chunk.p, team.get()))) return fail(rc);
     if (!pc.pages.empty())
       CKF(cudaMemcpyAsync(pgs.p, pc.pages.data(), pc.pages.size() * sizeof(qm_pq_page), cudaMemcpyHostToDevice,
                          ctx->stream));
@@ -446,10 +530,10 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
                          ctx->stream));
     size_t tbytes = temp.bytes;
     CKF(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pc.pages.size(),
-                           (const qm_pq_run *)rns.p, w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
+                           (const qm_pq_run *)rns.p, (int)pc.runs.size(), w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
                            (uint64_t *)ranks.p, temp.p, &tbytes, (unsigned char *)col.data, col.nulls,
                            ctx->sm_count, ctx->stream));
-    ctx->launches += 4;
+    ctx->launches += pc.runs.empty() ? 1 : 5;
     CKF(cudaStreamSynchronize(ctx->stream));  // the host vectors above go out of scope
   }
   DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};

@@ -67,6 +67,56 @@ class Page:
     parquet: bool = False
 
 
+@dataclass
+class PageTable:
+    """A column's pages as a reader has them: one host buffer holding the
+    page bytes (a column's byte range of a file) and per page its offset and
+    length in it (PageInfo.byteOffset / byteLength), rowCount, nullCount and,
+    optionally, dataOffsetInPage (-1 = absent) and the Parquet flag."""
+    buf: Any
+    offsets: np.ndarray
+    lengths: np.ndarray
+    row_counts: np.ndarray
+    null_counts: np.ndarray | None = None
+    data_offsets: np.ndarray | None = None
+    parquet: np.ndarray | None = None
+
+
+# numpy image of qm_page (checked against the ctypes mirror at import)
+_PAGE_DTYPE = np.dtype([("buf", np.uint64), ("bytes", np.int64), ("row_count", np.int64), ("null_count", np.int64),
+                        ("data_offset", np.int64), ("parquet", np.int32), ("reserved", np.int32)])
+assert _PAGE_DTYPE.itemsize == C.sizeof(A.QmPage) and all(
+    _PAGE_DTYPE.fields[f][1] == getattr(A.QmPage, f).offset for f, _ in A.QmPage._fields_)
+
+
+def _page_records(pages) -> tuple[np.ndarray, list]:
+    """qm_page records of a PageTable or a list of Page, and the objects that
+    must stay alive while they are used."""
+    if isinstance(pages, PageTable):
+        b = _host_bytes(pages.buf)
+        n = len(pages.offsets)
+        offs = np.asarray(pages.offsets, dtype=np.int64)
+        lens = np.asarray(pages.lengths, dtype=np.int64)
+        if n and (offs.min() < 0 or (offs + lens).max() > b.nbytes or lens.min() < 0):
+            raise ValueError("page ranges outside the buffer")
+        rec = np.zeros(n, dtype=_PAGE_DTYPE)
+        rec["buf"] = np.uint64(b.ctypes.data) + offs.astype(np.uint64)
+        rec["bytes"] = lens
+        rec["row_count"] = pages.row_counts
+        rec["null_count"] = 0 if pages.null_counts is None else pages.null_counts
+        rec["data_offset"] = -1 if pages.data_offsets is None else pages.data_offsets
+        rec["parquet"] = 0 if pages.parquet is None else pages.parquet
+        return rec, [b]
+    rec = np.zeros(len(pages), dtype=_PAGE_DTYPE)
+    keep = []
+    for k, pg in enumerate(pages):
+        b = _host_bytes(pg.buf)
+        keep.append(b)
+        rec[k] = (b.__array_interface__["data"][0] if b.nbytes else 0, b.nbytes, pg.row_count, pg.null_count,
+                  -1 if pg.data_offset is None else pg.data_offset, 1 if pg.parquet else 0, 0)
+    return rec, keep
+
+
 def _host_bytes(obj) -> np.ndarray:
     a = obj if isinstance(obj, np.ndarray) else np.frombuffer(obj, dtype=np.uint8)
     if not a.flags.c_contiguous:
@@ -385,29 +435,21 @@ class Context:
         t._dtypes = [c[1] for c in chunks]
         return t
 
-    def table_from_pages(self, columns: list[tuple[str, int, list[Page]]]) -> "Table":
+    def table_from_pages(self, columns: list[tuple[str, int, Any]]) -> "Table":
         """A table from scan pages: per column (name, QM dtype, its pages in
-        order), decoded on the device and concatenated page after page."""
+        order as a list of Page or a PageTable), decoded on the device and
+        concatenated page after page."""
         n = len(columns)
         arr = (A.QmPageColumn * n)()
         keep = []
         for i, (name, dtype, pages) in enumerate(columns):
             nb = name.encode()
-            pa = (A.QmPage * max(len(pages), 1))()
-            keep += [nb, pa]
-            for k, pg in enumerate(pages):
-                b = _host_bytes(pg.buf)
-                keep.append(b)
-                pa[k].buf = b.ctypes.data if b.nbytes else None
-                pa[k].bytes = b.nbytes
-                pa[k].row_count = pg.row_count
-                pa[k].null_count = pg.null_count
-                pa[k].data_offset = -1 if pg.data_offset is None else pg.data_offset
-                pa[k].parquet = 1 if pg.parquet else 0
+            rec, k = _page_records(pages)
+            keep += [nb, rec, k]
             arr[i].name = nb
             arr[i].dtype = dtype
-            arr[i].n_pages = len(pages)
-            arr[i].pages = pa
+            arr[i].n_pages = len(rec)
+            arr[i].pages = rec.ctypes.data_as(C.POINTER(A.QmPage))
         h = C.c_void_p()
         self.check(self.lib.qm_table_from_pages(self.h, n, arr, C.byref(h)))
         rows = C.c_int64()

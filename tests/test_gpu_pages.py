@@ -11,7 +11,7 @@ import pytest
 import oracle
 from oracle.pages import decode_column_pages
 from querymode_b200 import _abi as A
-from querymode_b200.engine import Column, Page
+from querymode_b200.engine import Column, Page, PageTable
 from querymode_b200.query import AggregateOp, FilterOp, QueryDescriptor
 from tests.helpers import assert_same
 from tests.page_util import as_tuples, encode_column, encode_page
@@ -133,3 +133,23 @@ def test_bad_descriptors(ctx):
     with pytest.raises(A.QmError) as e:
         ctx.table_from_pages([("a", A.QM_I32, [Page(bytes(8), 2, 0, -5)])])
     assert e.value.status == A.QM_ERR_INVALID
+
+
+def test_page_table_matches_page_list(ctx):
+    """A column's pages back to back in one buffer with a page table decode
+    as the same pages passed one by one."""
+    rng = np.random.default_rng(21)
+    pages = random_pages(rng, "int64", 30)
+    pages = [p for p in pages if not p.parquet]
+    bufs = [bytes(p.buf) for p in pages]
+    lens = np.array([len(b) for b in bufs], dtype=np.int64)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.int64)
+    pt = PageTable(np.frombuffer(b"".join(bufs), dtype=np.uint8), offs, lens,
+                   np.array([p.row_count for p in pages]), np.array([p.null_count for p in pages]),
+                   np.array([-1 if p.data_offset is None else p.data_offset for p in pages]))
+    t1 = ctx.table_from_pages([("c", A.QM_I64, pages)])
+    t2 = ctx.table_from_pages([("c", A.QM_I64, pt)])
+    v1, n1 = t1.read_column("c")
+    v2, n2 = t2.read_column("c")
+    assert np.array_equal(v1, v2) and np.array_equal(n1, n2)
+    check_column(t2, "c", "int64", pages)
