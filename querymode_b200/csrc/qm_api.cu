@@ -835,6 +835,8 @@ int ilog2_ceil(int64_t x) {
 }
 
 constexpr size_t LOCAL_BUDGET = 40 * 1024;  // bytes of the block-local hash table
+constexpr size_t LOCAL_WIDE_BUDGET = 80 * 1024;  // ... when the estimated groups overflow it
+constexpr int64_t LOCAL_WIDE_MAX_GROUPS = 10000;
 // A dense (direct) key range whose table fits this many bytes is aggregated
 // entirely in shared memory, even at one block per SM: every row then stays
 // on the shared-memory path instead of the L2 atomics of the global table.
@@ -873,6 +875,11 @@ void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning
   if (tu.local_slots > 0 || (tu.local_slots == 0 && est_groups <= ((int64_t)1 << 20))) {
     int L = 1;
     while ((int64_t)(L * 2) * (per_slot + 8) <= (int64_t)LOCAL_BUDGET) L *= 2;
+    // More groups than that table admits (half its slots): a wider table,
+    // still two blocks per SM, keeps them in shared memory (256-1,000
+    // int64 groups at 75 % selectivity: 3.9 -> 1.9 ms over 15 queries).
+    if (tu.local_slots == 0 && est_groups > L / 2 && est_groups <= LOCAL_WIDE_MAX_GROUPS)
+      while ((int64_t)(L * 2) * (per_slot + 8) <= (int64_t)LOCAL_WIDE_BUDGET) L *= 2;
     if (tu.local_slots > 0) {
       L = tu.local_slots;
       while (L > 1 && (int64_t)L * (per_slot + 8) > (int64_t)200 * 1024) L /= 2;  // fit shared memory
