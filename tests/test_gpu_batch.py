@@ -67,3 +67,26 @@ def test_batch_equals_single_queries(ctx):
             assert_same(g, r)
     finally:
         b.close()
+
+
+def test_batch_dense_keys_beyond_shared_memory(ctx):
+    # dense int32 keys whose direct tables exceed shared memory (block-local
+    # hash, then the global table) beside ones that fit, NULL keys included
+    rng = np.random.default_rng(13)
+    tables, queries = [], []
+    for card, n in ((9_000, 1_500_000), (20_000, 2_000_000), (300, 400_000), (4_000, 600_000)):
+        cols = {"key": Column(rng.integers(0, card, n).astype(np.int32), rng.random(n) < 0.001),
+                "f": rng.integers(0, 10_000, n).astype(np.int32), "v": rng.lognormal(size=n)}
+        tables.append(cols)
+        queries.append(QueryDescriptor(filters=[FilterOp("f", "lt", 7000)], group_by=["key"],
+                                       aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*"),
+                                                   AggregateOp("min", "v"), AggregateOp("max", "v")]))
+    handles = [ctx.table(t) for t in tables]
+    refs = [oracle.run(t, q) for t, q in zip(tables, queries)]
+    b = ctx.batch(handles, queries)
+    try:
+        for run in range(2):
+            for i, (g, r) in enumerate(zip(b.run(), refs)):
+                assert_same(g, r, ctx_msg=f"run {run} query {i}")
+    finally:
+        b.close()
