@@ -92,6 +92,49 @@ struct PinnedPool {
   }
 };
 
+// Device blocks of destroyed tables' columns, kept (up to a cap) for the
+// next table's columns of about the same size: tables created and dropped
+// per host batch or per ingest then cost no cudaMalloc / cudaFree (and
+// cudaFree synchronises the device).  Emptied whenever an allocation fails.
+struct DevPool {
+  std::mutex mu;
+  std::vector<std::pair<void *, size_t>> free;
+  size_t cached = 0;
+  static size_t round(size_t b) {
+    return (std::max<size_t>(b, 256) + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
+  }
+  void *take(size_t bytes, size_t &got) {
+    std::lock_guard<std::mutex> lk(mu);
+    const size_t want = round(bytes);
+    int best = -1;
+    for (int i = 0; i < (int)free.size(); i++)
+      if (free[i].second >= want && free[i].second <= want + want / 4 &&
+          (best < 0 || free[i].second < free[best].second))
+        best = i;
+    if (best < 0) return nullptr;
+    void *p = free[best].first;
+    got = free[best].second;
+    cached -= got;
+    free.erase(free.begin() + best);
+    return p;
+  }
+  bool keep(void *p, size_t bytes, size_t cap) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (cached + bytes > cap || free.size() >= 256) return false;
+    free.push_back({p, bytes});
+    cached += bytes;
+    return true;
+  }
+  bool trim() {
+    std::lock_guard<std::mutex> lk(mu);
+    const bool any = !free.empty();
+    for (auto &f : free) cudaFree(f.first);
+    free.clear();
+    cached = 0;
+    return any;
+  }
+};
+
 }  // namespace
 
 struct qm_ctx {
@@ -115,6 +158,11 @@ struct qm_ctx {
   std::vector<DevBuf> staged;  // per-column uploads of pushed host batches
   HostBuf hout, hstatus;
   std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
+  DevPool dpool;  // column blocks of destroyed tables
+  // side stream for the statistics of columns being uploaded
+  cudaStream_t aux = nullptr;
+  cudaEvent_t aux_ev = nullptr;
+  DevBuf ustat;
 };
 
 namespace {
@@ -154,7 +202,12 @@ int ensure(qm_ctx *ctx, DevBuf &b, size_t bytes) {
   cudaError_t e = cudaMalloc(&b.p, want);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return set_err(ctx, QM_ERR_OOM, "cudaMalloc(%zu): %s", want, cudaGetErrorString(e));
+    if (ctx->dpool.trim()) e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      b.p = nullptr;
+      return set_err(ctx, QM_ERR_OOM, "cudaMalloc(%zu): %s", want, cudaGetErrorString(e));
+    }
   }
   b.bytes = want;
   return QM_OK;
@@ -198,6 +251,7 @@ struct DevCol {
   void *data = nullptr;
   uint32_t *nulls = nullptr;
   bool own_data = false, own_nulls = false;
+  size_t data_block = 0, nulls_block = 0;  // pooled block sizes (0: plain cudaMalloc)
   bool has_minmax = false;
   long long mn = 0, mx = 0;
   bool has_hll = false;
@@ -218,22 +272,43 @@ struct qm_table {
 
 namespace {
 
-void free_col(DevCol &c) {
-  if (c.own_data && c.data) cudaFree(c.data);
-  if (c.own_nulls && c.nulls) cudaFree(c.nulls);
+// Device memory for a table column: a pooled block of about its size, else
+// a new 2 MiB-rounded one (the pool is emptied and the allocation retried
+// when the device is full).  `block` receives the block's size.
+void *col_alloc(qm_ctx *ctx, size_t bytes, size_t &block) {
+  void *p = ctx->dpool.take(bytes, block);
+  if (p) return p;
+  block = DevPool::round(bytes);
+  if (cudaMalloc(&p, block) != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+    if (ctx->dpool.trim() && cudaMalloc(&p, block) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+  }
+  return p;
+}
+
+// Blocks kept for reuse: at most an eighth of the device's memory.
+void col_release(qm_ctx *ctx, void *p, size_t block) {
+  if (!p) return;
+  if (!ctx || !block || !ctx->dpool.keep(p, block, (size_t)ctx->hbm_bytes / 8)) cudaFree(p);
+}
+
+void free_col(qm_ctx *ctx, DevCol &c) {
+  if (c.own_data && c.data) col_release(ctx, c.data, c.data_block);
+  if (c.own_nulls && c.nulls) col_release(ctx, c.nulls, c.nulls_block);
   c.data = nullptr;
   c.nulls = nullptr;
 }
 
 // Copy a QMCB-style byte bitmap into a 32-bit-word device bitmap.
-int upload_nulls(qm_ctx *ctx, const uint8_t *host_bits, int64_t n, uint32_t **out) {
+int upload_nulls(qm_ctx *ctx, const uint8_t *host_bits, int64_t n, uint32_t **out, size_t &block) {
   size_t words = (size_t)((n + 31) / 32) + 1;
-  uint32_t *d = nullptr;
-  cudaError_t e = cudaMalloc(&d, words * 4);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return set_err(ctx, QM_ERR_OOM, "null bitmap alloc: %s", cudaGetErrorString(e));
-  }
+  uint32_t *d = (uint32_t *)col_alloc(ctx, words * 4, block);
+  if (!d) return set_err(ctx, QM_ERR_OOM, "null bitmap alloc (%zu bytes)", words * 4);
+  *out = d;
   CK(cudaMemsetAsync(d, 0, words * 4, ctx->stream));
   if (n > 0) CK(cudaMemcpyAsync(d, host_bits, (size_t)((n + 7) / 8), cudaMemcpyHostToDevice, ctx->stream));
   *out = d;
@@ -253,34 +328,26 @@ int make_col(qm_ctx *ctx, int64_t n, const qm_column &src, DevCol &c) {
       // a device bitmap must already be readable as 32-bit words: copy it
       // into an owned, word-padded buffer
       size_t words = (size_t)((n + 31) / 32) + 1;
-      uint32_t *d = nullptr;
-      cudaError_t e = cudaMalloc(&d, words * 4);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(ctx, QM_ERR_OOM, "null bitmap alloc");
-      }
+      uint32_t *d = (uint32_t *)col_alloc(ctx, words * 4, c.nulls_block);
+      if (!d) return set_err(ctx, QM_ERR_OOM, "null bitmap alloc (%zu bytes)", words * 4);
+      c.nulls = d;
+      c.own_nulls = true;
       CK(cudaMemsetAsync(d, 0, words * 4, ctx->stream));
       if (n > 0)
         CK(cudaMemcpyAsync(d, src.null_bitmap, (size_t)((n + 7) / 8), cudaMemcpyDeviceToDevice, ctx->stream));
-      c.nulls = d;
-      c.own_nulls = true;
     }
     return QM_OK;
   }
   size_t bytes = (size_t)n * dtype_size(src.dtype);
-  void *d = nullptr;
-  cudaError_t e = cudaMalloc(&d, std::max<size_t>(bytes, 16));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return set_err(ctx, QM_ERR_OOM, "column %s: cudaMalloc(%zu): %s", src.name, bytes, cudaGetErrorString(e));
-  }
+  void *d = col_alloc(ctx, std::max<size_t>(bytes, 16), c.data_block);
+  if (!d) return set_err(ctx, QM_ERR_OOM, "column %s: device memory (%zu bytes)", src.name, bytes);
   c.data = d;
   c.own_data = true;
   if (bytes) CK(cudaMemcpyAsync(d, src.data, bytes, cudaMemcpyHostToDevice, ctx->stream));
   if (src.null_bitmap) {
-    int rc = upload_nulls(ctx, src.null_bitmap, n, &c.nulls);
-    if (rc) return rc;
     c.own_nulls = true;
+    int rc = upload_nulls(ctx, src.null_bitmap, n, &c.nulls, c.nulls_block);
+    if (rc) return rc;
   }
   return QM_OK;
 }
@@ -1880,9 +1947,10 @@ int qm_ctx_destroy(qm_ctx *ctx) {
                     &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare, &ctx->fbits, &ctx->fcounts,
                     &ctx->franks, &ctx->post_last, &ctx->post_hi, &ctx->post_lo, &ctx->post_idx,
                     &ctx->post_idx2, &ctx->post_k1, &ctx->post_k2, &ctx->post_l1, &ctx->post_l2,
-                    &ctx->post_temp, &ctx->out2, &ctx->zstat, &ctx->zones};
+                    &ctx->post_temp, &ctx->out2, &ctx->zstat, &ctx->zones, &ctx->ustat};
   for (DevBuf *b : bufs) release(*b);
   for (auto &b : ctx->staged) release(b);
+  ctx->dpool.trim();
   if (ctx->hout.p) cudaFreeHost(ctx->hout.p);
   if (ctx->hstatus.p) cudaFreeHost(ctx->hstatus.p);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -1890,6 +1958,8 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   if (ctx->evs0) cudaEventDestroy(ctx->evs0);
   if (ctx->evs1) cudaEventDestroy(ctx->evs1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
+  if (ctx->aux_ev) cudaEventDestroy(ctx->aux_ev);
   delete ctx;
   return QM_OK;
 }
@@ -1924,6 +1994,9 @@ int qm_ctx_device_info(const qm_ctx *ctx, int32_t *sm_count, int64_t *hbm_bytes)
   return QM_OK;
 }
 
+// Tables of at least this many rows get their column statistics at upload.
+constexpr int64_t EAGER_STATS_ROWS = (int64_t)4 << 20;
+
 int qm_table_create(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column *cols, qm_table **out) {
   if (!ctx || !out || n_rows < 0 || n_cols < 0 || (n_cols > 0 && !cols))
     return set_err(ctx, QM_ERR_INVALID, "qm_table_create: bad arguments");
@@ -1934,26 +2007,76 @@ int qm_table_create(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_column
   qm_table *t = new qm_table();
   t->ctx = ctx;
   t->n_rows = n_rows;
+  // The planner's column statistics (min / max of integer columns, max |x|
+  // of float columns, zone maps) of host-uploaded columns are computed on a
+  // side stream behind each column's copy, while the next columns cross the
+  // host link, instead of on the first query with a synchronise each.
+  const int64_t zones = (n_rows + QM_ZONE_ROWS - 1) / QM_ZONE_ROWS;
+  const size_t per = 32 + (size_t)zones * 24;
+  bool eager = n_rows >= EAGER_STATS_ROWS;
+  HostBuf hs;
+  if (eager) {
+    if ((!ctx->aux && cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess) ||
+        (!ctx->aux_ev && cudaEventCreateWithFlags(&ctx->aux_ev, cudaEventDisableTiming) != cudaSuccess) ||
+        ensure(ctx, ctx->ustat, per * std::max(n_cols, 1)) != QM_OK || !ctx->pool->acquire(per * std::max(n_cols, 1), hs)) {
+      cudaGetLastError();
+      eager = false;  // the statistics stay lazy
+    }
+  }
+  std::vector<char> staged((size_t)n_cols, 0);
+  auto fail = [&](int rc) {
+    if (eager) cudaStreamSynchronize(ctx->aux);
+    ctx->pool->release(hs);
+    qm_table_destroy(t);
+    return rc;
+  };
   for (int i = 0; i < n_cols; i++) {
     for (auto &c : t->cols)
-      if (c.name == cols[i].name) {
-        qm_table_destroy(t);
-        return set_err(ctx, QM_ERR_INVALID, "duplicate column %s", cols[i].name);
-      }
+      if (c.name == cols[i].name) return fail(set_err(ctx, QM_ERR_INVALID, "duplicate column %s", cols[i].name));
     DevCol c;
     int rc = make_col(ctx, n_rows, cols[i], c);
     if (rc) {
-      free_col(c);
-      qm_table_destroy(t);
-      return rc;
+      free_col(ctx, c);
+      return fail(rc);
     }
     t->cols.push_back(c);
+    if (eager && !cols[i].on_device) {
+      uint8_t *d = (uint8_t *)ctx->ustat.p + per * i;
+      int64_t *z = (int64_t *)(d + 32);
+      cudaError_t e = cudaEventRecord(ctx->aux_ev, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux, ctx->aux_ev, 0);
+      if (e == cudaSuccess)
+        e = is_int(c.dtype) ? qm_launch_minmax(c.data, c.dtype, c.nulls, n_rows, (long long *)d, ctx->sm_count, ctx->aux)
+                            : qm_launch_maxabs(c.data, c.dtype, c.nulls, n_rows, (unsigned long long *)(d + 16),
+                                               ctx->sm_count, ctx->aux);
+      if (e == cudaSuccess) e = qm_launch_zone_stats(c.data, c.dtype, c.nulls, n_rows, z, z + zones, z + 2 * zones, ctx->aux);
+      if (e == cudaSuccess) e = cudaMemcpyAsync((uint8_t *)hs.p + per * i, d, per, cudaMemcpyDeviceToHost, ctx->aux);
+      if (e != cudaSuccess) return fail(set_err(ctx, QM_ERR_CUDA, "column statistics: %s", cudaGetErrorString(e)));
+      staged[i] = 1;
+    }
   }
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) {
-    qm_table_destroy(t);
-    return set_err(ctx, QM_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+  if (e == cudaSuccess && eager) e = cudaStreamSynchronize(ctx->aux);
+  if (e != cudaSuccess) return fail(set_err(ctx, QM_ERR_CUDA, "upload: %s", cudaGetErrorString(e)));
+  for (int i = 0; i < n_cols; i++) {
+    if (!staged[i]) continue;
+    DevCol &c = t->cols[i];
+    const uint8_t *h = (const uint8_t *)hs.p + per * i;
+    if (is_int(c.dtype)) {
+      memcpy(&c.mn, h, 8);
+      memcpy(&c.mx, h + 8, 8);
+      c.has_minmax = true;
+    } else {
+      memcpy(&c.maxabs, h + 16, 8);
+      c.has_maxabs = true;
+    }
+    const int64_t *z = (const int64_t *)(h + 32);
+    c.zmin.assign(z, z + zones);
+    c.zmax.assign(z + zones, z + 2 * zones);
+    c.zcount.assign(z + 2 * zones, z + 3 * zones);
+    c.has_zones = true;
   }
+  ctx->pool->release(hs);
   *out = t;
   return QM_OK;
 }
@@ -2040,7 +2163,7 @@ int qm_table_destroy(qm_table *t) {
   if (!t) return QM_OK;
   if (t->ctx) cudaSetDevice(t->ctx->device);
   if (t->ctx) cudaStreamSynchronize(t->ctx->stream);
-  for (auto &c : t->cols) free_col(c);
+  for (auto &c : t->cols) free_col(t->ctx, c);
   delete t;
   return QM_OK;
 }

@@ -508,15 +508,18 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     col.name = c.name;
     col.dtype = c.dtype;
     const bool nullable = !pc.runs.empty();
-    if (cudaMalloc(&col.data, std::max<size_t>((size_t)rows * w, 16)) != cudaSuccess ||
-        (nullable && cudaMalloc((void **)&col.nulls, (size_t)std::max<int64_t>(words, 1) * 4) != cudaSuccess)) {
-      cudaGetLastError();
-      free_col(col);
+    col.data = col_alloc(ctx, std::max<size_t>((size_t)rows * w, 16), col.data_block);
+    col.own_data = col.data != nullptr;
+    if (nullable) {
+      col.nulls = (uint32_t *)col_alloc(ctx, (size_t)(words + 1) * 4, col.nulls_block);
+      col.own_nulls = col.nulls != nullptr;
+    }
+    if (!col.data || (nullable && !col.nulls)) {
+      free_col(ctx, col);
       return fail(set_err(ctx, QM_ERR_OOM, "column %s: device memory", c.name));
     }
-    col.own_data = true;
-    col.own_nulls = nullable;
     t->cols.push_back(col);
+    if (nullable) CKF(cudaMemsetAsync(col.nulls, 0, (size_t)(words + 1) * 4, ctx->stream));  // + the padding word
     if (pc.bytes >= ((int64_t)16 << 20) && !team) {
       const int hw = (int)std::thread::hardware_concurrency();
       team.reset(new HostTeam(std::max(1, std::min(16, hw / 2))));

@@ -491,3 +491,46 @@ def test_large_hash_table_update_passes(ctx):
         assert g.stats.retries == 0
         assert_same(g, oracle.run(cols, q, threads=16))
         assert g.stats.rows_selected == (n if not q.filters else int((cols["f"] < 8).sum()))
+
+
+def test_tables_recycle_device_blocks(ctx):
+    # tables created and dropped in turn reuse each other's device blocks
+    # (sizes within a quarter of each other); every table must see only its
+    # own cells and NULLs
+    rng = np.random.default_rng(91)
+    q = QueryDescriptor(filters=[FilterOp("f", "gte", 0)], group_by=["k"],
+                        aggregates=[AggregateOp("sum", "x"), AggregateOp("count", "x"), AggregateOp("min", "f")])
+    for it in range(6):
+        n = 1_000_000 + int(rng.integers(0, 200_000))
+        cols = {"k": rng.integers(0, 50, n).astype(np.int32),
+                "x": Column(rng.normal(size=n), rng.random(n) < (0.3 if it % 2 else 0.0) + 1e-9),
+                "f": Column(rng.integers(-5, 100, n).astype(np.int64), rng.random(n) < 0.05 * (it % 3))}
+        t = ctx.table(cols)
+        assert_same(t.run(q), oracle.run(cols, q), ctx_msg=f"table {it}")
+        t.close()
+
+
+def test_statistics_at_upload_match_lazy_ones(ctx):
+    # a host table of >= 4M rows gets its min / max, max |x| and zone maps
+    # while it uploads; the same columns borrowed from device memory get them
+    # on first use; both must plan to the oracle's results
+    import torch
+    rng = np.random.default_rng(101)
+    n = 5_000_000
+    ts = np.sort(rng.integers(0, 10**12, n)).astype(np.int64)
+    plain = {"ts": ts, "k": rng.integers(-300, 4000, n).astype(np.int32), "v": rng.normal(size=n) * 1e6,
+             "f": rng.random(n).astype(np.float32)}
+    nullable = dict(plain, ts=Column(ts, rng.random(n) < 0.001), v=Column(plain["v"], rng.random(n) < 0.01))
+    cut = int(ts[n // 4]), int(ts[n // 4 + 300_000])
+    qs = [QueryDescriptor(filters=[FilterOp("ts", "gte", cut[0]), FilterOp("ts", "lt", cut[1])], group_by=["k"],
+                          aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*"), AggregateOp("max", "f")]),
+          QueryDescriptor(filters=[FilterOp("f", "lt", 0.5)], group_by=["k"],
+                          aggregates=[AggregateOp("sum", "v"), AggregateOp("min", "ts"), AggregateOp("avg", "f")]),
+          QueryDescriptor(filters=[FilterOp("v", "gt", 1e6)], aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")])]
+    dev = {k: torch.from_numpy(v).cuda() for k, v in plain.items()}
+    tables = [("host", ctx.table(plain), plain), ("borrowed", ctx.table(dev), plain),
+              ("host with NULLs", ctx.table(nullable), nullable)]
+    for name, t, cols in tables:
+        for q in qs:
+            assert_same(t.run(q), oracle.run(cols, q, threads=8), ctx_msg=name)
+        t.close()
