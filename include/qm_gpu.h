@@ -375,16 +375,19 @@ int qm_batch_stats(const qm_batch *batch, double *device_ms, int64_t *rows,
 int qm_batch_destroy(qm_batch *batch);
 
 /* ---- Parquet column chunks ------------------------------------------------
- * Build a table from Parquet column chunks whose pages are PLAIN-encoded and
- * uncompressed (data page v1 or v2, definition levels for optional columns):
+ * Build a table from uncompressed Parquet column chunks: dictionary pages,
+ * data pages v1 or v2 with PLAIN values or RLE_DICTIONARY / RLE indices
+ * (encodings 8 and 3, the ones the reference reads as dictionary indices),
+ * definition levels for optional columns:
  * the bytes the reference's decodeParquetColumnChunk reads
  * (src/parquet-decode.ts:390-618), decoded into HBM with the same results —
  * rows per page, NULLs from definition level 0, the v1 level section
  * recognised as the reference recognises it.  The chunk is the bytes from
  * the chunk's first page header (ColumnMetaData.data_page_offset) for
  * total_compressed_size bytes; num_values is ColumnMetaData.num_values.
- * Dictionary pages, other encodings and compressed pages give
- * QM_ERR_UNSUPPORTED.  Every column must decode to the same row count. */
+ * Other encodings (PLAIN_DICTIONARY among them, which the reference would
+ * read as PLAIN) and compressed pages give QM_ERR_UNSUPPORTED.  Every column
+ * must decode to the same row count. */
 typedef struct {
   const char *name;
   int32_t dtype;         /* QM_I32 / QM_I64 / QM_F32 / QM_F64: INT32 / INT64 / FLOAT / DOUBLE */

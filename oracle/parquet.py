@@ -153,9 +153,18 @@ def decode_plain(b: bytes, dtype: str, n: int) -> list:
     return [struct.unpack_from(fmt, b, i * w)[0] for i in range(n)]
 
 
+def _dict_bit_width(n: int) -> int:
+    """ceil(log2(n)) as the reference computes it (0 for n <= 1)."""
+    return 0 if n <= 1 else (n - 1).bit_length()
+
+
 def decode_column_chunk(b: bytes, dtype: str, num_values: int) -> list:
+    """decodeParquetColumnChunk (src/parquet-decode.ts:390-618) for an
+    uncompressed chunk: dictionary pages, v1 / v2 data pages, PLAIN values or
+    RLE_DICTIONARY / RLE (encodings 8 and 3) indices into the dictionary."""
     values: list = []
     w = _FMT[dtype][1]
+    dictionary = None
     pos = 0
     while pos < len(b) and len(values) < num_values:
         h = parse_page_header(b, pos)
@@ -164,10 +173,15 @@ def decode_column_chunk(b: bytes, dtype: str, num_values: int) -> list:
         pos += h["header_size"]
         page = b[pos:pos + h["compressed"]]
         pos += h["compressed"]
+        if h["type"] == 2:  # DICTIONARY_PAGE
+            dictionary = decode_plain(page, dtype, h["num_values"])
+            continue
         if h["type"] not in (0, 3):
             continue
-        if h["encoding"] != 0:
-            raise NotImplementedError("only PLAIN pages")
+        enc = h["encoding"]
+        is_dict = enc in (8, 3)
+        if not is_dict and enc != 0:
+            raise NotImplementedError("encoding %d" % enc)
         defs = None
         off = 0
         if h["type"] == 0:
@@ -175,8 +189,13 @@ def decode_column_chunk(b: bytes, dtype: str, num_values: int) -> list:
                 plen = struct.unpack_from("<i", page, 0)[0]
                 max_def = max(64, -(-h["num_values"] // 4) + 8)
                 if 0 < plen <= max_def and plen < len(page) - 4:
-                    rem = len(page) - 4 - plen
-                    if 0 <= rem <= h["num_values"] * w:
+                    if is_dict and dictionary is not None:
+                        after = 4 + plen
+                        level = after < len(page) and page[after] == _dict_bit_width(len(dictionary))
+                    else:
+                        rem = len(page) - 4 - plen
+                        level = 0 <= rem <= h["num_values"] * w
+                    if level:
                         defs = decode_rle_bit_packed(page[4:4 + plen], 1, h["num_values"])
                         off = 4 + plen
         else:
@@ -184,14 +203,41 @@ def decode_column_chunk(b: bytes, dtype: str, num_values: int) -> list:
             if h["def_len"] > 0:
                 defs = decode_rle_bit_packed(page[d0:d0 + h["def_len"]], 1, h["num_values"])
             off = d0 + h["def_len"]
+
+        def is_null(i):
+            return defs is not None and i < len(defs) and defs[i] == 0
+
         nonnull = h["num_values"] if defs is None else sum(1 for d in defs if d > 0)
+        if is_dict:
+            if dictionary is None:
+                continue
+            bw = page[off] if off < len(page) else 0
+            if bw == 0:
+                first = dictionary[0] if dictionary else None
+                for i in range(h["num_values"]):
+                    if len(values) >= num_values:
+                        break
+                    values.append(None if is_null(i) else first)
+            else:
+                idx = decode_rle_bit_packed(page[off + 1:], bw, nonnull)
+                ip = 0
+                for i in range(h["num_values"]):
+                    if len(values) >= num_values:
+                        break
+                    if is_null(i):
+                        values.append(None)
+                    else:
+                        k = idx[ip] if ip < len(idx) else 0
+                        ip += 1
+                        values.append(dictionary[k] if k < len(dictionary) else None)
+            continue
         decoded = decode_plain(page[off:], dtype, nonnull)
         if defs is not None:
             dp = 0
             for i in range(h["num_values"]):
                 if len(values) >= num_values:
                     break
-                if i < len(defs) and defs[i] == 0:
+                if is_null(i):
                     values.append(None)
                 else:
                     values.append(decoded[dp] if dp < len(decoded) else None)

@@ -221,7 +221,7 @@ __device__ __forceinline__ void pq_warp_range(int64_t words, int64_t &w0, int64_
 struct PqCur {
   int p;
   int64_t row0, next0, val_off, avail;
-  int32_t run0, run1, slotted;
+  int32_t run0, run1, slotted, dict;
   __device__ __forceinline__ void load(const qm_pq_page *pages, int n_pages, int q) {
     p = q;
     const qm_pq_page &pg = pages[q];
@@ -231,6 +231,7 @@ struct PqCur {
     run0 = pg.run0;
     run1 = pg.run1;
     slotted = pg.slotted;
+    dict = pg.dict;
     next0 = q + 1 < n_pages ? pages[q + 1].row0 : INT64_MAX;
   }
   __device__ __forceinline__ bool advance(const qm_pq_page *pages, int n_pages, int64_t r) {
@@ -295,6 +296,38 @@ __global__ void __launch_bounds__(256) qm_pq_present(const uint8_t *chunk, const
   }
 }
 
+// Dictionary page: the address of the entry value j of the page maps to
+// (index j of its RLE / bit-packed index stream; index bytes at or past the
+// page's data end read as 0, indices past those decoded are 0), or null
+// where the index is outside the dictionary (NULL, as the reference's
+// `idx < dictionary.length ? dictionary[idx] : null`).
+__device__ __forceinline__ const uint8_t *pq_dict_entry(const uint8_t *chunk, const qm_pq_page &pg,
+                                                       const qm_pq_run *iruns, int64_t j, int width) {
+  uint64_t idx = 0;
+  if (j < pg.n_idx) {
+    int lo = pg.irun0, hi = pg.irun1 - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (iruns[mid].row0 <= j) lo = mid;
+      else hi = mid - 1;
+    }
+    const qm_pq_run &run = iruns[lo];
+    if (!run.packed) {
+      idx = (uint32_t)run.value;
+    } else {
+      const int64_t bit = (j - run.row0) * pg.bw;
+      const int64_t b0 = run.byte_off + (bit >> 3);
+      uint64_t word = 0;
+#pragma unroll
+      for (int i = 0; i < 5; ++i)
+        if (b0 + i < pg.data_end) word |= (uint64_t)chunk[b0 + i] << (8 * i);
+      idx = (word >> (bit & 7)) & (pg.bw >= 32 ? 0xffffffffull : ((1ull << pg.bw) - 1));
+    }
+  }
+  if (idx >= (uint64_t)pg.dict_n) return nullptr;
+  return chunk + pg.dict_off + (int64_t)idx * width;
+}
+
 // Values into rows, one lane per row, QM_PQ_UNROLL words per step with their
 // loads issued together (stores coalesced).  A present row r of page p
 // takes that page's value j: in a packed page j = rank(r) - rank(row0), in
@@ -303,8 +336,9 @@ __global__ void __launch_bounds__(256) qm_pq_present(const uint8_t *chunk, const
 // decoded[dPtr++] / values[vi++] running out does).
 #define QM_PQ_UNROLL 4
 __global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages,
-                                                     int width, int64_t n_rows, const uint32_t *present,
-                                                     const uint64_t *ranks, unsigned char *out, uint32_t *nulls) {
+                                                     const qm_pq_run *iruns, int width, int64_t n_rows,
+                                                     const uint32_t *present, const uint64_t *ranks,
+                                                     unsigned char *out, uint32_t *nulls) {
   const int lane = threadIdx.x & 31;
   const int64_t words = (n_rows + 31) / 32;
   int64_t w0, w1;
@@ -337,7 +371,10 @@ __global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const
             }
             j = (int64_t)ranks[w + u] + __popc(pw & ((1u << lane) - 1u)) - rank_f;
           }
-          if (j < c.avail) {
+          if (c.dict) {
+            src[u] = pq_dict_entry(chunk, pages[c.p], iruns, j, width);
+            live[u] = src[u] != nullptr;
+          } else if (j < c.avail) {
             live[u] = true;
             src[u] = chunk + c.val_off + j * width;
           }
@@ -897,7 +934,7 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
 }
 
 cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
-                                int n_runs, int width, int64_t n_rows, uint32_t *present, uint32_t *counts,
+                                int n_runs, const qm_pq_run *iruns, int width, int64_t n_rows, uint32_t *present, uint32_t *counts,
                                 uint64_t *ranks, void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls,
                                 int sm_count, cudaStream_t st) {
   const int64_t words = (n_rows + 31) / 32;
@@ -916,14 +953,14 @@ cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, i
   const int pblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_present);
   const int wblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_scatter);
   if (n_runs == 0) {  // no levels: every row present, values by row
-    qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, nullptr, nullptr, out, nulls);
+    qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, nullptr, nullptr, out, nulls);
     return cudaGetLastError();
   }
   qm_pq_present<<<pblocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
   qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
   cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
   if (e != cudaSuccess) return e;
-  qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, width, n_rows, present, ranks, out, nulls);
+  qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, present, ranks, out, nulls);
   return cudaGetLastError();
 }
 

@@ -180,6 +180,39 @@ int64_t pq_def_runs(const uint8_t *b, int64_t start, int64_t end, int64_t max_va
   return got;
 }
 
+// Run headers of the dictionary indices (bit width bw <= 32, at most
+// max_values of them; decodeRleBitPacked): row0 of a run is its first index
+// number; an RLE run keeps its value (ceil(bw / 8) little-endian bytes,
+// masked), a bit-packed one its first byte.  Returns the indices yielded.
+int64_t pq_index_runs(const uint8_t *b, int64_t start, int64_t end, int bw, int64_t max_values,
+                      std::vector<qm_pq_run> &runs) {
+  int64_t pos = start, got = 0;
+  const uint64_t mask = bw >= 32 ? 0xffffffffull : ((1ull << bw) - 1);
+  while (pos < end && got < max_values) {
+    ThriftIn r{b, end, pos};
+    const uint64_t header = r.varint();
+    if (r.bad) break;
+    pos = r.pos;
+    qm_pq_run run{};
+    run.row0 = got;
+    if ((header & 1) == 0) {
+      uint64_t v = 0;
+      for (int i = 0; i < (bw + 7) / 8 && pos < end; i++) v |= (uint64_t)b[pos++] << (8 * i);
+      run.value = (int32_t)(uint32_t)(v & mask);
+      run.count = std::min((int64_t)(header >> 1), max_values - got);
+    } else {
+      const int64_t groups = (int64_t)(header >> 1);
+      run.packed = 1;
+      run.byte_off = pos;
+      run.count = std::min(groups * 8, max_values - got);
+      pos += (groups * 8 * bw + 7) / 8;
+    }
+    if (run.count > 0) runs.push_back(run);
+    got += run.count;
+  }
+  return got;
+}
+
 int pq_width(int dtype) { return dtype == QM_I64 || dtype == QM_F64 ? 8 : 4; }
 
 // One column as the device decodes it: host byte segments laid end to end
@@ -194,6 +227,7 @@ struct PqColumn {
   int64_t bytes = 0;  // device buffer size
   std::vector<qm_pq_page> pages;
   std::vector<qm_pq_run> runs;
+  std::vector<qm_pq_run> iruns;  // dictionary index runs
   int64_t rows = 0;
   int64_t add_seg(const uint8_t *p, int64_t n) {
     const int64_t off = (bytes + 15) & ~(int64_t)15;
@@ -205,26 +239,37 @@ struct PqColumn {
 
 // Host parse of one Parquet column chunk (num_values values) into pages and
 // definition-level runs appended to col, its bytes at device offset base.
+// Dictionary pages set the dictionary of the data pages after them; data
+// pages are PLAIN or dictionary indices (RLE_DICTIONARY, or RLE: encodings
+// 8 and 3, as the reference reads them).
 int pq_parse_chunk(qm_ctx *ctx, const char *name, int dtype, const uint8_t *b, int64_t n, int64_t num_values,
                    int64_t base, PqColumn &col) {
   const int w = pq_width(dtype);
   std::vector<qm_pq_run> &runs = col.runs;
-  const size_t run_first = runs.size();
+  const size_t run_first = runs.size(), irun_first = col.iruns.size();
   int64_t pos = 0, rows = 0;
   const int64_t row_base = col.rows;
+  bool have_dict = false;
+  int64_t dict_off = 0, dict_n = 0;
   while (pos < n && rows < num_values) {
     PqHeader h;
     if (!pq_page_header(b, n, pos, h) || h.compressed <= 0) break;
     pos += h.header_size;
     const int64_t data = pos, data_end = std::min(n, pos + h.compressed);
     pos += h.compressed;
-    if (h.type == 2)
-      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dictionary-encoded pages are not decoded on the GPU", name);
-    if (h.type != 0 && h.type != 3) continue;  // other page types are skipped
-    if (h.encoding != 0)
-      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: page encoding %d (only PLAIN)", name, h.encoding);
+    if (h.type != 0 && h.type != 2 && h.type != 3) continue;  // other page types are skipped
     if (h.compressed != h.uncompressed)
       return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: compressed pages (pass an uncompressed chunk)", name);
+    if (h.type == 2) {  // DICTIONARY_PAGE: PLAIN values
+      have_dict = true;
+      dict_off = base + data;
+      dict_n = std::min(std::max<int64_t>(h.num_values, 0), (data_end - data) / w);
+      continue;
+    }
+    const bool is_dict = h.encoding == 8 || h.encoding == 3;
+    if (!is_dict && h.encoding != 0)
+      return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: page encoding %d (PLAIN or RLE_DICTIONARY)", name,
+                     h.encoding);
     const int64_t len = data_end - data;
     qm_pq_page pg{};
     pg.row0 = row_base + rows;
@@ -239,8 +284,17 @@ int pq_parse_chunk(qm_ctx *ctx, const char *name, int dtype, const uint8_t *b, i
         memcpy(&plen, b + data, 4);
         const int64_t max_def = std::max<int64_t>(64, (h.num_values + 3) / 4 + 8);
         if (plen > 0 && plen <= max_def && plen < len - 4) {
-          const int64_t rem = len - 4 - plen;
-          if (rem >= 0 && rem <= h.num_values * w) {
+          bool level;
+          if (is_dict && have_dict) {  // the byte after the levels must be the index bit width
+            const int64_t after = data + 4 + plen;
+            int expect = 0;
+            while (((int64_t)1 << expect) < dict_n) expect++;
+            level = after < data_end && b[after] == (dict_n <= 1 ? 0 : expect);
+          } else {
+            const int64_t rem = len - 4 - plen;
+            level = rem >= 0 && rem <= h.num_values * w;
+          }
+          if (level) {
             pq_def_runs(b, data + 4, data + 4 + plen, h.num_values, pg.row0, runs, nonnull);
             plain = data + 4 + plen;
             has_def = true;
@@ -256,24 +310,48 @@ int pq_parse_chunk(qm_ctx *ctx, const char *name, int dtype, const uint8_t *b, i
       plain = def0 + h.def_len;
     }
     pg.run1 = (int32_t)runs.size();
-    pg.val_off = base + plain;
-    pg.avail = std::max<int64_t>(0, (data_end - plain) / w);
-    if (has_def) {
-      pg.rows = h.num_values;
-      pg.avail = std::min(pg.avail, nonnull);  // decodePlainValues(plain, dtype, nonNullCount)
-    } else {
-      pg.rows = std::min(h.num_values, pg.avail);
+    if (!has_def) {
+      nonnull = h.num_values;
       pg.run1 = pg.run0;
+    }
+    if (is_dict) {
+      if (!have_dict) {  // indices without a dictionary yield nothing
+        runs.resize(pg.run0);
+        continue;
+      }
+      pg.dict = 1;
+      pg.dict_off = dict_off;
+      pg.dict_n = dict_n;
+      pg.data_end = base + data_end;
+      pg.bw = plain < data_end ? b[plain] : 0;
+      if (pg.bw > 32)
+        return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: dictionary index bit width %d", name, pg.bw);
+      pg.irun0 = pg.irun1 = (int32_t)col.iruns.size();
+      if (pg.bw > 0) pg.n_idx = pq_index_runs(b, plain + 1, data_end, pg.bw, nonnull, col.iruns);
+      pg.irun1 = (int32_t)col.iruns.size();
+      pg.rows = h.num_values;
+      pg.avail = pg.rows;
+    } else {
+      pg.val_off = base + plain;
+      pg.avail = std::max<int64_t>(0, (data_end - plain) / w);
+      if (has_def) {
+        pg.rows = h.num_values;
+        pg.avail = std::min(pg.avail, nonnull);  // decodePlainValues(plain, dtype, nonNullCount)
+      } else {
+        pg.rows = std::min(h.num_values, pg.avail);
+      }
     }
     pg.rows = std::min(pg.rows, num_values - rows);
     if (pg.rows <= 0) {
       runs.resize(pg.run0);
+      col.iruns.resize(pg.dict ? pg.irun0 : col.iruns.size());
       continue;
     }
     col.pages.push_back(pg);
     rows += pg.rows;
   }
   for (size_t i = run_first; i < runs.size(); i++) runs[i].byte_off += base;
+  for (size_t i = irun_first; i < col.iruns.size(); i++) col.iruns[i].byte_off += base;
   col.rows += rows;
   return QM_OK;
 }
@@ -495,19 +573,22 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     }
     const int64_t words = (rows + 31) / 32;
     size_t tb = 0;
-    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, 0, w, rows, nullptr, nullptr, nullptr, nullptr, &tb,
+    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb,
                             nullptr, nullptr, ctx->sm_count, ctx->stream));
     int rc;
     if ((rc = ensure(ctx, chunk, (size_t)pc.bytes + 16)) ||
         (rc = ensure(ctx, pgs, std::max<size_t>(pc.pages.size(), 1) * sizeof(qm_pq_page))) ||
-        (rc = ensure(ctx, rns, std::max<size_t>(pc.runs.size(), 1) * sizeof(qm_pq_run))) ||
+        (rc = ensure(ctx, rns, std::max<size_t>(pc.runs.size() + pc.iruns.size(), 1) * sizeof(qm_pq_run))) ||
         (rc = ensure(ctx, present, (size_t)(words + 1) * 4)) || (rc = ensure(ctx, counts, (size_t)(words + 1) * 4)) ||
         (rc = ensure(ctx, ranks, (size_t)(words + 1) * 8)) || (rc = ensure(ctx, temp, tb + 16)))
       return fail(rc);
     DevCol col;
     col.name = c.name;
     col.dtype = c.dtype;
-    const bool nullable = !pc.runs.empty();
+    // NULLs come from definition levels, and from dictionary indices past
+    // the dictionary
+    bool nullable = !pc.runs.empty();
+    for (const auto &pg : pc.pages) nullable = nullable || pg.dict;
     col.data = col_alloc(ctx, std::max<size_t>((size_t)rows * w, 16), col.data_block);
     col.own_data = col.data != nullptr;
     if (nullable) {
@@ -531,9 +612,12 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     if (!pc.runs.empty())
       CKF(cudaMemcpyAsync(rns.p, pc.runs.data(), pc.runs.size() * sizeof(qm_pq_run), cudaMemcpyHostToDevice,
                          ctx->stream));
+    if (!pc.iruns.empty())  // the index runs after the level runs
+      CKF(cudaMemcpyAsync((qm_pq_run *)rns.p + pc.runs.size(), pc.iruns.data(), pc.iruns.size() * sizeof(qm_pq_run),
+                          cudaMemcpyHostToDevice, ctx->stream));
     size_t tbytes = temp.bytes;
     CKF(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pc.pages.size(),
-                           (const qm_pq_run *)rns.p, (int)pc.runs.size(), w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
+                           (const qm_pq_run *)rns.p, (int)pc.runs.size(), (const qm_pq_run *)rns.p + pc.runs.size(), w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
                            (uint64_t *)ranks.p, temp.p, &tbytes, (unsigned char *)col.data, col.nulls,
                            ctx->sm_count, ctx->stream));
     ctx->launches += pc.runs.empty() ? 1 : 5;

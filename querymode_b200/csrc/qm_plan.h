@@ -256,6 +256,14 @@ struct qm_pq_page {
   int32_t run1;
   int32_t slotted;  // 1: one value slot per row (NULL rows too), value j = row - row0;
                     // 0: present rows' values packed, value j = rank among present rows
+  int32_t dict;     // 1: value j is dictionary entry index[j] (RLE_DICTIONARY page)
+  int64_t dict_off; // dict: the dictionary's PLAIN values in the chunk, and how many
+  int64_t dict_n;
+  int64_t data_end; // dict: end of the page's data (index bytes at or past it read as 0)
+  int64_t n_idx;    // dict: indices the page's index stream yields (index j >= n_idx: 0)
+  int32_t irun0;    // dict: its index runs [irun0, irun1) (row0 = first index number)
+  int32_t irun1;
+  int32_t bw;       // dict: index bit width (0: every index 0)
   int32_t reserved;
 };
 // A run of the RLE / bit-packed hybrid definition levels (bit width 1).

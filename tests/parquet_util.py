@@ -19,6 +19,28 @@ def write_plain(cols: dict, version: str, page_size: int = 4096) -> bytes:
     return buf.getvalue()
 
 
+def write_dict(cols: dict, version: str, page_size: int = 4096, dict_limit: int = 1 << 20) -> bytes:
+    """Dictionary-encoded (RLE_DICTIONARY indices; PLAIN pages after the
+    dictionary outgrows `dict_limit` bytes), uncompressed."""
+    arrays = {name: pa.array(vals, mask=mask) for name, (vals, mask) in cols.items()}
+    buf = io.BytesIO()
+    pq.write_table(pa.table(arrays), buf, use_dictionary=True, compression="NONE", data_page_version=version,
+                   data_page_size=page_size, dictionary_pagesize_limit=dict_limit, write_statistics=True)
+    return buf.getvalue()
+
+
+def dict_columns(n: int, seed: int):
+    """Few distinct values per column (dictionary-friendly), NULLs in some."""
+    rng = np.random.default_rng(seed)
+    return {
+        "i32": (rng.integers(-50, 50, n).astype(np.int32), rng.random(n) < 0.1),
+        "i64": ((rng.integers(0, 3000, n) * 7919 - 10**12).astype(np.int64), None),
+        "f32": (rng.integers(0, 7, n).astype(np.float32) / 4, rng.random(n) < 0.3),
+        "f64": (rng.integers(0, 20000, n) * 0.5, None),
+        "key": (((np.arange(n) * 7919) % 101).astype(np.int64), None),
+    }
+
+
 def chunks_of(raw: bytes):
     """(name, physical type, chunk bytes, num_values) of row group 0."""
     md = pq.ParquetFile(io.BytesIO(raw)).metadata.row_group(0)
