@@ -334,7 +334,10 @@ __device__ __forceinline__ const uint8_t *pq_dict_entry(const uint8_t *chunk, co
 // a slotted page (or any page of a column without levels: present == null)
 // j = r - row0.  j past the values present gives NULL (as the reference's
 // decoded[dPtr++] / values[vi++] running out does).
+// DICT: the column has dictionary pages (a separate instantiation, so the
+// PLAIN-only one keeps its registers).
 #define QM_PQ_UNROLL 4
+template <bool DICT>
 __global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages,
                                                      const qm_pq_run *iruns, int width, int64_t n_rows,
                                                      const uint32_t *present, const uint64_t *ranks,
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const
             }
             j = (int64_t)ranks[w + u] + __popc(pw & ((1u << lane) - 1u)) - rank_f;
           }
-          if (c.dict) {
+          if (DICT && c.dict) {
             src[u] = pq_dict_entry(chunk, pages[c.p], iruns, j, width);
             live[u] = src[u] != nullptr;
           } else if (j < c.avail) {
@@ -943,24 +946,28 @@ cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, i
   if (n_rows <= 0) return cudaSuccess;
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
   // one resident wave: every warp owns a fixed range of words
-  static int occ_present = 0, occ_scatter = 0;
+  static int occ_present = 0, occ_scatter[2] = {0, 0};
   if (!occ_present) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_present, qm_pq_present, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter, qm_pq_scatter, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[0], qm_pq_scatter<false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[1], qm_pq_scatter<true>, 256, 0);
     occ_present = std::max(occ_present, 1);
-    occ_scatter = std::max(occ_scatter, 1);
+    occ_scatter[0] = std::max(occ_scatter[0], 1);
+    occ_scatter[1] = std::max(occ_scatter[1], 1);
   }
+  const bool dict = iruns != nullptr;
+  const auto scatter = dict ? qm_pq_scatter<true> : qm_pq_scatter<false>;
   const int pblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_present);
-  const int wblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_scatter);
+  const int wblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_scatter[dict]);
   if (n_runs == 0) {  // no levels: every row present, values by row
-    qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, nullptr, nullptr, out, nulls);
+    scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, nullptr, nullptr, out, nulls);
     return cudaGetLastError();
   }
   qm_pq_present<<<pblocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
   qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
   cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
   if (e != cudaSuccess) return e;
-  qm_pq_scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, present, ranks, out, nulls);
+  scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, present, ranks, out, nulls);
   return cudaGetLastError();
 }
 

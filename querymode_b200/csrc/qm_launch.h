@@ -76,7 +76,9 @@ cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O,
                                   cudaStream_t st);
 // Decode a column from Parquet PLAIN pages (chunk bytes on the device; pages
 // and definition-level runs parsed on the host).  temp null: *temp_bytes
-// receives the scan's scratch size.  nulls may be null (no page has levels).
+// receives the scan's scratch size.  nulls may be null (no page has levels
+// and none is a dictionary page).  iruns: the dictionary pages' index runs,
+// null when no page is a dictionary page.
 cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
                                 int n_runs, const qm_pq_run *iruns, int width, int64_t n_rows, uint32_t *present, uint32_t *counts,
                                 uint64_t *ranks, void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls,

@@ -587,8 +587,9 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     col.dtype = c.dtype;
     // NULLs come from definition levels, and from dictionary indices past
     // the dictionary
-    bool nullable = !pc.runs.empty();
-    for (const auto &pg : pc.pages) nullable = nullable || pg.dict;
+    bool has_dict = false;
+    for (const auto &pg : pc.pages) has_dict = has_dict || pg.dict;
+    const bool nullable = !pc.runs.empty() || has_dict;
     col.data = col_alloc(ctx, std::max<size_t>((size_t)rows * w, 16), col.data_block);
     col.own_data = col.data != nullptr;
     if (nullable) {
@@ -617,7 +618,8 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
                           cudaMemcpyHostToDevice, ctx->stream));
     size_t tbytes = temp.bytes;
     CKF(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pc.pages.size(),
-                           (const qm_pq_run *)rns.p, (int)pc.runs.size(), (const qm_pq_run *)rns.p + pc.runs.size(), w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
+                           (const qm_pq_run *)rns.p, (int)pc.runs.size(),
+                           has_dict ? (const qm_pq_run *)rns.p + pc.runs.size() : nullptr, w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
                            (uint64_t *)ranks.p, temp.p, &tbytes, (unsigned char *)col.data, col.nulls,
                            ctx->sm_count, ctx->stream));
     ctx->launches += pc.runs.empty() ? 1 : 5;
