@@ -227,6 +227,13 @@ const char *qm_ctx_last_error(const qm_ctx *ctx);
 int qm_ctx_set_stream(qm_ctx *ctx, void *stream);
 /* Set (tuning != NULL) or clear (NULL) the context's launch-shape knobs. */
 int qm_ctx_set_tuning(qm_ctx *ctx, const qm_tuning *tuning);
+/* Device blocks of destroyed tables are kept by the context for the next
+ * tables of about their size (up to an eighth of the device's memory; given
+ * back by this library whenever one of its allocations fails, and at
+ * qm_ctx_destroy).  This frees them now, for a caller whose other allocators
+ * need the memory; *released (may be null) receives the bytes freed.  No
+ * counterpart in the reference (device memory management). */
+int qm_ctx_trim(qm_ctx *ctx, int64_t *released);
 /* Device properties the host planner and tests read. */
 int qm_ctx_device_info(const qm_ctx *ctx, int32_t *sm_count, int64_t *hbm_bytes);
 

@@ -151,6 +151,7 @@ SIGNATURES = [
     ("qm_ctx_destroy", C.c_int, [_P]),
     ("qm_ctx_last_error", C.c_char_p, [_P]),
     ("qm_ctx_set_stream", C.c_int, [_P, C.c_void_p]),
+    ("qm_ctx_trim", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("qm_ctx_set_tuning", C.c_int, [_P, C.c_void_p]),
     ("qm_ctx_device_info", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("qm_table_create", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn), _PP]),

@@ -1964,6 +1964,19 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   return QM_OK;
 }
 
+int qm_ctx_trim(qm_ctx *ctx, int64_t *released) {
+  if (!ctx) return QM_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  size_t bytes;
+  {
+    std::lock_guard<std::mutex> lk(ctx->dpool.mu);
+    bytes = ctx->dpool.cached;
+  }
+  ctx->dpool.trim();
+  if (released) *released = (int64_t)bytes;
+  return QM_OK;
+}
+
 int qm_ctx_set_tuning(qm_ctx *ctx, const qm_tuning *t) {
   if (!ctx) return QM_ERR_INVALID;
   if (!t) {

@@ -390,6 +390,13 @@ class Context:
         context's own stream."""
         self.check(self.lib.qm_ctx_set_stream(self.h, stream_handle or None))
 
+    def trim(self) -> int:
+        """Free the device blocks kept from destroyed tables; returns the
+        bytes freed."""
+        n = C.c_int64()
+        self.check(self.lib.qm_ctx_trim(self.h, C.byref(n)))
+        return n.value
+
     def set_tuning(self, local_slots: int = 0, dedupe: int = -1, blocks_per_sm: int = 0,
                    stage_depth: int = 0) -> None:
         """Launch-shape knobs of the fused scan (see qm_tuning); the

@@ -508,6 +508,8 @@ def test_tables_recycle_device_blocks(ctx):
         t = ctx.table(cols)
         assert_same(t.run(q), oracle.run(cols, q), ctx_msg=f"table {it}")
         t.close()
+    assert ctx.trim() > 0  # the last table's blocks were kept
+    assert ctx.trim() == 0
 
 
 def test_statistics_at_upload_match_lazy_ones(ctx):
