@@ -229,8 +229,19 @@ struct PqColumn {
   std::vector<qm_pq_run> runs;
   std::vector<qm_pq_run> iruns;  // dictionary index runs
   int64_t rows = 0;
+  // Device offset of a page's bytes.  A page that starts where the previous
+  // one ended in host memory extends its segment (pages of one buffer, as a
+  // reader fetched them, become one copy); a new segment starts at the next
+  // offset with the host address's alignment modulo 16.
   int64_t add_seg(const uint8_t *p, int64_t n) {
-    const int64_t off = (bytes + 15) & ~(int64_t)15;
+    if (!segs.empty() && n > 0 && segs.back().p + segs.back().bytes == p) {
+      PqSeg &g = segs.back();
+      const int64_t off = g.off + g.bytes;
+      g.bytes += n;
+      bytes = off + n;
+      return off;
+    }
+    const int64_t off = ((bytes + 15) & ~(int64_t)15) + (int64_t)((uintptr_t)p & 15);
     segs.push_back({p, n, off});
     bytes = off + n;
     return off;
@@ -477,8 +488,32 @@ void fill_window(const PqColumn &col, int64_t a, int64_t e, uint8_t *h, int64_t 
 // Host segments into the device buffer through two pinned staging buffers:
 // the column's byte image goes over in windows, a team of host threads
 // filling one buffer while the other is copied.
-int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev, HostTeam *team) {
+int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev, std::unique_ptr<HostTeam> &team_slot) {
   if (col.bytes <= 0) return QM_OK;
+  // Segments in page-locked memory go over directly, without staging.
+  bool pinned = true;
+  for (const PqSeg &g : col.segs) {
+    if (g.bytes <= 0) continue;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, g.p) != cudaSuccess || at.type != cudaMemoryTypeHost ||
+        cudaPointerGetAttributes(&at, g.p + g.bytes - 1) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      pinned = false;
+      break;
+    }
+  }
+  if (pinned) {
+    for (const PqSeg &g : col.segs)
+      if (g.bytes > 0 && cudaMemcpyAsync(dev + g.off, g.p, (size_t)g.bytes, cudaMemcpyHostToDevice, ctx->stream) !=
+                             cudaSuccess)
+        return set_err(ctx, QM_ERR_CUDA, "page upload: %s", cudaGetErrorString(cudaGetLastError()));
+    return QM_OK;  // the caller synchronises before its host vectors go
+  }
+  if (col.bytes >= ((int64_t)16 << 20) && !team_slot) {  // host threads fill the staging buffers
+    const int hw = (int)std::thread::hardware_concurrency();
+    team_slot.reset(new HostTeam(std::max(1, std::min(16, hw / 2))));
+  }
+  HostTeam *team = team_slot.get();
   const int64_t win = std::min<int64_t>(col.bytes, (int64_t)64 << 20);
   HostBuf hb[2];
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -517,6 +552,32 @@ int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev, HostTeam *te
   return rc;
 }
 
+// Scratch of one call in blocks of the context's pool (no cudaMalloc /
+// cudaFree per call once the pool holds them); back to the pool at the end,
+// after the call's last synchronise.
+struct PoolBuf {
+  qm_ctx *ctx;
+  void *p = nullptr;
+  size_t block = 0, bytes = 0;
+  explicit PoolBuf(qm_ctx *c) : ctx(c) {}
+  PoolBuf(const PoolBuf &) = delete;
+  PoolBuf &operator=(const PoolBuf &) = delete;
+  ~PoolBuf() { drop(); }
+  void drop() {
+    if (p) col_release(ctx, p, block);
+    p = nullptr;
+    block = bytes = 0;
+  }
+  int ensure(size_t n) {
+    if (p && bytes >= n) return QM_OK;
+    drop();
+    p = col_alloc(ctx, n, block);
+    if (!p) return set_err(ctx, QM_ERR_OOM, "device scratch (%zu bytes)", n);
+    bytes = block;
+    return QM_OK;
+  }
+};
+
 }  // namespace
 
 extern "C" {
@@ -533,12 +594,10 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
   cudaSetDevice(ctx->device);
   qm_table *t = new qm_table();
   t->ctx = ctx;
-  DevBuf chunk, pgs, rns, present, counts, ranks, temp;
+  PoolBuf chunk(ctx), pgs(ctx), rns(ctx), present(ctx), counts(ctx), ranks(ctx), temp(ctx);
   std::unique_ptr<HostTeam> team;  // fills the staging buffers of large columns
   auto fail = [&](int rc) {
-    DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};
-    for (DevBuf *x : bufs) release(*x);
-    qm_table_destroy(t);
+    qm_table_destroy(t);  // synchronises before the scratch goes back to the pool
     return rc;
   };
   for (int i = 0; i < n_cols; i++) {
@@ -576,11 +635,11 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb,
                             nullptr, nullptr, ctx->sm_count, ctx->stream));
     int rc;
-    if ((rc = ensure(ctx, chunk, (size_t)pc.bytes + 16)) ||
-        (rc = ensure(ctx, pgs, std::max<size_t>(pc.pages.size(), 1) * sizeof(qm_pq_page))) ||
-        (rc = ensure(ctx, rns, std::max<size_t>(pc.runs.size() + pc.iruns.size(), 1) * sizeof(qm_pq_run))) ||
-        (rc = ensure(ctx, present, (size_t)(words + 1) * 4)) || (rc = ensure(ctx, counts, (size_t)(words + 1) * 4)) ||
-        (rc = ensure(ctx, ranks, (size_t)(words + 1) * 8)) || (rc = ensure(ctx, temp, tb + 16)))
+    if ((rc = chunk.ensure((size_t)pc.bytes + 16)) ||
+        (rc = pgs.ensure(std::max<size_t>(pc.pages.size(), 1) * sizeof(qm_pq_page))) ||
+        (rc = rns.ensure(std::max<size_t>(pc.runs.size() + pc.iruns.size(), 1) * sizeof(qm_pq_run))) ||
+        (rc = present.ensure((size_t)(words + 1) * 4)) || (rc = counts.ensure((size_t)(words + 1) * 4)) ||
+        (rc = ranks.ensure((size_t)(words + 1) * 8)) || (rc = temp.ensure(tb + 16)))
       return fail(rc);
     DevCol col;
     col.name = c.name;
@@ -602,11 +661,7 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     }
     t->cols.push_back(col);
     if (nullable) CKF(cudaMemsetAsync(col.nulls, 0, (size_t)(words + 1) * 4, ctx->stream));  // + the padding word
-    if (pc.bytes >= ((int64_t)16 << 20) && !team) {
-      const int hw = (int)std::thread::hardware_concurrency();
-      team.reset(new HostTeam(std::max(1, std::min(16, hw / 2))));
-    }
-    if ((rc = upload_segments(ctx, pc, (uint8_t *)chunk.p, team.get()))) return fail(rc);
+    if ((rc = upload_segments(ctx, pc, (uint8_t *)chunk.p, team))) return fail(rc);
     if (!pc.pages.empty())
       CKF(cudaMemcpyAsync(pgs.p, pc.pages.data(), pc.pages.size() * sizeof(qm_pq_page), cudaMemcpyHostToDevice,
                          ctx->stream));
@@ -625,8 +680,6 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     ctx->launches += pc.runs.empty() ? 1 : 5;
     CKF(cudaStreamSynchronize(ctx->stream));  // the host vectors above go out of scope
   }
-  DevBuf *bufs[] = {&chunk, &pgs, &rns, &present, &counts, &ranks, &temp};
-  for (DevBuf *x : bufs) release(*x);
   *out = t;
   return QM_OK;
 }

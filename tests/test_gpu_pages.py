@@ -153,3 +153,27 @@ def test_page_table_matches_page_list(ctx):
     v2, n2 = t2.read_column("c")
     assert np.array_equal(v1, v2) and np.array_equal(n1, n2)
     check_column(t2, "c", "int64", pages)
+
+
+def test_pinned_page_buffers(ctx):
+    """Pages in page-locked memory go to the device without staging; back to
+    back in one buffer they are one copy, at the buffer's own alignment."""
+    import torch
+    rng = np.random.default_rng(23)
+    for dtype in ("int32", "int64", "float64"):
+        pages = [p for p in random_pages(rng, dtype, 25) if not p.parquet]
+        bufs = [bytes(p.buf) for p in pages]
+        lens = np.array([len(b) for b in bufs], dtype=np.int64)
+        offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.int64)
+        joined = np.frombuffer(b"".join(bufs), dtype=np.uint8)
+        pinned = torch.from_numpy(joined.copy()).pin_memory().numpy()
+        args = (offs, lens, np.array([p.row_count for p in pages]), np.array([p.null_count for p in pages]),
+                np.array([-1 if p.data_offset is None else p.data_offset for p in pages]))
+        t1 = ctx.table_from_pages([("c", QM[dtype], PageTable(joined, *args))])
+        t2 = ctx.table_from_pages([("c", QM[dtype], PageTable(pinned, *args))])
+        v1, n1 = t1.read_column("c")
+        v2, n2 = t2.read_column("c")
+        assert np.array_equal(v1.view(np.uint8), v2.view(np.uint8)) and np.array_equal(n1, n2), dtype
+        check_column(t2, "c", dtype, pages)
+        t1.close()
+        t2.close()
