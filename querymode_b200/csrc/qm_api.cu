@@ -315,6 +315,11 @@ int upload_nulls(qm_ctx *ctx, const uint8_t *host_bits, int64_t n, uint32_t **ou
   return QM_OK;
 }
 
+// Host bytes to device memory on the context's stream: page-locked and small
+// sources by one copy, large pageable ones staged through pinned buffers by
+// host threads (defined with the page ingest).
+int upload_host_bytes(qm_ctx *ctx, const void *src, size_t n, void *dst);
+
 int make_col(qm_ctx *ctx, int64_t n, const qm_column &src, DevCol &c) {
   if (!src.name) return set_err(ctx, QM_ERR_INVALID, "column without a name");
   if (!valid_dtype(src.dtype))
@@ -343,7 +348,10 @@ int make_col(qm_ctx *ctx, int64_t n, const qm_column &src, DevCol &c) {
   if (!d) return set_err(ctx, QM_ERR_OOM, "column %s: device memory (%zu bytes)", src.name, bytes);
   c.data = d;
   c.own_data = true;
-  if (bytes) CK(cudaMemcpyAsync(d, src.data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if (bytes) {
+    int rc = upload_host_bytes(ctx, src.data, bytes, d);
+    if (rc) return rc;
+  }
   if (src.null_bitmap) {
     c.own_nulls = true;
     int rc = upload_nulls(ctx, src.null_bitmap, n, &c.nulls, c.nulls_block);

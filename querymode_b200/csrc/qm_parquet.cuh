@@ -552,6 +552,21 @@ int upload_segments(qm_ctx *ctx, const PqColumn &col, uint8_t *dev, std::unique_
   return rc;
 }
 
+int upload_host_bytes(qm_ctx *ctx, const void *src, size_t n, void *dst) {
+  cudaPointerAttributes at;
+  const bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (pinned || n < ((size_t)64 << 20)) {
+    CK(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, ctx->stream));
+    return QM_OK;
+  }
+  PqColumn col;
+  col.segs.push_back({(const uint8_t *)src, (int64_t)n, 0});
+  col.bytes = (int64_t)n;
+  std::unique_ptr<HostTeam> team;
+  return upload_segments(ctx, col, (uint8_t *)dst, team);
+}
+
 // Scratch of one call in blocks of the context's pool (no cudaMalloc /
 // cudaFree per call once the pool holds them); back to the pool at the end,
 // after the call's last synchronise.

@@ -536,3 +536,17 @@ def test_statistics_at_upload_match_lazy_ones(ctx):
         for q in qs:
             assert_same(t.run(q), oracle.run(cols, q, threads=8), ctx_msg=name)
         t.close()
+
+
+def test_large_pageable_columns_staged(ctx):
+    # host columns of >= 64 MB in pageable memory go through pinned staging
+    # buffers filled by host threads; the table must hold the same cells
+    rng = np.random.default_rng(111)
+    n = 9_000_000
+    cols = {"k": rng.integers(0, 1000, n).astype(np.int64), "v": rng.normal(size=n),
+            "f": Column(rng.integers(0, 100, n).astype(np.int64), rng.random(n) < 0.01)}
+    t = ctx.table(cols)
+    q = QueryDescriptor(filters=[FilterOp("f", "lt", 50)], group_by=["k"],
+                        aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*"), AggregateOp("max", "f")])
+    assert_same(t.run(q), oracle.run(cols, q, threads=8))
+    t.close()
