@@ -177,3 +177,24 @@ def test_pinned_page_buffers(ctx):
         check_column(t2, "c", dtype, pages)
         t1.close()
         t2.close()
+
+
+def test_empty_inputs(ctx):
+    """Empty pages, an empty page table and a Parquet chunk of no values make
+    a table of 0 rows; the ungrouped aggregate over it answers as the oracle."""
+    from tests.parquet_util import chunks_of, write_plain
+    raw = write_plain({"c": (np.zeros(0, dtype=np.int64), None)}, "1.0")
+    _, _, chunk, nv = chunks_of(raw)[0]
+    empty_pt = PageTable(np.zeros(0, dtype=np.uint8), np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.int64))
+    specs = [[("c", A.QM_I64, [Page(b""), Page(b"", 0, 0), Page(bytes([0xFF]), 9, 1)])],
+             [("c", A.QM_I64, empty_pt)],
+             [("c", A.QM_I64, [Page(chunk, nv, 0, None, True)])],
+             [("c", A.QM_I64, [])]]
+    q = QueryDescriptor(aggregates=[AggregateOp("sum", "c"), AggregateOp("count", "*"), AggregateOp("max", "c")])
+    for spec in specs:
+        t = ctx.table_from_pages(spec)
+        assert t.n_rows == 0
+        vals, nulls = t.read_column("c")
+        assert len(vals) == 0 and len(nulls) == 0
+        assert_same(t.run(q), oracle.run({"c": np.zeros(0, dtype=np.int64)}, q))
+        t.close()
