@@ -14,24 +14,38 @@ import struct
 
 
 class _Thrift:
+    """Thrift compact protocol with the reference's reading rules
+    (ThriftReader, src/parquet.ts:44-183): varints of at most 5 bytes keep
+    the low 32 bits, i32 fields are their zigzag as an int32, the buffer's
+    end ends a struct, unknown types take no bytes."""
+
     def __init__(self, b: bytes, pos: int):
         self.b, self.pos, self.last, self.stack = b, pos, 0, []
 
+    def byte_at(self, i: int) -> int:
+        return self.b[i] if i < len(self.b) else 0  # JS reads undefined: 0 in bit operations
+
     def varint(self) -> int:
         v = shift = 0
-        while True:
+        while self.pos < len(self.b):
             c = self.b[self.pos]
             self.pos += 1
-            v |= (c & 0x7F) << shift
+            v = (v | ((c & 0x7F) << shift)) & 0xFFFFFFFF
             if not c & 0x80:
                 return v
             shift += 7
+            if shift >= 35:
+                return v
+        return v
 
     def zigzag(self) -> int:
         v = self.varint()
-        return (v >> 1) ^ -(v & 1)
+        r = (v >> 1) ^ (-(v & 1) & 0xFFFFFFFF)
+        return r - (1 << 32) if r & 0x80000000 else r
 
     def field(self):
+        if self.pos >= len(self.b):
+            return None
         h = self.b[self.pos]
         self.pos += 1
         if h == 0:
@@ -41,39 +55,51 @@ class _Thrift:
         self.last = fid
         return fid, t
 
-    def skip(self, t: int):
-        if t in (1, 2):
+    def skip(self, t: int, depth: int = 0):
+        if depth > 64:
             return
         if t == 3:
             self.pos += 1
-        elif t in (4, 5, 6):
+        elif t in (4, 5):
             self.varint()
+        elif t == 6:
+            while self.pos < len(self.b):
+                c = self.b[self.pos]
+                self.pos += 1
+                if not c & 0x80:
+                    break
         elif t == 7:
             self.pos += 8
         elif t == 8:
             n = self.varint()
             self.pos += n
         elif t in (9, 10):
-            h = self.b[self.pos]
+            h = self.byte_at(self.pos)
             self.pos += 1
             size = h >> 4
             if size == 15:
                 size = self.varint()
-            for _ in range(size):
-                self.skip(h & 0x0F)
+            i = 0
+            # past the buffer's end only the position changes, and it is past
+            # already; elements of no bytes (bools, unknown types) change nothing
+            while i < size and self.pos < len(self.b) and 3 <= (h & 0x0F) <= 12:
+                self.skip(h & 0x0F, depth + 1)
+                i += 1
         elif t == 11:
             size = self.varint()
             if size:
-                kv = self.b[self.pos]
+                kv = self.byte_at(self.pos)
                 self.pos += 1
-                for _ in range(size):
-                    self.skip(kv >> 4)
-                    self.skip(kv & 0x0F)
+                i = 0
+                while i < size and self.pos < len(self.b) and (3 <= kv >> 4 <= 12 or 3 <= (kv & 0x0F) <= 12):
+                    self.skip(kv >> 4, depth + 1)
+                    self.skip(kv & 0x0F, depth + 1)
+                    i += 1
         elif t == 12:
             self.stack.append(self.last)
             self.last = 0
             while (f := self.field()) is not None:
-                self.skip(f[1])
+                self.skip(f[1], depth + 1)
             self.last = self.stack.pop()
 
 
@@ -103,6 +129,10 @@ def parse_page_header(b: bytes, offset: int) -> dict:
                     h["def_len"] = r.zigzag()
                 elif fid == 8 and gid == 6:
                     h["rep_len"] = r.zigzag()
+                elif fid == 8 and gid in (2, 3):
+                    r.zigzag()  # num_nulls, num_rows: read as i32 whatever their type
+                elif fid == 8 and gid == 7:
+                    pass  # is_compressed: in the type nibble
                 else:
                     r.skip(gt)
             r.last = r.stack.pop()
@@ -112,24 +142,44 @@ def parse_page_header(b: bytes, offset: int) -> dict:
     return h
 
 
+def _run_varint(b: bytes, pos: int) -> tuple[int, int]:
+    """readVarint (src/footer.ts:183-200): to the terminator or the end, the
+    low 32 bits."""
+    v = shift = 0
+    while pos < len(b):
+        c = b[pos]
+        pos += 1
+        if shift < 32:
+            v = (v | ((c & 0x7F) << shift)) & 0xFFFFFFFF
+        if not c & 0x80:
+            break
+        shift += 7
+    return v, pos
+
+
 def decode_rle_bit_packed(b: bytes, bit_width: int, max_values: int) -> list[int]:
+    """decodeRleBitPacked (src/parquet-decode.ts:119-188).  A run's count is
+    its header shifted as a signed 32-bit number (the reference's
+    `header >> 1`); a negative bit-packed count, after which the reference
+    would step back and read the same bytes again without end, ends the
+    stream."""
     values: list[int] = []
     pos = 0
     mask = (1 << bit_width) - 1
     while pos < len(b) and len(values) < max_values:
-        r = _Thrift(b, pos)
-        header = r.varint()
-        pos = r.pos
+        header, pos = _run_varint(b, pos)
+        half = (header - (1 << 32) if header & 0x80000000 else header) >> 1
         if header & 1 == 0:
-            count = header >> 1
             val = 0
             for i in range((bit_width + 7) // 8):
                 if pos < len(b):
                     val |= b[pos] << (8 * i)
                     pos += 1
-            values += [val & mask] * min(count, max_values - len(values))
+            values += [val & mask] * max(0, min(half, max_values - len(values)))
         else:
-            groups = header >> 1
+            if half < 0:
+                break
+            groups = half
             n = min(groups * 8, max_values - len(values))
             bitpos = pos * 8
             for _ in range(n):

@@ -13,42 +13,47 @@
 
 namespace {
 
-// Thrift compact protocol reader (enough for PageHeader and to skip the rest).
+// Thrift compact protocol reader with the reference's reading rules
+// (ThriftReader, src/parquet.ts:44-183): varints of at most 5 bytes keep the
+// low 32 bits; i32 fields are their zigzag as an int32; the buffer's end
+// ends a struct; fields are told apart by id alone; unknown types take no
+// bytes.  Positions may run past the end (the page then has no data).
 struct ThriftIn {
   const uint8_t *b;
   int64_t n, pos;
-  bool bad = false;
-  int16_t last = 0;
-  std::vector<int16_t> stack;
+  int32_t last = 0;
+  std::vector<int32_t> stack;
 
-  uint64_t varint() {
-    uint64_t v = 0;
+  uint8_t byte_at(int64_t i) const { return i < n ? b[i] : 0; }  // JS reads undefined, 0 in bit operations
+  uint32_t varint32() {
+    uint32_t r = 0;
     int shift = 0;
-    while (pos < n && shift < 64) {
+    while (pos < n) {
       const uint8_t c = b[pos++];
-      v |= (uint64_t)(c & 0x7f) << shift;
-      if (!(c & 0x80)) return v;
+      r |= (uint32_t)(c & 0x7f) << shift;
+      if (!(c & 0x80)) return r;
       shift += 7;
+      if (shift >= 35) return r;
     }
-    bad = true;
-    return v;
+    return r;
   }
-  int64_t zigzag() {
-    const uint64_t v = varint();
-    return (int64_t)(v >> 1) ^ -(int64_t)(v & 1);
+  int32_t zigzag32() {
+    const uint32_t v = varint32();
+    return (int32_t)((v >> 1) ^ (0u - (v & 1)));
   }
-  // next field of the current struct: false at STOP
+  void skip_varint64() {  // readVarint64: to the terminator or the end
+    while (pos < n)
+      if (!(b[pos++] & 0x80)) return;
+  }
+  // next field of the current struct: false at STOP or at the buffer's end
   bool field(int &id, int &type) {
-    if (pos >= n) {
-      bad = true;
-      return false;
-    }
+    if (pos >= n) return false;
     const uint8_t h = b[pos++];
     if (h == 0) return false;
     type = h & 0x0f;
     const int delta = h >> 4;
-    id = delta ? last + delta : (int)zigzag();
-    last = (int16_t)id;
+    id = delta ? last + delta : zigzag32();
+    last = id;
     return true;
   }
   void begin() {
@@ -59,35 +64,37 @@ struct ThriftIn {
     last = stack.empty() ? 0 : stack.back();
     if (!stack.empty()) stack.pop_back();
   }
+  // Types that consume a byte at least when the buffer has one left (bools in
+  // the type nibble and unknown types take none).
+  static bool takes_bytes(int type) { return type >= 3 && type <= 12; }
+  // A list or map past the buffer's end changes nothing but the position,
+  // which is past the end already: its remaining elements are not walked.
   void skip(int type, int depth = 0) {
-    if (depth > 32) {
-      bad = true;
-      return;
-    }
+    if (depth > 64) return;  // deeper nesting than any page header: treat as skipped
     switch (type) {
-      case 1: case 2: break;  // bool in the type nibble
       case 3: pos += 1; break;
-      case 4: case 5: case 6: varint(); break;
+      case 4: case 5: varint32(); break;
+      case 6: skip_varint64(); break;
       case 7: pos += 8; break;
       case 8: {
-        const int64_t len = (int64_t)varint();
+        const uint32_t len = varint32();
         pos += len;
         break;
       }
       case 9: case 10: {
-        if (pos >= n) { bad = true; return; }
-        const uint8_t h = b[pos++];
-        int64_t size = h >> 4;
-        if (size == 15) size = (int64_t)varint();
-        for (int64_t i = 0; i < size && !bad; i++) skip(h & 0x0f, depth + 1);
+        const uint8_t h = byte_at(pos++);
+        uint32_t size = h >> 4;
+        if (size == 15) size = varint32();
+        if (!takes_bytes(h & 0x0f)) break;  // elements of no bytes: the loop would change nothing
+        for (uint32_t i = 0; i < size && pos < n; i++) skip(h & 0x0f, depth + 1);
         break;
       }
       case 11: {
-        const int64_t size = (int64_t)varint();
+        const uint32_t size = varint32();
         if (size > 0) {
-          if (pos >= n) { bad = true; return; }
-          const uint8_t kv = b[pos++];
-          for (int64_t i = 0; i < size && !bad; i++) {
+          const uint8_t kv = byte_at(pos++);
+          if (!takes_bytes(kv >> 4) && !takes_bytes(kv & 0x0f)) break;
+          for (uint32_t i = 0; i < size && pos < n; i++) {
             skip(kv >> 4, depth + 1);
             skip(kv & 0x0f, depth + 1);
           }
@@ -97,13 +104,12 @@ struct ThriftIn {
       case 12: {
         begin();
         int id, t;
-        while (!bad && field(id, t)) skip(t, depth + 1);
+        while (field(id, t)) skip(t, depth + 1);
         end();
         break;
       }
-      default: bad = true;
+      default: break;  // bools (in the type nibble) and unknown types take no bytes
     }
-    if (pos > n) bad = true;
   }
 };
 
@@ -115,23 +121,26 @@ struct PqHeader {
   int64_t header_size = 0;
 };
 
-// parsePageHeader: fields 1-3, data page (5), dictionary page (7), v2 (8).
+// parsePageHeader (src/parquet-decode.ts:239-276): fields 1-3, data page (5),
+// dictionary page (7), v2 (8), each by field id whatever its type.
 bool pq_page_header(const uint8_t *b, int64_t n, int64_t off, PqHeader &h) {
   ThriftIn r{b, n, off};
   int id, t;
-  while (!r.bad && r.field(id, t)) {
-    if (id == 1 && t == 5) h.type = (int)r.zigzag();
-    else if (id == 2 && t == 5) h.uncompressed = r.zigzag();
-    else if (id == 3 && t == 5) h.compressed = r.zigzag();
-    else if ((id == 5 || id == 7 || id == 8) && t == 12) {
+  while (r.field(id, t)) {
+    if (id == 1) h.type = r.zigzag32();
+    else if (id == 2) h.uncompressed = r.zigzag32();
+    else if (id == 3) h.compressed = r.zigzag32();
+    else if (id == 5 || id == 7 || id == 8) {
       r.begin();
       int fid, ft;
-      while (!r.bad && r.field(fid, ft)) {
-        if (fid == 1 && ft == 5) h.num_values = r.zigzag();
-        else if (id == 8 && fid == 4 && ft == 5) h.encoding = (int)r.zigzag();
-        else if (id != 8 && fid == 2 && ft == 5) h.encoding = (int)r.zigzag();
-        else if (id == 8 && fid == 5 && ft == 5) h.def_len = r.zigzag();
-        else if (id == 8 && fid == 6 && ft == 5) h.rep_len = r.zigzag();
+      while (r.field(fid, ft)) {
+        if (fid == 1) h.num_values = r.zigzag32();
+        else if (id != 8 && fid == 2) h.encoding = r.zigzag32();
+        else if (id == 8 && (fid == 2 || fid == 3)) r.zigzag32();
+        else if (id == 8 && fid == 4) h.encoding = r.zigzag32();
+        else if (id == 8 && fid == 5) h.def_len = r.zigzag32();
+        else if (id == 8 && fid == 6) h.rep_len = r.zigzag32();
+        else if (id == 8 && fid == 7) { /* is_compressed: in the type nibble */ }
         else r.skip(ft);
       }
       r.end();
@@ -139,76 +148,99 @@ bool pq_page_header(const uint8_t *b, int64_t n, int64_t off, PqHeader &h) {
       r.skip(t);
     }
   }
-  if (r.bad) return false;
   h.header_size = r.pos - off;
   return true;
 }
 
+// The varint of an RLE / bit-packed run header (readVarint, src/footer.ts:
+// 183-200): to the terminator or the end, the low 32 bits.
+uint32_t pq_run_varint(const uint8_t *b, int64_t end, int64_t &pos) {
+  uint32_t r = 0;
+  int shift = 0;
+  while (pos < end) {
+    const uint8_t c = b[pos++];
+    if (shift < 32) r |= (uint32_t)(c & 0x7f) << shift;
+    if (!(c & 0x80)) return r;
+    shift += 7;
+  }
+  return r;
+}
+
 // Run headers of an RLE / bit-packed hybrid stream of bit width 1 holding at
-// most max_values levels (decodeRleBitPacked): appended to runs with rows
-// from row0.  Returns the levels the stream yields.
+// most max_values levels (decodeRleBitPacked, src/parquet-decode.ts:119-188):
+// appended to runs with rows from row0.  A header's count is its value
+// shifted as a signed 32-bit number, as the reference's `header >> 1`; a
+// negative bit-packed count, after which the reference would step back and
+// read the same bytes again without end, ends the stream.  Returns the
+// levels the stream yields.
 int64_t pq_def_runs(const uint8_t *b, int64_t start, int64_t end, int64_t max_values, int64_t row0,
                     std::vector<qm_pq_run> &runs, int64_t &present) {
   int64_t pos = start, got = 0;
   present = 0;
   while (pos < end && got < max_values) {
-    ThriftIn r{b, end, pos};
-    const uint64_t header = r.varint();
-    if (r.bad) break;
-    pos = r.pos;
+    const uint32_t header = pq_run_varint(b, end, pos);
+    const int64_t half = (int64_t)((int32_t)header >> 1);
     qm_pq_run run{};
     run.row0 = row0 + got;
     if ((header & 1) == 0) {
-      const int64_t count = (int64_t)(header >> 1);
       run.value = pos < end ? (b[pos] & 1) : 0;
       pos += 1;
-      run.count = std::min(count, max_values - got);
-      present += run.value ? run.count : 0;
+      run.count = std::min(half, max_values - got);
+      present += run.value && run.count > 0 ? run.count : 0;
     } else {
-      const int64_t groups = (int64_t)(header >> 1);
+      if (half < 0) break;
+      const int64_t groups = half;
       run.packed = 1;
       run.byte_off = pos;
       run.count = std::min(groups * 8, max_values - got);
       run.value = (int32_t)std::max<int64_t>(0, std::min<int64_t>(end - pos, groups));
-      for (int64_t k = 0; k < run.count; k++)
-        if ((k >> 3) < run.value && ((b[pos + (k >> 3)] >> (k & 7)) & 1)) present++;
+      // levels past the bytes present read as 0: count over the bytes there are
+      const int64_t nbytes = std::min<int64_t>(run.value, (run.count + 7) / 8);
+      for (int64_t q = 0; q < nbytes; q++) {
+        uint32_t byte = b[pos + q];
+        if (q == (run.count - 1) / 8 && (run.count & 7)) byte &= (1u << (run.count & 7)) - 1;
+        present += __builtin_popcount(byte);
+      }
       pos += groups;
     }
-    if (run.count > 0) runs.push_back(run);
-    got += run.count;
+    if (run.count > 0) {
+      runs.push_back(run);
+      got += run.count;
+    }
   }
   return got;
 }
 
 // Run headers of the dictionary indices (bit width bw <= 32, at most
-// max_values of them; decodeRleBitPacked): row0 of a run is its first index
-// number; an RLE run keeps its value (ceil(bw / 8) little-endian bytes,
-// masked), a bit-packed one its first byte.  Returns the indices yielded.
+// max_values of them; decodeRleBitPacked as above): row0 of a run is its
+// first index number; an RLE run keeps its value (ceil(bw / 8) little-endian
+// bytes, masked), a bit-packed one its first byte.  Returns the indices
+// yielded.
 int64_t pq_index_runs(const uint8_t *b, int64_t start, int64_t end, int bw, int64_t max_values,
                       std::vector<qm_pq_run> &runs) {
   int64_t pos = start, got = 0;
   const uint64_t mask = bw >= 32 ? 0xffffffffull : ((1ull << bw) - 1);
   while (pos < end && got < max_values) {
-    ThriftIn r{b, end, pos};
-    const uint64_t header = r.varint();
-    if (r.bad) break;
-    pos = r.pos;
+    const uint32_t header = pq_run_varint(b, end, pos);
+    const int64_t half = (int64_t)((int32_t)header >> 1);
     qm_pq_run run{};
     run.row0 = got;
     if ((header & 1) == 0) {
       uint64_t v = 0;
       for (int i = 0; i < (bw + 7) / 8 && pos < end; i++) v |= (uint64_t)b[pos++] << (8 * i);
       run.value = (int32_t)(uint32_t)(v & mask);
-      run.count = std::min((int64_t)(header >> 1), max_values - got);
+      run.count = std::min(half, max_values - got);
     } else {
-      const int64_t groups = (int64_t)(header >> 1);
+      if (half < 0) break;
       run.packed = 1;
       run.byte_off = pos;
-      run.count = std::min(groups * 8, max_values - got);
-      pos += (groups * 8 * bw + 7) / 8;
+      run.count = std::min(half * 8, max_values - got);
+      pos += (half * 8 * bw + 7) / 8;
     }
-    if (run.count > 0) runs.push_back(run);
-    got += run.count;
+    if (run.count > 0) {
+      runs.push_back(run);
+      got += run.count;
+    }
   }
   return got;
 }
@@ -266,8 +298,9 @@ int pq_parse_chunk(qm_ctx *ctx, const char *name, int dtype, const uint8_t *b, i
     PqHeader h;
     if (!pq_page_header(b, n, pos, h) || h.compressed <= 0) break;
     pos += h.header_size;
-    const int64_t data = pos, data_end = std::min(n, pos + h.compressed);
-    pos += h.compressed;
+    // a page running past the chunk is cut at its end, and ends the chunk
+    const int64_t data = pos, data_end = h.compressed < n - pos ? pos + h.compressed : n;
+    pos = data_end;
     if (h.type != 0 && h.type != 2 && h.type != 3) continue;  // other page types are skipped
     if (h.compressed != h.uncompressed)
       return set_err(ctx, QM_ERR_UNSUPPORTED, "column %s: compressed pages (pass an uncompressed chunk)", name);
@@ -313,12 +346,17 @@ int pq_parse_chunk(qm_ctx *ctx, const char *name, int dtype, const uint8_t *b, i
         }
       }
     } else {
-      const int64_t def0 = data + h.rep_len;
+      // the level sections as the reference slices them (subarray: a
+      // negative offset counts from the page's end, every offset is cut to it)
+      auto jsx = [&](int64_t x) { return x < 0 ? std::max<int64_t>(len + x, 0) : std::min<int64_t>(x, len); };
+      const int64_t lim = (int64_t)1 << 40;
+      const int64_t rep = std::max(-lim, std::min(lim, h.rep_len)), def = std::max(-lim, std::min(lim, h.def_len));
+      const int64_t d0 = jsx(rep), d1 = std::max(d0, jsx(rep + def));
       if (h.def_len > 0) {
-        pq_def_runs(b, def0, std::min(data_end, def0 + h.def_len), h.num_values, pg.row0, runs, nonnull);
+        pq_def_runs(b, data + d0, data + d1, h.num_values, pg.row0, runs, nonnull);
         has_def = true;
       }
-      plain = def0 + h.def_len;
+      plain = data + jsx(rep + def);
     }
     pg.run1 = (int32_t)runs.size();
     if (!has_def) {
