@@ -249,6 +249,10 @@ int qm_table_from_qmcb(qm_ctx *ctx, const uint8_t *buf, size_t len,
                        qm_table **out);
 int qm_table_destroy(qm_table *table);
 int qm_table_num_rows(const qm_table *table, int64_t *out);
+/* The table's columns: how many, and column i's name (owned by the table)
+ * and dtype.  No counterpart in the reference (inspection and tests). */
+int qm_table_num_columns(const qm_table *table, int32_t *out);
+int qm_table_column(const qm_table *table, int32_t column, const char **name, int32_t *dtype);
 
 /* ---- one-shot query over a registered table ---------------------------- */
 /* filter -> GROUP BY -> finalize over all rows of `table` as one batch.

@@ -181,6 +181,8 @@ SIGNATURES = [
     ("qm_batch_stats", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                  C.POINTER(C.c_int32)]),
     ("qm_batch_destroy", C.c_int, [_P]),
+    ("qm_table_num_columns", C.c_int, [_P, C.POINTER(C.c_int32)]),
+    ("qm_table_column", C.c_int, [_P, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_int32)]),
     ("qm_table_from_parquet", C.c_int, [_P, C.c_int32, C.POINTER(QmParquetColumn), _PP]),
     ("qm_table_from_pages", C.c_int, [_P, C.c_int32, C.POINTER(QmPageColumn), _PP]),
     ("qm_table_read_column", C.c_int, [_P, C.c_int32, C.c_void_p, C.c_void_p]),

@@ -2159,12 +2159,14 @@ int qm_table_from_qmcb(qm_ctx *ctx, const uint8_t *buf, size_t len, qm_table **o
         if (pos + 4 > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB vector column");
         uint32_t dim;
         memcpy(&dim, buf + pos, 4);
+        // rows x dim x 4 can pass 2^64: a column larger than the buffer is truncated
+        if (rows && dim > (len / 4) / rows) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB vector column");
         sz = 4 + (size_t)rows * dim * 4;
         break;
       }
       default: sz = 0;
     }
-    if (pos + sz > len) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB column %s", d.name.c_str());
+    if (pos > len || sz > len - pos) return set_err(ctx, QM_ERR_INVALID, "truncated QMCB column %s", d.name.c_str());
     if (valid_dtype(d.dtype)) {
       names.push_back(d.name);
       qm_column c;
@@ -2192,6 +2194,19 @@ int qm_table_destroy(qm_table *t) {
 int qm_table_num_rows(const qm_table *t, int64_t *out) {
   if (!t || !out) return QM_ERR_INVALID;
   *out = t->n_rows;
+  return QM_OK;
+}
+
+int qm_table_num_columns(const qm_table *t, int32_t *out) {
+  if (!t || !out) return QM_ERR_INVALID;
+  *out = (int32_t)t->cols.size();
+  return QM_OK;
+}
+
+int qm_table_column(const qm_table *t, int32_t column, const char **name, int32_t *dtype) {
+  if (!t || column < 0 || column >= (int32_t)t->cols.size()) return QM_ERR_INVALID;
+  if (name) *name = t->cols[column].name.c_str();
+  if (dtype) *dtype = t->cols[column].dtype;
   return QM_OK;
 }
 

@@ -495,7 +495,17 @@ class Context:
         self.check(self.lib.qm_table_from_qmcb(self.h, b, len(b), C.byref(h)))
         n = C.c_int64()
         self.lib.qm_table_num_rows(h, C.byref(n))
-        return Table(self, h, n.value, [])
+        k = C.c_int32()
+        self.check(self.lib.qm_table_num_columns(h, C.byref(k)))
+        names, dtypes = [], []
+        for i in range(k.value):
+            nm, dt = C.c_char_p(), C.c_int32()
+            self.check(self.lib.qm_table_column(h, i, C.byref(nm), C.byref(dt)))
+            names.append(nm.value.decode("utf-8", "replace"))
+            dtypes.append(dt.value)
+        t = Table(self, h, n.value, names)
+        t._dtypes = dtypes
+        return t
 
     # -- filter-only ---------------------------------------------------------
     def filter_select(self, columns: Mapping[str, Any], query: QueryDescriptor,

@@ -550,3 +550,44 @@ def test_large_pageable_columns_staged(ctx):
                         aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*"), AggregateOp("max", "f")])
     assert_same(t.run(q), oracle.run(cols, q, threads=8))
     t.close()
+
+
+def test_corrupt_qmcb_refused_or_decoded(ctx):
+    # byte flips and truncations of a QMCB buffer: each call builds a table or
+    # returns QM_ERR_INVALID / UNSUPPORTED, never reads past the buffer; a table
+    # it builds holds the cells the host decoder reads from the same bytes
+    from querymode_b200 import _abi as A
+    from querymode_b200 import qmcb
+    rng = np.random.default_rng(41)
+    n = 500
+    cols = {"k": Column(rng.integers(0, 9, n).astype(np.int32), rng.random(n) < 0.1),
+            "v": rng.normal(size=n), "w": rng.integers(0, 10, n).astype(np.int64)}
+    buf = qmcb.encode(cols)
+    built = compared = 0
+    for trial in range(200):
+        b = bytearray(buf)
+        for _ in range(int(rng.integers(1, 4))):
+            b[int(rng.integers(0, 40 if trial % 2 else len(b)))] = int(rng.integers(0, 256))
+        if trial % 5 == 0:
+            b = b[:int(rng.integers(1, len(b)))]
+        try:
+            t = ctx.table_from_qmcb(bytes(b))
+        except A.QmError as e:
+            assert e.status in (A.QM_ERR_INVALID, A.QM_ERR_UNSUPPORTED)
+            continue
+        except (ValueError, UnicodeDecodeError):
+            continue
+        built += 1
+        try:
+            dec = qmcb.decode(bytes(b))
+        except Exception:
+            t.close()
+            continue
+        for i, name in enumerate(t.names):
+            if name in dec.names:
+                vals, nulls = t.read_column(name)
+                want = dec.column(name)
+                assert np.array_equal(vals.view(np.uint8), np.asarray(want.values).view(np.uint8)), name
+                compared += 1
+        t.close()
+    assert built > 0 and compared > 0
