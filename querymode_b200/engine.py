@@ -233,12 +233,25 @@ class Stats:
 class Result:
     """Typed result columns (keys first, then aggregates in query order)."""
 
-    def __init__(self, columns: list[ResultColumn], n_rows: int, stats: Stats | None = None,
-                 qmcb: bytes | None = None):
-        self.columns = columns
+    def __init__(self, columns: list[ResultColumn] | None, n_rows: int, stats: Stats | None = None,
+                 qmcb: bytes | None = None, build=None):
+        self._columns = columns
+        self._build = build  # makes the columns on first use (views of a result handle)
         self.n_rows = n_rows
         self.stats = stats
         self.qmcb = qmcb
+
+    @property
+    def columns(self) -> list[ResultColumn]:
+        if self._columns is None:
+            self._columns = self._build()
+            self._build = None
+        return self._columns
+
+    @columns.setter
+    def columns(self, cols: list[ResultColumn]) -> None:
+        self._columns = cols
+        self._build = None
 
     def take(self, order) -> "Result":
         """The rows at `order` (a list of row indices), as a new Result."""
@@ -267,11 +280,18 @@ class Result:
         lib.qm_result_num_rows(handle, C.byref(n))
         lib.qm_result_num_columns(handle, C.byref(nc))
         owner = _ResultOwner(lib, handle) if owned else None
-        cols = []
-        for i in range(nc.value):
-            rc = A.QmResultCol()
-            lib.qm_result_column(handle, i, C.byref(rc))
-            cols.append(_view_col(rc, n.value, owner) if owned else _read_col(rc, n.value))
+
+        def build():
+            cols = []
+            for i in range(nc.value):
+                rc = A.QmResultCol()
+                lib.qm_result_column(handle, i, C.byref(rc))
+                cols.append(_view_col(rc, n.value, owner) if owned else _read_col(rc, n.value))
+            return cols
+
+        # owned results keep their handle (through `owner`) until the columns
+        # are made and dropped; copies are made now, before the handle goes
+        cols = None if owned else build()
         st = A.QmStats()
         lib.qm_result_stats(handle, C.byref(st))
         stats = Stats(st.rows_scanned, st.rows_selected, st.groups, st.bytes_scanned, st.device_ms,
@@ -282,6 +302,9 @@ class Result:
             ln = C.c_size_t()
             if lib.qm_result_qmcb(handle, C.byref(p), C.byref(ln)) == A.QM_OK:
                 qmcb = C.string_at(p, ln.value)
+        if owned:
+            keep = owner  # the handle lives as long as the result may still build views of it
+            return cls(None, n.value, stats, qmcb, build=lambda: (keep, build())[1])
         return cls(cols, n.value, stats, qmcb)
 
 
