@@ -7,6 +7,7 @@
 //   qm_select_masks /   filter-only selection vector (ascending row indices)
 //   qm_select_write
 //   qm_minmax_kernel    integer column min / max (planning statistics)
+#include <thrust/iterator/transform_iterator.h>
 #include <cub/cub.cuh>
 
 #include <climits>
@@ -1035,6 +1036,19 @@ cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O,
   return cudaGetLastError();
 }
 
+struct PopcWord {
+  __host__ __device__ uint64_t operator()(uint32_t w) const {
+#ifdef __CUDA_ARCH__
+    return (uint64_t)__popc(w);
+#else
+    return (uint64_t)__builtin_popcount(w);
+#endif
+  }
+};
+inline thrust::transform_iterator<PopcWord, const uint32_t *> popc_words_it(const uint32_t *bitmap) {
+  return thrust::make_transform_iterator(bitmap, PopcWord());
+}
+
 cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
                                  uint32_t *bitmap, int64_t words, uint32_t *counts, uint64_t *ranks, void *temp,
                                  size_t temp_bytes, int sm_count, cudaStream_t st) {
@@ -1042,13 +1056,13 @@ cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int s
   if (e != cudaSuccess) return e;
   int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
   qm_mark_first<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap);
-  blocks = (int)std::min<int64_t>((words + 256) / 256, (int64_t)sm_count * 8);
-  qm_popc_words<<<std::max(blocks, 1), 256, 0, st>>>(bitmap, words, counts);
-  return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, ranks, (int)(words + 1), st);
+  // the words' popcounts go straight into the scan (no counts pass)
+  (void)counts;
+  return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, popc_words_it(bitmap), ranks, (int)(words + 1), st);
 }
 
 cudaError_t qm_rank_temp_bytes(int64_t words, size_t *bytes) {
-  return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
+  return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, popc_words_it(nullptr), (uint64_t *)nullptr,
                                        (int)(words + 1));
 }
 
