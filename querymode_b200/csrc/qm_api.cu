@@ -1404,7 +1404,19 @@ int post_aggregate(qm_ctx *ctx, const Plan &pl, const qm_outspec &O, int64_t G, 
 }
 
 // groups_known >= 0: launch_rank already ran and its count was read.
-int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1) {
+// Results of at most this many bytes laid out for every slot of the table
+// are emitted and copied before the status is read (one synchronise per
+// query instead of two; finish_table's `spec`).
+constexpr size_t SPEC_RESULT_BYTES = (size_t)8 << 20;
+
+// spec (speculative, ranked queries without post-aggregate clauses): the
+// result is laid out for every slot of the table, emitted and copied before
+// the status has been read; the status (enqueued by the caller into
+// ctx->hstatus) and the group count come with the same synchronise.  On a
+// device error *out stays null and *spec holds the status: the caller
+// regrows and runs again.
+int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1,
+                 qm_status *spec = nullptr) {
   const Plan &pl = gt.pl;
   const Exec &ex = gt.ex;
   int64_t G = 0;
@@ -1414,7 +1426,9 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   if (pl.key.mode == QK_NONE) {
     G = 1;  // ungrouped: exactly one row (src/partial-agg.ts:313-320)
   } else if (ranked) {
-    if (groups_known >= 0) {
+    if (spec) {
+      G = ex.total_slots;  // the layout's rows; the group count comes with the status
+    } else if (groups_known >= 0) {
       G = groups_known;
     } else {
       int rc = launch_rank(ctx, gt);
@@ -1508,6 +1522,17 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   }
   float tail_ms = 0;
   cudaEventElapsedTime(&tail_ms, ctx->ev0, ctx->ev1);
+  if (spec) {
+    memcpy(spec, ctx->hstatus.p, sizeof(qm_status));
+    take_scan_time(ctx, gt, spec->error == QM_DEV_OK);
+    if (spec->error != QM_DEV_OK) {
+      delete R;
+      *out = nullptr;
+      return QM_OK;
+    }
+    gt.selected = spec->rows_selected;
+    G = (int64_t)*(uint64_t *)((char *)ctx->hstatus.p + 32);
+  }
 
   R->n_rows = G;
   const uint8_t *h = (const uint8_t *)R->buf.p;
@@ -2252,12 +2277,24 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
     const bool ranked = ranked_finish(gt);
     if (ranked && (rc = launch_rank(ctx, gt))) return rc;
     qm_status st;
-    if ((rc = read_status(ctx, &st))) return rc;
-    take_scan_time(ctx, gt, st.error == QM_DEV_OK);
-    if (st.error == QM_DEV_OK) {
-      gt.selected = st.rows_selected;
-      if (ranked) groups = (int64_t)*(uint64_t *)((char *)ctx->hstatus.p + 32);
-      break;
+    qm_outspec Ocap = pl.outs;
+    if (ranked && !pl.post && result_layout(pl, Ocap, gt.ex.total_slots) <= SPEC_RESULT_BYTES) {
+      // small result: emitted and copied with the status, one synchronise
+      CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->status.p, sizeof(qm_status), cudaMemcpyDeviceToHost, ctx->stream));
+      if ((rc = finish_table(ctx, gt, out, 0.f, -1, &st))) return rc;
+      if (*out) {
+        (*out)->stats.rows_scanned = t->n_rows;
+        (*out)->stats.bytes_scanned = pl.bytes_per_row * t->n_rows;
+        return QM_OK;
+      }
+    } else {
+      if ((rc = read_status(ctx, &st))) return rc;
+      take_scan_time(ctx, gt, st.error == QM_DEV_OK);
+      if (st.error == QM_DEV_OK) {
+        gt.selected = st.rows_selected;
+        if (ranked) groups = (int64_t)*(uint64_t *)((char *)ctx->hstatus.p + 32);
+        break;
+      }
     }
     if (attempt >= 4) return set_err(ctx, QM_ERR_CUDA, "group table overflow after %d regrowths", attempt);
     gt.retries++;
