@@ -1490,7 +1490,8 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   if (ranked) {
     if (G > 0)
       CK(qm_launch_emit_ranked(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
-                               (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, pl.key, ex.n_slots, O,
+                               (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, rank_words(gt),
+                               pl.key, ex.n_slots, O,
                                (unsigned char *)ctx->out.p, ctx->sm_count, ctx->stream));
   } else {
     CK(qm_launch_emit(gt.table, ex.stride, slots, G, pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p,
@@ -2250,6 +2251,7 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
   gt.rows_done = 0;
   int64_t groups = -1;
   for (int attempt = 0;; attempt++) {
+    gt.rows_done = 0;  // every attempt scans the table from its first row
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(qm_status), ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if ((rc = setup_table(ctx, gt, est, direct_size, false))) return rc;

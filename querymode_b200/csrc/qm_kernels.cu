@@ -166,13 +166,17 @@ __global__ void qm_emit_groups(const uint64_t *t, int stride, const uint32_t *sl
 // First-seen ranking without a sort: bit `first row` of every occupied slot
 // in a row bitmap (each row belongs to one group, so bits are distinct);
 // the prefix popcount of the bitmap then gives each group's output row.
+// (a FIRST row outside the bitmap's `words` words is left unmarked: it can
+// only come from a table the status reports as failed, whose result is
+// discarded)
 __global__ void qm_mark_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
-                              uint32_t *bitmap) {
+                              uint32_t *bitmap, int64_t words) {
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots_total;
        s += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t *w = t + s * stride + 1;
     if (w[count_word] == 0) continue;
     const uint64_t f = w[first_word];
+    if ((f >> 5) >= (uint64_t)words) continue;
     atomicOr(bitmap + (f >> 5), 1u << (f & 31));
   }
 }
@@ -183,13 +187,15 @@ __global__ void qm_popc_words(const uint32_t *bitmap, int64_t words, uint32_t *c
 }
 
 __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
-                               const uint32_t *bitmap, const uint64_t *ranks, const __grid_constant__ qm_keyspec K,
-                               int64_t n_slots, const __grid_constant__ qm_outspec O, unsigned char *out) {
+                               const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
+                               const __grid_constant__ qm_keyspec K, int64_t n_slots,
+                               const __grid_constant__ qm_outspec O, unsigned char *out) {
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots_total;
        s += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t *w = t + s * stride + 1;
     if (w[count_word] == 0) continue;
     const uint64_t f = w[first_word];
+    if ((f >> 5) >= (uint64_t)words) continue;  // not marked (see qm_mark_first)
     const int64_t i = (int64_t)ranks[f >> 5] + __popc(bitmap[f >> 5] & ((1u << (f & 31)) - 1u));
     emit_group<false>(t, stride, (uint64_t)s, i, K, n_slots, O, out, nullptr, nullptr);
   }
@@ -1055,7 +1061,7 @@ cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int s
   cudaError_t e = cudaMemsetAsync(bitmap, 0, sizeof(uint32_t) * (size_t)(words + 1), st);
   if (e != cudaSuccess) return e;
   int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
-  qm_mark_first<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap);
+  qm_mark_first<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap, words);
   // the words' popcounts go straight into the scan (no counts pass)
   (void)counts;
   return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, popc_words_it(bitmap), ranks, (int)(words + 1), st);
@@ -1067,12 +1073,12 @@ cudaError_t qm_rank_temp_bytes(int64_t words, size_t *bytes) {
 }
 
 cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
-                                  int first_word, const uint32_t *bitmap, const uint64_t *ranks, const qm_keyspec &K,
-                                  int64_t n_slots, const qm_outspec &O, unsigned char *out, int sm_count,
-                                  cudaStream_t st) {
+                                  int first_word, const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
+                                  const qm_keyspec &K, int64_t n_slots, const qm_outspec &O, unsigned char *out,
+                                  int sm_count, cudaStream_t st) {
   const int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
   qm_emit_ranked<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap, ranks,
-                                                      K, n_slots, O, out);
+                                                      words, K, n_slots, O, out);
   return cudaGetLastError();
 }
 

@@ -59,9 +59,9 @@ cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int s
                                  size_t temp_bytes, int sm_count, cudaStream_t st);
 cudaError_t qm_rank_temp_bytes(int64_t words, size_t *bytes);
 cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
-                                  int first_word, const uint32_t *bitmap, const uint64_t *ranks, const qm_keyspec &K,
-                                  int64_t n_slots, const qm_outspec &O, unsigned char *out, int sm_count,
-                                  cudaStream_t st);
+                                  int first_word, const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
+                                  const qm_keyspec &K, int64_t n_slots, const qm_outspec &O, unsigned char *out,
+                                  int sm_count, cudaStream_t st);
 // Post-aggregate ORDER BY / LIMIT over emitted result rows (see qm_kernels.cu).
 cudaError_t qm_launch_sort_keys(const unsigned char *data, const uint32_t *nulls, int dtype, int desc, int64_t G,
                                 uint32_t *last, uint64_t *hi, uint64_t *lo, uint32_t *idx, int sm_count, cudaStream_t st);

@@ -591,3 +591,26 @@ def test_corrupt_qmcb_refused_or_decoded(ctx):
                 compared += 1
         t.close()
     assert built > 0 and compared > 0
+
+
+def test_retries_after_stale_statistics(ctx):
+    # borrowed device columns rewritten in place after their statistics were
+    # cached: the next query plans a direct range the keys leave (retry as a
+    # hash table), then a hash table too small for them (retry larger); the
+    # small result takes the one-synchronise path, whose failed attempts must
+    # be discarded, and the answer must equal the oracle's on the new data
+    import torch
+    rng = np.random.default_rng(121)
+    n = 400_000
+    k0 = rng.integers(0, 100, n).astype(np.int64)
+    v = rng.normal(size=n)
+    dk = torch.from_numpy(k0).cuda()
+    t = ctx.table({"k": dk, "v": torch.from_numpy(v).cuda()})
+    q = QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")])
+    assert_same(t.run(q), oracle.run({"k": k0, "v": v}, q))
+    k1 = rng.integers(-1000, 2000, n).astype(np.int64)
+    dk.copy_(torch.from_numpy(k1))
+    g = t.run(q)
+    assert g.stats.retries >= 1, g.stats
+    assert_same(g, oracle.run({"k": k1, "v": v}, q))
+    t.close()
