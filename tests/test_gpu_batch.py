@@ -90,3 +90,34 @@ def test_batch_dense_keys_beyond_shared_memory(ctx):
                 assert_same(g, r, ctx_msg=f"run {run} query {i}")
     finally:
         b.close()
+
+
+def test_batch_overflow_reruns_alone(ctx):
+    # a batch planned on borrowed device columns whose keys are then rewritten
+    # to far more distinct values than the cached estimate: the query's
+    # batched table overflows, and it is run again alone (where its table
+    # regrows) to the oracle's answer
+    import torch
+    rng = np.random.default_rng(17)
+    n = 300_000
+    k0 = rng.integers(-(1 << 62), 1 << 62, 50).astype(np.int64)[rng.integers(0, 50, n)]
+    v = rng.normal(size=n)
+    dk = torch.from_numpy(k0).cuda()
+    t = ctx.table({"key": dk, "v": torch.from_numpy(v).cuda()})
+    q = QueryDescriptor(group_by=["key"], aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")])
+    other = {"key": rng.integers(0, 7, 1000).astype(np.int32), "v": rng.normal(size=1000)}
+    t2 = ctx.table(other)
+    b = ctx.batch([t, t2], [q, q])
+    try:
+        for g, r in zip(b.run(), [oracle.run({"key": k0, "v": v}, q), oracle.run(other, q)]):
+            assert_same(g, r)
+        k1 = rng.integers(-(1 << 62), 1 << 62, 5000).astype(np.int64)[rng.integers(0, 5000, n)]
+        dk.copy_(torch.from_numpy(k1))
+        res = b.run()
+        assert res[0].stats.retries >= 1, res[0].stats  # run alone, regrown
+        assert_same(res[0], oracle.run({"key": k1, "v": v}, q))
+        assert_same(res[1], oracle.run(other, q))
+    finally:
+        b.close()
+        t.close()
+        t2.close()
