@@ -5,6 +5,7 @@ import base64
 import json
 import math
 import os
+import struct
 
 import pytest
 
@@ -87,3 +88,32 @@ def test_dictionary_files_match_pyarrow(version, dict_limit):
         assert len(vals) == len(want)
         same = all(_same(a, b) for a, b in zip(vals, want))
         assert same != (growing and name in ("i64", "f64")), name
+
+
+def test_corrupt_chunks_terminate():
+    # byte flips and truncations: the restatement ends (decoding, or raising
+    # where it would read past the bytes) and never spins on a corrupt count
+    import time
+
+    import numpy as np
+
+    from tests.parquet_util import dict_columns, write_dict
+    rng = np.random.default_rng(32)
+    raws = [write_plain(sample_columns(2000, 2), "1.0", page_size=512),
+            write_dict(dict_columns(2000, 4), "1.0", page_size=512),
+            write_dict(dict_columns(2000, 5), "2.0", page_size=512)]
+    t0 = time.time()
+    for raw in raws:
+        for nm, ph, ch, nv in chunks_of(raw):
+            for trial in range(40):
+                b = bytearray(ch)
+                for _ in range(int(rng.integers(1, 8))):
+                    b[int(rng.integers(0, len(b)))] = int(rng.integers(0, 256))
+                if trial % 4 == 0:
+                    b = b[:int(rng.integers(1, len(b)))]
+                try:
+                    vals = decode_column_chunk(bytes(b), PHYS[ph], nv)
+                    assert len(vals) <= nv
+                except (IndexError, ValueError, NotImplementedError, struct.error):
+                    pass
+    assert time.time() - t0 < 60
