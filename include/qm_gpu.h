@@ -434,11 +434,26 @@ typedef struct {
   int32_t reserved;
 } qm_page;
 
+/* Value types of PLAIN pages narrower than the table's dtypes, widened on
+ * the device as the reference's numbers hold them (decodePlainValues,
+ * src/parquet-decode.ts:280-386): int8 / uint8 / int16 / uint16 into QM_I32
+ * columns, uint32 into QM_F64 (a JS number, exact), float16 into QM_F32
+ * (exact).  QM_PT_SAME: the pages hold the column's dtype. */
+#define QM_PT_SAME 0
+#define QM_PT_INT8 1
+#define QM_PT_UINT8 2
+#define QM_PT_INT16 3
+#define QM_PT_UINT16 4
+#define QM_PT_UINT32 5
+#define QM_PT_FLOAT16 6
+
 typedef struct {
   const char *name;
   int32_t dtype;        /* QM_I32 / QM_I64 / QM_F32 / QM_F64 */
   int32_t n_pages;
   const qm_page *pages;
+  int32_t page_type;    /* QM_PT_*: the value type of its (non-Parquet) pages */
+  int32_t reserved;
 } qm_page_column;
 
 int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols, qm_table **out);

@@ -194,7 +194,10 @@ def decode_rle_bit_packed(b: bytes, bit_width: int, max_values: int) -> list[int
     return values
 
 
-_FMT = {"int32": ("<i", 4), "int64": ("<q", 8), "float32": ("<f", 4), "float64": ("<d", 8)}
+_FMT = {"int32": ("<i", 4), "int64": ("<q", 8), "float32": ("<f", 4), "float64": ("<d", 8),
+        # narrower page types of decodePlainValues (src/parquet-decode.ts:288-348); float16 as its exact value
+        "int8": ("<b", 1), "uint8": ("<B", 1), "int16": ("<h", 2), "uint16": ("<H", 2), "uint32": ("<I", 4),
+        "float16": ("<e", 2)}
 
 
 def decode_plain(b: bytes, dtype: str, n: int) -> list:

@@ -29,6 +29,7 @@ STATUS_NAMES = {
 
 # dtypes (QMCB tags, src/columnar.ts:22-33) + the result-only 128-bit integer
 QM_F64 = 0
+QM_PT_SAME, QM_PT_INT8, QM_PT_UINT8, QM_PT_INT16, QM_PT_UINT16, QM_PT_UINT32, QM_PT_FLOAT16 = 0, 1, 2, 3, 4, 5, 6
 QM_I64 = 1
 QM_I32 = 6
 QM_F32 = 7
@@ -136,7 +137,8 @@ class QmPage(C.Structure):
 
 
 class QmPageColumn(C.Structure):
-    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("n_pages", C.c_int32), ("pages", C.POINTER(QmPage))]
+    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int32), ("n_pages", C.c_int32), ("pages", C.POINTER(QmPage)),
+                ("page_type", C.c_int32), ("reserved", C.c_int32)]
 
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))

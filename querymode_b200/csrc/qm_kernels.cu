@@ -7,6 +7,7 @@
 //   qm_select_masks /   filter-only selection vector (ascending row indices)
 //   qm_select_write
 //   qm_minmax_kernel    integer column min / max (planning statistics)
+#include <cuda_fp16.h>
 #include <thrust/iterator/transform_iterator.h>
 #include <cub/cub.cuh>
 
@@ -341,14 +342,30 @@ __device__ __forceinline__ const uint8_t *pq_dict_entry(const uint8_t *chunk, co
 // a slotted page (or any page of a column without levels: present == null)
 // j = r - row0.  j past the values present gives NULL (as the reference's
 // decoded[dPtr++] / values[vi++] running out does).
-// DICT: the column has dictionary pages (a separate instantiation, so the
-// PLAIN-only one keeps its registers).
+// A page value of in_width bytes widened to the column's cell (conv: the
+// QM_PT_* page type; int8 / uint8 / int16 / uint16 to int32, uint32 to a
+// double, float16 to a float, each exact).
+__device__ __forceinline__ uint64_t pq_widen(uint64_t v, int conv) {
+  switch (conv) {
+    case 1: return (uint64_t)(uint32_t)(int32_t)(int8_t)(v & 0xff);
+    case 2: return v & 0xff;
+    case 3: return (uint64_t)(uint32_t)(int32_t)(int16_t)(v & 0xffff);
+    case 4: return v & 0xffff;
+    case 5: return (uint64_t)__double_as_longlong((double)(uint32_t)v);
+    case 6: return (uint64_t)__float_as_uint(__half2float(__ushort_as_half((unsigned short)(v & 0xffff))));
+    default: return v;
+  }
+}
+
+// DICT: the column has dictionary pages; WIDE: page values narrower than the
+// column's (in_width bytes, widened by conv).  Separate instantiations, so
+// the PLAIN one keeps its registers (five blocks per SM).
 #define QM_PQ_UNROLL 4
-template <bool DICT>
-__global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages,
-                                                     const qm_pq_run *iruns, int width, int64_t n_rows,
-                                                     const uint32_t *present, const uint64_t *ranks,
-                                                     unsigned char *out, uint32_t *nulls) {
+template <bool DICT, bool WIDE>
+__global__ void __launch_bounds__(256, (DICT || WIDE) ? 4 : 5)
+    qm_pq_scatter(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *iruns, int width,
+                  int in_width, int conv, int64_t n_rows, const uint32_t *present, const uint64_t *ranks,
+                  unsigned char *out, uint32_t *nulls) {
   const int lane = threadIdx.x & 31;
   const int64_t words = (n_rows + 31) / 32;
   int64_t w0, w1;
@@ -386,7 +403,7 @@ __global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const
             live[u] = src[u] != nullptr;
           } else if (j < c.avail) {
             live[u] = true;
-            src[u] = chunk + c.val_off + j * width;
+            src[u] = chunk + c.val_off + j * (WIDE ? in_width : width);
           }
         }
       }
@@ -397,7 +414,14 @@ __global__ void __launch_bounds__(256) qm_pq_scatter(const uint8_t *chunk, const
       v[u] = 0;
       if (live[u]) {
         const uint8_t *s = src[u];
-        if (((uintptr_t)s & (width - 1)) == 0) {
+        if (WIDE) {
+          if (((uintptr_t)s & (in_width - 1)) == 0) {
+            v[u] = in_width == 4 ? *(const uint32_t *)s : in_width == 2 ? *(const uint16_t *)s : *s;
+          } else {
+            for (int i = in_width - 1; i >= 0; --i) v[u] = (v[u] << 8) | s[i];
+          }
+          v[u] = pq_widen(v[u], conv);
+        } else if (((uintptr_t)s & (width - 1)) == 0) {
           v[u] = width == 8 ? *(const uint64_t *)s : *(const uint32_t *)s;
         } else {
           for (int i = width - 1; i >= 0; --i) v[u] = (v[u] << 8) | s[i];
@@ -944,7 +968,7 @@ cudaError_t qm_launch_select_masks(const qm_pred &P, int64_t n, const uint32_t *
 }
 
 cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
-                                int n_runs, const qm_pq_run *iruns, int width, int64_t n_rows, uint32_t *present, uint32_t *counts,
+                                int n_runs, const qm_pq_run *iruns, int width, int in_width, int conv, int64_t n_rows, uint32_t *present, uint32_t *counts,
                                 uint64_t *ranks, void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls,
                                 int sm_count, cudaStream_t st) {
   const int64_t words = (n_rows + 31) / 32;
@@ -953,28 +977,36 @@ cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, i
   if (n_rows <= 0) return cudaSuccess;
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
   // one resident wave: every warp owns a fixed range of words
-  static int occ_present = 0, occ_scatter[2] = {0, 0};
+  // variants: PLAIN, dictionary pages (Parquet), widened page values (Lance
+  // pages only, so never with dictionary pages)
+  static int occ_present = 0, occ_scatter[3] = {0, 0, 0};
   if (!occ_present) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_present, qm_pq_present, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[0], qm_pq_scatter<false>, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[1], qm_pq_scatter<true>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[0], qm_pq_scatter<false, false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[1], qm_pq_scatter<true, false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_scatter[2], qm_pq_scatter<false, true>, 256, 0);
     occ_present = std::max(occ_present, 1);
-    occ_scatter[0] = std::max(occ_scatter[0], 1);
-    occ_scatter[1] = std::max(occ_scatter[1], 1);
+    for (int &o : occ_scatter) o = std::max(o, 1);
   }
   const bool dict = iruns != nullptr;
-  const auto scatter = dict ? qm_pq_scatter<true> : qm_pq_scatter<false>;
+  const bool wide = conv != 0;
+  if (dict && wide) return cudaErrorInvalidValue;
+  const int var = dict ? 1 : (wide ? 2 : 0);
+  const auto scatter =
+      dict ? qm_pq_scatter<true, false> : (wide ? qm_pq_scatter<false, true> : qm_pq_scatter<false, false>);
   const int pblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_present);
-  const int wblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_scatter[dict]);
+  const int wblocks = (int)std::min<int64_t>((words + 7) / 8, (int64_t)sm_count * occ_scatter[var]);
   if (n_runs == 0) {  // no levels: every row present, values by row
-    scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, nullptr, nullptr, out, nulls);
+    scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, in_width, conv, n_rows, nullptr, nullptr, out,
+                                     nulls);
     return cudaGetLastError();
   }
   qm_pq_present<<<pblocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
   qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
   cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
   if (e != cudaSuccess) return e;
-  scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, n_rows, present, ranks, out, nulls);
+  scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, in_width, conv, n_rows, present, ranks, out,
+                                   nulls);
   return cudaGetLastError();
 }
 

@@ -80,7 +80,7 @@ cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O,
 // and none is a dictionary page).  iruns: the dictionary pages' index runs,
 // null when no page is a dictionary page.
 cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, int n_pages, const qm_pq_run *runs,
-                                int n_runs, const qm_pq_run *iruns, int width, int64_t n_rows, uint32_t *present, uint32_t *counts,
+                                int n_runs, const qm_pq_run *iruns, int width, int in_width, int conv, int64_t n_rows, uint32_t *present, uint32_t *counts,
                                 uint64_t *ranks, void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls,
                                 int sm_count, cudaStream_t st);
 cudaError_t qm_launch_zone_stats(const void *p, int dtype, const uint32_t *nulls, int64_t n, int64_t *zmin,

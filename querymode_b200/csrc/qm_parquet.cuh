@@ -661,17 +661,35 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     for (auto &e : t->cols)
       if (e.name == c.name) return fail(set_err(ctx, QM_ERR_INVALID, "duplicate column %s", c.name));
     const int w = pq_width(c.dtype);
+    // the pages' value width and its widening into the column's cells
+    int w_in = w, conv = 0;
+    switch (c.page_type) {
+      case QM_PT_SAME: break;
+      case QM_PT_INT8: case QM_PT_UINT8: w_in = 1; conv = c.page_type; break;
+      case QM_PT_INT16: case QM_PT_UINT16: case QM_PT_FLOAT16: w_in = 2; conv = c.page_type; break;
+      case QM_PT_UINT32: w_in = 4; conv = c.page_type; break;
+      default: return fail(set_err(ctx, QM_ERR_INVALID, "column %s: page type %d", c.name, c.page_type));
+    }
+    const int want = c.page_type == QM_PT_SAME     ? c.dtype
+                     : c.page_type == QM_PT_UINT32  ? QM_F64
+                     : c.page_type == QM_PT_FLOAT16 ? QM_F32
+                                                    : QM_I32;
+    if (want != c.dtype)
+      return fail(set_err(ctx, QM_ERR_INVALID, "column %s: page type %d widens into dtype %d, not %d", c.name,
+                          c.page_type, want, c.dtype));
     PqColumn pc;
     for (int k = 0; k < c.n_pages; k++) {
       const qm_page &pa = c.pages[k];
       if ((!pa.buf && pa.bytes > 0) || pa.bytes < 0 || pa.row_count < 0 || pa.null_count < 0 || pa.data_offset < -1)
         return fail(set_err(ctx, QM_ERR_INVALID, "column %s page %d: bad descriptor", c.name, k));
+      if (pa.parquet && conv)
+        return fail(set_err(ctx, QM_ERR_INVALID, "column %s: Parquet chunks hold the column's own dtype", c.name));
       const int64_t base = pc.add_seg(pa.buf, pa.bytes);
       if (pa.parquet) {
         int rc = pq_parse_chunk(ctx, c.name, c.dtype, pa.buf, pa.bytes, pa.row_count, base, pc);
         if (rc) return fail(rc);
       } else {
-        lance_page(pa, w, base, pc);
+        lance_page(pa, w_in, base, pc);
       }
       if (pc.rows > 0xffffffffLL || pc.runs.size() > (size_t)INT32_MAX)
         return fail(set_err(ctx, QM_ERR_UNSUPPORTED, "tables are limited to 2^32-1 rows"));
@@ -685,7 +703,7 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     }
     const int64_t words = (rows + 31) / 32;
     size_t tb = 0;
-    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, 0, nullptr, w, rows, nullptr, nullptr, nullptr, nullptr, &tb,
+    CKF(qm_launch_pq_decode(nullptr, nullptr, 0, nullptr, 0, nullptr, w, w_in, conv, rows, nullptr, nullptr, nullptr, nullptr, &tb,
                             nullptr, nullptr, ctx->sm_count, ctx->stream));
     int rc;
     if ((rc = chunk.ensure((size_t)pc.bytes + 16)) ||
@@ -727,7 +745,8 @@ int qm_table_from_pages(qm_ctx *ctx, int32_t n_cols, const qm_page_column *cols,
     size_t tbytes = temp.bytes;
     CKF(qm_launch_pq_decode((const uint8_t *)chunk.p, (const qm_pq_page *)pgs.p, (int)pc.pages.size(),
                            (const qm_pq_run *)rns.p, (int)pc.runs.size(),
-                           has_dict ? (const qm_pq_run *)rns.p + pc.runs.size() : nullptr, w, rows, (uint32_t *)present.p, (uint32_t *)counts.p,
+                           has_dict ? (const qm_pq_run *)rns.p + pc.runs.size() : nullptr, w, w_in, conv, rows,
+                           (uint32_t *)present.p, (uint32_t *)counts.p,
                            (uint64_t *)ranks.p, temp.p, &tbytes, (unsigned char *)col.data, col.nulls,
                            ctx->sm_count, ctx->stream));
     ctx->launches += pc.runs.empty() ? 1 : 5;

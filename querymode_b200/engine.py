@@ -465,14 +465,19 @@ class Context:
         t._dtypes = [c[1] for c in chunks]
         return t
 
-    def table_from_pages(self, columns: list[tuple[str, int, Any]]) -> "Table":
+    def table_from_pages(self, columns: list[tuple]) -> "Table":
         """A table from scan pages: per column (name, QM dtype, its pages in
-        order as a list of Page or a PageTable), decoded on the device and
-        concatenated page after page."""
+        order as a list of Page or a PageTable[, QM_PT_* page value type]),
+        decoded on the device and concatenated page after page.  Pages of a
+        narrower type (int8 / uint8 / int16 / uint16 into QM_I32, uint32 into
+        QM_F64, float16 into QM_F32) are widened as the reference's numbers
+        hold them."""
         n = len(columns)
         arr = (A.QmPageColumn * n)()
         keep = []
-        for i, (name, dtype, pages) in enumerate(columns):
+        for i, col in enumerate(columns):
+            name, dtype, pages = col[:3]
+            arr[i].page_type = col[3] if len(col) > 3 else A.QM_PT_SAME
             nb = name.encode()
             rec, k = _page_records(pages)
             keep += [nb, rec, k]

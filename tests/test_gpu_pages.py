@@ -198,3 +198,49 @@ def test_empty_inputs(ctx):
         assert len(vals) == 0 and len(nulls) == 0
         assert_same(t.run(q), oracle.run({"c": np.zeros(0, dtype=np.int64)}, q))
         t.close()
+
+
+NARROW = {"int8": (A.QM_PT_INT8, A.QM_I32, np.int8, np.int32), "uint8": (A.QM_PT_UINT8, A.QM_I32, np.uint8, np.int32),
+          "int16": (A.QM_PT_INT16, A.QM_I32, np.int16, np.int32), "uint16": (A.QM_PT_UINT16, A.QM_I32, np.uint16, np.int32),
+          "uint32": (A.QM_PT_UINT32, A.QM_F64, np.uint32, np.float64),
+          "float16": (A.QM_PT_FLOAT16, A.QM_F32, np.float16, np.float32)}
+
+
+@pytest.mark.parametrize("src", list(NARROW))
+def test_narrow_page_types(ctx, src):
+    """Pages of int8 / uint8 / int16 / uint16 / uint32 / float16 values are
+    widened on the device to the cells the reference's numbers hold (int32,
+    double, float), bit for bit against the oracle's decode."""
+    pt, qd, np_src, np_out = NARROW[src]
+    rng = np.random.default_rng(len(src) * 7 + pt)
+    pages = []
+    for k in range(30):
+        n = int(rng.integers(0, 2000))
+        if np_src == np.float16:
+            vals = rng.normal(size=n).astype(np.float16) * np.float16(100)
+            vals[rng.random(n) < 0.02] = np.nan
+        else:
+            info = np.iinfo(np_src)
+            vals = rng.integers(info.min, int(info.max) + 1, n).astype(np_src)
+        mask = rng.random(n) < rng.choice([0.0, 0.1, 0.6])
+        p = encode_page(vals, mask, ["plain", "packed", "slotted"][k % 3], pad=int(rng.choice([1, 8])))
+        if k % 5 == 4:  # cut short
+            p = Page(p.buf[:int(rng.integers(0, len(p.buf) + 1))], p.row_count, p.null_count, p.data_offset)
+        pages.append(p)
+    t = ctx.table_from_pages([("c", qd, pages, pt)])
+    vals, nulls = t.read_column("c")
+    want = decode_column_pages(as_tuples(pages), src)
+    assert len(vals) == len(want)
+    wn = np.array([w is None for w in want], dtype=bool)
+    assert np.array_equal(nulls, wn)
+    wv = np.array([0 if w is None else w for w in want], dtype=np.float64).astype(np_out)
+    if np_out in (np.float32, np.float64):
+        nan = np.isnan(wv)
+        assert np.array_equal(np.isnan(vals), nan)
+        vals, wv = vals[~nan], wv[~nan]
+    assert np.array_equal(vals.view(np.uint8), wv.view(np.uint8))
+    t.close()
+    # a page type widens into one dtype only
+    with pytest.raises(A.QmError) as e:
+        ctx.table_from_pages([("c", A.QM_I64, pages, pt)])
+    assert e.value.status == A.QM_ERR_INVALID

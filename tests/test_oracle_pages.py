@@ -59,3 +59,17 @@ def test_pages_concatenate():
              (bytes([0x02]) + struct.pack("<i", 9), 2, 1, None, False),
              (b"", 0, 0, None, False)]
     assert decode_column_pages(pages, "int32") == [1, 2, None, 9]
+
+
+def test_narrow_page_types():
+    # src/decode.test.ts:66-75: float16 0x3C00 reads as 1.0; and the other
+    # narrow types of decodePlainValues, little-endian
+    assert decode_page(struct.pack("<H", 0x3C00), "float16") == [1.0]
+    assert decode_page(struct.pack("<3e", -2.5, 0.0, 65504.0), "float16") == [-2.5, 0.0, 65504.0]
+    assert decode_page(bytes([0x80, 0x7F, 0xFF]), "int8") == [-128, 127, -1]
+    assert decode_page(bytes([0x80, 0x7F, 0xFF]), "uint8") == [128, 127, 255]
+    assert decode_page(struct.pack("<2h", -32768, 7), "int16") == [-32768, 7]
+    assert decode_page(struct.pack("<2H", 65535, 7), "uint16") == [65535, 7]
+    assert decode_page(struct.pack("<I", 4294967295), "uint32") == [4294967295]
+    # with a validity bitmap, packed
+    assert decode_page(bytes([0x05]) + bytes([3, 200]), "uint8", 1, 3) == [3, None, 200]
