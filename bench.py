@@ -59,6 +59,9 @@ def parse_args():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-ingest", action="store_true")
+    p.add_argument("--no-parity", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the orders_1m / wide_keys_200m lines")
+    p.add_argument("--config-steps", type=int, default=20)
     p.add_argument("--ingest-reps", type=int, default=3)
     p.add_argument("--serve-queries", type=int, default=1500, help="requests per offered load")
     p.add_argument("--serve-loads", default="0.25,0.5,0.75,0.95", help="offered loads as fractions of capacity")
@@ -209,6 +212,116 @@ def cpu_baseline(cols, q, sample_rows: int):
         "sample": f"first {n:,} rows of {WORKLOAD} ({n * BYTES_PER_ROW / 1e9:.2f} GB), oracle on {threads} threads",
         "single_thread_gbs": n1 * BYTES_PER_ROW / t_1 / 1e9,
     }
+
+
+def check_parity(res, cols, q) -> dict:
+    """The last timed step's result against the oracle's one-batch result over
+    the same table (the checker, run after the timed region)."""
+    import oracle
+    from tests.helpers import assert_same
+    t0 = time.perf_counter()
+    ref = oracle.run_full(cols, q)
+    try:
+        assert_same(res, ref)
+        ok, why = True, ""
+    except AssertionError as e:
+        ok, why = False, str(e)[:300]
+    return {"ok": ok, "groups": int(ref.n_rows), "oracle": "one batch, key-partitioned host threads",
+            "threads": os.cpu_count() or 1, "seconds": round(time.perf_counter() - t0, 2), "detail": why}
+
+
+def run_config(ctx, stream, name: str, cols: dict, q, bytes_per_row: int, steps: int, warmup: int,
+               cpu_rows: int, note: str) -> dict:
+    """One more of the measured workloads, on one GPU: device-resident table
+    (`value`: algorithmic bytes / CUDA-event time per query, result in host
+    memory), the scan kernel's roofline, the same query end to end from
+    pinned host columns (`e2e`), the oracle on a bounded sample of the host
+    cores (`cpu_baseline`) and the benched result against the oracle."""
+    import torch
+
+    import oracle
+    from querymode_b200.query import CQuery
+    n = len(next(iter(cols.values())))
+    cq = CQuery(q)
+    peak, peak_kind = load_peaks()
+    with torch.cuda.stream(stream):
+        t = ctx.table(cols)
+        for _ in range(max(3, warmup)):
+            res = t.run(cq)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        scan, launches = [], 0
+        e0.record(stream)
+        for _ in range(steps):
+            res = t.run(cq)
+            scan.append(res.stats.scan_ms)
+            launches += res.stats.launches
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        t.close()
+        # end to end from pinned host memory: upload, query, result download
+        pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in cols.items()}
+        h2d = sum(v.nbytes for v in pinned.values())
+        tt = ctx.table(pinned)
+        r = tt.run(cq)
+        tt.close()
+        d2h = sum(c.values.nbytes for c in r.columns)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        e2e_steps = 3
+        for _ in range(e2e_steps):
+            tt = ctx.table(pinned)
+            tt.run(cq)
+            tt.close()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / e2e_steps
+        del pinned
+    qbytes = n * bytes_per_row
+    scan_ms = float(np.mean(scan))
+    achieved = qbytes / (scan_ms / 1e3) / 1e9
+    sub = {k: np.ascontiguousarray(v[:cpu_rows]) for k, v in cols.items()}
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    oracle.run_full(sub, q, threads=threads)
+    cpu_s = time.perf_counter() - t0
+    parity = check_parity(res, cols, q)
+    return {
+        "workload": name, "rows": n, "bytes_per_row": bytes_per_row, "groups": int(res.n_rows),
+        "rows_selected": int(res.stats.rows_selected), "steps": steps, "warmup": max(3, warmup),
+        "ms_per_query": ms, "value": qbytes / (ms / 1e3) / 1e9, "unit": "GB/s", "rows_per_s": n / (ms / 1e3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel": "qm_scan_kernel", "kernel_ms": scan_ms},
+        "e2e": {"value": qbytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "steps": e2e_steps},
+        "cpu_baseline": {"value": len(next(iter(sub.values()))) * bytes_per_row / cpu_s / 1e9, "unit": "GB/s",
+                         "cores": threads, "kind": "port",
+                         "sample": f"first {len(next(iter(sub.values()))):,} rows, oracle one batch on {threads} threads"},
+        "parity": parity["ok"], "parity_check": parity, "gpu_launches": launches, "note": note,
+    }
+
+
+def run_configs(ctx, stream, args) -> dict:
+    """orders_1m (16 groups, launch-bound) and wide_keys_200m filtered /
+    unfiltered (16.7M groups, hash table beyond L2)."""
+    from querymode_b200 import datagen
+    out = {}
+    orders = datagen.orders(1_000_000, seed=0)
+    out["orders_1m"] = run_config(ctx, stream, "orders_1m", orders, datagen.orders_query(), 16, max(args.config_steps, 50),
+                                  args.warmup, 1_000_000,
+                                  "status = 1 GROUP BY region SUM(amount), COUNT(*); 16 groups; launch- and "
+                                  "sync-bound (16 MB per query)")
+    del orders
+    wide = datagen.wide_keys(200_000_000, seed=2, n_keys=1 << 24)
+    out["wide_keys_200m_filtered"] = run_config(
+        ctx, stream, "wide_keys_200m_filtered", wide, datagen.wide_keys_query(True), 20, args.config_steps, args.warmup,
+        20_000_000, "flag = 1 AND val > 0 (~0.5 %) GROUP BY key SUM(val), COUNT(*); key int64 over 2^24 values")
+    out["wide_keys_200m_unfiltered"] = run_config(
+        ctx, stream, "wide_keys_200m_unfiltered", wide, datagen.wide_keys_query(False), 16, max(3, args.config_steps // 4),
+        args.warmup, 20_000_000, "no filter, GROUP BY key SUM(val), COUNT(*): 16.7M groups, result 0.4 GB to the host")
+    return out
 
 
 def batch_tables_on_device(specs, device: int):
@@ -612,6 +725,10 @@ def main():
     total_bytes = sum_over_ranks(bytes_per_query * args.steps, world)
     value = total_bytes / (elapsed_max / 1e3) / 1e9
 
+    parity = None
+    if world == 1 and not args.no_parity:
+        parity = check_parity(res, cols, q)
+
     # roofline of the fused scan kernel (CUDA events around each launch)
     peak, peak_kind = load_peaks()
     scan_avg = float(np.mean(scan_ms)) if scan_ms else float("nan")
@@ -647,14 +764,21 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cols, q, min(args.cpu_sample_rows, n))
 
+    configs = None
+    if world == 1 and not args.no_configs:
+        table.close()
+        table = None
+        configs = run_configs(ctx, stream, args)
+
     ingest = None
     if world == 1 and not args.no_ingest:
         ingest = run_ingest(ctx, cols, args)
 
     batched = None
     if world == 1 and not args.no_batched:
-        table.close()
-        table = None
+        if table is not None:
+            table.close()
+            table = None
         batched = run_batched(ctx, stream, local, args)
     serving = None
     if world == 1 and not args.no_serving:
@@ -672,8 +796,11 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "qm_scan_kernel", "kernel_ms": scan_avg},
+            "parity": None if parity is None else parity["ok"],
+            "parity_check": parity,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "configs": configs,
             "batched": batched,
             "serving": serving,
             "ingest": ingest,

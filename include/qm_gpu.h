@@ -333,11 +333,16 @@ int qm_filter_select(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
  * available to it — this runs the query of qm_query_run over device-resident
  * columns without any device or pinned allocation: the group table and
  * every temporary live in one static device array of
- * QM_NOALLOC_SCRATCH_BYTES, held by each device from the first call on it
- * until the process exits.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  Every call shares and re-initialises the array, so calls
- * that overlap on the GPU race: serialise them.
+ * QM_NOALLOC_SCRATCH_BYTES, held by each device from the library's module
+ * load on it (its first call under lazy module loading) until the process
+ * exits.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it; make that first call before any
+ * stream capture, and make no call on a device after a cudaDeviceReset of
+ * it.  Every call shares and re-initialises the array, so calls that
+ * overlap on the GPU race: serialise them.
+ * Without column statistics, a GROUP BY over several columns is limited to
+ * two non-NULL int32 columns (QM_ERR_UNSUPPORTED otherwise; qm_query_run
+ * packs other integer keys by their value ranges).
  *   cols         device columns only (on_device = 1); a NULL bitmap must be
  *                4-byte aligned and readable as ceil(n_rows/32) 32-bit words
  *   max_groups   capacity of the outputs; queries whose groups (or whose

@@ -46,6 +46,9 @@ def lib() -> C.CDLL:
         L.oracle_run_mt.restype = C.c_int
         L.oracle_run_mt.argtypes = [C.c_int64, C.c_int32, C.POINTER(A.QmColumn), C.POINTER(A.QmQuery),
                                     C.c_int64, C.c_int32, C.POINTER(P)]
+        L.oracle_run_keypart.restype = C.c_int
+        L.oracle_run_keypart.argtypes = [C.c_int64, C.c_int32, C.POINTER(A.QmColumn), C.POINTER(A.QmQuery),
+                                         C.c_int32, C.POINTER(P)]
         L.oracle_filter_select.restype = C.c_int
         L.oracle_filter_select.argtypes = [C.c_int64, C.c_int32, C.POINTER(A.QmColumn),
                                            C.POINTER(A.QmQuery), C.POINTER(C.c_uint32), C.c_int64,
@@ -120,6 +123,24 @@ def run(columns, query: QueryDescriptor, batch_rows: int = 0, threads: int = 1) 
         L.oracle_result_destroy(h)
 
 
+def run_full(columns, query: QueryDescriptor, threads: int | None = None) -> OracleResult:
+    """The reference's one-batch result (run(..., batch_rows=0)) bit for bit,
+    on `threads` host threads (default: all): groups are split across threads
+    by key hash, each group's rows visited in row order, and the groups put
+    back in first-seen order.  For full-size checks of large tables."""
+    L = lib()
+    cs = _ColumnSet(columns)
+    cq = CQuery(query)
+    h = C.c_void_p()
+    st = L.oracle_run_keypart(cs.n_rows, cs.count, cs.array, cq.ref, threads or os.cpu_count() or 1, C.byref(h))
+    if st != 0:
+        raise A.QmError(st, L.oracle_last_error().decode())
+    try:
+        return _collect(L, h)
+    finally:
+        L.oracle_result_destroy(h)
+
+
 def filter_select(columns, query: QueryDescriptor, selection=None) -> np.ndarray:
     if selection is not None:
         sel = np.asarray(selection, dtype=np.int64)
@@ -142,4 +163,4 @@ def filter_select(columns, query: QueryDescriptor, selection=None) -> np.ndarray
     return out[:cnt.value].copy()
 
 
-__all__ = ["run", "filter_select", "build", "OracleResult", "ResultColumn"]
+__all__ = ["run", "run_full", "filter_select", "build", "OracleResult", "ResultColumn"]

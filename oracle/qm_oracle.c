@@ -799,6 +799,125 @@ int oracle_run_mt(int64_t n_rows, int32_t n_cols, const qm_column *cols,
   return 0;
 }
 
+/* ------------------------------------------------ key-partitioned threads */
+/* One batch over all rows (the in-memory route of MaterializedExecutor,
+ * src/client.ts:1023-1054) on n_threads host threads, with the single-thread
+ * result bit for bit: thread t takes the groups whose key hash falls in its
+ * part, visiting their rows in row order, so every group's float sum is the
+ * reference's sequential sum in row order.  The groups of all parts are then
+ * put in first-seen order (the Map insertion order of finalizePartialAgg,
+ * src/partial-agg.ts:320-349) by a merge on each group's first row.  For
+ * full-size checks of high-cardinality results, where merging per-thread
+ * maps of millions of groups would dominate. */
+typedef struct {
+  const oplan *P;
+  int part, n_parts;
+  uint8_t *row_part;  /* per row: its group's part, or 0xff when filtered out */
+  int64_t r0, r1;     /* rows this thread classifies */
+  omap acc;
+  int64_t *first;   /* first row of each group of acc */
+  int64_t n_first, cap_first;
+} okworker;
+
+/* Phase 1, by row ranges: the filter, and each passing row's part. */
+static void *keypart_classify(void *arg) {
+  okworker *w = (okworker *)arg;
+  const oplan *P = w->P;
+  const int nk = P->nk;
+  uint64_t kv[OR_MAX_KEYS] = {0};
+  uint8_t kn[OR_MAX_KEYS] = {0};
+  for (int64_t r = w->r0; r < w->r1; r++) {
+    if (!row_pass(P, r)) {
+      w->row_part[r] = 0xff;
+      continue;
+    }
+    for (int i = 0; i < nk; i++) key_part(P->kc[i], r, &kv[i], &kn[i]);
+    w->row_part[r] = (uint8_t)((key_hash(kv, kn, nk) >> 40) % (uint64_t)w->n_parts);
+  }
+  return NULL;
+}
+
+/* Phase 2, by part: the part's rows aggregated in row order. */
+static void *keypart_main(void *arg) {
+  okworker *w = (okworker *)arg;
+  const oplan *P = w->P;
+  const int nk = P->nk, na = P->na;
+  uint64_t kv[OR_MAX_KEYS] = {0};
+  uint8_t kn[OR_MAX_KEYS] = {0};
+  const uint8_t me = (uint8_t)w->part;
+  for (int64_t r = 0; r < P->n_rows; r++) {
+    if (w->row_part[r] != me) continue;
+    for (int i = 0; i < nk; i++) key_part(P->kc[i], r, &kv[i], &kn[i]);
+    const int64_t before = w->acc.n_groups;
+    int64_t g = omap_find_or_add(&w->acc, kv, kn);
+    if (w->acc.n_groups != before) {
+      if (w->n_first == w->cap_first) {
+        w->cap_first = w->cap_first ? 2 * w->cap_first : 1024;
+        w->first = (int64_t *)realloc(w->first, sizeof(int64_t) * w->cap_first);
+      }
+      w->first[w->n_first++] = r;
+    }
+    for (int a = 0; a < na; a++) feed(&w->acc.st[g * na + a], &P->ag[a], r);
+  }
+  return NULL;
+}
+
+int oracle_run_keypart(int64_t n_rows, int32_t n_cols, const qm_column *cols, const qm_query *q,
+                       int32_t n_threads, oresult **out) {
+  *out = NULL;
+  g_err[0] = 0;
+  if (q->n_group_by == 0 || n_threads <= 1) return oracle_run(n_rows, n_cols, cols, q, 0, out);
+  oplan P;
+  int rc = plan_build(&P, n_rows, n_cols, cols, q, 1);
+  if (rc) { plan_free(&P); return rc; }
+  const int nk = P.nk, na = P.na;
+  if (n_threads > 250) n_threads = 250;
+  okworker *W = (okworker *)calloc(n_threads, sizeof(okworker));
+  pthread_t *th = (pthread_t *)calloc(n_threads, sizeof(pthread_t));
+  uint8_t *row_part = (uint8_t *)malloc(n_rows > 0 ? (size_t)n_rows : 1);
+  for (int t = 0; t < n_threads; t++) {
+    W[t].P = &P; W[t].part = t; W[t].n_parts = n_threads; W[t].row_part = row_part;
+    W[t].r0 = n_rows * t / n_threads; W[t].r1 = n_rows * (t + 1) / n_threads;
+    pthread_create(&th[t], NULL, keypart_classify, &W[t]);
+  }
+  for (int t = 0; t < n_threads; t++) pthread_join(th[t], NULL);
+  for (int t = 0; t < n_threads; t++) {
+    omap_init(&W[t].acc, nk, na);
+    pthread_create(&th[t], NULL, keypart_main, &W[t]);
+  }
+  for (int t = 0; t < n_threads; t++) pthread_join(th[t], NULL);
+  free(row_part);
+  /* the parts' groups, each part already in first-row order, merged by first row */
+  int64_t G = 0;
+  for (int t = 0; t < n_threads; t++) G += W[t].acc.n_groups;
+  omap acc;
+  memset(&acc, 0, sizeof acc);
+  acc.n_keys = nk; acc.n_aggs = na; acc.n_groups = G; acc.alloc_groups = G ? G : 1;
+  acc.keys = (uint64_t *)malloc(sizeof(uint64_t) * acc.alloc_groups * nk);
+  acc.knull = (uint8_t *)malloc(acc.alloc_groups * nk);
+  acc.st = (ostate *)malloc(sizeof(ostate) * acc.alloc_groups * (na ? na : 1));
+  int64_t *pos = (int64_t *)calloc(n_threads, sizeof(int64_t));
+  for (int64_t g = 0; g < G; g++) {
+    int best = -1;
+    for (int t = 0; t < n_threads; t++)
+      if (pos[t] < W[t].acc.n_groups && (best < 0 || W[t].first[pos[t]] < W[best].first[pos[best]])) best = t;
+    const int64_t s = pos[best]++;
+    memcpy(acc.keys + g * nk, W[best].acc.keys + s * nk, sizeof(uint64_t) * nk);
+    memcpy(acc.knull + g * nk, W[best].acc.knull + s * nk, nk);
+    memcpy(acc.st + g * na, W[best].acc.st + s * na, sizeof(ostate) * na);
+  }
+  for (int t = 0; t < n_threads; t++) {
+    omap_free(&W[t].acc);
+    free(W[t].first);
+  }
+  free(pos);
+  *out = finalize(&P, &acc);
+  free(acc.keys); free(acc.knull); free(acc.st);
+  free(W); free(th);
+  plan_free(&P);
+  return 0;
+}
+
 /* Filter-only: ascending indices of passing rows (scanFilterIndices,
  * src/operators.ts:439-466). */
 int oracle_filter_select(int64_t n_rows, int32_t n_cols, const qm_column *cols,

@@ -2883,6 +2883,9 @@ bool g_noalloc_ready[128];
 
 // The device address of the scratch array on the current device (set up on
 // the first call per device; that call must come before any stream capture).
+// The address is kept for the life of the process: it does not survive a
+// cudaDeviceReset (or a primary context torn down and created again), after
+// which this entry point must not be called on that device.
 int noalloc_scratch(qm_ctx *ctx, unsigned char **out) {
   if (ctx->device < 0 || ctx->device >= 128) return set_err(ctx, QM_ERR_INVALID, "device ordinal out of range");
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
@@ -2914,6 +2917,11 @@ extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
   if (q->order_by || q->has_limit || q->offset)
     return set_err(ctx, QM_ERR_UNSUPPORTED, "ORDER BY / LIMIT / OFFSET run through qm_query_run");
   *out_groups = 0;
+  // no group needs less than 8 bytes of scratch: a larger capacity cannot
+  // fit, and bounding it here keeps the size arithmetic below from overflowing
+  if (max_groups > (int64_t)(QM_NOALLOC_SCRATCH_BYTES / 8))
+    return set_err(ctx, QM_ERR_CAPACITY, "max_groups = %lld cannot fit the %u-byte scratch array",
+                   (long long)max_groups, (unsigned)QM_NOALLOC_SCRATCH_BYTES);
   cudaSetDevice(ctx->device);
   unsigned char *scratch = nullptr;
   int rc = noalloc_scratch(ctx, &scratch);
@@ -2991,7 +2999,9 @@ extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
     a.n = n_rows;
     a.sel = nullptr;
     a.row_offset = 0;
-    const size_t smem = qm_scan_smem_bytes(ex.local_slots, ex.local_hash, pl.agg.n_words, 0, 0, ex.priv);
+    // per-warp copies pay only on large inputs (the rule of run_scan)
+    if (a.priv && n_rows < PRIV_MIN_ROWS) a.priv = 0;
+    const size_t smem = qm_scan_smem_bytes(ex.local_slots, ex.local_hash, pl.agg.n_words, 0, 0, a.priv);
     const int blocks = scan_blocks(ctx, smem, n_rows, false);
     CK(qm_launch_scan(a, blocks, smem, ctx->stream));
   }

@@ -11,10 +11,10 @@ form, the shape QueryDescriptor takes (filters AND-ed, filterGroups OR-ed).
 The string column `c` becomes int32 dictionary codes carrying its NULLs.
 Expected rows are turned into row indices of the source table.
 
-Run from the repository root with the reference checked out at
-/root/reference (the output is committed; tests never read the reference):
+Run from the repository root, naming the reference's checkout (the output
+is committed; tests never read the reference):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <path to the reference checkout>
 """
 from __future__ import annotations
 
@@ -23,7 +23,7 @@ import json
 import os
 import re
 
-REF = "/root/reference/wasm/tests/conformance/fixtures"
+FIXTURES = os.path.join("wasm", "tests", "conformance", "fixtures")  # inside the reference checkout
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "filter_fixtures.json")
 
 # The fixture table, restated from generate_sql_fixtures.py:33-46.
@@ -146,9 +146,9 @@ def row_index(data: dict, i: int) -> int:
     raise KeyError(key)
 
 
-def main() -> None:
+def main(reference: str) -> None:
     cases = []
-    for f in sorted(glob.glob(os.path.join(REF, "*.expected.json"))):
+    for f in sorted(glob.glob(os.path.join(reference, FIXTURES, "*.expected.json"))):
         fx = json.load(open(f))
         res = fx["result"]
         if not res.get("success"):
@@ -185,4 +185,7 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference checkout>")
+    main(sys.argv[1])

@@ -7,9 +7,9 @@ here as the expected values).  Also tests/golden/parquet_dict_id.bin.zlib +
 parquet_dict.json from wasm/tests/fixtures/benchmark_100k_uncompressed.parquet:
 its `id` column chunk (a dictionary page of 100,000 INT64 values and one v1
 data page of 17-bit RLE_DICTIONARY indices), zlib-compressed, whose values
-pyarrow decodes as 0..99,999.  Run where the reference is mounted:
+pyarrow decodes as 0..99,999.  Run where the reference is checked out:
 
-    python tests/golden/make_parquet_golden.py /root/reference
+    python tests/golden/make_parquet_golden.py <path to the reference checkout>
 """
 import base64
 import hashlib
@@ -60,4 +60,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_parquet_golden.py <path to the reference checkout>")
+    main(sys.argv[1])

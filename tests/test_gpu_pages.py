@@ -244,3 +244,24 @@ def test_narrow_page_types(ctx, src):
     with pytest.raises(A.QmError) as e:
         ctx.table_from_pages([("c", A.QM_I64, pages, pt)])
     assert e.value.status == A.QM_ERR_INVALID
+
+
+def test_uint32_pages_sum_exactly(ctx):
+    """uint32 page values are JS numbers in the reference's operator path
+    (decodePlainValues, src/parquet-decode.ts:280-386), so their SUM is a
+    float64 sum; values near 2^32 over many rows push every group's sum far
+    past 2^32 and stay exact below 2^53, bit for bit against the oracle."""
+    rng = np.random.default_rng(77)
+    n = 400_000
+    vals = rng.integers(4_000_000_000, 4_294_967_296, n, dtype=np.uint64).astype(np.uint32)
+    key = rng.integers(0, 7, n).astype(np.int32)
+    t = ctx.table_from_pages([("c", A.QM_F64, encode_column(vals, None, 10_000), A.QM_PT_UINT32),
+                              ("k", A.QM_I32, encode_column(key, None, 10_000))])
+    q = QueryDescriptor(group_by=["k"], aggregates=[AggregateOp("sum", "c"), AggregateOp("min", "c"),
+                                                    AggregateOp("max", "c"), AggregateOp("count", "*")])
+    got = t.run(q)
+    ref = oracle.run({"c": vals.astype(np.float64), "k": key}, q)
+    assert_same(got, ref, rel_tol=0.0)
+    sums = got.column("sum_c").values
+    assert (sums > 2.0 ** 32).all() and np.array_equal(sums, np.floor(sums))
+    t.close()

@@ -9,6 +9,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 from querymode_b200 import _abi as A
 from querymode_b200 import datagen
 from querymode_b200.engine import Result, ResultColumn, _ColumnSet, unpack_nulls
@@ -54,9 +55,11 @@ def test_noalloc_matches_query_run_on_two_calls(ctx):
     ref = ctx.table(cols).run(q)
     dev = {k: torch.from_numpy(v).cuda() for k, v in cols.items()}
     names = [(c.name, c.is_key) for c in ref.columns]
+    want = oracle.run(cols, q)
     for _ in range(2):
         got = run_noalloc(ctx, dev, q, 70_000, names)
         assert_same(got, ref, ordered=False)
+        assert_same(got, want, ordered=False)
 
 
 def test_noalloc_ungrouped_and_capacity_error(ctx):
@@ -78,3 +81,26 @@ def test_noalloc_ungrouped_and_capacity_error(ctx):
     with pytest.raises(A.QmError) as ei:
         run_noalloc(ctx, dev, qg, 1 << 26, [("k", True), ("sum_v", False)])
     assert ei.value.status == A.QM_ERR_CAPACITY
+
+
+def test_noalloc_key_packing_limit(ctx):
+    """Without column statistics two int64 group columns cannot be packed
+    into one key word: QM_ERR_UNSUPPORTED (qm_query_run packs them by their
+    value ranges); two non-NULL int32 columns concatenate and match the
+    oracle."""
+    import torch
+    rng = np.random.default_rng(9)
+    n = 100_000
+    cols = {"a": rng.integers(0, 40, n).astype(np.int64), "b": rng.integers(0, 30, n).astype(np.int64),
+            "c": rng.integers(-5, 5, n).astype(np.int32), "d": rng.integers(0, 9, n).astype(np.int32),
+            "v": rng.normal(size=n)}
+    dev = {k: torch.from_numpy(v).cuda() for k, v in cols.items()}
+    q64 = QueryDescriptor(group_by=["a", "b"], aggregates=[AggregateOp("sum", "v")])
+    with pytest.raises(A.QmError) as ei:
+        run_noalloc(ctx, dev, q64, 4096, [("a", True), ("b", True), ("sum_v", False)])
+    assert ei.value.status == A.QM_ERR_UNSUPPORTED
+    q32 = QueryDescriptor(group_by=["c", "d"], aggregates=[AggregateOp("sum", "v"), AggregateOp("count", "*")])
+    for _ in range(2):
+        got = run_noalloc(ctx, dev, q32, 4096, [("c", True), ("d", True), ("sum_v", False), ("count_*", False)])
+        assert_same(got, oracle.run(cols, q32), ordered=False)
+    assert_same(ctx.table(cols).run(q64), oracle.run(cols, q64))
