@@ -87,6 +87,18 @@ extern "C" {
  * (src/operators.ts:550-666): NULLs read as 0 and int32 thresholds pass
  * through ToInt32.  Default is the JS matchesFilter semantics. */
 #define QM_FLAG_WASM_SCAN_SEMANTICS 2
+/* Float SUM / AVG independent of the order rows are added in: each finite
+ * cell becomes an exact 128-bit fixed-point integer (units of 2^-k below the
+ * column's largest |x|, taken from its statistics) and the integers are
+ * summed, so the same query gives bit-identical sums on every run, alone or
+ * batched, whatever the launch shape.  The result is the exact sum of the
+ * cells rounded once (each cell off by at most 2^-(126 - log2 rows) of the
+ * column's largest |x|); NaN / Infinity cells follow the reference's
+ * sequential sum.  The reference's own sum is sequential in row order
+ * (src/partial-agg.ts:77), which a parallel sum matches only to rounding.
+ * Registered tables only (qm_query_run, batches, servers): streamed batches
+ * and qm_query_run_noalloc return QM_ERR_UNSUPPORTED. */
+#define QM_FLAG_DETERMINISTIC 4
 
 typedef struct qm_ctx qm_ctx;
 typedef struct qm_table qm_table;
@@ -306,6 +318,28 @@ int qm_agg_partial_export(qm_agg *agg, int64_t row_offset, uint64_t *dst, int64_
 int qm_agg_partial_merge(qm_agg *agg, const uint64_t *src, int64_t n_groups, int32_t row_words,
                          int64_t rows_end);
 
+/* The layout of this aggregation's partial rows: words per row and the word
+ * holding the group's first global row (-1 when the query keeps no
+ * first-seen order).  A finished result's rows come in ascending order of
+ * that word. */
+int qm_agg_partial_layout(const qm_agg *agg, int32_t *row_words, int32_t *first_word);
+/* A new, empty aggregation with src's plan and partial-row layout, taking
+ * only qm_agg_partial_merge: the receiving side of a key-partitioned
+ * exchange, where each rank merges and finalizes the groups of its key
+ * range.  (The reference reduces every fragment's partial on one node,
+ * src/query-do.ts:1896-1960, src/merge.ts:156-172; splitting the groups
+ * across ranks is this library's own step.) */
+int qm_agg_partial_begin(const qm_agg *src, qm_agg **out);
+/* Split n_rows partial rows (device memory of this context's GPU) into
+ * `parts` groups by the hash of their key word, so that every rank's rows
+ * of one group go to the same rank of an all-to-all exchange: dst (device,
+ * n_rows rows) receives part 0's rows, then part 1's, ...; part_rows (host,
+ * `parts` entries) receives each part's row count.  Rows of a special key
+ * (the empty-slot sentinel, NULL) go to part 0.  1 <= parts <= 4096.  No
+ * counterpart in the reference. */
+int qm_partial_partition(qm_ctx *ctx, const uint64_t *src, int64_t n_rows, int32_t row_words, int32_t parts,
+                         uint64_t *dst, int64_t *part_rows);
+
 /* ---- filter-only selection (FilterOperator / WASM filter drop-in) ------- */
 /* Evaluate the filters of `query` (aggregates and group_by ignored) over one
  * batch — over the rows listed by `selection` (ascending, n_selected) when it
@@ -385,6 +419,11 @@ int qm_batch_set_tuning(qm_batch *batch, int32_t chunk_tiles, int32_t local_kb,
  * (query, chunk of tiles) work items and read each query's plan at run
  * time (the chunk / local-table knobs below apply to it). */
 int qm_batch_set_mode(qm_batch *batch, int32_t mode);
+/* Waves of a batched run (0: by batch size, up to 8): the queries are cut
+ * into waves run back to back, each followed by the copy of its results to
+ * the host, which overlaps the later waves.  Queries whose results are large
+ * for the bytes they scan go first.  Re-captures the graph on the next run. */
+int qm_batch_set_waves(qm_batch *batch, int32_t waves);
 /* Device time of the last run, total rows and algorithmic bytes, chunks. */
 int qm_batch_stats(const qm_batch *batch, double *device_ms, int64_t *rows,
                    int64_t *bytes, int32_t *chunks);
@@ -471,17 +510,21 @@ int qm_table_read_column(const qm_table *table, int32_t column, void *values, ui
 /* ---- serving loop -----------------------------------------------------------
  * Continuous batching of single requests over resident tables.  The reference
  * serves each query in its own durable object (src/query-do.ts fan-out, one
- * single-threaded engine per object, src/wasm-engine.ts:181-186); here one
- * worker thread per server drains a request queue into batched persistent
- * launches (qm_batch_*) back to back: requests that arrive while a batch runs
- * form the next one.
+ * single-threaded engine per object, src/wasm-engine.ts:181-186); here a
+ * server runs several lanes, each a worker thread with its own CUDA stream:
+ * a free lane takes the requests queued at that moment as one batched launch
+ * (qm_batch_*), so requests that arrive while other batches run start on the
+ * next free lane and their device work overlaps the others'.  Each request
+ * completes as soon as its own result has been copied back.  A request over
+ * a table of more than max_batch_rows rows is heavy: it runs alone, and the
+ * light-only lane keeps small requests moving past it.
  *
  * HBM budget admission: the server counts the device bytes of every table
- * it has been given (resident) plus each queued request's working memory
- * (group table, bitmaps, packed result).  A batch takes queued requests in
- * arrival order while resident + working bytes stay within hbm_budget_bytes;
- * the rest wait for the next batch.  A request that cannot fit even alone
- * completes with QM_ERR_OOM.
+ * it has been given (resident) plus the working memory (group table,
+ * bitmaps, packed result) of every request on the GPU.  A lane admits
+ * queued requests in arrival order while resident + working bytes of all
+ * lanes stay within hbm_budget_bytes; the rest wait until memory frees up.
+ * A request that cannot fit even alone completes with QM_ERR_OOM.
  *
  * The server drives the context it is created on from its worker thread:
  * register tables first, and make no other call on that context (or its
@@ -494,11 +537,13 @@ typedef struct {
   int32_t max_batch;        /* requests per batched launch (1..4096)       */
   int32_t max_wait_us;      /* the oldest queued request waits at most this
                                long for others before a launch (0: none)   */
-  int64_t max_batch_rows;   /* rows a batch may scan (0: no limit); a batch
-                               always takes its first request.  Bounds the
-                               latency a large request adds to small ones
-                               sharing its batch                            */
-  int32_t reserved[2];
+  int64_t max_batch_rows;   /* rows a batch may scan (0: no limit); a
+                               request over a table of more rows is heavy:
+                               it runs alone, never on the light lane       */
+  int32_t lanes;            /* batches in flight at once, each on its own
+                               stream (0: 4); with more than one, the last
+                               lane takes light requests only               */
+  int32_t reserved;
 } qm_server_config;
 
 typedef struct {
@@ -512,8 +557,11 @@ typedef struct {
 typedef struct {
   int64_t submitted, completed, failed, cancelled, refused, batches;
   int64_t resident_bytes;     /* device bytes of the tables seen           */
-  int64_t peak_working_bytes; /* largest admitted batch's working memory   */
+  int64_t peak_working_bytes; /* most working memory of batches in flight  */
   int64_t queued;             /* requests waiting now                      */
+  int64_t peak_in_flight;     /* most requests on the GPU at once          */
+  int64_t heavy;              /* requests run alone as heavy               */
+  int64_t lanes;              /* lanes of the server                       */
 } qm_server_counters;
 
 int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out);

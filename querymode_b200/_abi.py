@@ -60,6 +60,7 @@ QM_NOALLOC_SCRATCH_BYTES = 32 << 20
 
 QM_FLAG_UNORDERED = 1
 QM_FLAG_WASM_SCAN_SEMANTICS = 2
+QM_FLAG_DETERMINISTIC = 4
 
 
 class QmColumn(C.Structure):
@@ -112,7 +113,7 @@ class QmStats(C.Structure):
 
 class QmServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_batch", C.c_int32), ("max_wait_us", C.c_int32),
-                ("max_batch_rows", C.c_int64), ("reserved", C.c_int32 * 2)]
+                ("max_batch_rows", C.c_int64), ("lanes", C.c_int32), ("reserved", C.c_int32)]
 
 
 class QmServerTiming(C.Structure):
@@ -123,7 +124,8 @@ class QmServerTiming(C.Structure):
 class QmServerCounters(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("cancelled", C.c_int64), ("refused", C.c_int64), ("batches", C.c_int64),
-                ("resident_bytes", C.c_int64), ("peak_working_bytes", C.c_int64), ("queued", C.c_int64)]
+                ("resident_bytes", C.c_int64), ("peak_working_bytes", C.c_int64), ("queued", C.c_int64),
+                ("peak_in_flight", C.c_int64), ("heavy", C.c_int64), ("lanes", C.c_int64)]
 
 
 class QmParquetColumn(C.Structure):
@@ -170,6 +172,10 @@ SIGNATURES = [
     ("qm_agg_partial_export", C.c_int, [_P, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(C.c_int64),
                                         C.POINTER(C.c_int32)]),
     ("qm_agg_partial_merge", C.c_int, [_P, C.c_void_p, C.c_int64, C.c_int32, C.c_int64]),
+    ("qm_agg_partial_layout", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("qm_agg_partial_begin", C.c_int, [_P, _PP]),
+    ("qm_partial_partition", C.c_int, [_P, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p,
+                                       C.POINTER(C.c_int64)]),
     ("qm_filter_select", C.c_int, [_P, C.c_int64, C.c_int32, C.POINTER(QmColumn),
                                    C.POINTER(QmQuery), C.POINTER(C.c_uint32), C.c_int64,
                                    C.POINTER(C.c_uint32), C.c_int64, C.POINTER(C.c_int64)]),
@@ -180,6 +186,7 @@ SIGNATURES = [
     ("qm_batch_run", C.c_int, [_P, C.POINTER(C.c_void_p)]),
     ("qm_batch_set_tuning", C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     ("qm_batch_set_mode", C.c_int, [_P, C.c_int32]),
+    ("qm_batch_set_waves", C.c_int, [_P, C.c_int32]),
     ("qm_batch_stats", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                  C.POINTER(C.c_int32)]),
     ("qm_batch_destroy", C.c_int, [_P]),

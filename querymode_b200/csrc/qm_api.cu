@@ -23,6 +23,7 @@
 #include <mutex>
 #include <string>
 #include <deque>
+#include <functional>
 #include <vector>
 
 #include "../../include/qm_gpu.h"
@@ -56,20 +57,28 @@ struct PinnedPool {
   // kept up to a byte cap: allocating or freeing pinned memory costs far
   // more than a query (and freeing synchronises the device).
   static constexpr size_t CACHE_CAP = (size_t)8 << 30;
+  static constexpr size_t MAX_BUFFERS = 256;
+  static size_t class_of(size_t bytes) {
+    size_t want = 64 * 1024;
+    while (want < bytes) want <<= 1;
+    return want;
+  }
   bool acquire(size_t bytes, HostBuf &out) {
+    const size_t want = class_of(bytes);
     {
+      // the smallest free buffer of at least the request's class, at most
+      // twice it (a large buffer is not spent on a small result)
       std::lock_guard<std::mutex> lk(mu);
       int best = -1;
       for (int i = 0; i < (int)free.size(); i++)
-        if (free[i].bytes >= bytes && (best < 0 || free[i].bytes < free[best].bytes)) best = i;
+        if (free[i].bytes >= want && free[i].bytes <= 2 * want && (best < 0 || free[i].bytes < free[best].bytes))
+          best = i;
       if (best >= 0) {
         out = free[best];
         free.erase(free.begin() + best);
         return true;
       }
     }
-    size_t want = 64 * 1024;
-    while (want < bytes) want <<= 1;
     if (cudaMallocHost(&out.p, want) != cudaSuccess) {
       cudaGetLastError();
       out = HostBuf();
@@ -78,16 +87,26 @@ struct PinnedPool {
     out.bytes = want;
     return true;
   }
+  // Kept for reuse up to the caps; beyond them the smallest buffers go
+  // first (the large ones cost the most to page-lock again).
   void release(HostBuf &b) {
     if (!b.p) return;
-    std::lock_guard<std::mutex> lk(mu);
-    size_t cached = b.bytes;
-    for (auto &f : free) cached += f.bytes;
-    if (cached <= CACHE_CAP && free.size() < 64) {
+    std::vector<void *> drop;
+    {
+      std::lock_guard<std::mutex> lk(mu);
       free.push_back(b);
-    } else {
-      cudaFreeHost(b.p);
+      size_t cached = 0;
+      for (auto &f : free) cached += f.bytes;
+      while ((cached > CACHE_CAP || free.size() > MAX_BUFFERS) && !free.empty()) {
+        int s = 0;
+        for (int i = 1; i < (int)free.size(); i++)
+          if (free[i].bytes < free[s].bytes) s = i;
+        cached -= free[s].bytes;
+        drop.push_back(free[s].p);
+        free.erase(free.begin() + s);
+      }
     }
+    for (void *p : drop) cudaFreeHost(p);
     b = HostBuf();
   }
 };
@@ -840,6 +859,13 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
           acc = add_acc(QA_FSUM, vc, 0);
           o.kind = ag.fn == QM_AGG_SUM ? QO_SUM_F : QO_AVG_F;
           o.dtype = QM_F64;
+          if (q->flags & QM_FLAG_DETERMINISTIC) {
+            // fixed-point sum: its non-finite cells go to a word of their own
+            const int nf = add_acc(QA_FNF, vc, 0);
+            if (nf < 0) return set_err(ctx, QM_ERR_UNSUPPORTED, "too many accumulators");
+            o.fixed = 1;
+            o.nf_word = A.acc[nf].word;
+          }
         }
         break;
       case QM_AGG_MIN:
@@ -870,7 +896,9 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
   for (int c = 0; c < A.n_vcols; c++) {
     qm_vcol &vc = A.vcol[c];
     vc.flags = 0;
-    vc.w_nn = vc.w_sum = vc.w_min = vc.w_max = vc.w_zero = -1;
+    vc.w_nn = vc.w_sum = vc.w_min = vc.w_max = vc.w_zero = vc.w_nf = -1;
+    vc.fx_exp = 0;
+    vc.fx_max = 0.0;
   }
   for (int i = 0; i < A.n_accs; i++) {
     const qm_acc &ac = A.acc[i];
@@ -883,6 +911,7 @@ int build_agg(qm_ctx *ctx, const qm_query *q, const ColEnv &env, Plan &pl, std::
       case QA_IMIN: case QA_FMIN: vc.flags |= VF_MIN; vc.w_min = ac.word; break;
       case QA_IMAX: case QA_FMAX: vc.flags |= VF_MAX; vc.w_max = ac.word; break;
       case QA_FZERO: vc.flags |= VF_ZERO; vc.w_zero = ac.word; break;
+      case QA_FNF: vc.w_nf = ac.word; break;
     }
   }
   return QM_OK;
@@ -1091,20 +1120,38 @@ int column_maxabs(qm_ctx *ctx, DevCol &c, int64_t n) {
   return QM_OK;
 }
 
-// Split constants of the float SUM columns of a table query (see qm_vcol).
-int plan_split_sums(qm_ctx *ctx, Plan &pl, int64_t n_rows) {
+// Split constants of the float SUM columns of a table query (see qm_vcol),
+// or, for a deterministic query, the unit of their fixed-point sums: with
+// every finite |x| < 2^e and fewer than 2^R rows, cells become integers
+// below 2^F (F = 125 - R) in units of 2^(e - F), so a group's sum stays
+// below 2^125 and each cell is off by at most half a unit, 2^(e - F - 1).
+int plan_split_sums(qm_ctx *ctx, Plan &pl, int64_t n_rows, bool deterministic) {
   int bits = 1;
   while (bits < 62 && ((int64_t)1 << bits) <= n_rows) bits++;
   const int k = bits + 1;  // a group has fewer than 2^(k-1) rows
   for (int c = 0; c < pl.agg.n_vcols; c++) {
     qm_vcol &vc = pl.agg.vcol[c];
     vc.split = 0.0;
-    if (!(vc.flags & VF_SUM) || is_int(vc.dtype) || !pl.vcolsrc[c]) continue;
+    if (!(vc.flags & VF_SUM) || is_int(vc.dtype)) continue;
+    if (!pl.vcolsrc[c]) {
+      if (deterministic) return set_err(ctx, QM_ERR_UNSUPPORTED, "deterministic float SUM needs a registered table");
+      continue;
+    }
     DevCol &col = *const_cast<DevCol *>(pl.vcolsrc[c]);
     int rc = column_maxabs(ctx, col, n_rows);
     if (rc) return rc;
     int e = 0;  // every finite |x| < 2^e
     if (col.maxabs > 0) e = std::ilogb(col.maxabs) + 1;
+    if (deterministic) {
+      const int F = 125 - bits;
+      vc.flags |= VF_FIXED;
+      vc.fx_exp = e - F;
+      vc.fx_max = std::ldexp(1.0, e);
+      for (int o = 0; o < pl.outs.n_out; o++)
+        if ((pl.outs.o[o].kind == QO_SUM_F || pl.outs.o[o].kind == QO_AVG_F) && pl.outs.o[o].word == vc.w_sum)
+          pl.outs.o[o].fx_exp = vc.fx_exp;
+      continue;
+    }
     if (e + k > 1000 || e + k < -960) continue;  // keep TwoSum at the ends of the range
     vc.split = 1.5 * std::ldexp(1.0, e + k);
   }
@@ -1847,7 +1894,7 @@ int plan_table_query(qm_ctx *ctx, qm_table *t, const qm_query *q, GroupTable &gt
   direct_size = 0;
   uint64_t space = 0;
   if ((rc = plan_key_packing(ctx, pl, t->n_rows, true, &space))) return rc;
-  if ((rc = plan_split_sums(ctx, pl, t->n_rows))) return rc;
+  if ((rc = plan_split_sums(ctx, pl, t->n_rows, (q->flags & QM_FLAG_DETERMINISTIC) != 0))) return rc;
   plan_narrow_sums(pl, t->n_rows);
   if (pl.key.n_cols == 0) {
     pl.key.mode = QK_NONE;
@@ -2300,6 +2347,14 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
     }
     if (attempt >= 4) return set_err(ctx, QM_ERR_CUDA, "group table overflow after %d regrowths", attempt);
     gt.retries++;
+    if (st.error == QM_DEV_STALE) {
+      // a fixed-point SUM cell beyond its column's cached range: the column
+      // changed since; take its statistics again and re-run
+      for (int c = 0; c < pl.agg.n_vcols; c++)
+        if (pl.vcolsrc[c]) const_cast<DevCol *>(pl.vcolsrc[c])->has_maxabs = false;
+      if ((rc = plan_split_sums(ctx, pl, t->n_rows, true))) return rc;
+      continue;
+    }
     if (st.error == QM_DEV_RANGE || pl.key.mode == QK_DIRECT) {
       pl.key.mode = QK_HASH;
     }
@@ -2519,6 +2574,8 @@ extern "C" {
 int qm_agg_begin(qm_ctx *ctx, const qm_query *q, qm_agg **out) {
   if (!ctx || !q || !out) return set_err(ctx, QM_ERR_INVALID, "qm_agg_begin: bad arguments");
   *out = nullptr;
+  if (q->flags & QM_FLAG_DETERMINISTIC)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "deterministic float SUM runs through qm_query_run, batches and servers");
   qm_agg *a = new qm_agg();
   a->ctx = ctx;
   // deep copy (names live in a->strs; reserve so c_str() stays valid)
@@ -2711,6 +2768,62 @@ int qm_agg_partial_merge(qm_agg *a, const uint64_t *src, int64_t n_groups, int32
   }
   gt.groups_upper += (int64_t)st.groups_inserted;
   gt.rows_done = std::max(gt.rows_done, rows_end);
+  return QM_OK;
+}
+
+int qm_agg_partial_layout(const qm_agg *a, int32_t *row_words, int32_t *first_word) {
+  if (!a || !row_words || !first_word) return QM_ERR_INVALID;
+  if (!a->planned) return set_err(a->ctx, QM_ERR_INVALID, "partial layout before the first push");
+  *row_words = a->gt.ex.stride + 1;
+  *first_word = a->gt.pl.agg.w_first >= 0 ? 2 + a->gt.pl.agg.w_first : -1;
+  return QM_OK;
+}
+
+int qm_agg_partial_begin(const qm_agg *src, qm_agg **out) {
+  if (!src || !out) return QM_ERR_INVALID;
+  *out = nullptr;
+  qm_ctx *ctx = src->ctx;
+  if (!src->planned) return set_err(ctx, QM_ERR_INVALID, "partial begin from an aggregation without a push");
+  cudaSetDevice(ctx->device);
+  qm_agg *a = nullptr;
+  int rc = qm_agg_begin(ctx, &src->q, &a);
+  if (rc) return rc;
+  a->gt.pl = src->gt.pl;
+  a->schema = src->schema;
+  if ((rc = setup_table(ctx, a->gt, 1, 0, true))) {
+    qm_agg_destroy(a);
+    return rc;
+  }
+  a->planned = true;
+  *out = a;
+  return QM_OK;
+}
+
+int qm_partial_partition(qm_ctx *ctx, const uint64_t *src, int64_t n_rows, int32_t row_words, int32_t parts,
+                         uint64_t *dst, int64_t *part_rows) {
+  if (!ctx || n_rows < 0 || (n_rows > 0 && (!src || !dst)) || row_words < 2 || parts < 1 || parts > 4096 ||
+      !part_rows)
+    return set_err(ctx, QM_ERR_INVALID, "qm_partial_partition: bad arguments");
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = ensure(ctx, ctx->counts, sizeof(unsigned long long) * 2 * parts)) ||
+      (rc = ensure_host(ctx, ctx->hout, sizeof(unsigned long long) * parts)))
+    return rc;
+  unsigned long long *cnt = (unsigned long long *)ctx->counts.p, *cur = cnt + parts;
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * parts, ctx->stream));
+  CK(qm_launch_partition_count(src, n_rows, row_words, parts, cnt, ctx->sm_count, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->hout.p, cnt, sizeof(unsigned long long) * parts, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<unsigned long long> start(parts);
+  unsigned long long acc = 0;
+  for (int p = 0; p < parts; p++) {
+    start[p] = acc;
+    part_rows[p] = (int64_t)((unsigned long long *)ctx->hout.p)[p];
+    acc += (unsigned long long)part_rows[p];
+  }
+  CK(cudaMemcpyAsync(cur, start.data(), sizeof(unsigned long long) * parts, cudaMemcpyHostToDevice, ctx->stream));
+  CK(qm_launch_partition_scatter(src, n_rows, row_words, parts, cur, dst, ctx->sm_count, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return QM_OK;
 }
 
@@ -2916,6 +3029,8 @@ extern "C" int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols,
   if (n_rows > 0xffffffffLL) return set_err(ctx, QM_ERR_UNSUPPORTED, "batches are limited to 2^32-1 rows");
   if (q->order_by || q->has_limit || q->offset)
     return set_err(ctx, QM_ERR_UNSUPPORTED, "ORDER BY / LIMIT / OFFSET run through qm_query_run");
+  if (q->flags & QM_FLAG_DETERMINISTIC)
+    return set_err(ctx, QM_ERR_UNSUPPORTED, "deterministic float SUM needs column statistics: qm_query_run");
   *out_groups = 0;
   // no group needs less than 8 bytes of scratch: a larger capacity cannot
   // fit, and bounding it here keeps the size arithmetic below from overflowing
@@ -3127,10 +3242,34 @@ struct OwnedQuery {  // holds pointers into itself: never copied or moved
 
 }  // namespace
 
+// One wave of a batched run: a contiguous slice [q0, q1) of the batch's
+// queries in wave order, with its own finalize buffers, so that its packed
+// results cross the host link while later waves scan.
+struct BatchWave {
+  int q0 = 0, q1 = 0;     // positions in the batch's wave order
+  int64_t slots = 0;      // group-table slots of its queries
+  int64_t bm_words = 0;   // words of its first-row bitmap
+  qm_batch_dev dev{};
+  DevBuf d_slot0, d_chunks, d_bitmap, d_popc, d_ranks, d_temp, d_meta, d_packed, d_nullbytes;
+  HostBuf h_meta;         // pinned: the wave's layout, copied back with its work
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaEvent_t done = nullptr;  // the wave's device work ended (results packed, layout copied)
+  std::shared_ptr<SharedPinned> host;  // its packed results in host memory
+  ~BatchWave() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (done) cudaEventDestroy(done);
+    DevBuf *bufs[] = {&d_slot0, &d_chunks, &d_bitmap, &d_popc, &d_ranks, &d_temp, &d_meta, &d_packed, &d_nullbytes};
+    for (DevBuf *b : bufs) release(*b);
+    if (h_meta.p) cudaFreeHost(h_meta.p);
+  }
+};
+
 struct qm_batch {
   qm_ctx *ctx = nullptr;
   int n = 0;
-  std::vector<GroupTable> gts;
+  std::vector<GroupTable> gts;  // per query, in the caller's order
   std::vector<qm_bq> bq;
   std::vector<int64_t> rows;
   std::vector<int64_t> est;  // planner's group estimate per query
@@ -3141,59 +3280,127 @@ struct qm_batch {
     size_t smem;
   };
   std::vector<Launch> launches;       // mode 1: one specialised scan per query
-  std::vector<int> launch_order;      // largest first
+  std::vector<int> order;             // wave position -> query
+  std::vector<int> pos;               // query -> wave position
+  std::vector<int> wave_of;           // wave position -> wave
+  std::vector<std::unique_ptr<BatchWave>> waves;
+  int waves_req = 0;                  // waves asked for (0: by batch size)
   std::vector<cudaStream_t> side;     // mode 1: branches the launches spread over
   std::vector<cudaEvent_t> side_ev;
   cudaEvent_t fork_ev = nullptr;
+  cudaStream_t stream = nullptr;      // the batch's work (null: the context's stream)
+  cudaStream_t copy_stream = nullptr; // result copies
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+  std::vector<cudaEvent_t> q_ev;      // per-query copies landed (per-request completion)
   int mode = 1;  // 0: one persistent kernel over (query, chunk) work items; 1: per-query launches
   std::vector<const qm_table *> tabs;  // query i's table and a copy of the
   std::vector<std::unique_ptr<OwnedQuery>> queries;  // query, to rerun it alone
-  DevBuf arena, d_bq, d_slot0, d_chunks, d_counter, d_status, d_bitmap, d_popc, d_ranks, d_temp, d_meta,
-      d_packed, d_nullbytes;
-  HostBuf h_meta, h_status;
-  qm_batch_dev dev{};
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
+  DevBuf arena, d_bq, d_counter, d_status;
+  HostBuf h_status;  // pinned, wave order
   int chunk_tiles = 512;
   int local_kb = 40;
   int bps = 0;
+  size_t scan_smem = 0;
+  int scan_blocks = 1;
+  int local_bytes = 0;
   float last_ms = 0;
   int64_t bytes_scanned = 0;
   int64_t total_rows = 0;
   ~qm_batch() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (graph) cudaGraphDestroy(graph);
+    waves.clear();
     for (cudaStream_t st : side) cudaStreamDestroy(st);
     for (cudaEvent_t ev : side_ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : q_ev) cudaEventDestroy(ev);
     if (fork_ev) cudaEventDestroy(fork_ev);
-    DevBuf *bufs[] = {&arena, &d_bq, &d_slot0, &d_chunks, &d_counter, &d_status, &d_bitmap, &d_popc, &d_ranks,
-                      &d_temp, &d_meta, &d_packed, &d_nullbytes};
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_end) cudaEventDestroy(ev_end);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    DevBuf *bufs[] = {&arena, &d_bq, &d_counter, &d_status};
     for (DevBuf *b : bufs) release(*b);
-    if (h_meta.p) cudaFreeHost(h_meta.p);
     if (h_status.p) cudaFreeHost(h_status.p);
   }
+  cudaStream_t st() const { return stream ? stream : ctx->stream; }
 };
 
 namespace {
 
 void drop_graph(qm_batch *b) {
-  if (b->gexec) cudaGraphExecDestroy(b->gexec);
-  if (b->graph) cudaGraphDestroy(b->graph);
-  b->gexec = nullptr;
-  b->graph = nullptr;
+  for (auto &w : b->waves) {
+    if (w->gexec) cudaGraphExecDestroy(w->gexec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    w->gexec = nullptr;
+    w->graph = nullptr;
+  }
 }
 
-// (Re)build chunks, table layout and device descriptors for the current knobs.
+// Result bytes of query i as planned (its group estimate, capped by rows).
+int64_t est_result_bytes(const qm_batch *b, int i) {
+  const qm_bq &q = b->bq[i];
+  const int64_t G = q.none ? 1 : std::min<int64_t>(std::max<int64_t>(b->est[i], 1), std::max<int64_t>(b->rows[i], 1));
+  int64_t w = 0;
+  for (int k = 0; k < q.outs.n_out; k++) w += q.width[k];
+  return G * w;
+}
+
+// Wave order and boundaries: queries whose results are large for the bytes
+// they scan first (their copies start early and overlap the rest), queries
+// with small results last (the copy after the last wave is short); waves of
+// about equal scanned bytes.
+void plan_waves(qm_batch *b) {
+  const int n = b->n;
+  int W = b->waves_req > 0 ? b->waves_req : std::max(1, std::min(8, n / 16));
+  W = std::max(1, std::min(W, n));
+  b->order.resize(n);
+  for (int i = 0; i < n; i++) b->order[i] = i;
+  std::vector<double> ratio(n);
+  std::vector<int64_t> sb(n);
+  int64_t total = 0;
+  for (int i = 0; i < n; i++) {
+    sb[i] = std::max<int64_t>(b->gts[i].pl.bytes_per_row * b->rows[i], 1) + 4096;
+    ratio[i] = (double)est_result_bytes(b, i) / (double)sb[i];
+    total += sb[i];
+  }
+  if (W > 1)
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return ratio[x] > ratio[y]; });
+  std::vector<int> cut;  // first wave position of each wave
+  cut.push_back(0);
+  int64_t acc = 0;
+  for (int j = 0; j < n; j++) {
+    acc += sb[b->order[j]];
+    const int w = (int)cut.size();
+    if (w < W && j + 1 < n && (double)acc >= (double)total * w / W) cut.push_back(j + 1);
+  }
+  cut.push_back(n);
+  const int nw = (int)cut.size() - 1;
+  while ((int)b->waves.size() > nw) b->waves.pop_back();
+  while ((int)b->waves.size() < nw) b->waves.emplace_back(new BatchWave());
+  b->pos.assign(n, 0);
+  b->wave_of.assign(n, 0);
+  for (int w = 0; w < nw; w++) {
+    BatchWave &wv = *b->waves[w];
+    wv.q0 = cut[w];
+    wv.q1 = cut[w + 1];
+    // largest query first inside a wave (the parallel branches finish together)
+    std::stable_sort(b->order.begin() + wv.q0, b->order.begin() + wv.q1,
+                     [&](int x, int y) { return b->rows[x] > b->rows[y]; });
+    for (int j = wv.q0; j < wv.q1; j++) b->wave_of[j] = w;
+  }
+  for (int j = 0; j < n; j++) b->pos[b->order[j]] = j;
+}
+
+// (Re)build waves, chunks, table layout and device descriptors for the
+// current knobs.
 int batch_layout(qm_batch *b) {
   qm_ctx *ctx = b->ctx;
   const int n = b->n;
+  cudaStream_t st = b->st();
   const size_t local_budget = (size_t)b->local_kb * 1024;
-  int64_t slots = 0, words = 0, bm_words = 0, packed_max = 0, nullbytes_max = 0;
-  std::vector<int64_t> slot0(n), table_off(n);
+  int64_t words = 0;
+  std::vector<int64_t> table_off(n);
   for (int i = 0; i < n; i++) {
     GroupTable &gt = b->gts[i];
     Exec &ex = gt.ex;
-    // block-local table within the batch's shared-memory budget
+    // block-local table within the batch's shared-memory budget (mode 0)
     const int64_t per_slot = (int64_t)gt.pl.agg.n_words * 8;
     if (ex.local_slots > 0) {
       int64_t need = (int64_t)ex.local_slots * (per_slot + (ex.local_hash ? 8 : 0));
@@ -3206,115 +3413,134 @@ int batch_layout(qm_batch *b) {
         ex.local_hash = 1;
       }
     }
-    slot0[i] = slots;
     table_off[i] = words;
-    slots += ex.total_slots;
     words += ex.total_slots * ex.stride;
-    qm_bq &q = b->bq[i];
-    q.bm_word0 = bm_words;
-    q.bm_words = b->rows[i] / 32 + 1;
-    bm_words += q.bm_words;
-    const int64_t gmax = q.none ? 1 : std::min<int64_t>(ex.total_slots, std::max<int64_t>(b->rows[i], 1));
-    packed_max += region_bytes(gmax, q);
-    for (int k = 0; k < q.outs.n_out; k++)
-      if (q.nullable[k]) nullbytes_max += (gmax + 15) & ~(int64_t)15;
   }
+  plan_waves(b);
   int rc;
   if ((rc = ensure(ctx, b->arena, (size_t)words * 8 + 64))) return rc;
   if ((rc = ensure(ctx, b->d_status, sizeof(qm_status) * n))) return rc;
+  if ((rc = ensure(ctx, b->d_bq, sizeof(qm_bq) * n))) return rc;
+  if ((rc = ensure(ctx, b->d_counter, sizeof(int) * (b->waves.size() + 1)))) return rc;
+  if ((rc = ensure_host(ctx, b->h_status, sizeof(qm_status) * n))) return rc;
+  std::vector<qm_bq> dbq(n);
   for (int i = 0; i < n; i++) {
     GroupTable &gt = b->gts[i];
     gt.table = (uint64_t *)b->arena.p + table_off[i];
     qm_bq &q = b->bq[i];
-    fill_args(gt, q.a, (qm_status *)b->d_status.p + i);
-    q.a.priv = 0;  // the batched kernel keeps one block-local copy
+    fill_args(gt, q.a, (qm_status *)b->d_status.p + b->pos[i]);
+    q.a.priv = 0;  // the persistent kernel keeps one block-local copy
     q.a.n = b->rows[i];
     q.a.sel = nullptr;
     q.a.row_offset = 0;
     memset(&q.a.stage, 0, sizeof q.a.stage);
   }
-  // chunks: each query's tiles cut into runs of chunk_tiles
-  std::vector<qm_chunk> chunks;
-  for (int i = 0; i < n; i++) {
-    const int64_t tiles = (b->rows[i] + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
-    for (int64_t t0 = 0; t0 < tiles; t0 += b->chunk_tiles) {
-      qm_chunk c;
-      c.q = i;
-      c.pad = 0;
-      c.tile0 = t0;
-      c.tile1 = std::min<int64_t>(tiles, t0 + b->chunk_tiles);
-      chunks.push_back(c);
-    }
-  }
-  // the largest local table of the batch sets the kernel's shared memory
+  // the largest local table of the batch sets the persistent kernel's shared memory
   int local_bytes = 0;
   for (int i = 0; i < n; i++) {
     const Exec &ex = b->gts[i].ex;
     if (ex.local_slots > 0)
       local_bytes = std::max<int>(local_bytes, ex.local_slots * (b->gts[i].pl.agg.n_words * 8 + (ex.local_hash ? 8 : 0)));
   }
-  size_t temp = 0;
-  CK(qm_batch_scan_temp_bytes(bm_words, &temp));
-  if ((rc = ensure(ctx, b->d_bq, sizeof(qm_bq) * n)) || (rc = ensure(ctx, b->d_slot0, sizeof(int64_t) * n)) ||
-      (rc = ensure(ctx, b->d_chunks, sizeof(qm_chunk) * std::max<size_t>(chunks.size(), 1))) ||
-      (rc = ensure(ctx, b->d_counter, 16)) || (rc = ensure(ctx, b->d_bitmap, sizeof(uint32_t) * (bm_words + 1))) ||
-      (rc = ensure(ctx, b->d_popc, sizeof(uint32_t) * (bm_words + 1))) ||
-      (rc = ensure(ctx, b->d_ranks, sizeof(uint64_t) * (bm_words + 1))) || (rc = ensure(ctx, b->d_temp, temp + 16)) ||
-      (rc = ensure(ctx, b->d_meta, sizeof(qm_batch_meta))) || (rc = ensure(ctx, b->d_packed, (size_t)packed_max + 64)) ||
-      (rc = ensure(ctx, b->d_nullbytes, (size_t)nullbytes_max + 64)) ||
-      (rc = ensure_host(ctx, b->h_meta, sizeof(qm_batch_meta))) || (rc = ensure_host(ctx, b->h_status, sizeof(qm_status) * n)))
-    return rc;
-  CK(cudaMemcpyAsync(b->d_bq.p, b->bq.data(), sizeof(qm_bq) * n, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(b->d_slot0.p, slot0.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
-  if (!chunks.empty())
-    CK(cudaMemcpyAsync(b->d_chunks.p, chunks.data(), sizeof(qm_chunk) * chunks.size(), cudaMemcpyHostToDevice,
-                       ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  qm_batch_dev &d = b->dev;
-  d.n = n;
-  d.sm_count = ctx->sm_count;
-  d.bq = (qm_bq *)b->d_bq.p;
-  d.slot0 = (int64_t *)b->d_slot0.p;
-  d.total_slots = slots;
-  d.chunks = (qm_chunk *)b->d_chunks.p;
-  d.n_chunks = (int)chunks.size();
-  d.counter = (int *)b->d_counter.p;
-  d.statuses = (qm_status *)b->d_status.p;
-  d.bitmap = (uint32_t *)b->d_bitmap.p;
-  d.bm_words = bm_words;
-  d.popc = (uint32_t *)b->d_popc.p;
-  d.ranks = (uint64_t *)b->d_ranks.p;
-  d.scan_temp = b->d_temp.p;
-  d.scan_temp_bytes = temp;
-  d.meta = (qm_batch_meta *)b->d_meta.p;
-  d.meta_host = (qm_batch_meta *)b->h_meta.p;
-  d.meta_bytes = sizeof(qm_batch_meta);
-  d.packed = (unsigned char *)b->d_packed.p;
-  d.nullbytes = (unsigned char *)b->d_nullbytes.p;
-  d.local_bytes = local_bytes;
-  d.scan_smem = qm_batch_smem_bytes(local_bytes);
+  b->local_bytes = local_bytes;
+  b->scan_smem = qm_batch_smem_bytes(local_bytes);
   int bps = 1;
   {
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    if (qm_batch_configure(d.scan_smem, &bps) != cudaSuccess) {
+    if (qm_batch_configure(b->scan_smem, &bps) != cudaSuccess) {
       cudaGetLastError();
-      return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", d.scan_smem);
+      return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", b->scan_smem);
     }
   }
   if (bps < 1) bps = 1;
   if (b->bps > 0 && b->bps < bps) bps = b->bps;
-  d.scan_blocks = std::max(1, std::min(ctx->sm_count * bps, d.n_chunks));
+  // per wave: slots, bitmap slices, chunks and finalize buffers
+  for (size_t w = 0; w < b->waves.size(); w++) {
+    BatchWave &wv = *b->waves[w];
+    std::vector<int64_t> slot0;
+    std::vector<qm_chunk> chunks;
+    int64_t slots = 0, bm_words = 0, packed_max = 0, nullbytes_max = 0;
+    for (int j = wv.q0; j < wv.q1; j++) {
+      const int i = b->order[j];
+      const Exec &ex = b->gts[i].ex;
+      qm_bq q = b->bq[i];
+      slot0.push_back(slots);
+      slots += ex.total_slots;
+      q.bm_word0 = bm_words;
+      q.bm_words = b->rows[i] / 32 + 1;
+      bm_words += q.bm_words;
+      const int64_t gmax = q.none ? 1 : std::min<int64_t>(ex.total_slots, std::max<int64_t>(b->rows[i], 1));
+      packed_max += region_bytes(gmax, q);
+      for (int k = 0; k < q.outs.n_out; k++)
+        if (q.nullable[k]) nullbytes_max += (gmax + 15) & ~(int64_t)15;
+      dbq[j] = q;
+      b->bq[i].bm_word0 = q.bm_word0;
+      b->bq[i].bm_words = q.bm_words;
+      const int64_t tiles = (b->rows[i] + QM_TILE_ROWS - 1) / QM_TILE_ROWS;
+      for (int64_t t0 = 0; t0 < tiles; t0 += b->chunk_tiles) {
+        qm_chunk c;
+        c.q = j - wv.q0;
+        c.pad = 0;
+        c.tile0 = t0;
+        c.tile1 = std::min<int64_t>(tiles, t0 + b->chunk_tiles);
+        chunks.push_back(c);
+      }
+    }
+    wv.slots = slots;
+    wv.bm_words = bm_words;
+    size_t temp = 0;
+    CK(qm_batch_scan_temp_bytes(bm_words, &temp));
+    if ((rc = ensure(ctx, wv.d_slot0, sizeof(int64_t) * slot0.size())) ||
+        (rc = ensure(ctx, wv.d_chunks, sizeof(qm_chunk) * std::max<size_t>(chunks.size(), 1))) ||
+        (rc = ensure(ctx, wv.d_bitmap, sizeof(uint32_t) * (bm_words + 1))) ||
+        (rc = ensure(ctx, wv.d_popc, sizeof(uint32_t) * (bm_words + 1))) ||
+        (rc = ensure(ctx, wv.d_ranks, sizeof(uint64_t) * (bm_words + 1))) || (rc = ensure(ctx, wv.d_temp, temp + 16)) ||
+        (rc = ensure(ctx, wv.d_meta, sizeof(qm_batch_meta))) ||
+        (rc = ensure(ctx, wv.d_packed, (size_t)packed_max + 64)) ||
+        (rc = ensure(ctx, wv.d_nullbytes, (size_t)nullbytes_max + 64)) ||
+        (rc = ensure_host(ctx, wv.h_meta, sizeof(qm_batch_meta))))
+      return rc;
+    CK(cudaMemcpyAsync(wv.d_slot0.p, slot0.data(), sizeof(int64_t) * slot0.size(), cudaMemcpyHostToDevice, st));
+    if (!chunks.empty())
+      CK(cudaMemcpyAsync(wv.d_chunks.p, chunks.data(), sizeof(qm_chunk) * chunks.size(), cudaMemcpyHostToDevice, st));
+    if (!wv.done) CK(cudaEventCreateWithFlags(&wv.done, cudaEventDisableTiming));
+    qm_batch_dev &d = wv.dev;
+    d.n = wv.q1 - wv.q0;
+    d.sm_count = ctx->sm_count;
+    d.bq = (qm_bq *)b->d_bq.p + wv.q0;
+    d.slot0 = (int64_t *)wv.d_slot0.p;
+    d.total_slots = slots;
+    d.chunks = (qm_chunk *)wv.d_chunks.p;
+    d.n_chunks = (int)chunks.size();
+    d.counter = (int *)b->d_counter.p + w;
+    d.statuses = (qm_status *)b->d_status.p + wv.q0;
+    d.bitmap = (uint32_t *)wv.d_bitmap.p;
+    d.bm_words = bm_words;
+    d.popc = (uint32_t *)wv.d_popc.p;
+    d.ranks = (uint64_t *)wv.d_ranks.p;
+    d.scan_temp = wv.d_temp.p;
+    d.scan_temp_bytes = temp;
+    d.meta = (qm_batch_meta *)wv.d_meta.p;
+    d.meta_host = (qm_batch_meta *)wv.h_meta.p;
+    d.meta_bytes = sizeof(qm_batch_meta);
+    d.packed = (unsigned char *)wv.d_packed.p;
+    d.nullbytes = (unsigned char *)wv.d_nullbytes.p;
+    d.local_bytes = local_bytes;
+    d.scan_smem = b->scan_smem;
+    d.scan_blocks = std::max(1, std::min(ctx->sm_count * bps, d.n_chunks));
+  }
+  CK(cudaMemcpyAsync(b->d_bq.p, dbq.data(), sizeof(qm_bq) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
   // mode 1: each query's own specialised scan, with the planner's block-local
   // layout, on one of several stream branches
   b->launches.resize(n);
-  b->launch_order.resize(n);
   for (int i = 0; i < n; i++) {
     GroupTable g;
     g.pl = b->gts[i].pl;
     g.ex = b->ex_plan[i];
     g.table = b->gts[i].table;
     qm_batch::Launch &L = b->launches[i];
-    fill_args(g, L.a, (qm_status *)b->d_status.p + i);
+    fill_args(g, L.a, (qm_status *)b->d_status.p + b->pos[i]);
     L.a.n = b->rows[i];
     L.a.sel = nullptr;
     L.a.row_offset = 0;
@@ -3322,46 +3548,204 @@ int batch_layout(qm_batch *b) {
     if (L.a.priv && L.a.n < PRIV_MIN_ROWS) L.a.priv = 0;
     L.smem = qm_scan_smem_bytes(g.ex.local_slots, g.ex.local_hash, g.pl.agg.n_words, 0, 0, L.a.priv);
     L.blocks = scan_blocks(ctx, L.smem, L.a.n, false);
-    b->launch_order[i] = i;
   }
-  std::sort(b->launch_order.begin(), b->launch_order.end(),
-            [&](int x, int y) { return b->rows[x] > b->rows[y]; });
   const int k = std::min(n, 16);
   while ((int)b->side.size() < k) {
-    cudaStream_t st;
+    cudaStream_t s2;
     cudaEvent_t ev;
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    b->side.push_back(st);
+    b->side.push_back(s2);
     b->side_ev.push_back(ev);
   }
   if (!b->fork_ev) CK(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+  if (!b->copy_stream) CK(cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking));
+  if (!b->ev_start) CK(cudaEventCreate(&b->ev_start));
+  if (!b->ev_end) CK(cudaEventCreate(&b->ev_end));
   drop_graph(b);
   return QM_OK;
 }
 
-// Issue the whole batched run on the context's stream (captured into the
-// batch's graph, or launched directly).
-int batch_launch(qm_batch *b) {
+// Issue one wave's device work on stream st: clear its tables and bitmaps,
+// scan its queries, rank / lay out / emit / pack their results and copy its
+// layout and statuses to pinned host memory.
+int wave_launch(qm_batch *b, BatchWave &wv, cudaStream_t st) {
   qm_ctx *ctx = b->ctx;
-  cudaStream_t st = ctx->stream;
   if (b->mode == 0) {
-    CK(qm_batch_launch_all(b->dev, st));
-    return QM_OK;
+    CK(qm_batch_launch_all(wv.dev, st));
+  } else {
+    CK(qm_batch_launch_init(wv.dev, st));
+    const int nq = wv.q1 - wv.q0;
+    const int k = std::min<int>(nq, (int)b->side.size());
+    CK(cudaEventRecord(b->fork_ev, st));
+    for (int j = 0; j < k; j++) CK(cudaStreamWaitEvent(b->side[j], b->fork_ev, 0));
+    for (int j = 0; j < nq; j++) {
+      const qm_batch::Launch &L = b->launches[b->order[wv.q0 + j]];
+      CK(qm_launch_scan(L.a, L.blocks, L.smem, b->side[j % k]));
+    }
+    for (int j = 0; j < k; j++) {
+      CK(cudaEventRecord(b->side_ev[j], b->side[j]));
+      CK(cudaStreamWaitEvent(st, b->side_ev[j], 0));
+    }
+    CK(qm_batch_launch_finalize(wv.dev, st));
   }
-  CK(qm_batch_launch_init(b->dev, st));
-  const int k = std::min<int>(b->n, (int)b->side.size());
-  CK(cudaEventRecord(b->fork_ev, st));
-  for (int j = 0; j < k; j++) CK(cudaStreamWaitEvent(b->side[j], b->fork_ev, 0));
-  for (int j = 0; j < b->n; j++) {
-    const qm_batch::Launch &L = b->launches[b->launch_order[j]];
-    CK(qm_launch_scan(L.a, L.blocks, L.smem, b->side[j % k]));
+  CK(cudaMemcpyAsync((qm_status *)b->h_status.p + wv.q0, wv.dev.statuses, sizeof(qm_status) * (wv.q1 - wv.q0),
+                     cudaMemcpyDeviceToHost, st));
+  return QM_OK;
+}
+
+// Issue every wave on the batch's stream (each through its captured graph,
+// or with plain launches when use_graph is false), each followed by its
+// `done` event.  Nothing waits here.
+int batch_issue(qm_batch *b, bool use_graph) {
+  qm_ctx *ctx = b->ctx;
+  cudaStream_t st = b->st();
+  CK(cudaEventRecord(b->ev_start, st));
+  for (auto &wp : b->waves) {
+    BatchWave &wv = *wp;
+    if (use_graph) {
+      if (!wv.gexec) {
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc = wave_launch(b, wv, st);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc || e != cudaSuccess) {
+          if (g) cudaGraphDestroy(g);
+          cudaGetLastError();
+          return rc ? rc : set_err(ctx, QM_ERR_CUDA, "capturing the batched launch: %s", cudaGetErrorString(e));
+        }
+        wv.graph = g;
+        CK(cudaGraphInstantiate(&wv.gexec, g, 0));
+      }
+      CK(cudaGraphLaunch(wv.gexec, st));
+    } else {
+      int rc = wave_launch(b, wv, st);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(wv.done, st));
   }
-  for (int j = 0; j < k; j++) {
-    CK(cudaEventRecord(b->side_ev[j], b->side[j]));
-    CK(cudaStreamWaitEvent(st, b->side_ev[j], 0));
+  return QM_OK;
+}
+
+// Query i's result from its wave's packed results in host memory.
+qm_result *batch_result(qm_batch *b, int i, const BatchWave &wv, const qm_status &s, float scan_ms) {
+  const int j = b->pos[i];
+  const qm_batch_meta *meta = (const qm_batch_meta *)wv.h_meta.p;
+  const qm_bq &qb = b->bq[i];
+  const Plan &pl = b->gts[i].pl;
+  const int64_t G = meta->groups[j - wv.q0];
+  const uint8_t *h = (const uint8_t *)wv.host->buf.p;
+  qm_result *R = new qm_result();
+  R->shared = wv.host;
+  R->n_rows = G;
+  int64_t off = meta->base[j - wv.q0];
+  for (int k = 0; k < qb.outs.n_out; k++) {
+    qm_result::Col c;
+    c.name = pl.meta[k].name;
+    c.dtype = qb.outs.o[k].dtype;
+    c.is_key = pl.meta[k].is_key;
+    c.bytes = (size_t)G * qb.width[k];
+    c.data = h + off;
+    off += ((int64_t)c.bytes + 15) & ~(int64_t)15;
+    if (qb.nullable[k]) {
+      c.nulls = h + off;
+      const size_t nb = (size_t)((G + 7) / 8);
+      for (size_t x = 0; x < nb && !c.has_nulls; x++) c.has_nulls = c.nulls[x] != 0;
+      off += ((G + 31) / 32 * 4 + 15) & ~(int64_t)15;
+    }
+    R->cols.push_back(std::move(c));
   }
-  CK(qm_batch_launch_finalize(b->dev, st));
+  R->stats.rows_scanned = b->rows[i];
+  R->stats.rows_selected = (int64_t)s.rows_selected;
+  R->stats.groups = G;
+  R->stats.bytes_scanned = pl.bytes_per_row * b->rows[i];
+  R->stats.scan_ms = scan_ms;
+  R->stats.strategy = b->gts[i].ex.strategy;
+  R->stats.launches = b->mode == 0 ? 8 : 7 + (wv.q1 - wv.q0);
+  return R;
+}
+
+// A query's device status as a code; overflowed tables and stale column
+// statistics are re-run alone (QM_ERR_CAPACITY), where both are repaired.
+int status_code(const qm_status &s) {
+  if (s.error == 0) return QM_OK;
+  return s.error == QM_DEV_OVERFLOW || s.error == QM_DEV_STALE ? QM_ERR_CAPACITY : QM_ERR_CUDA;
+}
+
+// Wait for each wave in turn and copy its packed results back on the copy
+// stream while later waves still run; then build one result per query.
+// With per_query, each query's region is copied by its own copy and
+// on_done(i, code, result) is called as soon as that copy has landed (the
+// results of one wave complete one by one); otherwise results[i] and
+// codes[i] are filled once every copy has landed.
+int batch_collect(qm_batch *b, qm_result **results, int *codes, bool per_query = false,
+                  const std::function<void(int, int, qm_result *)> &on_done = nullptr) {
+  qm_ctx *ctx = b->ctx;
+  const int n = b->n;
+  if (per_query && (int)b->q_ev.size() < n) {
+    while ((int)b->q_ev.size() < n) {
+      cudaEvent_t ev;
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      b->q_ev.push_back(ev);
+    }
+  }
+  const qm_status *stv = (const qm_status *)b->h_status.p;
+  for (auto &wp : b->waves) {
+    BatchWave &wv = *wp;
+    cudaError_t e = cudaEventSynchronize(wv.done);
+    if (e != cudaSuccess) return set_err(ctx, QM_ERR_CUDA, "batched run: %s", cudaGetErrorString(e));
+    const qm_batch_meta *meta = (const qm_batch_meta *)wv.h_meta.p;
+    const size_t total = (size_t)meta->total;
+    auto holder = std::make_shared<SharedPinned>();
+    holder->pool = ctx->pool;
+    if (!ctx->pool->acquire(total + 16, holder->buf)) return set_err(ctx, QM_ERR_OOM, "pinned batch results");
+    wv.host = holder;
+    CK(cudaStreamWaitEvent(b->copy_stream, wv.done, 0));
+    if (!per_query) {
+      if (total)
+        CK(cudaMemcpyAsync(holder->buf.p, wv.dev.packed, total, cudaMemcpyDeviceToHost, b->copy_stream));
+      continue;
+    }
+    for (int j = wv.q0; j < wv.q1; j++) {
+      const int64_t base = meta->base[j - wv.q0], bytes = meta->bytes[j - wv.q0];
+      if (bytes > 0)
+        CK(cudaMemcpyAsync((char *)holder->buf.p + base, wv.dev.packed + base, (size_t)bytes, cudaMemcpyDeviceToHost,
+                           b->copy_stream));
+      CK(cudaEventRecord(b->q_ev[j], b->copy_stream));
+    }
+  }
+  CK(cudaEventRecord(b->ev_end, b->copy_stream));
+  if (per_query) {
+    for (auto &wp : b->waves) {
+      BatchWave &wv = *wp;
+      for (int j = wv.q0; j < wv.q1; j++) {
+        cudaError_t e = cudaEventSynchronize(b->q_ev[j]);
+        if (e != cudaSuccess) return set_err(ctx, QM_ERR_CUDA, "batched results: %s", cudaGetErrorString(e));
+        const int i = b->order[j];
+        const int code = status_code(stv[j]);
+        qm_result *R = code == QM_OK ? batch_result(b, i, wv, stv[j], 0.f) : nullptr;
+        if (results) results[i] = R;
+        if (codes) codes[i] = code;
+        if (on_done) on_done(i, code, R);
+      }
+    }
+  }
+  cudaError_t e = cudaEventSynchronize(b->ev_end);
+  if (e != cudaSuccess) return set_err(ctx, QM_ERR_CUDA, "batched results: %s", cudaGetErrorString(e));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, b->ev_start, b->ev_end);
+  b->last_ms = ms;
+  if (!per_query) {
+    for (int j = 0; j < n; j++) {
+      const int i = b->order[j];
+      const BatchWave &wv = *b->waves[b->wave_of[j]];
+      codes[i] = status_code(stv[j]);
+      results[i] = codes[i] == QM_OK ? batch_result(b, i, wv, stv[j], ms) : nullptr;
+      if (results[i]) results[i]->stats.device_ms = ms;
+    }
+  }
+  // the results hold the host buffers now (they return to the pool with them)
+  for (auto &wp : b->waves) wp->host.reset();
   return QM_OK;
 }
 
@@ -3438,97 +3822,6 @@ int64_t batch_query_bytes(const qm_batch *b, int i) {
   return table + res + b->rows[i] / 8 * 3 + 4096;
 }
 
-// Run the laid-out batch (through its captured graph, or with plain
-// launches when use_graph is false) and build one result per query.
-// codes[i] receives each query's status; results[i] is null where it failed.
-int batch_execute(qm_batch *b, qm_result **results, int *codes, bool use_graph) {
-  qm_ctx *ctx = b->ctx;
-  cudaSetDevice(ctx->device);
-  if (use_graph && !b->gexec) {
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = batch_launch(b);
-    cudaError_t e2 = rc ? cudaSuccess
-                        : cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n,
-                                          cudaMemcpyDeviceToHost, ctx->stream);
-    cudaGraph_t g = nullptr;
-    cudaError_t e3 = cudaStreamEndCapture(ctx->stream, &g);
-    if (rc || e2 != cudaSuccess || e3 != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      cudaGetLastError();
-      return set_err(ctx, QM_ERR_CUDA, "capturing the batched launch: %s",
-                     cudaGetErrorString(e2 != cudaSuccess ? e2 : e3));
-    }
-    b->graph = g;
-    CK(cudaGraphInstantiate(&b->gexec, g, 0));
-  }
-  CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  if (use_graph) {
-    CK(cudaGraphLaunch(b->gexec, ctx->stream));
-  } else {
-    int rc = batch_launch(b);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(b->h_status.p, b->dev.statuses, sizeof(qm_status) * b->n, cudaMemcpyDeviceToHost,
-                       ctx->stream));
-  }
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  float ms = 0;
-  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  const qm_status *st = (const qm_status *)b->h_status.p;
-  for (int i = 0; i < b->n; i++) {
-    results[i] = nullptr;
-    codes[i] = st[i].error == 0 ? QM_OK : (st[i].error == QM_DEV_OVERFLOW ? QM_ERR_CAPACITY : QM_ERR_CUDA);
-  }
-  const qm_batch_meta *meta = (const qm_batch_meta *)b->h_meta.p;
-  auto holder = std::make_shared<SharedPinned>();
-  holder->pool = ctx->pool;
-  const size_t total = (size_t)meta->total;
-  if (!ctx->pool->acquire(total + 16, holder->buf)) return set_err(ctx, QM_ERR_OOM, "pinned batch results");
-  if (total) CK(cudaMemcpyAsync(holder->buf.p, b->dev.packed, total, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  float ms2 = 0;
-  cudaEventElapsedTime(&ms2, ctx->ev0, ctx->ev1);
-  b->last_ms = ms2;
-  const uint8_t *h = (const uint8_t *)holder->buf.p;
-  for (int i = 0; i < b->n; i++) {
-    if (codes[i] != QM_OK) continue;
-    const qm_bq &qb = b->bq[i];
-    const Plan &pl = b->gts[i].pl;
-    const int64_t G = meta->groups[i];
-    qm_result *R = new qm_result();
-    R->shared = holder;
-    R->n_rows = G;
-    int64_t off = meta->base[i];
-    for (int k = 0; k < qb.outs.n_out; k++) {
-      qm_result::Col c;
-      c.name = pl.meta[k].name;
-      c.dtype = qb.outs.o[k].dtype;
-      c.is_key = pl.meta[k].is_key;
-      c.bytes = (size_t)G * qb.width[k];
-      c.data = h + off;
-      off += ((int64_t)c.bytes + 15) & ~(int64_t)15;
-      if (qb.nullable[k]) {
-        c.nulls = h + off;
-        const size_t nb = (size_t)((G + 7) / 8);
-        for (size_t x = 0; x < nb && !c.has_nulls; x++) c.has_nulls = c.nulls[x] != 0;
-        off += ((G + 31) / 32 * 4 + 15) & ~(int64_t)15;
-      }
-      R->cols.push_back(std::move(c));
-    }
-    R->stats.rows_scanned = b->rows[i];
-    R->stats.rows_selected = (int64_t)st[i].rows_selected;
-    R->stats.groups = G;
-    R->stats.bytes_scanned = b->gts[i].pl.bytes_per_row * b->rows[i];
-    R->stats.device_ms = ms2;
-    R->stats.scan_ms = ms;
-    R->stats.strategy = b->gts[i].ex.strategy;
-    R->stats.launches = 9;
-    results[i] = R;
-  }
-  return QM_OK;
-}
-
 }  // namespace
 
 extern "C" {
@@ -3578,11 +3871,30 @@ int qm_batch_set_tuning(qm_batch *b, int32_t chunk_tiles, int32_t local_kb, int3
   return batch_layout(b);
 }
 
+int qm_batch_set_waves(qm_batch *b, int32_t waves) {
+  if (!b || waves < 0) return QM_ERR_INVALID;
+  cudaSetDevice(b->ctx->device);
+  b->waves_req = waves;
+  for (int i = 0; i < b->n; i++) choose_layout(b->gts[i].pl, b->est[i], b->gts[i].ex, b->ctx->tuning);
+  return batch_layout(b);
+}
+
 int qm_batch_run(qm_batch *b, qm_result **results) {
   if (!b || !results) return QM_ERR_INVALID;
+  cudaSetDevice(b->ctx->device);
   std::vector<int> codes(b->n, QM_OK);
-  int rc = batch_execute(b, results, codes.data(), true);
-  if (rc) return rc;
+  for (int i = 0; i < b->n; i++) results[i] = nullptr;
+  int rc = batch_issue(b, true);
+  if (!rc) rc = batch_collect(b, results, codes.data());
+  if (rc) {
+    cudaStreamSynchronize(b->st());
+    cudaStreamSynchronize(b->copy_stream);
+    for (int k = 0; k < b->n; k++) {
+      delete results[k];
+      results[k] = nullptr;
+    }
+    return rc;
+  }
   for (int i = 0; i < b->n; i++)
     if (codes[i] == QM_ERR_CAPACITY) {
       // more groups than the batched table was sized for: this query alone,
@@ -3596,7 +3908,7 @@ int qm_batch_run(qm_batch *b, qm_result **results) {
         results[k] = nullptr;
       }
       return set_err(b->ctx, codes[i], "query %d of the batch: device status %d (group estimate too small)", i,
-                     ((const qm_status *)b->h_status.p)[i].error);
+                     ((const qm_status *)b->h_status.p)[b->pos[i]].error);
     }
   return QM_OK;
 }
@@ -3606,14 +3918,19 @@ int qm_batch_stats(const qm_batch *b, double *device_ms, int64_t *rows, int64_t 
   if (device_ms) *device_ms = b->last_ms;
   if (rows) *rows = b->total_rows;
   if (bytes) *bytes = b->bytes_scanned;
-  if (chunks) *chunks = b->dev.n_chunks;
+  if (chunks) {
+    int c = 0;
+    for (auto &w : b->waves) c += w->dev.n_chunks;
+    *chunks = c;
+  }
   return QM_OK;
 }
 
 int qm_batch_destroy(qm_batch *b) {
   if (!b) return QM_OK;
   cudaSetDevice(b->ctx->device);
-  cudaStreamSynchronize(b->ctx->stream);
+  cudaStreamSynchronize(b->st());
+  if (b->copy_stream) cudaStreamSynchronize(b->copy_stream);
   delete b;
   return QM_OK;
 }

@@ -45,6 +45,48 @@ __global__ void qm_export_partial(const uint64_t *t, int stride, const uint32_t 
   }
 }
 
+// Key-partitioned exchange of partial rows: the part of a row is the hash of
+// its key word modulo the part count (rows of a special key go to part 0),
+// so every rank's rows of one group meet on one rank.
+__device__ __forceinline__ int partial_part(const uint64_t *row, int parts) {
+  return row[1] != 0 ? 0 : (int)(fmix64(row[0] ^ 0x9e3779b97f4a7c15ULL) % (uint64_t)parts);
+}
+
+__global__ void qm_partition_count(const uint64_t *src, int64_t n, int rw, int parts, unsigned long long *counts) {
+  extern __shared__ unsigned long long hist[];
+  for (int p = threadIdx.x; p < parts; p += blockDim.x) hist[p] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&hist[partial_part(src + i * rw, parts)], 1ULL);
+  __syncthreads();
+  for (int p = threadIdx.x; p < parts; p += blockDim.x)
+    if (hist[p]) atomicAdd(&counts[p], hist[p]);
+}
+
+// Rows to their part's region: lanes of a warp bound for the same part take
+// consecutive places with one atomic (the order inside a part is free: the
+// merge does not depend on it).
+__global__ void qm_partition_scatter(const uint64_t *src, int64_t n, int rw, int parts,
+                                     unsigned long long *cursor, uint64_t *dst) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    const bool live = i < n;
+    const unsigned act = __ballot_sync(QM_FULL, live);
+    if (!live) continue;
+    const int p = partial_part(src + i * rw, parts);
+    const unsigned peers = __match_any_sync(act, p);
+    const int leader = __ffs(peers) - 1;
+    unsigned long long at = 0;
+    if (lane == leader) at = atomicAdd(&cursor[p], (unsigned long long)__popc(peers));
+    at = __shfl_sync(peers, at, leader) + __popc(peers & ((1u << lane) - 1));
+    const uint64_t *r = src + i * rw;
+    uint64_t *o = dst + (int64_t)at * rw;
+    for (int k = 0; k < rw; ++k) o[k] = r[k];
+  }
+}
+
 // Fold partial rows into the group table (slots found / claimed as in the
 // scan); integer sums are 128-bit, float sums compensated (TwoSum).
 __global__ void qm_merge_partial(const __grid_constant__ qm_scan_args a, const uint64_t *src, int64_t n) {
@@ -77,7 +119,14 @@ __global__ void qm_merge_partial(const __grid_constant__ qm_scan_args a, const u
           }
           break;
         case QA_FSUM:
-          fsum_add(g0, g1, __longlong_as_double((long long)v0), __longlong_as_double((long long)v[ac.word + 1]));
+          if (A.vcol[ac.vcol].flags & VF_FIXED) {
+            if (v0 || v[ac.word + 1]) add128(g0, g1, v0, (int64_t)v[ac.word + 1]);
+          } else {
+            fsum_add(g0, g1, __longlong_as_double((long long)v0), __longlong_as_double((long long)v[ac.word + 1]));
+          }
+          break;
+        case QA_FNF:
+          if (v0) atomicOr(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
           break;
         case QA_IMIN:
         case QA_FMIN:
@@ -1143,6 +1192,22 @@ cudaError_t qm_launch_export_partial(const uint64_t *t, int stride, const uint32
   if (G <= 0) return cudaSuccess;
   const int blocks = (int)std::min<int64_t>((G + 255) / 256, (int64_t)sm_count * 8);
   qm_export_partial<<<blocks, 256, 0, st>>>(t, stride, slots, G, n_slots, key_mode, A, row_offset, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_partition_count(const uint64_t *src, int64_t n, int rw, int parts, unsigned long long *counts,
+                                      int sm_count, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 4);
+  qm_partition_count<<<blocks, 256, parts * sizeof(unsigned long long), st>>>(src, n, rw, parts, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_partition_scatter(const uint64_t *src, int64_t n, int rw, int parts, unsigned long long *cursor,
+                                        uint64_t *dst, int sm_count, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 8);
+  qm_partition_scatter<<<blocks, 256, 0, st>>>(src, n, rw, parts, cursor, dst);
   return cudaGetLastError();
 }
 

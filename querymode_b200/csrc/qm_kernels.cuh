@@ -592,6 +592,66 @@ __device__ __forceinline__ void two_sum_acc(double &s, double &c, double x) {
   s = t;
 }
 
+// ---- fixed-point float sums (VF_FIXED) -------------------------------------
+// A finite x as round(x / 2^fxe) (ties to even), a 128-bit two's-complement
+// integer.  Planning keeps |x| < 2^(fxe + 126), so the value fits; sums of
+// these integers are exact and do not depend on the order of the adds.
+__device__ __forceinline__ void fx_parts(double x, int fxe, uint64_t &lo, int64_t &hi) {
+  const uint64_t b = (uint64_t)__double_as_longlong(x);
+  const int ex = (int)((b >> 52) & 0x7ff);
+  uint64_t m = b & ((1ULL << 52) - 1);
+  int e2 = -1074;  // zero or subnormal: m * 2^-1074
+  if (ex != 0) {
+    m |= 1ULL << 52;
+    e2 = ex - 1075;
+  }
+  const int sh = e2 - fxe;  // x = m * 2^sh units
+  unsigned __int128 v = 0;
+  if (m != 0) {
+    if (sh >= 0) {
+      v = (unsigned __int128)m << sh;
+    } else if (sh > -64) {
+      const int r = -sh;
+      uint64_t q = m >> r;
+      const uint64_t rem = m & ((1ULL << r) - 1), half = 1ULL << (r - 1);
+      if (rem > half || (rem == half && (q & 1))) q++;
+      v = q;
+    }
+  }
+  if (b >> 63) v = (unsigned __int128)0 - v;
+  lo = (uint64_t)v;
+  hi = (int64_t)(uint64_t)(v >> 64);
+}
+
+// One cell of a fixed-point SUM column: its integer value, or its
+// non-finite bit (NaN 1, +Infinity 2, -Infinity 4); `stale` when the cell is
+// beyond the planned range.
+__device__ __forceinline__ void fx_cell(const qm_vcol &vc, double x, uint64_t &lo, int64_t &hi, uint32_t &nf,
+                                        bool &stale) {
+  lo = 0;
+  hi = 0;
+  nf = 0;
+  if (isnan(x)) {
+    nf = 1;
+  } else if (isinf(x)) {
+    nf = x > 0 ? 2u : 4u;
+  } else if (fabs(x) >= vc.fx_max) {
+    stale = true;
+  } else {
+    fx_parts(x, vc.fx_exp, lo, hi);
+  }
+}
+
+// A fixed-point sum's value: NaN if a NaN or both infinities were seen, else
+// the infinity seen, else the integer scaled back (rounded once, to nearest).
+__device__ __forceinline__ double i128_to_f64(uint64_t lo, int64_t hi);
+__device__ __forceinline__ double fx_value(uint64_t lo, int64_t hi, uint64_t nf, int fxe) {
+  if ((nf & 1) || (nf & 6) == 6) return __longlong_as_double(0x7ff8000000000000LL);
+  if (nf & 2) return __longlong_as_double(0x7ff0000000000000LL);
+  if (nf & 4) return __longlong_as_double((long long)0xfff0000000000000ULL);
+  return ldexp(i128_to_f64(lo, hi), fxe);
+}
+
 __device__ __forceinline__ uint64_t pick(const uint64_t (&v)[QM_MAX_VCOLS], int i) {
   uint64_t r = 0;
 #pragma unroll
@@ -718,7 +778,8 @@ __device__ __forceinline__ T group_reduce(T v, unsigned act, unsigned peers, int
 // iters = (largest peer group in act) - 1.
 __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local, unsigned act,
                                           unsigned peers, int iters, int lane, uint64_t grow,
-                                          const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull, bool plain = false) {
+                                          const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull, bool plain = false,
+                                          qm_status *st = nullptr) {
   const bool full = peers == QM_FULL;
   auto umin = [](uint64_t x, uint64_t y) { return min(x, y); };
   auto imin = [](int64_t x, int64_t y) { return min(x, y); };
@@ -786,7 +847,54 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
       }
       case QA_FSUM: {
         const double v = valid ? __longlong_as_double((long long)raw) : 0.0;
-        const double split = A.vcol[ac.vcol].split;
+        const qm_vcol &fv = A.vcol[ac.vcol];
+        if (fv.flags & VF_FIXED) {
+          uint64_t lo;
+          int64_t hi;
+          uint32_t nf;
+          bool stale = false;
+          fx_cell(fv, v, lo, hi, nf, stale);
+          if (stale && st) set_error(st, QM_DEV_STALE);
+          if (full) {
+            nf = warp_allreduce(nf, [](uint32_t x, uint32_t y) { return x | y; });
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+              const uint64_t xl = __shfl_xor_sync(QM_FULL, lo, o);
+              const int64_t xh = __shfl_xor_sync(QM_FULL, hi, o);
+              const uint64_t nlo = lo + xl;
+              hi += xh + (nlo < lo ? 1 : 0);
+              lo = nlo;
+            }
+          } else {
+            const uint64_t lo0 = lo;
+            const int64_t hi0 = hi;
+            const uint32_t nf0 = nf;
+            unsigned rem = peers & ~(1u << lane);
+            for (int it = 0; it < iters; ++it) {
+              const int src = rem ? __ffs(rem) - 1 : lane;
+              const uint64_t xl = __shfl_sync(act, lo0, src);
+              const int64_t xh = __shfl_sync(act, hi0, src);
+              const uint32_t xn = __shfl_sync(act, nf0, src);
+              if (rem) {
+                const uint64_t nlo = lo + xl;
+                hi += xh + (nlo < lo ? 1 : 0);
+                lo = nlo;
+                nf |= xn;
+                rem &= rem - 1;
+              }
+            }
+          }
+          if (tp) {
+            if (lo != 0 || hi != 0) acc_add128(w0, w1, lo, hi, plain);
+            if (nf) {
+              uint64_t *wn = tp + (int64_t)fv.w_nf * ws;
+              if (plain) *wn |= nf;
+              else atomicOr(reinterpret_cast<unsigned long long *>(wn), (unsigned long long)nf);
+            }
+          }
+          break;
+        }
+        const double split = fv.split;
         if (split != 0.0) {
           double h, l;
           split_parts(v, split, h, l);
@@ -868,7 +976,8 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
 #endif
 template <int NV = QM_NV_ANY>
 __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
-                                        uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull) {
+                                        uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull,
+                                        qm_status *st = nullptr) {
   // In the global table, the FIRST word and the MIN / MAX words of the first
   // two value columns are read up front, in one L2 round trip; the atomics
   // then go out only where the row beats the word read.  A word only moves
@@ -927,8 +1036,20 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
       const double d = __longlong_as_double((long long)vb[c]);
       if (f & VF_SUM) {
         uint64_t *w0 = tp + (int64_t)vc.w_sum * ws;
-        if (vc.split != 0.0) split_add(w0, w0 + ws, d, vc.split);
-        else fsum_add(w0, w0 + ws, d, 0.0);
+        if (f & VF_FIXED) {
+          uint64_t lo;
+          int64_t hi;
+          uint32_t nf;
+          bool stale = false;
+          fx_cell(vc, d, lo, hi, nf, stale);
+          if (stale && st) set_error(st, QM_DEV_STALE);
+          if (lo != 0 || hi != 0) add128(w0, w0 + ws, lo, hi);
+          if (nf) atomicOr(reinterpret_cast<unsigned long long *>(tp + (int64_t)vc.w_nf * ws), (unsigned long long)nf);
+        } else if (vc.split != 0.0) {
+          split_add(w0, w0 + ws, d, vc.split);
+        } else {
+          fsum_add(w0, w0 + ws, d, 0.0);
+        }
       }
       if ((f & (VF_MIN | VF_MAX)) && !isnan(d)) {  // NaN never wins '<' / '>'
         const int64_t o = f2ord(d == 0.0 ? 0.0 : d);
@@ -948,7 +1069,7 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
 template <int NV = QM_NV_ANY>
 __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp, int L, unsigned lmask, unsigned peers,
                                                int lane, uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS],
-                                               uint32_t vnull, uint64_t *scr) {
+                                               uint32_t vnull, uint64_t *scr, qm_status *st = nullptr) {
   const bool leader = lane == __ffs(peers) - 1;
   if (leader) atomicAdd(reinterpret_cast<unsigned long long *>(tp + (int64_t)A.w_count * L), (unsigned long long)__popc(peers));
   if (A.w_first >= 0) min_u64(tp + (int64_t)A.w_first * L, grow);
@@ -984,6 +1105,30 @@ __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp
           } else if (lo != 0) {
             atomicAdd(reinterpret_cast<unsigned long long *>(w0), (unsigned long long)lo);  // int32 cells: fits
           }
+        }
+        __syncwarp(lmask);
+      } else if (f & VF_FIXED) {
+        const double d = valid ? __longlong_as_double((long long)raw) : 0.0;
+        uint64_t lo;
+        int64_t hi;
+        uint32_t nf;
+        bool stale = false;
+        fx_cell(vc, d, lo, hi, nf, stale);
+        if (stale && st) set_error(st, QM_DEV_STALE);
+        if (nf) atomicOr(reinterpret_cast<unsigned long long *>(tp + (int64_t)vc.w_nf * L), (unsigned long long)nf);
+        scr[lane] = lo;
+        scr[32 + lane] = (uint64_t)hi;
+        __syncwarp(lmask);
+        if (leader) {
+          uint64_t slo = 0;
+          int64_t shi = 0;
+          for (unsigned m = peers; m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            const uint64_t nlo = slo + scr[src];
+            shi += (int64_t)scr[32 + src] + (nlo < slo ? 1 : 0);
+            slo = nlo;
+          }
+          if (slo != 0 || shi != 0) add128(w0, w0 + L, slo, shi);
         }
         __syncwarp(lmask);
       } else {
@@ -1070,8 +1215,14 @@ __device__ __forceinline__ void merge_local(const qm_aggspec &A, const uint64_t 
         else if (v0 && ac.narrow) atomicAdd(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
         else if (v0) add128(g0, g1, v0, (int64_t)v0 < 0 ? -1 : 0);
         break;
+      case QA_FNF:
+        if (v0) atomicOr(reinterpret_cast<unsigned long long *>(g0), (unsigned long long)v0);
+        break;
       case QA_FSUM:
-        if (A.vcol[ac.vcol].split != 0.0) {
+        if (A.vcol[ac.vcol].flags & VF_FIXED) {
+          const uint64_t v1 = lp[(int64_t)(ac.word + 1) * L];
+          if (v0 || v1) add128(g0, g1, v0, (int64_t)v1);
+        } else if (A.vcol[ac.vcol].split != 0.0) {
           const double h = __longlong_as_double((long long)v0);
           const double l = __longlong_as_double((long long)lp[(int64_t)(ac.word + 1) * L]);
           if (h != 0.0 || isnan(h)) atomicAdd(reinterpret_cast<double *>(g0), h);
@@ -1109,8 +1260,11 @@ __device__ __forceinline__ void merge_plain(const qm_aggspec &A, uint64_t *dst, 
         if (ac.wide) acc_add128(dst + w0, dst + w1, src[w0], (int64_t)src[w1], true);
         else dst[w0] += src[w0];
         break;
+      case QA_FNF: dst[w0] |= src[w0]; break;
       case QA_FSUM:
-        if (A.vcol[ac.vcol].split != 0.0) {
+        if (A.vcol[ac.vcol].flags & VF_FIXED) {
+          acc_add128(dst + w0, dst + w1, src[w0], (int64_t)src[w1], true);
+        } else if (A.vcol[ac.vcol].split != 0.0) {
           acc_add_f64(dst + w0, __longlong_as_double((long long)src[w0]), true);
           acc_add_f64(dst + w1, __longlong_as_double((long long)src[w1]), true);
         } else {
@@ -1164,7 +1318,7 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
       }
     }
     const int iters = (int)__reduce_max_sync(act, (unsigned)__popc(peers)) - 1;
-    apply_row(A, tp, ws, local, act, peers, iters, lane, grow, vb, vnull, local && a.priv);
+    apply_row(A, tp, ws, local, act, peers, iters, lane, grow, vb, vnull, local && a.priv, a.status);
     return;
   }
   uint64_t grow = 0, key = 0;
@@ -1187,11 +1341,11 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
   if (loc) peers = __match_any_sync(lmask, ls);
   const bool merge = __any_sync(QM_FULL, (peers & (peers - 1)) != 0);
   if (loc) {
-    if (merge) agg_row_merged<NV>(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr);
-    else agg_row<NV>(A, lw + ls, L, true, grow, vb, vnull);
+    if (merge) agg_row_merged<NV>(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr, a.status);
+    else agg_row<NV>(A, lw + ls, L, true, grow, vb, vnull, a.status);
   } else if (active && !(L > 0 && !a.local_hash)) {
     const int64_t gs = global_slot(a, key, special);
-    if (gs >= 0) agg_row<NV>(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull);
+    if (gs >= 0) agg_row<NV>(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull, a.status);
   }
 }
 
@@ -1291,7 +1445,8 @@ __device__ __forceinline__ void emit_group(const uint64_t *t, int stride, uint64
     switch (o.kind) {
       case QO_SUM_F:
       case QO_AVG_F: {
-        double s2 = __longlong_as_double((long long)w[o.word]) + __longlong_as_double((long long)w[o.word + 1]);
+        double s2 = o.fixed ? fx_value(w[o.word], (int64_t)w[o.word + 1], w[o.nf_word], o.fx_exp)
+                            : __longlong_as_double((long long)w[o.word]) + __longlong_as_double((long long)w[o.word + 1]);
         reinterpret_cast<double *>(col)[i] = o.kind == QO_SUM_F ? s2 : s2 / (double)nn;
         break;
       }

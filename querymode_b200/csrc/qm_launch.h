@@ -52,6 +52,12 @@ cudaError_t qm_launch_export_partial(const uint64_t *t, int stride, const uint32
                                      cudaStream_t st);
 cudaError_t qm_launch_merge_partial(const qm_scan_args &a, const uint64_t *src, int64_t n, int sm_count,
                                     cudaStream_t st);
+// Partial rows by key-hash part: per-part counts, then the rows into their
+// parts' regions (cursor: each part's first row, advanced by the scatter).
+cudaError_t qm_launch_partition_count(const uint64_t *src, int64_t n, int rw, int parts, unsigned long long *counts,
+                                      int sm_count, cudaStream_t st);
+cudaError_t qm_launch_partition_scatter(const uint64_t *src, int64_t n, int rw, int parts, unsigned long long *cursor,
+                                        uint64_t *dst, int sm_count, cudaStream_t st);
 // First-seen ranking of the occupied slots through a row bitmap and its
 // prefix popcount (ranks[words] = number of groups), then the emit by rank.
 cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,

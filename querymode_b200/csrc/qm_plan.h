@@ -108,6 +108,8 @@ enum qm_acc_kind : int32_t {
   QA_FMIN = 7,   // order-preserving i64 image of a double (-0 as +0)
   QA_FMAX = 8,
   QA_FZERO = 9,  // min over zero cells of (row << 1 | sign bit), u64
+  QA_FNF = 10,   // non-finite cells of a fixed-point float SUM (atomic OR):
+                 // bit 0 NaN, bit 1 +Infinity, bit 2 -Infinity
 };
 
 struct qm_acc {
@@ -130,6 +132,9 @@ struct qm_acc {
 #define VF_ZERO 16  // QA_FZERO (float MIN / MAX)
 #define VF_WIDE 32  // 128-bit integer sum even block-locally (int64 cells)
 #define VF_NARROW 64  // signed 64-bit integer sum in the global table too
+#define VF_FIXED 128  // float SUM as an exact 128-bit fixed-point integer
+                      // (units of 2^fx_exp): integer adds, so the sum does not
+                      // depend on the order of the rows (deterministic)
 
 struct qm_vcol {
   const void *data;
@@ -142,6 +147,13 @@ struct qm_vcol {
   // xh = (x + split) - split, a multiple of ulp(split) whose sums are exact in
   // any order, and xl = x - xh.  0: compensate each add with TwoSum instead.
   double split;
+  // VF_FIXED: a finite cell x becomes round(x / 2^fx_exp) as a 128-bit
+  // integer in the two QA_FSUM words (lo u64, hi i64); |x| must stay below
+  // fx_max (else the kernel reports QM_DEV_STALE: the column's statistics
+  // are out of date); non-finite cells set bits of word w_nf.
+  int32_t fx_exp;
+  int32_t w_nf;
+  double fx_max;
 };
 
 struct qm_aggspec {
@@ -182,6 +194,9 @@ struct qm_out {
   int32_t zero_word;// QA_FZERO word for float MIN/MAX, else -1
   int32_t src;      // key column index for QO_KEY
   int32_t narrow;   // QO_SUM_I2F / QO_AVG_I2F over a narrow (64-bit) sum
+  int32_t fixed;    // QO_SUM_F / QO_AVG_F over a fixed-point sum (VF_FIXED)
+  int32_t fx_exp;   //   its unit's exponent
+  int32_t nf_word;  //   its QA_FNF word
   int32_t pad;
   int64_t offset;   // byte offset of the column in the output buffer
   int64_t null_offset; // byte offset of its 32-bit-word null bitmap, or -1
@@ -206,6 +221,8 @@ struct qm_status {
 #define QM_DEV_OVERFLOW 1  // hash probe limit hit: regrow and re-run
 #define QM_DEV_RANGE 2     // direct-mapped key outside the planned range
 #define QM_DEV_TIMEOUT 3   // a bounded wait on an asynchronous copy gave up
+#define QM_DEV_STALE 4     // a fixed-point SUM cell beyond the planned range:
+                           // the column changed since its statistics were taken
 
 // Filter columns copied tile by tile into shared memory with bulk async
 // copies (cp.async.bulk + mbarrier), double buffered per warp.

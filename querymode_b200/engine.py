@@ -559,12 +559,26 @@ class Context:
     def aggregate(self, query: QueryDescriptor) -> "AggStream":
         return AggStream(self, query)
 
+    def partition_partial(self, rows, parts: int):
+        """Partial rows (an int64 CUDA tensor [n, row_words] from
+        AggStream.export_partial) split by key hash into `parts` parts:
+        (the rows part after part, each part's row count)."""
+        import torch
+        rows = rows.contiguous()
+        out = torch.empty_like(rows)
+        counts = (C.c_int64 * parts)()
+        torch.cuda.current_stream(rows.device).synchronize()
+        self.check(self.lib.qm_partial_partition(self.h, C.c_void_p(rows.data_ptr()) if rows.numel() else None,
+                                                 rows.shape[0], rows.shape[1], parts,
+                                                 C.c_void_p(out.data_ptr()) if rows.numel() else None, counts))
+        return out, [int(c) for c in counts]
+
     def batch(self, tables: list["Table"], queries: list[QueryDescriptor]) -> "Batch":
         return Batch(self, tables, queries)
 
     def server(self, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0,
-               max_batch_rows: int = 0) -> "Server":
-        return Server(self, hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows)
+               max_batch_rows: int = 0, lanes: int = 0) -> "Server":
+        return Server(self, hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows, lanes)
 
 
 class Table:
@@ -668,6 +682,26 @@ class AggStream:
         self.ctx.check(self.ctx.lib.qm_agg_partial_merge(self.h, C.c_void_p(rows.data_ptr()) if rows.numel() else None,
                                                          rows.shape[0], rows.shape[1], rows_end))
 
+    def partial_layout(self) -> tuple[int, int]:
+        """(words per partial row, word of the group's first global row or -1)."""
+        w = C.c_int32()
+        f = C.c_int32()
+        self.ctx.check(self.ctx.lib.qm_agg_partial_layout(self.h, C.byref(w), C.byref(f)))
+        return w.value, f.value
+
+    def partial_begin(self) -> "AggStream":
+        """A new empty aggregation with this one's plan, for merging the
+        partial rows of one key range (the receiving side of a
+        key-partitioned exchange)."""
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.qm_agg_partial_begin(self.h, C.byref(h)))
+        other = AggStream.__new__(AggStream)
+        other.ctx = self.ctx
+        other.cq = self.cq
+        other.h = h
+        self.ctx._adopt(other)
+        return other
+
     def finish(self, with_qmcb: bool = False) -> Result:
         r = C.c_void_p()
         self.ctx.check(self.ctx.lib.qm_agg_finish(self.h, C.byref(r)))
@@ -717,6 +751,11 @@ class Batch:
         """1: one specialised scan launch per query on parallel graph
         branches (default); 0: one persistent kernel over all queries."""
         self.ctx.check(self.ctx.lib.qm_batch_set_mode(self.h, mode))
+
+    def set_waves(self, waves: int) -> None:
+        """Cut the batch into `waves` waves (0: by batch size), each one's
+        results copied to the host while the later waves run."""
+        self.ctx.check(self.ctx.lib.qm_batch_set_waves(self.h, waves))
 
     def run(self) -> "BatchResults":
         out = (C.c_void_p * self.n)()
@@ -778,15 +817,18 @@ class BatchResults:
 
 
 class Server:
-    """A qm_server: a native worker thread that batches submitted requests
-    over resident tables into persistent launches, within an HBM budget.
-    While it runs, the context is the worker's: register tables first."""
+    """A qm_server: native lanes (worker threads, each with its own CUDA
+    stream) that take submitted requests over resident tables as batched
+    launches while other lanes' batches run, within an HBM budget.  Requests
+    over tables of more than max_batch_rows rows run alone; the last lane
+    takes small requests only.  While it runs, the context is the server's:
+    register tables first."""
 
     def __init__(self, ctx: Context, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0,
-                 max_batch_rows: int = 0):
+                 max_batch_rows: int = 0, lanes: int = 0):
         self.ctx = ctx
         self.lib = ctx.lib
-        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows)
+        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows, lanes)
         h = C.c_void_p()
         ctx.check(self.lib.qm_server_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h

@@ -121,3 +121,23 @@ def test_batch_overflow_reruns_alone(ctx):
         b.close()
         t.close()
         t2.close()
+
+
+@pytest.mark.parametrize("mode", [1, 0])
+def test_batch_waves_keep_results(ctx, mode):
+    """The batch cut into 1, 3 or 8 waves (each wave's results copied back
+    while later waves run), per-query launches and the persistent kernel:
+    every query still equals the oracle, on capture and on replay."""
+    tables, queries = mixed_batch(seed=21, n=30)
+    handles = [ctx.table(t) for t in tables]
+    refs = [oracle.run(t, q) for t, q in zip(tables, queries)]
+    b = ctx.batch(handles, queries)
+    try:
+        b.set_mode(mode)
+        for waves in (3, 8, 1, 0):
+            b.set_waves(waves)
+            for run in range(2):
+                for i, (g, r) in enumerate(zip(b.run(), refs)):
+                    assert_same(g, r, ctx_msg=f"mode {mode} waves {waves} run {run} query {i}")
+    finally:
+        b.close()

@@ -153,3 +153,38 @@ def test_batch_row_cap_keeps_results():
         assert srv.stats()["batches"] > 24 * 400_000 // cap // 4
     finally:
         srv.close()
+
+
+def test_request_overlaps_heavy_batch():
+    """A light request submitted while a heavy request (a 16.7M-group
+    aggregate over 40M rows, run alone) is on the GPU starts on another lane
+    at once and completes first; both equal their results alone."""
+    import time
+    ctx = Context(0)
+    heavy_t = ctx.table(datagen.wide_keys(40_000_000, seed=31, n_keys=1 << 24))
+    light_t = ctx.table(datagen.orders(400_000, seed=31))
+    hq, lq = datagen.wide_keys_query(False), datagen.orders_query()
+    heavy_alone, light_alone = heavy_t.run(hq), light_t.run(lq)
+    srv = ctx.server(hbm_budget_bytes=40 << 30, max_batch=16, max_batch_rows=10_000_000, lanes=3)
+    try:
+        for _ in range(2):  # warm: buffers of both shapes on every lane
+            for t in [srv.submit(heavy_t, hq), srv.submit(light_t, lq)]:
+                srv.wait(t)
+        h = srv.submit(heavy_t, hq)
+        time.sleep(0.002)  # the heavy request is on the GPU
+        t0 = time.perf_counter()
+        lt = srv.submit(light_t, lq)
+        lres, ltm = srv.wait(lt)
+        light_s = time.perf_counter() - t0
+        with pytest.raises(A.QmError) as e:  # the heavy request is still running
+            srv.wait(h, timeout_s=1e-6)
+        assert e.value.status == A.QM_ERR_TIMEOUT
+        hres, htm = srv.wait(h)
+        assert_same(lres, light_alone)
+        assert_same(hres, heavy_alone)
+        assert ltm["batch_size"] == 1 and htm["batch_size"] == 1
+        assert light_s * 1e6 < htm["total_us"]
+        st = srv.stats()
+        assert st["heavy"] >= 3 and st["lanes"] == 3 and st["peak_in_flight"] >= 2
+    finally:
+        srv.close()
