@@ -63,8 +63,12 @@ def parse_args():
     p.add_argument("--no-configs", action="store_true", help="skip the orders_1m / wide_keys_200m lines")
     p.add_argument("--config-steps", type=int, default=20)
     p.add_argument("--ingest-reps", type=int, default=3)
-    p.add_argument("--serve-queries", type=int, default=1500, help="requests per offered load")
-    p.add_argument("--serve-loads", default="0.25,0.5,0.75,0.95", help="offered loads as fractions of capacity")
+    p.add_argument("--serve-queries", type=int, default=1600, help="requests per offered load and repeat")
+    p.add_argument("--serve-repeats", type=int, default=3)
+    p.add_argument("--serve-burst", type=int, default=800, help="requests of the closed capacity burst")
+    p.add_argument("--serve-plain", type=int, default=400, help="requests of the plain per-query comparison")
+    p.add_argument("--serve-lanes", type=int, default=4)
+    p.add_argument("--serve-loads", default="0.25,0.5,0.75,0.9", help="offered loads as fractions of capacity")
     p.add_argument("--batch-queries", type=int, default=256)
     p.add_argument("--batch-reps", type=int, default=3)
     return p.parse_args()
@@ -404,19 +408,34 @@ def run_batched(ctx, stream, local: int, args) -> dict:
 
 
 def serving_tables(device: int) -> dict:
-    """The serving mix's resident tables, generated on the device (seeded):
-    the orders / events / wide-keys shapes at 1M-200M rows."""
+    """The serving mix's eight resident tables, generated on the device
+    (seeded): the orders / events / wide-keys shapes at 1M-200M rows, each
+    with payload columns the mix's queries do not read (as a table holds more
+    columns than one query touches), ~59 GB in all."""
     import torch
     dev = f"cuda:{device}"
     g = torch.Generator(device=dev)
 
-    def orders(n, seed):
+    def payload(n, spec):
+        out = {}
+        for name, dt in spec:
+            if dt == "i64":
+                out[name] = torch.randint(0, 1 << 40, (n,), dtype=torch.int64, device=dev, generator=g)
+            elif dt == "i32":
+                out[name] = torch.randint(0, 1 << 20, (n,), dtype=torch.int32, device=dev, generator=g)
+            else:
+                out[name] = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+        return out
+
+    def orders(n, seed, extra=()):
         g.manual_seed(seed)
-        return {"status": torch.randint(0, 3, (n,), dtype=torch.int32, device=dev, generator=g),
+        cols = {"status": torch.randint(0, 3, (n,), dtype=torch.int32, device=dev, generator=g),
                 "region": torch.randint(0, 16, (n,), dtype=torch.int32, device=dev, generator=g),
                 "amount": torch.empty(n, dtype=torch.float64, device=dev).log_normal_(3.0, 1.0, generator=g)}
+        cols.update(payload(n, extra))
+        return cols
 
-    def events(n, seed, n_keys=65_536):
+    def events(n, seed, n_keys=65_536, extra=()):
         g.manual_seed(seed)
         w = torch.arange(1, n_keys + 1, dtype=torch.float64, device=dev) ** -1.1
         cdf = torch.cumsum(w, 0)
@@ -426,22 +445,33 @@ def serving_tables(device: int) -> dict:
         for i in range(0, n, 1 << 25):
             u = torch.rand(min(1 << 25, n - i), dtype=torch.float64, device=dev, generator=g)
             key[i:i + len(u)] = perm[torch.searchsorted(cdf, u, right=True).clamp_(max=n_keys - 1)]
-        return {"key": key,
+        cols = {"key": key,
                 "qty": torch.randint(1, 101, (n,), dtype=torch.int32, device=dev, generator=g),
                 "price": torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 1000.0,
                 "ts": torch.randint(datagen_year_start(), datagen_year_start() + 365 * 86_400_000, (n,),
                                     dtype=torch.int64, device=dev, generator=g)}
+        cols.update(payload(n, extra))
+        return cols
 
-    def wide(n, seed, n_keys=1 << 24):
+    def wide(n, seed, n_keys=1 << 24, extra=()):
         g.manual_seed(seed)
-        return {"key": torch.randint(0, n_keys, (n,), dtype=torch.int64, device=dev, generator=g),
+        cols = {"key": torch.randint(0, n_keys, (n,), dtype=torch.int64, device=dev, generator=g),
                 "val": torch.randn(n, dtype=torch.float64, device=dev, generator=g) * 1e3,
                 "flag": (torch.rand(n, device=dev, generator=g) < 0.01).to(torch.int32)}
+        cols.update(payload(n, extra))
+        return cols
 
-    return {"orders_1m": ("orders", orders(1_000_000, 40)), "orders_200m": ("orders", orders(200_000_000, 41)),
-            "events_100m": ("events", events(100_000_000, 42)), "events_200m_a": ("events", events(200_000_000, 43)),
-            "events_200m_b": ("events", events(200_000_000, 44)), "wide_50m": ("wide", wide(50_000_000, 45)),
-            "wide_200m_a": ("wide", wide(200_000_000, 46)), "wide_200m_b": ("wide", wide(200_000_000, 47))}
+    ord_x = (("customer", "i64"), ("discount", "f64"), ("channel", "i32"), ("ship_ts", "i64"))
+    ev_x = (("user", "i64"), ("session", "i64"), ("amount", "f64"), ("referrer", "i64"))
+    wide_x = (("aux", "i64"), ("w", "f64"), ("z", "f64"))
+    return {"orders_1m": ("orders", orders(1_000_000, 40)),
+            "orders_200m": ("orders", orders(200_000_000, 41, ord_x)),
+            "events_100m": ("events", events(100_000_000, 42, extra=ev_x)),
+            "events_200m_a": ("events", events(200_000_000, 43, extra=ev_x)),
+            "events_200m_b": ("events", events(200_000_000, 44, extra=ev_x)),
+            "wide_50m": ("wide", wide(50_000_000, 45, extra=wide_x)),
+            "wide_200m_a": ("wide", wide(200_000_000, 46, extra=wide_x)),
+            "wide_200m_b": ("wide", wide(200_000_000, 47, extra=wide_x))}
 
 
 def datagen_year_start() -> int:
@@ -451,9 +481,10 @@ def datagen_year_start() -> int:
 
 def run_serving(local: int, args) -> dict:
     """Poisson arrivals of single requests mixing the orders / events /
-    wide-keys queries over 8 resident tables, served by the native
-    continuous-batching loop under a 150 GB HBM budget; latency = submit ->
-    result in host memory, per offered load."""
+    wide-keys queries over 8 resident tables (~59 GB), served by the native
+    multi-lane continuous-batching server under a 150 GB HBM budget; latency
+    = submit -> result in host memory, per offered load, each load repeated;
+    against the same request mix run as plain per-query launches."""
     import threading
 
     import torch
@@ -491,17 +522,19 @@ def run_serving(local: int, args) -> dict:
             return t, wide_full
         return t, wide_q[int(r.integers(2))]
 
-    # batches of small requests; a 200M-row request is scanned alone (it
-    # fills the GPU by itself, and batching it would hold back the others)
-    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0, max_batch_rows=1 << 27)
+    # requests over tables above 2^27 rows run alone (heavy); the last of
+    # the lanes takes small requests only
+    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0, max_batch_rows=1 << 27,
+                      lanes=args.serve_lanes)
     try:
-        # warm-up: every table and query kind once (column statistics are cached)
-        warm = []
-        for name, (kind, t) in handles.items():
-            qs = orders_q if kind == "orders" else (events_q[:2] if kind == "events" else wide_q + [wide_full])
-            warm += [srv.submit(t, q) for q in qs]
-        for tk in warm:
-            srv.wait(tk)
+        # warm-up: every table and query kind on every lane (column statistics are cached)
+        for _ in range(args.serve_lanes):
+            warm = []
+            for name, (kind, t) in handles.items():
+                qs = orders_q if kind == "orders" else (events_q[:2] if kind == "events" else wide_q + [wide_full])
+                warm += [srv.submit(t, q) for q in qs]
+            for tk in warm:
+                srv.wait(tk)
 
         def serve(reqs, rate):
             """Submit reqs at Poisson arrivals of `rate` per second (all at
@@ -535,32 +568,55 @@ def run_serving(local: int, args) -> dict:
             return np.array(lat), np.array(bs), done_at[0] - t0
 
         # capacity: a closed burst of requests (after one untimed burst, which
-        # grows the server's buffers to the mix's working set)
-        serve([draw(rng) for _ in range(100)], None)
-        burst = [draw(rng) for _ in range(max(200, args.serve_queries // 4))]
+        # grows the lanes' buffers to the mix's working set)
+        serve([draw(rng) for _ in range(200)], None)
+        burst = [draw(rng) for _ in range(args.serve_burst)]
         _, bsz, span = serve(burst, None)
         capacity = len(burst) / span
         loads = []
+        served = 0
         for frac in [float(x) for x in args.serve_loads.split(",")]:
-            reqs = [draw(rng) for _ in range(args.serve_queries)]
-            lat, bsz, span = serve(reqs, capacity * frac)
-            loads.append({"offered_qps": round(capacity * frac, 1), "achieved_qps": round(len(reqs) / span, 1),
-                          "p50_ms": round(float(np.percentile(lat, 50)) / 1e3, 3),
-                          "p95_ms": round(float(np.percentile(lat, 95)) / 1e3, 3),
-                          "p99_ms": round(float(np.percentile(lat, 99)) / 1e3, 3),
-                          "mean_batch": round(float(bsz.mean()), 2)})
+            reps = []
+            for _ in range(args.serve_repeats):
+                reqs = [draw(rng) for _ in range(args.serve_queries)]
+                lat, bsz, span = serve(reqs, capacity * frac)
+                served += len(reqs)
+                reps.append({"achieved_qps": round(len(reqs) / span, 1),
+                             "p50_ms": round(float(np.percentile(lat, 50)) / 1e3, 3),
+                             "p95_ms": round(float(np.percentile(lat, 95)) / 1e3, 3),
+                             "p99_ms": round(float(np.percentile(lat, 99)) / 1e3, 3),
+                             "mean_batch": round(float(bsz.mean()), 2)})
+            med = lambda k: round(float(np.median([r[k] for r in reps])), 3)
+            loads.append({"offered_qps": round(capacity * frac, 1), "achieved_qps": med("achieved_qps"),
+                          "p50_ms": med("p50_ms"), "p95_ms": med("p95_ms"), "p99_ms": med("p99_ms"),
+                          "mean_batch": med("mean_batch"), "p99_ms_repeats": [r["p99_ms"] for r in reps],
+                          "repeats": reps})
         st = srv.stats()
     finally:
         srv.close()
-        sctx.close()
-        del tabs, handles
-        torch.cuda.empty_cache()
-    return {"tables": 8, "table_gb": round(table_bytes / 1e9, 2), "hbm_budget_gb": 150,
-            "capacity_qps": round(capacity, 1), "queries_per_load": args.serve_queries, "loads": loads,
-            "server": {k: st[k] for k in ("completed", "failed", "refused", "batches", "peak_working_bytes")},
+    # the same request mix as plain per-query launches (Table.run, result
+    # in host memory), closed loop
+    plain_reqs = [draw(rng) for _ in range(args.serve_plain)]
+    for t, q in plain_reqs[:20]:
+        t.run(q)
+    t0 = time.perf_counter()
+    for t, q in plain_reqs:
+        t.run(q)
+    plain_qps = len(plain_reqs) / (time.perf_counter() - t0)
+    sctx.close()
+    del tabs, handles
+    torch.cuda.empty_cache()
+    return {"tables": 8, "table_gb": round(table_bytes / 1e9, 2), "hbm_budget_gb": 150, "lanes": st["lanes"],
+            "capacity_qps": round(capacity, 1), "plain_qps": round(plain_qps, 1),
+            "served_vs_plain": round(capacity / plain_qps, 2),
+            "queries": served + len(burst), "queries_per_load": args.serve_queries * args.serve_repeats,
+            "repeats": args.serve_repeats, "loads": loads,
+            "server": {k: st[k] for k in ("completed", "failed", "refused", "batches", "peak_working_bytes",
+                                          "peak_in_flight", "heavy")},
             "mix": "uniform over 8 tables (orders 1M/200M, events 100M/200M/200M, wide 50M/200M/200M); "
                    "orders: status filter by region; events: 30-day window + qty, 48 windows; wide: flag (+val) "
-                   "filters, 1% unfiltered 16M-group; Poisson arrivals (seed 4)"}
+                   "filters, 1% unfiltered 16M-group; Poisson arrivals (seed 4); plain: the same mix, one "
+                   "Table.run after another"}
 
 
 def run_ingest(ctx, cols: dict, args) -> dict:
@@ -687,8 +743,8 @@ def main():
 
     if world > 1:
         # one query over the union of the ranks' shards: every rank scans its
-        # resident shard, the partial group states are all-gathered over
-        # NCCL and rank 0 merges them and finalizes
+        # resident shard, the partial group states are gathered to rank 0
+        # over NCCL and rank 0 merges them and finalizes
         from querymode_b200.distributed import aggregate_sharded
 
         def step():
@@ -792,7 +848,7 @@ def main():
             "config": {"workload": WORKLOAD, "rows_per_gpu": n, "bytes_per_row": BYTES_PER_ROW,
                        "groups": int(res.n_rows), "rows_selected": int(res.stats.rows_selected),
                        "l2": f"inputs {n * BYTES_PER_ROW / 1e9:.2f} GB per GPU > 126 MB L2 (no flush needed)",
-                       "parallelism": f"dp{world}" + (" (row shards, partial states all-gathered over NCCL, merged on rank 0)" if world > 1 else "")},
+                       "parallelism": f"dp{world}" + (" (row shards, partial states gathered to rank 0 over NCCL, merged there)" if world > 1 else "")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "qm_scan_kernel", "kernel_ms": scan_avg},

@@ -242,9 +242,11 @@ int qm_ctx_set_tuning(qm_ctx *ctx, const qm_tuning *tuning);
 /* Device blocks of destroyed tables are kept by the context for the next
  * tables of about their size (up to an eighth of the device's memory; given
  * back by this library whenever one of its allocations fails, and at
- * qm_ctx_destroy).  This frees them now, for a caller whose other allocators
- * need the memory; *released (may be null) receives the bytes freed.  No
- * counterpart in the reference (device memory management). */
+ * qm_ctx_destroy).  Batch and serving buffers come from the device's
+ * stream-ordered memory pool and stay in it when freed.  This frees both
+ * now, for a caller whose other allocators need the memory; *released (may
+ * be null) receives the table-block bytes freed.  No counterpart in the
+ * reference (device memory management). */
 int qm_ctx_trim(qm_ctx *ctx, int64_t *released);
 /* Device properties the host planner and tests read. */
 int qm_ctx_device_info(const qm_ctx *ctx, int32_t *sm_count, int64_t *hbm_bytes);

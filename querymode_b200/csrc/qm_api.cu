@@ -232,6 +232,31 @@ int ensure(qm_ctx *ctx, DevBuf &b, size_t bytes) {
   return QM_OK;
 }
 
+// ensure() for buffers used on one stream only: grown with stream-ordered
+// allocation (cudaFreeAsync / cudaMallocAsync on that stream), so growing
+// one batch's buffers does not synchronise the device under the other
+// batches in flight (a serving lane growing to a larger request).
+int ensure_on(qm_ctx *ctx, DevBuf &b, size_t bytes, cudaStream_t st) {
+  if (b.bytes >= bytes && b.p) return QM_OK;
+  const size_t old_bytes = b.p ? b.bytes : 0;
+  if (b.p) {
+    cudaFreeAsync(b.p, st);
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 256);
+  if (old_bytes) want = std::max(want, old_bytes + old_bytes / 2);
+  if (want > ((size_t)1 << 21)) want = (want + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
+  cudaError_t e = cudaMallocAsync(&b.p, want, st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return set_err(ctx, QM_ERR_OOM, "cudaMallocAsync(%zu): %s", want, cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  return QM_OK;
+}
+
 int ensure_host(qm_ctx *ctx, HostBuf &b, size_t bytes) {
   if (b.bytes >= bytes && b.p) return QM_OK;
   if (b.p) cudaFreeHost(b.p);
@@ -2011,6 +2036,17 @@ int qm_ctx_create(int32_t device, qm_ctx **out) {
   }
   ctx->sm_count = prop.multiProcessorCount;
   ctx->hbm_bytes = (int64_t)prop.totalGlobalMem;
+  {
+    // stream-ordered allocations (batch buffers) stay in the device's pool
+    // when freed, for the next batch of that size, instead of going back to
+    // the driver at every synchronisation; qm_ctx_trim hands them back
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   if (ensure(ctx, ctx->status, sizeof(qm_status))) {
     delete ctx;
     return QM_ERR_OOM;
@@ -2054,6 +2090,12 @@ int qm_ctx_trim(qm_ctx *ctx, int64_t *released) {
     bytes = ctx->dpool.cached;
   }
   ctx->dpool.trim();
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(pool, 0);
+  }
+  cudaGetLastError();
   if (released) *released = (int64_t)bytes;
   return QM_OK;
 }
@@ -3418,11 +3460,13 @@ int batch_layout(qm_batch *b) {
   }
   plan_waves(b);
   int rc;
-  if ((rc = ensure(ctx, b->arena, (size_t)words * 8 + 64))) return rc;
-  if ((rc = ensure(ctx, b->d_status, sizeof(qm_status) * n))) return rc;
-  if ((rc = ensure(ctx, b->d_bq, sizeof(qm_bq) * n))) return rc;
-  if ((rc = ensure(ctx, b->d_counter, sizeof(int) * (b->waves.size() + 1)))) return rc;
-  if ((rc = ensure_host(ctx, b->h_status, sizeof(qm_status) * n))) return rc;
+  if ((rc = ensure_on(ctx, b->arena, (size_t)words * 8 + 64, st))) return rc;
+  if ((rc = ensure_on(ctx, b->d_status, sizeof(qm_status) * n, st))) return rc;
+  if ((rc = ensure_on(ctx, b->d_bq, sizeof(qm_bq) * n, st))) return rc;
+  if ((rc = ensure_on(ctx, b->d_counter, sizeof(int) * (b->waves.size() + 1), st))) return rc;
+  // sized for the largest batch once: regrowing pinned memory frees the old
+  // buffer, which synchronises the device under other batches in flight
+  if ((rc = ensure_host(ctx, b->h_status, sizeof(qm_status) * QM_BATCH_MAX))) return rc;
   std::vector<qm_bq> dbq(n);
   for (int i = 0; i < n; i++) {
     GroupTable &gt = b->gts[i];
@@ -3490,14 +3534,14 @@ int batch_layout(qm_batch *b) {
     wv.bm_words = bm_words;
     size_t temp = 0;
     CK(qm_batch_scan_temp_bytes(bm_words, &temp));
-    if ((rc = ensure(ctx, wv.d_slot0, sizeof(int64_t) * slot0.size())) ||
-        (rc = ensure(ctx, wv.d_chunks, sizeof(qm_chunk) * std::max<size_t>(chunks.size(), 1))) ||
-        (rc = ensure(ctx, wv.d_bitmap, sizeof(uint32_t) * (bm_words + 1))) ||
-        (rc = ensure(ctx, wv.d_popc, sizeof(uint32_t) * (bm_words + 1))) ||
-        (rc = ensure(ctx, wv.d_ranks, sizeof(uint64_t) * (bm_words + 1))) || (rc = ensure(ctx, wv.d_temp, temp + 16)) ||
-        (rc = ensure(ctx, wv.d_meta, sizeof(qm_batch_meta))) ||
-        (rc = ensure(ctx, wv.d_packed, (size_t)packed_max + 64)) ||
-        (rc = ensure(ctx, wv.d_nullbytes, (size_t)nullbytes_max + 64)) ||
+    if ((rc = ensure_on(ctx, wv.d_slot0, sizeof(int64_t) * slot0.size(), st)) ||
+        (rc = ensure_on(ctx, wv.d_chunks, sizeof(qm_chunk) * std::max<size_t>(chunks.size(), 1), st)) ||
+        (rc = ensure_on(ctx, wv.d_bitmap, sizeof(uint32_t) * (bm_words + 1), st)) ||
+        (rc = ensure_on(ctx, wv.d_popc, sizeof(uint32_t) * (bm_words + 1), st)) ||
+        (rc = ensure_on(ctx, wv.d_ranks, sizeof(uint64_t) * (bm_words + 1), st)) ||
+        (rc = ensure_on(ctx, wv.d_temp, temp + 16, st)) || (rc = ensure_on(ctx, wv.d_meta, sizeof(qm_batch_meta), st)) ||
+        (rc = ensure_on(ctx, wv.d_packed, (size_t)packed_max + 64, st)) ||
+        (rc = ensure_on(ctx, wv.d_nullbytes, (size_t)nullbytes_max + 64, st)) ||
         (rc = ensure_host(ctx, wv.h_meta, sizeof(qm_batch_meta))))
       return rc;
     CK(cudaMemcpyAsync(wv.d_slot0.p, slot0.data(), sizeof(int64_t) * slot0.size(), cudaMemcpyHostToDevice, st));

@@ -948,7 +948,10 @@ cudaError_t qm_launch_scan(const qm_scan_args &a, int blocks, size_t smem_bytes,
   cudaError_t e = scan_attrs_once();
   if (e != cudaSuccess) return e;
   const int dd = a.dedupe != 0 ? 1 : 0;
-  if (!a.sel && a.stage.n == 0 && a.agg.n_vcols <= QM_SPEC_NV_MAX) {
+  // fixed-point (deterministic) sums run in the run-time-plan kernels only
+  bool fixed = false;
+  for (int c = 0; c < a.agg.n_vcols; ++c) fixed = fixed || (a.agg.vcol[c].flags & VF_FIXED) != 0;
+  if (!a.sel && a.stage.n == 0 && a.agg.n_vcols <= QM_SPEC_NV_MAX && !fixed) {
     int kk = key_kind(a.key);
     if (kk == QM_KK_NONE && !dd) kk = QM_KK_ANY;
     switch (a.agg.n_vcols) {

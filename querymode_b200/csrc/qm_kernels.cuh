@@ -430,6 +430,31 @@ __device__ __forceinline__ uint32_t eval_pred(const qm_pred &P, const ROWS &row,
 #define QM_NV_ANY (QM_MAX_VCOLS + 1)
 #define QM_NV_BOUND(NV) ((NV) > QM_MAX_VCOLS ? QM_MAX_VCOLS : (NV))
 
+// The payload columns of a tile (key columns, then value columns) into L2
+// ahead of the survivors' gathers.
+#ifndef QM_PREFETCH_PAYLOAD
+#define QM_PREFETCH_PAYLOAD 0
+#endif
+template <int NV, int KK>
+__device__ __forceinline__ void prefetch_payload_l2(const qm_keyspec &K, const qm_aggspec &A, int64_t e0, int lane) {
+  auto line = [&](const void *data, int dtype) {
+    const int elem = (dtype == QM_I32 || dtype == QM_F32) ? 4 : 8;
+    if (lane < QM_TILE_ROWS * elem / 128) {
+      const char *p = reinterpret_cast<const char *>(data) + e0 * elem + lane * 128;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
+  };
+  if (KK == QM_KK_I64) line(K.data[0], QM_I64);
+  else if (KK == QM_KK_I32) line(K.data[0], QM_I32);
+  else if (KK != QM_KK_NONE)
+    for (int i = 0; i < K.n_cols; ++i) line(K.data[i], K.dtype[i]);
+  const int nv = NV > QM_MAX_VCOLS ? A.n_vcols : NV;
+#pragma unroll
+  for (int c = 0; c < QM_NV_BOUND(NV); ++c)
+    if (c < nv) line(A.vcol[c].data, A.vcol[c].dtype);
+}
+
+
 template <int KK = QM_KK_ANY>
 __device__ __forceinline__ uint64_t row_key(const qm_keyspec &K, int64_t r, int &special) {
   special = 0;
@@ -776,6 +801,10 @@ __device__ __forceinline__ T group_reduce(T v, unsigned act, unsigned peers, int
 // accumulator word w lives at tp[w * ws].  Every lane of `act` executes this
 // (the shuffles need them); only group leaders, with tp != nullptr, write.
 // iters = (largest peer group in act) - 1.
+// FX: the kernel carries the fixed-point (VF_FIXED) sum paths; kernels
+// specialised for a column count and key kind leave them out (their plans
+// never use them, and the extra paths cost the hot loop instructions).
+template <bool FX = true>
 __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local, unsigned act,
                                           unsigned peers, int iters, int lane, uint64_t grow,
                                           const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull, bool plain = false,
@@ -848,7 +877,7 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
       case QA_FSUM: {
         const double v = valid ? __longlong_as_double((long long)raw) : 0.0;
         const qm_vcol &fv = A.vcol[ac.vcol];
-        if (fv.flags & VF_FIXED) {
+        if (FX && (fv.flags & VF_FIXED)) {
           uint64_t lo;
           int64_t hi;
           uint32_t nf;
@@ -974,7 +1003,7 @@ __device__ __forceinline__ void apply_row(const qm_aggspec &A, uint64_t *tp, int
 #ifndef QM_GLOBAL_READ_TEST
 #define QM_GLOBAL_READ_TEST 0
 #endif
-template <int NV = QM_NV_ANY>
+template <int NV = QM_NV_ANY, bool FX = true>
 __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int ws, bool local,
                                         uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull,
                                         qm_status *st = nullptr) {
@@ -1036,7 +1065,7 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
       const double d = __longlong_as_double((long long)vb[c]);
       if (f & VF_SUM) {
         uint64_t *w0 = tp + (int64_t)vc.w_sum * ws;
-        if (f & VF_FIXED) {
+        if (FX && (f & VF_FIXED)) {
           uint64_t lo;
           int64_t hi;
           uint32_t nf;
@@ -1066,7 +1095,7 @@ __device__ __forceinline__ void agg_row(const qm_aggspec &A, uint64_t *tp, int w
 // contributions through the warp's shared scratch, and the group leader adds
 // them once; MIN / MAX / FIRST stay per lane (64-bit min/max atomics resolve
 // conflicts in hardware, and most are skipped by the read test).
-template <int NV = QM_NV_ANY>
+template <int NV = QM_NV_ANY, bool FX = true>
 __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp, int L, unsigned lmask, unsigned peers,
                                                int lane, uint64_t grow, const uint64_t (&vb)[QM_MAX_VCOLS],
                                                uint32_t vnull, uint64_t *scr, qm_status *st = nullptr) {
@@ -1107,7 +1136,7 @@ __device__ __forceinline__ void agg_row_merged(const qm_aggspec &A, uint64_t *tp
           }
         }
         __syncwarp(lmask);
-      } else if (f & VF_FIXED) {
+      } else if (FX && (f & VF_FIXED)) {
         const double d = valid ? __longlong_as_double((long long)raw) : 0.0;
         uint64_t lo;
         int64_t hi;
@@ -1283,7 +1312,7 @@ __device__ __forceinline__ void merge_plain(const qm_aggspec &A, uint64_t *dst, 
 // Aggregates one survivor per lane (lanes with active = false sit out).
 // DD: 0 / 1 = the plan's dedupe flag fixed at compile time (separate kernels
 // keep each path's registers and code apart), 2 = read it from the plan.
-template <int DD = 2, int NV = QM_NV_ANY, int KK = QM_KK_ANY>
+template <int DD = 2, int NV = QM_NV_ANY, int KK = QM_KK_ANY, bool FX = true>
 __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
                                             int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
   const qm_aggspec &A = a.agg;
@@ -1318,7 +1347,7 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
       }
     }
     const int iters = (int)__reduce_max_sync(act, (unsigned)__popc(peers)) - 1;
-    apply_row(A, tp, ws, local, act, peers, iters, lane, grow, vb, vnull, local && a.priv, a.status);
+    apply_row<FX>(A, tp, ws, local, act, peers, iters, lane, grow, vb, vnull, local && a.priv, FX ? a.status : nullptr);
     return;
   }
   uint64_t grow = 0, key = 0;
@@ -1341,11 +1370,11 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
   if (loc) peers = __match_any_sync(lmask, ls);
   const bool merge = __any_sync(QM_FULL, (peers & (peers - 1)) != 0);
   if (loc) {
-    if (merge) agg_row_merged<NV>(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr, a.status);
-    else agg_row<NV>(A, lw + ls, L, true, grow, vb, vnull, a.status);
+    if (merge) agg_row_merged<NV, FX>(A, lw + ls, L, lmask, peers, lane, grow, vb, vnull, scr, FX ? a.status : nullptr);
+    else agg_row<NV, FX>(A, lw + ls, L, true, grow, vb, vnull, FX ? a.status : nullptr);
   } else if (active && !(L > 0 && !a.local_hash)) {
     const int64_t gs = global_slot(a, key, special);
-    if (gs >= 0) agg_row<NV>(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull, a.status);
+    if (gs >= 0) agg_row<NV, FX>(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull, FX ? a.status : nullptr);
   }
 }
 

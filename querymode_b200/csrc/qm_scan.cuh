@@ -39,7 +39,8 @@ __host__ __device__ inline smem_layout make_smem_layout(int local_slots, int loc
 template <bool SEL, int DD, int NV, int KK>
 __device__ __forceinline__ void drain_round(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
                                             int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
-  drain_round_any<DD, NV, KK>(a, lkeys, lw, L, l_used, lane, active, row, scr);
+  // the fixed-point sum paths only in the run-time-plan kernels
+  drain_round_any<DD, NV, KK, (NV > QM_MAX_VCOLS)>(a, lkeys, lw, L, l_used, lane, active, row, scr);
 }
 
 // The fused scan.  Each warp takes tiles of QM_TILE_ROWS rows round robin,
@@ -156,7 +157,10 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
       // full dense tile: the lane's rows are r0 .. r0+7
       const int64_t r0 = e0 + (int64_t)lane * QM_R;
       const int64_t nxt = v + gwarps < n_virtual ? tile_of(v + gwarps) * QM_TILE_ROWS : a.n;
-      if (nxt + QM_TILE_ROWS <= a.n) prefetch_tile_l2(a.pred, nxt, lane);
+      if (nxt + QM_TILE_ROWS <= a.n) {
+        prefetch_tile_l2(a.pred, nxt, lane);
+        if (QM_PREFETCH_PAYLOAD) prefetch_payload_l2<NV, KK>(a.key, A, nxt, lane);
+      }
       m = eval_pred_contig(a.pred, r0, (1u << QM_R) - 1);
       const uint32_t cnt = __popc(m);
       uint32_t off = cnt;
