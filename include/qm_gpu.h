@@ -219,6 +219,12 @@ typedef struct {
   int32_t blocks_per_sm; /* resident blocks per SM: 0 auto (occupancy), else a cap */
   int32_t stage_depth;   /* filter-column tiles in flight per warp (bulk async
                             copies into shared memory): <= 0 off, 2..4 */
+  int32_t partitioned;   /* 1: partitioned aggregation (survivors written to key
+                            partitions, each aggregated in shared memory) for
+                            grouped queries whose table exceeds shared memory
+                            and which select at least a quarter of the rows;
+                            0 (default): the fused scan */
+  int32_t reserved;
 } qm_tuning;
 
 /* ---- library / context ---------------------------------------------------- */

@@ -95,7 +95,7 @@ class QmQuery(C.Structure):
 
 class QmTuning(C.Structure):
     _fields_ = [("local_slots", C.c_int32), ("dedupe", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("stage_depth", C.c_int32)]
+                ("stage_depth", C.c_int32), ("partitioned", C.c_int32), ("reserved", C.c_int32)]
 
 
 class QmResultCol(C.Structure):

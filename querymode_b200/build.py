@@ -17,7 +17,7 @@ from concurrent.futures import ThreadPoolExecutor
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libqm_gpu.so")
-SOURCES = ["qm_api.cu", "qm_kernels.cu", "qm_batch.cu"] + [f"qm_scan_nv{n}.cu" for n in range(5)]
+SOURCES = ["qm_api.cu", "qm_kernels.cu", "qm_batch.cu", "qm_part.cu"] + [f"qm_scan_nv{n}.cu" for n in range(5)]
 HEADERS = ["qm_plan.h", "qm_launch.h", "qm_kernels.cuh", "qm_batch.h", "qm_scan.cuh", "qm_scan_spec.cuh",
            "qm_server.cuh", "qm_parquet.cuh", os.path.join("..", "..", "include", "qm_gpu.h")]
 

@@ -1309,22 +1309,17 @@ __device__ __forceinline__ void merge_plain(const qm_aggspec &A, uint64_t *dst, 
   }
 }
 
-// Aggregates one survivor per lane (lanes with active = false sit out).
-// DD: 0 / 1 = the plan's dedupe flag fixed at compile time (separate kernels
-// keep each path's registers and code apart), 2 = read it from the plan.
-template <int DD = 2, int NV = QM_NV_ANY, int KK = QM_KK_ANY, bool FX = true>
-__device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
-                                            int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
+// Applies one survivor per lane (key word, special flag, global row and
+// gathered cells; lanes with active = false sit out) to the block-local
+// table or else the global table.
+template <int DD = 2, int NV = QM_NV_ANY, bool FX = true>
+__device__ __forceinline__ void drain_apply(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L, int *l_used,
+                                            int lane, bool active, uint64_t key, int special, uint64_t grow,
+                                            const uint64_t (&vb)[QM_MAX_VCOLS], uint32_t vnull, uint64_t *scr) {
   const qm_aggspec &A = a.agg;
   if (DD == 2 ? a.dedupe != 0 : DD == 1) {
     const unsigned act = __ballot_sync(QM_FULL, active);
     if (!active) return;
-    const uint64_t grow = (uint64_t)(a.row_offset + row);
-    int special;
-    const uint64_t key = row_key<KK>(a.key, row, special);
-    uint64_t vb[QM_MAX_VCOLS];
-    uint32_t vnull;
-    gather_values<NV>(A, row, vb, vnull);
     unsigned peers = __match_any_sync(act, key);
     if (__any_sync(act, special != 0)) peers &= __match_any_sync(act, special);
     const bool leader = lane == __ffs(peers) - 1;
@@ -1350,19 +1345,10 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
     apply_row<FX>(A, tp, ws, local, act, peers, iters, lane, grow, vb, vnull, local && a.priv, FX ? a.status : nullptr);
     return;
   }
-  uint64_t grow = 0, key = 0;
-  int special = 0;
-  uint64_t vb[QM_MAX_VCOLS];
-  uint32_t vnull = 0;
   int ls = -1;
-  if (active) {
-    grow = (uint64_t)(a.row_offset + row);
-    key = row_key<KK>(a.key, row, special);
-    gather_values<NV>(A, row, vb, vnull);
-    if (L > 0) {
-      if (!a.local_hash) ls = (int)global_slot(a, key, special);
-      else if (special == 0) ls = local_find(lkeys, L, key, l_used);
-    }
+  if (active && L > 0) {
+    if (!a.local_hash) ls = (int)global_slot(a, key, special);
+    else if (special == 0) ls = local_find(lkeys, L, key, l_used);
   }
   const bool loc = active && ls >= 0;
   const unsigned lmask = __ballot_sync(QM_FULL, loc);
@@ -1376,6 +1362,25 @@ __device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t 
     const int64_t gs = global_slot(a, key, special);
     if (gs >= 0) agg_row<NV, FX>(A, a.table + gs * a.stride + 1, 1, false, grow, vb, vnull, FX ? a.status : nullptr);
   }
+}
+
+// Aggregates one survivor per lane (lanes with active = false sit out):
+// gathers its key and value cells, then drain_apply.
+// DD: 0 / 1 = the plan's dedupe flag fixed at compile time (separate kernels
+// keep each path's registers and code apart), 2 = read it from the plan.
+template <int DD = 2, int NV = QM_NV_ANY, int KK = QM_KK_ANY, bool FX = true>
+__device__ __forceinline__ void drain_round_any(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw, int L,
+                                                int *l_used, int lane, bool active, int64_t row, uint64_t *scr) {
+  uint64_t grow = 0, key = 0;
+  int special = 0;
+  uint64_t vb[QM_MAX_VCOLS];
+  uint32_t vnull = 0;
+  if (active) {
+    grow = (uint64_t)(a.row_offset + row);
+    key = row_key<KK>(a.key, row, special);
+    gather_values<NV>(a.agg, row, vb, vnull);
+  }
+  drain_apply<DD, NV, FX>(a, lkeys, lw, L, l_used, lane, active, key, special, grow, vb, vnull, scr);
 }
 
 

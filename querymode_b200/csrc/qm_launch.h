@@ -100,3 +100,13 @@ cudaError_t qm_launch_check_selection(const uint32_t *sel, int64_t n_sel, int64_
                                       int sm_count, cudaStream_t stream);
 cudaError_t qm_launch_maxabs(const void *p, int dtype, const uint32_t *nulls, int64_t n, unsigned long long *out,
                              int sm_count, cudaStream_t st);
+
+// Partitioned aggregation (qm_part.cu): the counting pass (pass 0) or the
+// scatter pass (pass 1) over the plan's rows, the per-partition offsets, and
+// the aggregation of each partition's records.
+size_t qm_part_scan_smem(int parts);
+int qm_part_scan_blocks(int sm_count, int parts);
+cudaError_t qm_launch_part_scan(int pass, const qm_scan_args &a, const qm_part_spec &ps, cudaStream_t st);
+cudaError_t qm_launch_part_offsets(const qm_part_spec &ps, cudaStream_t st);
+size_t qm_part_agg_smem(int local_slots, int local_hash, int n_words);
+cudaError_t qm_launch_part_agg(const qm_scan_args &a, const qm_part_spec &ps, int sm_count, cudaStream_t st);

@@ -262,6 +262,32 @@ struct qm_scan_args {
   qm_staging stage;
 };
 
+// ---- partitioned aggregation --------------------------------------------------
+// For group tables larger than a block's shared memory: a counting pass and
+// a scatter pass write every survivor as a record into its key partition
+// (direct keys: a window of 2^shift slots; hashed keys: the top `bits` bits
+// of the key's hash; special keys and direct keys outside the table: the
+// last partition, `parts`), then one block per partition aggregates its
+// records in a shared-memory table and merges it into the group table once.
+// A record is 2 + value-column words: the key word; row (bits 0-31), special
+// flag (32-39), NULL bits of the cells (40-47); the value cells.
+struct qm_part_spec {
+  int32_t parts;       // partitions of ordinary keys (partition `parts` takes the rest)
+  int32_t direct;      // 1: partition = slot >> shift; 0: partition = hash >> (64 - bits)
+  int32_t shift;
+  int32_t bits;
+  int32_t rec_words;
+  int32_t blocks;      // grid of the counting and scatter passes (the same in both)
+  int32_t local_slots; // slots of a partition's shared-memory table
+  int32_t pad;
+  int64_t rec_cap;     // records the buffer holds (a survivor past it is an overflow)
+  uint32_t *counts;    // [(parts + 1) x blocks] survivors per partition and block
+  uint64_t *offsets;   // [(parts + 1) x blocks] first record of each partition and block
+  uint64_t *bases;     // [parts + 2] first record of each partition; then the total
+  uint64_t *records;
+  int *counter;        // partitions claimed by the aggregating blocks
+};
+
 // ---- Parquet column chunk decode (PLAIN pages) --------------------------------
 // A page of a column chunk after its header was parsed on the host.
 struct qm_pq_page {

@@ -421,10 +421,10 @@ class Context:
         return n.value
 
     def set_tuning(self, local_slots: int = 0, dedupe: int = -1, blocks_per_sm: int = 0,
-                   stage_depth: int = 0) -> None:
+                   stage_depth: int = 0, partitioned: int = 0) -> None:
         """Launch-shape knobs of the fused scan (see qm_tuning); the
         defaults restore the planner's choices."""
-        t = A.QmTuning(local_slots, dedupe, blocks_per_sm, stage_depth)
+        t = A.QmTuning(local_slots, dedupe, blocks_per_sm, stage_depth, partitioned)
         self._tuning = t
         self.check(self.lib.qm_ctx_set_tuning(self.h, C.byref(t)))
 
