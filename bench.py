@@ -62,6 +62,9 @@ def parse_args():
     p.add_argument("--no-parity", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the orders_1m / wide_keys_200m lines")
     p.add_argument("--config-steps", type=int, default=20)
+    p.add_argument("--configs", default="orders,filtered,unfiltered",
+                   help="which of the orders_1m / wide_keys filtered / unfiltered lines to run")
+    p.add_argument("--wide-rows", type=int, default=200_000_000, help="rows of the wide_keys lines")
     p.add_argument("--ingest-reps", type=int, default=3)
     p.add_argument("--serve-queries", type=int, default=1600, help="requests per offered load and repeat")
     p.add_argument("--serve-repeats", type=int, default=3)
@@ -312,19 +315,27 @@ def run_configs(ctx, stream, args) -> dict:
     unfiltered (16.7M groups, hash table beyond L2)."""
     from querymode_b200 import datagen
     out = {}
-    orders = datagen.orders(1_000_000, seed=0)
-    out["orders_1m"] = run_config(ctx, stream, "orders_1m", orders, datagen.orders_query(), 16, max(args.config_steps, 50),
-                                  args.warmup, 1_000_000,
-                                  "status = 1 GROUP BY region SUM(amount), COUNT(*); 16 groups; launch- and "
-                                  "sync-bound (16 MB per query)")
-    del orders
-    wide = datagen.wide_keys(200_000_000, seed=2, n_keys=1 << 24)
-    out["wide_keys_200m_filtered"] = run_config(
-        ctx, stream, "wide_keys_200m_filtered", wide, datagen.wide_keys_query(True), 20, args.config_steps, args.warmup,
-        20_000_000, "flag = 1 AND val > 0 (~0.5 %) GROUP BY key SUM(val), COUNT(*); key int64 over 2^24 values")
-    out["wide_keys_200m_unfiltered"] = run_config(
-        ctx, stream, "wide_keys_200m_unfiltered", wide, datagen.wide_keys_query(False), 16, max(3, args.config_steps // 4),
-        args.warmup, 20_000_000, "no filter, GROUP BY key SUM(val), COUNT(*): 16.7M groups, result 0.4 GB to the host")
+    which = set(args.configs.split(","))
+    if "orders" in which:
+        orders = datagen.orders(1_000_000, seed=0)
+        out["orders_1m"] = run_config(ctx, stream, "orders_1m", orders, datagen.orders_query(), 16,
+                                      max(args.config_steps, 50), args.warmup, 1_000_000,
+                                      "status = 1 GROUP BY region SUM(amount), COUNT(*); 16 groups; launch- and "
+                                      "sync-bound (16 MB per query)")
+        del orders
+    if not which & {"filtered", "unfiltered"}:
+        return out
+    wide = datagen.wide_keys(args.wide_rows, seed=2, n_keys=1 << 24)
+    wname = "wide_keys_200m" if args.wide_rows == 200_000_000 else f"wide_keys_{args.wide_rows}"
+    if "filtered" in which:
+        out[f"{wname}_filtered"] = run_config(
+            ctx, stream, f"{wname}_filtered", wide, datagen.wide_keys_query(True), 20, args.config_steps, args.warmup,
+            20_000_000, "flag = 1 AND val > 0 (~0.5 %) GROUP BY key SUM(val), COUNT(*); key int64 over 2^24 values")
+    if "unfiltered" in which:
+        out[f"{wname}_unfiltered"] = run_config(
+            ctx, stream, f"{wname}_unfiltered", wide, datagen.wide_keys_query(False), 16,
+            max(3, args.config_steps // 4), args.warmup, 20_000_000,
+            "no filter, GROUP BY key SUM(val), COUNT(*): 16.7M groups, result 0.4 GB to the host")
     return out
 
 

@@ -559,7 +559,8 @@ typedef struct {
   int64_t run_us;     /* launch -> result in host memory                   */
   int64_t total_us;   /* submit -> result in host memory                   */
   int32_t batch_size; /* requests in its batch                             */
-  int32_t reserved;
+  int32_t plan_us;    /* its lane planning and laying out the batch (host,
+                         part of queued_us)                               */
 } qm_server_timing;
 
 typedef struct {

@@ -118,7 +118,7 @@ class QmServerConfig(C.Structure):
 
 class QmServerTiming(C.Structure):
     _fields_ = [("queued_us", C.c_int64), ("run_us", C.c_int64), ("total_us", C.c_int64),
-                ("batch_size", C.c_int32), ("reserved", C.c_int32)]
+                ("batch_size", C.c_int32), ("plan_us", C.c_int32)]
 
 
 class QmServerCounters(C.Structure):

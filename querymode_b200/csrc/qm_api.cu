@@ -3432,6 +3432,13 @@ struct BatchWave {
   int64_t slots = 0;      // group-table slots of its queries
   int64_t bm_words = 0;   // words of its first-row bitmap
   qm_batch_dev dev{};
+  // mode 0: one persistent launch per query class present in the wave, over
+  // chunks [chunk0, chunk0 + n_chunks) of the wave's chunk list
+  struct ClassLaunch {
+    int cls, chunk0, n_chunks, blocks, local_bytes;
+    size_t smem;
+  };
+  std::vector<ClassLaunch> classes;
   DevBuf d_slot0, d_chunks, d_bitmap, d_popc, d_ranks, d_temp, d_meta, d_packed, d_nullbytes;
   HostBuf h_meta;         // pinned: the wave's layout, copied back with its work
   cudaGraph_t graph = nullptr;
@@ -3482,9 +3489,6 @@ struct qm_batch {
   int chunk_tiles = 512;
   int local_kb = 40;
   int bps = 0;
-  size_t scan_smem = 0;
-  int scan_blocks = 1;
-  int local_bytes = 0;
   float last_ms = 0;
   int64_t bytes_scanned = 0;
   int64_t total_rows = 0;
@@ -3603,7 +3607,7 @@ int batch_layout(qm_batch *b) {
   if ((rc = ensure_on(ctx, b->arena, (size_t)words * 8 + 64, st))) return rc;
   if ((rc = ensure_on(ctx, b->d_status, sizeof(qm_status) * n, st))) return rc;
   if ((rc = ensure_on(ctx, b->d_bq, sizeof(qm_bq) * n, st))) return rc;
-  if ((rc = ensure_on(ctx, b->d_counter, sizeof(int) * (b->waves.size() + 1), st))) return rc;
+  if ((rc = ensure_on(ctx, b->d_counter, sizeof(int) * QM_BATCH_CLASS_SLOTS * b->waves.size(), st))) return rc;
   // sized for the largest batch once: regrowing pinned memory frees the old
   // buffer, which synchronises the device under other batches in flight
   if ((rc = ensure_host(ctx, b->h_status, sizeof(qm_status) * QM_BATCH_MAX))) return rc;
@@ -3619,30 +3623,42 @@ int batch_layout(qm_batch *b) {
     q.a.row_offset = 0;
     memset(&q.a.stage, 0, sizeof q.a.stage);
   }
-  // the largest local table of the batch sets the persistent kernel's shared memory
-  int local_bytes = 0;
+  // per query class (dedupe flag, value columns, key kind): the largest local
+  // table of its queries sets that persistent kernel's shared memory
+  std::vector<int> cls(n);
+  int class_local[QM_BATCH_CLASSES_N] = {0};
   for (int i = 0; i < n; i++) {
     const Exec &ex = b->gts[i].ex;
+    cls[i] = qm_batch_class_of(b->bq[i].a);
     if (ex.local_slots > 0)
-      local_bytes = std::max<int>(local_bytes, ex.local_slots * (b->gts[i].pl.agg.n_words * 8 + (ex.local_hash ? 8 : 0)));
+      class_local[cls[i]] = std::max<int>(
+          class_local[cls[i]], ex.local_slots * (b->gts[i].pl.agg.n_words * 8 + (ex.local_hash ? 8 : 0)));
   }
-  b->local_bytes = local_bytes;
-  b->scan_smem = qm_batch_smem_bytes(local_bytes);
-  int bps = 1;
-  {
-    std::lock_guard<std::mutex> lk(g_cfg_mu);
-    if (qm_batch_configure(b->scan_smem, &bps) != cudaSuccess) {
-      cudaGetLastError();
-      return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", b->scan_smem);
+  size_t class_smem[QM_BATCH_CLASSES_N];
+  int class_bps[QM_BATCH_CLASSES_N];
+  for (int c = 0; c < QM_BATCH_CLASSES_N; c++) {
+    class_smem[c] = qm_batch_smem_bytes(class_local[c]);
+    class_bps[c] = 0;
+    bool used = false;
+    for (int i = 0; i < n && !used; i++) used = cls[i] == c;
+    if (!used) continue;
+    int bps = 1;
+    {
+      std::lock_guard<std::mutex> lk(g_cfg_mu);
+      if (qm_batch_class_configure(c, class_smem[c], &bps) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", class_smem[c]);
+      }
     }
+    if (bps < 1) bps = 1;
+    if (b->bps > 0 && b->bps < bps) bps = b->bps;
+    class_bps[c] = bps;
   }
-  if (bps < 1) bps = 1;
-  if (b->bps > 0 && b->bps < bps) bps = b->bps;
-  // per wave: slots, bitmap slices, chunks and finalize buffers
+  // per wave: slots, bitmap slices, chunks (grouped by class) and finalize buffers
   for (size_t w = 0; w < b->waves.size(); w++) {
     BatchWave &wv = *b->waves[w];
     std::vector<int64_t> slot0;
-    std::vector<qm_chunk> chunks;
+    std::vector<qm_chunk> by_class[QM_BATCH_CLASSES_N];
     int64_t slots = 0, bm_words = 0, packed_max = 0, nullbytes_max = 0;
     for (int j = wv.q0; j < wv.q1; j++) {
       const int i = b->order[j];
@@ -3667,8 +3683,22 @@ int batch_layout(qm_batch *b) {
         c.pad = 0;
         c.tile0 = t0;
         c.tile1 = std::min<int64_t>(tiles, t0 + b->chunk_tiles);
-        chunks.push_back(c);
+        by_class[cls[i]].push_back(c);
       }
+    }
+    std::vector<qm_chunk> chunks;
+    wv.classes.clear();
+    for (int c = 0; c < QM_BATCH_CLASSES_N; c++) {
+      if (by_class[c].empty()) continue;
+      BatchWave::ClassLaunch L;
+      L.cls = c;
+      L.chunk0 = (int)chunks.size();
+      L.n_chunks = (int)by_class[c].size();
+      L.local_bytes = class_local[c];
+      L.smem = class_smem[c];
+      L.blocks = std::max(1, std::min(ctx->sm_count * class_bps[c], L.n_chunks));
+      wv.classes.push_back(L);
+      chunks.insert(chunks.end(), by_class[c].begin(), by_class[c].end());
     }
     wv.slots = slots;
     wv.bm_words = bm_words;
@@ -3696,7 +3726,7 @@ int batch_layout(qm_batch *b) {
     d.total_slots = slots;
     d.chunks = (qm_chunk *)wv.d_chunks.p;
     d.n_chunks = (int)chunks.size();
-    d.counter = (int *)b->d_counter.p + w;
+    d.counter = (int *)b->d_counter.p + QM_BATCH_CLASS_SLOTS * w;
     d.statuses = (qm_status *)b->d_status.p + wv.q0;
     d.bitmap = (uint32_t *)wv.d_bitmap.p;
     d.bm_words = bm_words;
@@ -3709,9 +3739,6 @@ int batch_layout(qm_batch *b) {
     d.meta_bytes = sizeof(qm_batch_meta);
     d.packed = (unsigned char *)wv.d_packed.p;
     d.nullbytes = (unsigned char *)wv.d_nullbytes.p;
-    d.local_bytes = local_bytes;
-    d.scan_smem = b->scan_smem;
-    d.scan_blocks = std::max(1, std::min(ctx->sm_count * bps, d.n_chunks));
   }
   CK(cudaMemcpyAsync(b->d_bq.p, dbq.data(), sizeof(qm_bq) * n, cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
@@ -3756,7 +3783,24 @@ int batch_layout(qm_batch *b) {
 int wave_launch(qm_batch *b, BatchWave &wv, cudaStream_t st) {
   qm_ctx *ctx = b->ctx;
   if (b->mode == 0) {
-    CK(qm_batch_launch_all(wv.dev, st));
+    const qm_batch_dev &d = wv.dev;
+    CK(qm_batch_launch_init(d, st));
+    const int k = std::min<int>((int)wv.classes.size(), (int)b->side.size());
+    if (k > 1) {
+      CK(cudaEventRecord(b->fork_ev, st));
+      for (int j = 0; j < k; j++) CK(cudaStreamWaitEvent(b->side[j], b->fork_ev, 0));
+    }
+    for (size_t c = 0; c < wv.classes.size(); c++) {
+      const BatchWave::ClassLaunch &L = wv.classes[c];
+      CK(qm_batch_launch_class(L.cls, d.bq, d.chunks + L.chunk0, L.n_chunks, d.counter + c, L.local_bytes,
+                               L.blocks, L.smem, k > 1 ? b->side[c % k] : st));
+    }
+    if (k > 1)
+      for (int j = 0; j < k; j++) {
+        CK(cudaEventRecord(b->side_ev[j], b->side[j]));
+        CK(cudaStreamWaitEvent(st, b->side_ev[j], 0));
+      }
+    CK(qm_batch_launch_finalize(d, st));
   } else {
     CK(qm_batch_launch_init(wv.dev, st));
     const int nq = wv.q1 - wv.q0;

@@ -11,8 +11,6 @@
 // prefix popcount of the query's bitmap of first rows at the group's own
 // first row.  Each query's rows are written at their rank into one packed
 // buffer (columns, then NULL bitmaps), so one copy returns every result.
-#include <cub/cub.cuh>
-
 #include "qm_batch.h"
 #include "qm_launch.h"
 #include "qm_kernels.cuh"
@@ -68,6 +66,10 @@ __device__ void batch_flush(const qm_scan_args &a, uint64_t *lkeys, uint64_t *lw
   }
 }
 
+// DD / NV / KK: the dedupe flag, value-column count and key kind of the
+// queries this instantiation takes (QM_NV_ANY / QM_KK_ANY / DD 2: read from
+// each query's plan); a batch runs one persistent launch per class present.
+template <int DD, int NV, int KK>
 __global__ void __launch_bounds__(QM_SCAN_THREADS)
     qm_batch_scan(const qm_bq *__restrict__ bq, const qm_chunk *__restrict__ chunks, int n_chunks, int *counter,
                   int local_bytes) {
@@ -154,14 +156,14 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
         const int64_t row = queue[qn - 32 + lane];
         __syncwarp();
         qn -= 32;
-        drain_round_any(P, lkeys, lw, L, &l_used, lane, true, row, scr);
+        drain_round_any<DD, NV, KK, (NV > QM_MAX_VCOLS)>(P, lkeys, lw, L, &l_used, lane, true, row, scr);
       }
     }
     if (qn > 0) {
       const bool active = lane < qn;
       const int64_t row = active ? (int64_t)queue[lane] : 0;
       __syncwarp();
-      drain_round_any(P, lkeys, lw, L, &l_used, lane, active, row, scr);
+      drain_round_any<DD, NV, KK, (NV > QM_MAX_VCOLS)>(P, lkeys, lw, L, &l_used, lane, active, row, scr);
     }
     __syncthreads();
   }
@@ -184,10 +186,6 @@ __global__ void qm_batch_mark(const qm_bq *bq, const int64_t *slot0, int n, int6
   }
 }
 
-__global__ void qm_batch_popc(const uint32_t *bitmap, int64_t words, uint32_t *counts) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= words; i += (int64_t)gridDim.x * blockDim.x)
-    counts[i] = i < words ? __popc(bitmap[i]) : 0;
-}
 
 __host__ __device__ inline int64_t align16(int64_t x) { return (x + 15) & ~(int64_t)15; }
 
@@ -274,11 +272,62 @@ using namespace qm;
 
 size_t qm_batch_smem_bytes(int local_bytes) { return batch_smem(local_bytes, QM_SCAN_THREADS / 32).bytes; }
 
-cudaError_t qm_batch_configure(size_t smem, int *blocks_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(qm_batch_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+namespace {
+
+template <int DD, int NV, int KK>
+cudaError_t batch_class_configure(size_t smem, int *blocks_per_sm) {
+  cudaError_t e =
+      cudaFuncSetAttribute(qm_batch_scan<DD, NV, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_batch_scan, QM_SCAN_THREADS, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_batch_scan<DD, NV, KK>, QM_SCAN_THREADS,
+                                                       smem);
 }
+
+// The class instantiations: value-column counts 1 and 2 and key kinds int32 /
+// int64 specialised, everything else through the run-time-plan kernel.
+#define QM_BATCH_CLASSES(X)                                                                              \
+  X(0, 1, QM_KK_I32) X(0, 1, QM_KK_I64) X(0, 2, QM_KK_I32) X(0, 2, QM_KK_I64) X(1, 1, QM_KK_I32)         \
+  X(1, 1, QM_KK_I64) X(1, 2, QM_KK_I32) X(1, 2, QM_KK_I64)
+
+}  // namespace
+
+int qm_batch_class_of(const qm_scan_args &a) {
+  bool fixed = false;
+  for (int c = 0; c < a.agg.n_vcols; ++c) fixed = fixed || (a.agg.vcol[c].flags & VF_FIXED) != 0;
+  const qm_keyspec &K = a.key;
+  int kk = QM_KK_ANY;
+  if (K.n_cols == 1 && K.pack == QP_RAW && K.nulls[0] == nullptr)
+    kk = K.dtype[0] == QM_I64 ? QM_KK_I64 : K.dtype[0] == QM_I32 ? QM_KK_I32 : QM_KK_ANY;
+  const int nv = a.agg.n_vcols;
+  if (!fixed && (nv == 1 || nv == 2) && kk != QM_KK_ANY)
+    return 1 + (a.dedupe ? 4 : 0) + (nv == 2 ? 2 : 0) + (kk == QM_KK_I64 ? 1 : 0);
+  return 0;  // the run-time-plan kernel
+}
+
+cudaError_t qm_batch_class_configure(int cls, size_t smem, int *blocks_per_sm) {
+  int c = 1;
+#define QM_CFG_(DD, NV, KK) \
+  if (cls == c++) return batch_class_configure<DD, NV, KK>(smem, blocks_per_sm);
+  QM_BATCH_CLASSES(QM_CFG_)
+#undef QM_CFG_
+  return batch_class_configure<2, QM_NV_ANY, QM_KK_ANY>(smem, blocks_per_sm);
+}
+
+cudaError_t qm_batch_launch_class(int cls, const qm_bq *bq, const qm_chunk *chunks, int n_chunks, int *counter,
+                                  int local_bytes, int blocks, size_t smem, cudaStream_t st) {
+  int c = 1;
+#define QM_LAUNCH_(DD, NV, KK)                                                                            \
+  if (cls == c++) {                                                                                       \
+    qm_batch_scan<DD, NV, KK><<<blocks, QM_SCAN_THREADS, smem, st>>>(bq, chunks, n_chunks, counter, local_bytes); \
+    return cudaGetLastError();                                                                            \
+  }
+  QM_BATCH_CLASSES(QM_LAUNCH_)
+#undef QM_LAUNCH_
+  qm_batch_scan<2, QM_NV_ANY, QM_KK_ANY><<<blocks, QM_SCAN_THREADS, smem, st>>>(bq, chunks, n_chunks, counter,
+                                                                              local_bytes);
+  return cudaGetLastError();
+}
+
 
 static int grid_for(int64_t n, int sm_count, int per_sm) {
   int64_t b = (n + 255) / 256;
@@ -289,31 +338,16 @@ static int grid_for(int64_t n, int sm_count, int per_sm) {
 cudaError_t qm_batch_launch_init(const qm_batch_dev &d, cudaStream_t st) {
   cudaError_t e;
   if ((e = cudaMemsetAsync(d.statuses, 0, sizeof(qm_status) * d.n, st))) return e;
-  if ((e = cudaMemsetAsync(d.counter, 0, sizeof(int), st))) return e;
+  if ((e = cudaMemsetAsync(d.counter, 0, sizeof(int) * QM_BATCH_CLASS_SLOTS, st))) return e;
   if ((e = cudaMemsetAsync(d.bitmap, 0, sizeof(uint32_t) * (d.bm_words + 1), st))) return e;
   qm_batch_init<<<grid_for(d.total_slots, d.sm_count, 16), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots);
   return cudaGetLastError();
 }
 
-cudaError_t qm_batch_launch_persistent(const qm_batch_dev &d, cudaStream_t st) {
-  qm_batch_scan<<<d.scan_blocks, QM_SCAN_THREADS, d.scan_smem, st>>>(d.bq, d.chunks, d.n_chunks, d.counter,
-                                                                     d.local_bytes);
-  return cudaGetLastError();
-}
-
-cudaError_t qm_batch_launch_all(const qm_batch_dev &d, cudaStream_t st) {
-  cudaError_t e;
-  if ((e = qm_batch_launch_init(d, st))) return e;
-  if ((e = qm_batch_launch_persistent(d, st))) return e;
-  return qm_batch_launch_finalize(d, st);
-}
-
 cudaError_t qm_batch_launch_finalize(const qm_batch_dev &d, cudaStream_t st) {
   cudaError_t e;
   qm_batch_mark<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap);
-  qm_batch_popc<<<grid_for(d.bm_words + 1, d.sm_count, 8), 256, 0, st>>>(d.bitmap, d.bm_words, d.popc);
-  size_t tb = d.scan_temp_bytes;
-  if ((e = cub::DeviceScan::ExclusiveSum(d.scan_temp, tb, d.popc, d.ranks, (int)(d.bm_words + 1), st))) return e;
+  if ((e = qm_scan_popc_words(d.bitmap, d.bm_words, d.ranks, d.scan_temp, d.scan_temp_bytes, st))) return e;
   qm_batch_layout<<<1, 32, 0, st>>>(d.bq, d.n, d.ranks, d.meta);
   qm_batch_emit<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap,
                                                                          d.ranks, d.packed, d.nullbytes);
@@ -324,6 +358,6 @@ cudaError_t qm_batch_launch_finalize(const qm_batch_dev &d, cudaStream_t st) {
 }
 
 cudaError_t qm_batch_scan_temp_bytes(int64_t words, size_t *bytes) {
-  return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
-                                       (int)(words + 1));
+  *bytes = qm_scan_temp_bytes_for(words);
+  return cudaSuccess;
 }

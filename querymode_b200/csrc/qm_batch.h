@@ -56,19 +56,22 @@ struct qm_batch_dev {
   size_t meta_bytes;
   unsigned char *packed;
   unsigned char *nullbytes;
-  int scan_blocks;
-  size_t scan_smem;
-  int local_bytes;
 };
 
 size_t qm_batch_smem_bytes(int local_bytes);
-cudaError_t qm_batch_configure(size_t smem, int *blocks_per_sm);
-// The three phases of a batched run: clear statuses, bitmaps and group
-// tables; the persistent scan over every query's chunks (or, instead, one
-// specialised scan launch per query issued by the host); rank, lay out,
-// emit and pack the results.
+// Per-class persistent launches: a query's class (dedupe flag, value-column
+// count, key kind, fixed-point sums) picks a specialised instantiation of
+// the persistent kernel (0: the run-time-plan one).  A wave keeps one work
+// counter per class (QM_BATCH_CLASS_SLOTS counters from dev.counter).
+#define QM_BATCH_CLASS_SLOTS 16
+#define QM_BATCH_CLASSES_N 9
+int qm_batch_class_of(const qm_scan_args &a);
+cudaError_t qm_batch_class_configure(int cls, size_t smem, int *blocks_per_sm);
+cudaError_t qm_batch_launch_class(int cls, const qm_bq *bq, const qm_chunk *chunks, int n_chunks, int *counter,
+                                  int local_bytes, int blocks, size_t smem, cudaStream_t st);
+// The phases of a batched run: clear statuses, counters, bitmaps and group
+// tables; the persistent scans (qm_batch_launch_class, one per class) or one
+// specialised scan launch per query; rank, lay out, emit and pack the results.
 cudaError_t qm_batch_launch_init(const qm_batch_dev &d, cudaStream_t st);
-cudaError_t qm_batch_launch_persistent(const qm_batch_dev &d, cudaStream_t st);
 cudaError_t qm_batch_launch_finalize(const qm_batch_dev &d, cudaStream_t st);
-cudaError_t qm_batch_launch_all(const qm_batch_dev &d, cudaStream_t st);
 cudaError_t qm_batch_scan_temp_bytes(int64_t words, size_t *bytes);

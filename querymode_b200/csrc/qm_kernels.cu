@@ -8,7 +8,6 @@
 //   qm_select_write
 //   qm_minmax_kernel    integer column min / max (planning statistics)
 #include <cuda_fp16.h>
-#include <thrust/iterator/transform_iterator.h>
 #include <cub/cub.cuh>
 
 #include <climits>
@@ -231,10 +230,6 @@ __global__ void qm_mark_first(const uint64_t *t, int64_t n_slots_total, int stri
   }
 }
 
-__global__ void qm_popc_words(const uint32_t *bitmap, int64_t words, uint32_t *counts) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= words; i += (int64_t)gridDim.x * blockDim.x)
-    counts[i] = i < words ? __popc(bitmap[i]) : 0;
-}
 
 __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
                                const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
@@ -884,6 +879,134 @@ __global__ void qm_minmax_init(long long *out) {
 // ---------------------------------------------------------------- launchers
 using namespace qm;
 
+// ---- exclusive scan (u32 or popcounts of u32 words -> u64) -------------------
+// Three phases without waits between blocks: every block sums its tile of
+// SCAN_TILE inputs; one block turns the tile sums into tile offsets; every
+// block scans its tile again (thread sums, warp shuffles, one shared-memory
+// pass over the warps) and adds its tile's offset.  out[n] receives the
+// total.  POPC: the inputs are bitmap words and count their set bits.
+#define QM_SCAN_BLOCK 256
+#define QM_SCAN_PER 8
+#define QM_SCAN_TILE (QM_SCAN_BLOCK * QM_SCAN_PER)
+
+template <bool POPC>
+__device__ __forceinline__ uint64_t scan_in(const uint32_t *in, int64_t i, int64_t n) {
+  if (i >= n) return 0;
+  const uint32_t x = in[i];
+  return POPC ? (uint64_t)__popc(x) : (uint64_t)x;
+}
+
+template <bool POPC>
+__global__ void __launch_bounds__(QM_SCAN_BLOCK) qm_scan_tile_sums(const uint32_t *in, int64_t n, uint64_t *sums) {
+  __shared__ uint64_t wsum[QM_SCAN_BLOCK / 32];
+  const int64_t base = (int64_t)blockIdx.x * QM_SCAN_TILE + (int64_t)threadIdx.x * QM_SCAN_PER;
+  uint64_t t = 0;
+#pragma unroll
+  for (int k = 0; k < QM_SCAN_PER; ++k) t += scan_in<POPC>(in, base + k, n);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(QM_FULL, t, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t b = 0;
+    for (int w = 0; w < QM_SCAN_BLOCK / 32; ++w) b += wsum[w];
+    sums[blockIdx.x] = b;
+  }
+}
+
+// one block: tile sums -> exclusive tile offsets (in place), total at sums[tiles]
+__global__ void __launch_bounds__(1024) qm_scan_tile_offsets(uint64_t *sums, int64_t tiles) {
+  __shared__ uint64_t part[1024];
+  const int64_t per = (tiles + blockDim.x - 1) / blockDim.x;
+  const int64_t b0 = (int64_t)threadIdx.x * per;
+  uint64_t t = 0;
+  for (int64_t i = 0; i < per; ++i)
+    if (b0 + i < tiles) t += sums[b0 + i];
+  part[threadIdx.x] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t acc = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      const uint64_t x = part[i];
+      part[i] = acc;
+      acc += x;
+    }
+    sums[tiles] = acc;
+  }
+  __syncthreads();
+  uint64_t acc = part[threadIdx.x];
+  for (int64_t i = 0; i < per; ++i)
+    if (b0 + i < tiles) {
+      const uint64_t x = sums[b0 + i];
+      sums[b0 + i] = acc;
+      acc += x;
+    }
+}
+
+template <bool POPC>
+__global__ void __launch_bounds__(QM_SCAN_BLOCK)
+    qm_scan_tiles(const uint32_t *in, int64_t n, const uint64_t *offsets, uint64_t *out, int write_total) {
+  __shared__ uint64_t wsum[QM_SCAN_BLOCK / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * QM_SCAN_TILE + (int64_t)threadIdx.x * QM_SCAN_PER;
+  uint64_t v[QM_SCAN_PER];
+  uint64_t t = 0;
+#pragma unroll
+  for (int k = 0; k < QM_SCAN_PER; ++k) {
+    v[k] = scan_in<POPC>(in, base + k, n);
+    t += v[k];
+  }
+  uint64_t x = t;  // inclusive scan of thread sums across the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(QM_FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t acc = 0;
+    for (int w = 0; w < QM_SCAN_BLOCK / 32; ++w) {
+      const uint64_t y = wsum[w];
+      wsum[w] = acc;
+      acc += y;
+    }
+  }
+  __syncthreads();
+  uint64_t run = offsets[blockIdx.x] + wsum[warp] + x - t;  // exclusive offset of this thread's first input
+#pragma unroll
+  for (int k = 0; k < QM_SCAN_PER; ++k) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+  if (write_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = offsets[gridDim.x];
+}
+
+// Scratch bytes of qm_scan_u64 over n inputs.
+size_t qm_scan_temp_bytes_for(int64_t n) {
+  return (size_t)(((n + QM_SCAN_TILE - 1) / QM_SCAN_TILE) + 2) * sizeof(uint64_t);
+}
+
+// out[i] = sum of inputs before i, i < n; with write_total also out[n] = the
+// total (out then holds n + 1 entries).
+template <bool POPC>
+cudaError_t qm_scan_u64(const uint32_t *in, int64_t n, uint64_t *out, void *temp, size_t temp_bytes,
+                        cudaStream_t st, bool write_total = true) {
+  const int64_t tiles = std::max<int64_t>((n + QM_SCAN_TILE - 1) / QM_SCAN_TILE, 1);
+  if (temp_bytes < qm_scan_temp_bytes_for(n)) return cudaErrorInvalidValue;
+  uint64_t *sums = static_cast<uint64_t *>(temp);
+  qm_scan_tile_sums<POPC><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums);
+  qm_scan_tile_offsets<<<1, 1024, 0, st>>>(sums, tiles);
+  qm_scan_tiles<POPC><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums, out, write_total ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_scan_popc_words(const uint32_t *bitmap, int64_t words, uint64_t *ranks, void *temp, size_t temp_bytes,
+                               cudaStream_t st) {
+  return qm_scan_u64<true>(bitmap, words, ranks, temp, temp_bytes, st);
+}
+
+
 size_t qm_scan_smem_bytes(int local_slots, int local_hash, int n_words, int stage_tile_bytes, int stage_depth,
                           int priv) {
   return make_smem_layout(local_slots, local_hash, n_words, QM_SCAN_THREADS / 32, stage_tile_bytes, stage_depth, priv)
@@ -1024,8 +1147,10 @@ cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, i
                                 uint64_t *ranks, void *temp, size_t *temp_bytes, unsigned char *out, uint32_t *nulls,
                                 int sm_count, cudaStream_t st) {
   const int64_t words = (n_rows + 31) / 32;
-  if (!temp) return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, (const uint32_t *)nullptr, (uint64_t *)nullptr,
-                                                  (int)(words + 1));
+  if (!temp) {
+    *temp_bytes = qm_scan_temp_bytes_for(words);
+    return cudaSuccess;
+  }
   if (n_rows <= 0) return cudaSuccess;
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
   // one resident wave: every warp owns a fixed range of words
@@ -1054,8 +1179,9 @@ cudaError_t qm_launch_pq_decode(const uint8_t *chunk, const qm_pq_page *pages, i
     return cudaGetLastError();
   }
   qm_pq_present<<<pblocks, 256, 0, st>>>(chunk, pages, n_pages, runs, n_rows, present);
-  qm_popc_words<<<blocks, 256, 0, st>>>(present, words, counts);
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, ranks, (int)(words + 1), st);
+  (void)counts;
+  (void)blocks;
+  cudaError_t e = qm_scan_u64<true>(present, words, ranks, temp, *temp_bytes, st);
   if (e != cudaSuccess) return e;
   scatter<<<wblocks, 256, 0, st>>>(chunk, pages, n_pages, iruns, width, in_width, conv, n_rows, present, ranks, out,
                                    nulls);
@@ -1126,18 +1252,6 @@ cudaError_t qm_launch_gather_rows(const unsigned char *src, const qm_outspec &O,
   return cudaGetLastError();
 }
 
-struct PopcWord {
-  __host__ __device__ uint64_t operator()(uint32_t w) const {
-#ifdef __CUDA_ARCH__
-    return (uint64_t)__popc(w);
-#else
-    return (uint64_t)__builtin_popcount(w);
-#endif
-  }
-};
-inline thrust::transform_iterator<PopcWord, const uint32_t *> popc_words_it(const uint32_t *bitmap) {
-  return thrust::make_transform_iterator(bitmap, PopcWord());
-}
 
 cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
                                  uint32_t *bitmap, int64_t words, uint32_t *counts, uint64_t *ranks, void *temp,
@@ -1148,12 +1262,12 @@ cudaError_t qm_launch_rank_first(const uint64_t *t, int64_t n_slots_total, int s
   qm_mark_first<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap, words);
   // the words' popcounts go straight into the scan (no counts pass)
   (void)counts;
-  return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, popc_words_it(bitmap), ranks, (int)(words + 1), st);
+  return qm_scan_u64<true>(bitmap, words, ranks, temp, temp_bytes, st);
 }
 
 cudaError_t qm_rank_temp_bytes(int64_t words, size_t *bytes) {
-  return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, popc_words_it(nullptr), (uint64_t *)nullptr,
-                                       (int)(words + 1));
+  *bytes = qm_scan_temp_bytes_for(words);
+  return cudaSuccess;
 }
 
 cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int stride, int count_word,
@@ -1166,9 +1280,15 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
   return cudaGetLastError();
 }
 
+// Exclusive scan of n u32 counts into u64 offsets (out[n - 1] + in[n - 1]
+// lands in out[n]).  temp null: *temp_bytes receives the scratch size.
 cudaError_t qm_exclusive_scan_u32(void *temp, size_t *temp_bytes, const uint32_t *in, uint64_t *out, int64_t n,
                                   cudaStream_t st) {
-  return cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, in, out, (int)n, st);
+  if (!temp) {
+    *temp_bytes = qm_scan_temp_bytes_for(n);
+    return cudaSuccess;
+  }
+  return qm_scan_u64<false>(in, n, out, temp, *temp_bytes, st, false);
 }
 
 cudaError_t qm_launch_select_write(int64_t n_tiles, const uint32_t *sel, const uint32_t *masks,

@@ -110,3 +110,9 @@ cudaError_t qm_launch_part_scan(int pass, const qm_scan_args &a, const qm_part_s
 cudaError_t qm_launch_part_offsets(const qm_part_spec &ps, cudaStream_t st);
 size_t qm_part_agg_smem(int local_slots, int local_hash, int n_words);
 cudaError_t qm_launch_part_agg(const qm_scan_args &a, const qm_part_spec &ps, int sm_count, cudaStream_t st);
+
+// The library's exclusive scan: scratch bytes for n inputs, and ranks of a
+// bitmap (ranks[i] = set bits in words before i, ranks[words] = all of them).
+size_t qm_scan_temp_bytes_for(int64_t n);
+cudaError_t qm_scan_popc_words(const uint32_t *bitmap, int64_t words, uint64_t *ranks, void *temp, size_t temp_bytes,
+                               cudaStream_t st);

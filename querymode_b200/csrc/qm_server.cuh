@@ -32,7 +32,7 @@ struct Request {
   int code = QM_OK;
   std::string msg;
   qm_result *res = nullptr;
-  srv_clock::time_point t_submit, t_launch, t_done;
+  srv_clock::time_point t_submit, t_take, t_launch, t_done;
   int batch_size = 0;
 };
 
@@ -117,6 +117,7 @@ struct qm_server {
       }
       rows += r.table->n_rows;
       r.state = RQ_RUNNING;
+      r.t_take = srv_clock::now();
       take.push_back(*it);
       it = queue.erase(it);
       if (take.back()->heavy || (int)take.size() >= cfg.max_batch) break;
@@ -407,6 +408,7 @@ int qm_server_wait(qm_server *s, uint64_t ticket, int64_t timeout_us, qm_result 
     timing->run_us = launched ? us_between(r->t_launch, r->t_done) : 0;
     timing->total_us = us_between(r->t_submit, r->t_done);
     timing->batch_size = r->batch_size;
+    timing->plan_us = launched ? (int32_t)us_between(r->t_take, r->t_launch) : 0;
   }
   if (msg && msg_len) snprintf(msg, msg_len, "%s", r->msg.c_str());
   if (out) *out = r->res;

@@ -855,7 +855,7 @@ class Server:
         tmo = -1 if timeout_s is None else int(timeout_s * 1e6)
         status = self.lib.qm_server_wait(self.h, ticket, tmo, C.byref(out), C.byref(tm), msg, len(msg))
         timing = {"queued_us": tm.queued_us, "run_us": tm.run_us, "total_us": tm.total_us,
-                  "batch_size": tm.batch_size}
+                  "batch_size": tm.batch_size, "plan_us": tm.plan_us}
         if status != A.QM_OK:
             raise A.QmError(status, msg.value.decode(errors="replace"))
         return Result.from_handle(self.lib, out, owned=True), timing
