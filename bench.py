@@ -70,10 +70,15 @@ def parse_args():
     p.add_argument("--serve-repeats", type=int, default=3)
     p.add_argument("--serve-burst", type=int, default=800, help="requests of the closed capacity burst")
     p.add_argument("--serve-plain", type=int, default=400, help="requests of the plain per-query comparison")
-    p.add_argument("--serve-lanes", type=int, default=4)
+    p.add_argument("--serve-lanes", type=int, default=8)
+    p.add_argument("--serve-max-rows", type=int, default=1 << 29, help="rows a serving batch may scan")
+    p.add_argument("--serve-max-groups", type=int, default=1 << 22,
+                   help="a request planned at more groups runs alone (heavy)")
     p.add_argument("--serve-loads", default="0.25,0.5,0.75,0.9", help="offered loads as fractions of capacity")
     p.add_argument("--batch-queries", type=int, default=256)
     p.add_argument("--batch-reps", type=int, default=3)
+    p.add_argument("--batch-choice", default="",
+                   help="mode,chunk_tiles,local_kb,blocks_per_sm,waves for the batch instead of the autotuner's search")
     return p.parse_args()
 
 
@@ -238,7 +243,7 @@ def check_parity(res, cols, q) -> dict:
 
 
 def run_config(ctx, stream, name: str, cols: dict, q, bytes_per_row: int, steps: int, warmup: int,
-               cpu_rows: int, note: str) -> dict:
+               cpu_rows: int, note: str, args=None) -> dict:
     """One more of the measured workloads, on one GPU: device-resident table
     (`value`: algorithmic bytes / CUDA-event time per query, result in host
     memory), the scan kernel's roofline, the same query end to end from
@@ -268,7 +273,42 @@ def run_config(ctx, stream, name: str, cols: dict, q, bytes_per_row: int, steps:
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
         t.close()
-        # end to end from pinned host memory: upload, query, result download
+    e2e = None
+    if not (args and args.no_e2e):
+        e2e = run_config_e2e(ctx, stream, cols, cq, n * bytes_per_row)
+    qbytes = n * bytes_per_row
+    scan_ms = float(np.mean(scan))
+    achieved = qbytes / (scan_ms / 1e3) / 1e9
+    cpu = None
+    if not (args and args.no_cpu):
+        sub = {k: np.ascontiguousarray(v[:cpu_rows]) for k, v in cols.items()}
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.run_full(sub, q, threads=threads)
+        cpu_s = time.perf_counter() - t0
+        sub_rows = len(next(iter(sub.values())))
+        cpu = {"value": sub_rows * bytes_per_row / cpu_s / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"first {sub_rows:,} rows, oracle one batch on {threads} threads"}
+    parity = None if (args and args.no_parity) else check_parity(res, cols, q)
+    return {
+        "workload": name, "rows": n, "bytes_per_row": bytes_per_row, "groups": int(res.n_rows),
+        "rows_selected": int(res.stats.rows_selected), "steps": steps, "warmup": max(3, warmup),
+        "ms_per_query": ms, "value": qbytes / (ms / 1e3) / 1e9, "unit": "GB/s", "rows_per_s": n / (ms / 1e3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel": "qm_scan_kernel", "kernel_ms": scan_ms},
+        "e2e": e2e, "cpu_baseline": cpu,
+        "parity": None if parity is None else parity["ok"], "parity_check": parity, "gpu_launches": launches,
+        "note": note,
+    }
+
+
+def run_config_e2e(ctx, stream, cols: dict, cq, qbytes: int) -> dict:
+    """The query end to end from pinned host columns: upload, query, result
+    download, every step, CUDA events on the context's stream."""
+    import torch
+    with torch.cuda.stream(stream):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in cols.items()}
         h2d = sum(v.nbytes for v in pinned.values())
         tt = ctx.table(pinned)
@@ -286,28 +326,8 @@ def run_config(ctx, stream, name: str, cols: dict, q, bytes_per_row: int, steps:
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / e2e_steps
         del pinned
-    qbytes = n * bytes_per_row
-    scan_ms = float(np.mean(scan))
-    achieved = qbytes / (scan_ms / 1e3) / 1e9
-    sub = {k: np.ascontiguousarray(v[:cpu_rows]) for k, v in cols.items()}
-    threads = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    oracle.run_full(sub, q, threads=threads)
-    cpu_s = time.perf_counter() - t0
-    parity = check_parity(res, cols, q)
-    return {
-        "workload": name, "rows": n, "bytes_per_row": bytes_per_row, "groups": int(res.n_rows),
-        "rows_selected": int(res.stats.rows_selected), "steps": steps, "warmup": max(3, warmup),
-        "ms_per_query": ms, "value": qbytes / (ms / 1e3) / 1e9, "unit": "GB/s", "rows_per_s": n / (ms / 1e3),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "kernel": "qm_scan_kernel", "kernel_ms": scan_ms},
-        "e2e": {"value": qbytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "steps": e2e_steps},
-        "cpu_baseline": {"value": len(next(iter(sub.values()))) * bytes_per_row / cpu_s / 1e9, "unit": "GB/s",
-                         "cores": threads, "kind": "port",
-                         "sample": f"first {len(next(iter(sub.values()))):,} rows, oracle one batch on {threads} threads"},
-        "parity": parity["ok"], "parity_check": parity, "gpu_launches": launches, "note": note,
-    }
+    return {"value": qbytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "steps": e2e_steps}
 
 
 def run_configs(ctx, stream, args) -> dict:
@@ -321,7 +341,7 @@ def run_configs(ctx, stream, args) -> dict:
         out["orders_1m"] = run_config(ctx, stream, "orders_1m", orders, datagen.orders_query(), 16,
                                       max(args.config_steps, 50), args.warmup, 1_000_000,
                                       "status = 1 GROUP BY region SUM(amount), COUNT(*); 16 groups; launch- and "
-                                      "sync-bound (16 MB per query)")
+                                      "sync-bound (16 MB per query)", args)
         del orders
     if not which & {"filtered", "unfiltered"}:
         return out
@@ -330,12 +350,13 @@ def run_configs(ctx, stream, args) -> dict:
     if "filtered" in which:
         out[f"{wname}_filtered"] = run_config(
             ctx, stream, f"{wname}_filtered", wide, datagen.wide_keys_query(True), 20, args.config_steps, args.warmup,
-            20_000_000, "flag = 1 AND val > 0 (~0.5 %) GROUP BY key SUM(val), COUNT(*); key int64 over 2^24 values")
+            20_000_000, "flag = 1 AND val > 0 (~0.5 %) GROUP BY key SUM(val), COUNT(*); key int64 over 2^24 values",
+            args)
     if "unfiltered" in which:
         out[f"{wname}_unfiltered"] = run_config(
             ctx, stream, f"{wname}_unfiltered", wide, datagen.wide_keys_query(False), 16,
             max(3, args.config_steps // 4), args.warmup, 20_000_000,
-            "no filter, GROUP BY key SUM(val), COUNT(*): 16.7M groups, result 0.4 GB to the host")
+            "no filter, GROUP BY key SUM(val), COUNT(*): 16.7M groups, result 0.4 GB to the host", args)
     return out
 
 
@@ -375,7 +396,13 @@ def run_batched(ctx, stream, local: int, args) -> dict:
     tables = [ctx.table(t) for t in dev_tables]
     cqs = [CQuery(datagen.batch_query(s)) for s in specs]
     batch = ctx.batch(tables, cqs)
-    tuned = autotune.tune_batch(batch, reps=1, device_name=torch.cuda.get_device_name(local))
+    if args.batch_choice:
+        keys = ("mode", "chunk_tiles", "local_kb", "blocks_per_sm", "waves")
+        choice = dict(zip(keys, (int(x) for x in args.batch_choice.split(","))))
+        autotune.apply_choice(batch, choice)
+        tuned = {"choice": choice, "search_s": 0.0, "trials": []}
+    else:
+        tuned = autotune.tune_batch(batch, reps=1, device_name=torch.cuda.get_device_name(local))
 
     def timed(fn, reps):
         e0 = torch.cuda.Event(enable_timing=True)
@@ -404,6 +431,7 @@ def run_batched(ctx, stream, local: int, args) -> dict:
         "plain_ms": plain_ms, "batched_ms": batch_ms, "plain_qps": n / (plain_ms / 1e3),
         "batched_qps": n / (batch_ms / 1e3), "speedup": plain_ms / batch_ms,
         "batched_scan_gbs": st["bytes"] / (st["device_ms"] / 1e3) / 1e9,
+        "batched_scan_frac": st["bytes"] / (st["device_ms"] / 1e3) / 1e9 / load_peaks()[0],
         "plain_wall_ms": plain_wall, "batched_wall_ms": batch_wall,
         "autotune": {"choice": tuned["choice"], "search_s": round(tuned["search_s"], 2),
                      "trials": len(tuned["trials"])},
@@ -533,10 +561,12 @@ def run_serving(local: int, args) -> dict:
             return t, wide_full
         return t, wide_q[int(r.integers(2))]
 
-    # requests over tables above 2^27 rows run alone (heavy); the last of
-    # the lanes takes small requests only
-    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0, max_batch_rows=1 << 27,
-                      lanes=args.serve_lanes)
+    # a batch scans at most --serve-max-rows rows; requests planned at more
+    # than --serve-max-groups groups (the 16M-group aggregate) run alone
+    # (heavy); the last of the lanes takes light requests only
+    srv = sctx.server(hbm_budget_bytes=150_000_000_000, max_batch=64, max_wait_us=0,
+                      max_batch_rows=args.serve_max_rows, lanes=args.serve_lanes,
+                      max_batch_groups=args.serve_max_groups)
     try:
         # warm-up: every table and query kind on every lane (column statistics are cached)
         for _ in range(args.serve_lanes):
@@ -578,10 +608,13 @@ def run_serving(local: int, args) -> dict:
             th.join()
             return np.array(lat), np.array(bs), done_at[0] - t0
 
-        # capacity: a closed burst of requests (after one untimed burst, which
-        # grows the lanes' buffers to the mix's working set)
-        serve([draw(rng) for _ in range(200)], None)
+        # capacity: closed bursts of requests.  The first burst grows the
+        # lanes' buffers and the pinned result pool to the mix's working set
+        # (reported as the cold capacity); the last one is the steady state.
         burst = [draw(rng) for _ in range(args.serve_burst)]
+        _, _, span = serve(burst, None)
+        cold_capacity = len(burst) / span
+        serve(burst, None)
         _, bsz, span = serve(burst, None)
         capacity = len(burst) / span
         loads = []
@@ -608,7 +641,7 @@ def run_serving(local: int, args) -> dict:
     # the same request mix as plain per-query launches (Table.run, result
     # in host memory), closed loop
     plain_reqs = [draw(rng) for _ in range(args.serve_plain)]
-    for t, q in plain_reqs[:20]:
+    for t, q in plain_reqs:  # one untimed pass: buffers and pinned pool at the mix's size
         t.run(q)
     t0 = time.perf_counter()
     for t, q in plain_reqs:
@@ -618,7 +651,9 @@ def run_serving(local: int, args) -> dict:
     del tabs, handles
     torch.cuda.empty_cache()
     return {"tables": 8, "table_gb": round(table_bytes / 1e9, 2), "hbm_budget_gb": 150, "lanes": st["lanes"],
-            "capacity_qps": round(capacity, 1), "plain_qps": round(plain_qps, 1),
+            "max_batch_rows": args.serve_max_rows, "max_batch_groups": args.serve_max_groups,
+            "capacity_qps": round(capacity, 1), "cold_capacity_qps": round(cold_capacity, 1),
+            "plain_qps": round(plain_qps, 1),
             "served_vs_plain": round(capacity / plain_qps, 2),
             "queries": served + len(burst), "queries_per_load": args.serve_queries * args.serve_repeats,
             "repeats": args.serve_repeats, "loads": loads,

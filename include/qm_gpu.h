@@ -551,7 +551,10 @@ typedef struct {
   int32_t lanes;            /* batches in flight at once, each on its own
                                stream (0: 4); with more than one, the last
                                lane takes light requests only               */
-  int32_t reserved;
+  int32_t max_batch_groups; /* a request the planner sizes at more groups
+                               than this (e.g. a 16M-group aggregate) is
+                               heavy too: it runs alone, never on the light
+                               lane (0: no limit)                          */
 } qm_server_config;
 
 typedef struct {

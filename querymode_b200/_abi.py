@@ -113,7 +113,7 @@ class QmStats(C.Structure):
 
 class QmServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_batch", C.c_int32), ("max_wait_us", C.c_int32),
-                ("max_batch_rows", C.c_int64), ("lanes", C.c_int32), ("reserved", C.c_int32)]
+                ("max_batch_rows", C.c_int64), ("lanes", C.c_int32), ("max_batch_groups", C.c_int32)]
 
 
 class QmServerTiming(C.Structure):

@@ -1509,8 +1509,12 @@ constexpr size_t SPEC_RESULT_BYTES = (size_t)8 << 20;
 // ctx->hstatus) and the group count come with the same synchronise.  On a
 // device error *out stays null and *spec holds the status: the caller
 // regrows and runs again.
+// rows_resident: the plan's key columns hold every row the first-row bitmap
+// indexes (a query over a resident table), so a large direct-indexed result
+// can be emitted in output order by walking that bitmap.
+constexpr int64_t WALK_MIN_SLOTS = (int64_t)1 << 20;
 int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1,
-                 qm_status *spec = nullptr) {
+                 qm_status *spec = nullptr, bool rows_resident = false) {
   const Plan &pl = gt.pl;
   const Exec &ex = gt.ex;
   int64_t G = 0;
@@ -1580,8 +1584,17 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   qm_result *R = new qm_result();
   R->pool = ctx->pool;
   R->buf = hbuf;
-  CK(cudaMemsetAsync(ctx->out.p, 0, off + 16, ctx->stream));
-  if (ranked) {
+  // NULL flags are set bit by bit: clear the bitmaps (every data cell of the
+  // G rows is written by the emit)
+  for (int k = 0; k < O.n_out; k++)
+    if (O.o[k].null_offset >= 0)
+      CK(cudaMemsetAsync((char *)ctx->out.p + O.o[k].null_offset, 0, null_words_bytes, ctx->stream));
+  if (ranked && rows_resident && pl.key.mode == QK_DIRECT && ex.n_slots >= WALK_MIN_SLOTS) {
+    if (G > 0)
+      CK(qm_launch_emit_walk(gt.table, ex.stride, (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p,
+                             rank_words(gt), pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p, ctx->sm_count,
+                             ctx->stream));
+  } else if (ranked) {
     if (G > 0)
       CK(qm_launch_emit_ranked(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
                                (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, rank_words(gt),
@@ -2509,10 +2522,13 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
     if (ranked && (rc = launch_rank(ctx, gt))) return rc;
     qm_status st;
     qm_outspec Ocap = pl.outs;
-    if (ranked && !pl.post && result_layout(pl, Ocap, gt.ex.total_slots) <= SPEC_RESULT_BYTES) {
-      // small result: emitted and copied with the status, one synchronise
+    // a dense direct-indexed table (its groups fill most slots) costs no more
+    // to copy laid out for every slot than for its groups
+    const bool dense = pl.key.mode == QK_DIRECT && est * 4 >= gt.ex.total_slots * 3;
+    if (ranked && !pl.post && (dense || result_layout(pl, Ocap, gt.ex.total_slots) <= SPEC_RESULT_BYTES)) {
+      // small or dense result: emitted and copied with the status, one synchronise
       CK(cudaMemcpyAsync(ctx->hstatus.p, ctx->status.p, sizeof(qm_status), cudaMemcpyDeviceToHost, ctx->stream));
-      if ((rc = finish_table(ctx, gt, out, 0.f, -1, &st))) return rc;
+      if ((rc = finish_table(ctx, gt, out, 0.f, -1, &st, true))) return rc;
       if (*out) {
         (*out)->stats.rows_scanned = t->n_rows;
         (*out)->stats.bytes_scanned = pl.bytes_per_row * t->n_rows;
@@ -2543,7 +2559,7 @@ int qm_query_run(qm_ctx *ctx, const qm_table *table, const qm_query *q, qm_resul
     est = std::max<int64_t>(est * 4, (int64_t)st.groups_inserted * 2);
   }
   gt.rows_done = t->n_rows;
-  rc = finish_table(ctx, gt, out, 0.f, groups);
+  rc = finish_table(ctx, gt, out, 0.f, groups, nullptr, true);
   if (rc) return rc;
   (*out)->stats.rows_scanned = t->n_rows;
   (*out)->stats.bytes_scanned = pl.bytes_per_row * t->n_rows;

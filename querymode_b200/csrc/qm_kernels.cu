@@ -246,6 +246,31 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
   }
 }
 
+// The same output in output order, for a direct-indexed table whose key
+// columns still hold every row the first-row bitmap indexes: output row i is
+// the group whose first row is the i-th set bit, and that row's key is the
+// group's slot.  Consecutive threads take consecutive bitmap words, so the
+// output columns are written in runs (the slot-order emit scatters every
+// 8-byte cell to its rank, and a result of millions of groups then costs a
+// partial-sector write per cell).
+__global__ void qm_emit_walk(const uint64_t *t, int stride, const uint32_t *bitmap, const uint64_t *ranks,
+                             int64_t words, const __grid_constant__ qm_keyspec K, int64_t n_slots,
+                             const __grid_constant__ qm_outspec O, unsigned char *out) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t b = bitmap[w];
+    if (b == 0) continue;
+    int64_t i = (int64_t)ranks[w];
+    for (; b; b &= b - 1, ++i) {
+      const int64_t r = w * 32 + (__ffs(b) - 1);
+      int special;
+      const uint64_t key = row_key<QM_KK_ANY>(K, r, special);
+      const uint64_t s = special == 2 ? (uint64_t)n_slots : key - (uint64_t)K.base;
+      if (s > (uint64_t)n_slots) continue;  // not a group of this table (a failed run's bitmap)
+      emit_group<false>(t, stride, s, i, K, n_slots, O, out, nullptr, nullptr);
+    }
+  }
+}
+
 // ---- Parquet PLAIN pages -> a column ----------------------------------------
 // (src/parquet-decode.ts:390-618: decodeParquetColumnChunk's PLAIN path, and
 // decodePage, src/decode.ts:251-331)
@@ -914,32 +939,45 @@ __global__ void __launch_bounds__(QM_SCAN_BLOCK) qm_scan_tile_sums(const uint32_
   }
 }
 
-// one block: tile sums -> exclusive tile offsets (in place), total at sums[tiles]
+// one block: tile sums -> exclusive tile offsets (in place), total at
+// sums[tiles].  Each thread sums a run of tiles; the runs' sums are scanned
+// by warp shuffles (lanes, then the warps' totals in warp 0).
 __global__ void __launch_bounds__(1024) qm_scan_tile_offsets(uint64_t *sums, int64_t tiles) {
-  __shared__ uint64_t part[1024];
+  __shared__ uint64_t wtot[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t per = (tiles + blockDim.x - 1) / blockDim.x;
   const int64_t b0 = (int64_t)threadIdx.x * per;
   uint64_t t = 0;
   for (int64_t i = 0; i < per; ++i)
     if (b0 + i < tiles) t += sums[b0 + i];
-  part[threadIdx.x] = t;
+  uint64_t x = t;  // inclusive scan of the runs across the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(QM_FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wtot[warp] = x;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    uint64_t acc = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      const uint64_t x = part[i];
-      part[i] = acc;
-      acc += x;
+  if (warp == 0) {
+    const int nw = (int)(blockDim.x >> 5);
+    const uint64_t w = lane < nw ? wtot[lane] : 0;
+    uint64_t z = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(QM_FULL, z, o);
+      if (lane >= o) z += y;
     }
-    sums[tiles] = acc;
+    if (lane < nw) wtot[lane] = z - w;  // exclusive
+    if (lane == 31) sums[tiles] = z;
   }
   __syncthreads();
-  uint64_t acc = part[threadIdx.x];
+  uint64_t acc = wtot[warp] + x - t;  // exclusive offset of this thread's run
+  __syncthreads();  // every run's sums read before any is overwritten
   for (int64_t i = 0; i < per; ++i)
     if (b0 + i < tiles) {
-      const uint64_t x = sums[b0 + i];
+      const uint64_t v = sums[b0 + i];
       sums[b0 + i] = acc;
-      acc += x;
+      acc += v;
     }
 }
 
@@ -1277,6 +1315,14 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
   const int blocks = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
   qm_emit_ranked<<<std::max(blocks, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap, ranks,
                                                       words, K, n_slots, O, out);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_emit_walk(const uint64_t *t, int stride, const uint32_t *bitmap, const uint64_t *ranks,
+                                int64_t words, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
+                                unsigned char *out, int sm_count, cudaStream_t st) {
+  const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
+  qm_emit_walk<<<std::max(blocks, 1), 256, 0, st>>>(t, stride, bitmap, ranks, words, K, n_slots, O, out);
   return cudaGetLastError();
 }
 

@@ -1418,10 +1418,23 @@ __device__ __forceinline__ void set_null(unsigned char *out, int64_t null_offset
 // BYTES: NULL flags go to one byte per output row at nullbytes + nboff[k]
 // (every nullable output writes 0 or 1, so no clearing is needed);
 // otherwise set bits in the word bitmap at out + null_offset.
+// A NULL output cell: its flag, and zero in the data cell (the output
+// buffer is not cleared beforehand).
+__device__ __forceinline__ void zero_cell(unsigned char *col, int dtype, int64_t i) {
+  if (dtype == QM_I32 || dtype == QM_F32) {
+    reinterpret_cast<uint32_t *>(col)[i] = 0;
+  } else if (dtype == QM_I128) {
+    reinterpret_cast<uint64_t *>(col)[2 * i] = 0;
+    reinterpret_cast<uint64_t *>(col)[2 * i + 1] = 0;
+  } else {
+    reinterpret_cast<uint64_t *>(col)[i] = 0;
+  }
+}
 #define NULL_OUT()                                  \
   do {                                              \
     if (BYTES) nullbytes[nboff[k] + i] = 1;         \
     else set_null(out, o.null_offset, i);           \
+    zero_cell(col, o.dtype, i);                     \
   } while (0)
 template <bool BYTES>
 __device__ __forceinline__ void emit_group(const uint64_t *t, int stride, uint64_t s, int64_t i, const qm_keyspec &K,

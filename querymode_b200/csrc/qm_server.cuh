@@ -143,7 +143,7 @@ struct qm_server {
   // when nothing was admitted because the batches in flight hold the budget.
   bool run_batch(Lane &ln, std::vector<std::shared_ptr<Request>> &take) {
     qm_batch *b = ln.batch;
-    std::vector<std::shared_ptr<Request>> admitted, deferred;
+    std::vector<std::shared_ptr<Request>> admitted, deferred, heavy_back;
     int64_t working = 0;
     {
       std::unique_lock<std::mutex> cl(ctx_mu);
@@ -165,6 +165,13 @@ struct qm_server {
           complete(r, rc, ctx->err, nullptr);
           continue;
         }
+        if (cfg.max_batch_groups > 0 && !r->heavy && b->est[k] > cfg.max_batch_groups &&
+            (take.size() > 1 || ln.light_only)) {
+          // planned heavy: back to the queue, where it runs alone on a lane that takes heavy requests
+          r->heavy = true;
+          heavy_back.push_back(r);
+          continue;
+        }
         const int64_t need = batch_query_bytes(b, k);
         if (need > budget_alone) {
           char m[200];
@@ -181,6 +188,10 @@ struct qm_server {
         admitted.push_back(r);
       }
       if (!deferred.empty()) requeue_front(deferred);
+      if (!heavy_back.empty()) {
+        requeue_front(heavy_back);
+        cv_work.notify_all();
+      }
       const int n = (int)admitted.size();
       if (n == 0) return deferred.empty();
       // the planned queries are b's first n entries
@@ -305,9 +316,10 @@ int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out) 
   if (!ctx || !cfg || !out) return QM_ERR_INVALID;
   *out = nullptr;
   if (cfg->max_batch < 1 || cfg->max_batch > QM_BATCH_MAX || cfg->hbm_budget_bytes <= 0 || cfg->max_wait_us < 0 ||
-      cfg->lanes < 0 || cfg->lanes > 64)
+      cfg->lanes < 0 || cfg->lanes > 64 || cfg->max_batch_groups < 0)
     return set_err(ctx, QM_ERR_INVALID,
-                   "server config: max_batch 1..%d, a positive budget, max_wait_us >= 0, lanes 0..64", QM_BATCH_MAX);
+                   "server config: max_batch 1..%d, a positive budget, max_wait_us >= 0, lanes 0..64, "
+                   "max_batch_groups >= 0", QM_BATCH_MAX);
   cudaSetDevice(ctx->device);
   qm_server *s = new qm_server();
   s->ctx = ctx;

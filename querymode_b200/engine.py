@@ -577,8 +577,8 @@ class Context:
         return Batch(self, tables, queries)
 
     def server(self, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0,
-               max_batch_rows: int = 0, lanes: int = 0) -> "Server":
-        return Server(self, hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows, lanes)
+               max_batch_rows: int = 0, lanes: int = 0, max_batch_groups: int = 0) -> "Server":
+        return Server(self, hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows, lanes, max_batch_groups)
 
 
 class Table:
@@ -820,15 +820,16 @@ class Server:
     """A qm_server: native lanes (worker threads, each with its own CUDA
     stream) that take submitted requests over resident tables as batched
     launches while other lanes' batches run, within an HBM budget.  Requests
-    over tables of more than max_batch_rows rows run alone; the last lane
-    takes small requests only.  While it runs, the context is the server's:
+    over tables of more than max_batch_rows rows, or planned at more than
+    max_batch_groups groups, run alone; the last lane takes small requests
+    only.  While it runs, the context is the server's:
     register tables first."""
 
     def __init__(self, ctx: Context, hbm_budget_bytes: int, max_batch: int = 64, max_wait_us: int = 0,
-                 max_batch_rows: int = 0, lanes: int = 0):
+                 max_batch_rows: int = 0, lanes: int = 0, max_batch_groups: int = 0):
         self.ctx = ctx
         self.lib = ctx.lib
-        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows, lanes)
+        cfg = A.QmServerConfig(hbm_budget_bytes, max_batch, max_wait_us, max_batch_rows, lanes, max_batch_groups)
         h = C.c_void_p()
         ctx.check(self.lib.qm_server_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h

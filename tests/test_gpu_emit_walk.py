@@ -1,0 +1,73 @@
+"""Large direct-indexed results emitted in output order (the first-row bitmap
+walk used for resident tables of at least 2^20 group slots) against the
+oracle: keys and first-seen order, COUNT, integer SUM and float MIN / MAX
+bit-exact, float SUM / AVG within the path's tolerance (tests/helpers.py).
+Covers NULL keys (the direct table's NULL slot), digit-packed two-column keys
+with a nullable column, a filter that leaves most slots empty, and a
+post-aggregate ORDER BY / LIMIT over the walked result (finalizePartialAgg,
+src/partial-agg.ts:306-352; first-seen group order, src/types.ts:10-18)."""
+import numpy as np
+import pytest
+
+import dataclasses
+
+import oracle
+from oracle.post import post_aggregate
+from querymode_b200.engine import Column
+from querymode_b200.query import AggregateOp, FilterOp, QueryDescriptor
+from tests.helpers import assert_same
+
+pytestmark = pytest.mark.gpu
+
+AGGS = [AggregateOp("sum", "v"), AggregateOp("count", "*"), AggregateOp("min", "v"), AggregateOp("max", "w"),
+        AggregateOp("avg", "v"), AggregateOp("sum", "w")]
+
+
+def run(ctx, cols, q):
+    t = ctx.table(cols)
+    g = t.run(q)
+    t.close()
+    return g
+
+
+def test_int64_keys_with_nulls(ctx):
+    rng = np.random.default_rng(11)
+    n = 6_000_000
+    key = Column(rng.integers(-1000, (1 << 21) - 1000, n).astype(np.int64), rng.random(n) < 0.05)
+    cols = {"key": key, "v": rng.normal(size=n) * 10, "w": rng.integers(-50, 50, n).astype(np.int32)}
+    q = QueryDescriptor(group_by=["key"], aggregates=AGGS)
+    g = run(ctx, cols, q)
+    assert g.n_rows > 1_500_000
+    assert_same(g, oracle.run_full(cols, q), ctx_msg="int64 keys with NULLs")
+
+
+def test_two_packed_keys_nullable(ctx):
+    rng = np.random.default_rng(12)
+    n = 5_000_000
+    cols = {"a": rng.integers(0, 1500, n).astype(np.int32),
+            "b": Column(rng.integers(0, 1000, n).astype(np.int64), rng.random(n) < 0.02),
+            "v": rng.random(n), "w": rng.integers(0, 7, n).astype(np.int32)}
+    q = QueryDescriptor(group_by=["a", "b"], aggregates=AGGS)
+    g = run(ctx, cols, q)
+    assert g.n_rows > 1_000_000
+    assert_same(g, oracle.run_full(cols, q), ctx_msg="packed keys")
+
+
+def test_filtered_sparse_slots(ctx):
+    rng = np.random.default_rng(13)
+    n = 8_000_000
+    cols = {"key": rng.integers(0, 1 << 22, n).astype(np.int32), "f": rng.integers(0, 100, n).astype(np.int32),
+            "v": rng.normal(size=n), "w": rng.integers(-9, 9, n).astype(np.int32)}
+    q = QueryDescriptor(filters=[FilterOp("f", "lt", 60)], group_by=["key"], aggregates=AGGS)
+    assert_same(run(ctx, cols, q), oracle.run_full(cols, q), ctx_msg="filtered")
+
+
+def test_order_by_limit_after_walk(ctx):
+    rng = np.random.default_rng(14)
+    n = 4_000_000
+    cols = {"key": rng.integers(0, 1 << 21, n).astype(np.int64), "v": rng.normal(size=n),
+            "w": rng.integers(0, 1000, n).astype(np.int32)}
+    q = QueryDescriptor(group_by=["key"], aggregates=AGGS)
+    want = post_aggregate(oracle.run_full(cols, q), "sum_w", True, 1000, 0)
+    got = run(ctx, cols, dataclasses.replace(q, sort_column="sum_w", sort_desc=True, limit=1000))
+    assert_same(got, want, ctx_msg="order by / limit")

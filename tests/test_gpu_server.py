@@ -188,3 +188,31 @@ def test_request_overlaps_heavy_batch():
         assert st["heavy"] >= 3 and st["lanes"] == 3 and st["peak_in_flight"] >= 2
     finally:
         srv.close()
+
+
+def test_planned_groups_make_a_request_heavy():
+    """With max_batch_groups, a request the planner sizes at more groups (a
+    16M-key aggregate over a table small enough to batch by rows) is sent
+    back and runs alone on a lane that takes heavy requests; the light
+    requests submitted with it still batch together; all equal their
+    results alone."""
+    ctx = Context(0)
+    heavy_t = ctx.table(datagen.wide_keys(8_000_000, seed=32, n_keys=1 << 24))
+    light_t = ctx.table(datagen.orders(300_000, seed=32))
+    hq, lq = datagen.wide_keys_query(False), datagen.orders_query()
+    heavy_alone, light_alone = heavy_t.run(hq), light_t.run(lq)
+    srv = ctx.server(hbm_budget_bytes=40 << 30, max_batch=16, max_batch_rows=0, lanes=2, max_batch_groups=1 << 20)
+    try:
+        for _ in range(3):
+            tickets = [srv.submit(light_t, lq) for _ in range(6)] + [srv.submit(heavy_t, hq)] + \
+                      [srv.submit(light_t, lq) for _ in range(6)]
+            timings = []
+            for i, t in enumerate(tickets):
+                res, tm = srv.wait(t)
+                assert_same(res, heavy_alone if i == 6 else light_alone)
+                timings.append(tm)
+            assert timings[6]["batch_size"] == 1
+        st = srv.stats()
+        assert st["heavy"] >= 3 and st["failed"] == 0
+    finally:
+        srv.close()
