@@ -404,12 +404,12 @@ int qm_query_run_noalloc(qm_ctx *ctx, int64_t n_rows, int32_t n_cols, const qm_c
 typedef struct qm_batch qm_batch;
 
 /* Plan n independent filter -> GROUP BY queries, query i over table i, for
- * one persistent fused launch (the reference runs them as n separate
- * executions, each a full pipeline, src/client.ts:1003-1085).  Blocks claim
- * (query, row range) chunks of uneven queries from a shared counter; the
- * whole run — table init, scan, first-seen ordering, finalize — is captured
- * as a CUDA graph on the first qm_batch_run and replayed afterwards.  At
- * most 4096 queries. */
+ * one batched run (the reference runs them as n separate executions, each a
+ * full pipeline, src/client.ts:1003-1085).  The queries are cut into waves;
+ * each wave — table init, scans, first-seen ordering, finalize — is captured
+ * as a CUDA graph on the first qm_batch_run and replayed afterwards, and its
+ * packed results cross to host memory while later waves run (see
+ * qm_batch_set_mode for the two ways a wave scans).  At most 4096 queries. */
 int qm_batch_create(qm_ctx *ctx, int32_t n, const qm_table *const *tables,
                     const qm_query *const *queries, qm_batch **out);
 /* Run the batch; results[i] receives query i's result (destroy each). */
@@ -423,9 +423,11 @@ int qm_batch_set_tuning(qm_batch *batch, int32_t chunk_tiles, int32_t local_kb,
 /* How the batch scans: 1 (default) one scan launch per query, each
  * specialised for its plan (value-column count, key kind) with the
  * planner's block-local table, spread over parallel stream branches of the
- * graph, largest query first; 0 one persistent kernel whose blocks claim
- * (query, chunk of tiles) work items and read each query's plan at run
- * time (the chunk / local-table knobs below apply to it). */
+ * graph, largest query first; 0 persistent kernels, one per query class
+ * (dedupe flag, value-column count, key kind) on parallel branches, whose
+ * blocks claim (query, chunk of tiles) work items from the class's counter
+ * and load each query's plan into shared memory (the chunk / local-table
+ * knobs of qm_batch_set_tuning apply to them). */
 int qm_batch_set_mode(qm_batch *batch, int32_t mode);
 /* Waves of a batched run (0: by batch size, up to 8): the queries are cut
  * into waves run back to back, each followed by the copy of its results to

@@ -9,7 +9,8 @@
 // Finalize is batched too and needs no sort: a group's first-seen rank is
 // the number of groups of its query whose first row is smaller, i.e. the
 // prefix popcount of the query's bitmap of first rows at the group's own
-// first row.  Each query's rows are written at their rank into one packed
+// first row.  Each query's rows are written in that order (slot numbers
+// scattered to their ranks, then rows emitted in order) into one packed
 // buffer (columns, then NULL bitmaps), so one copy returns every result.
 #include "qm_batch.h"
 #include "qm_launch.h"
@@ -27,14 +28,30 @@ __device__ __forceinline__ int find_query(const int64_t *slot0, int n, int64_t g
   return lo;
 }
 
+// Each warp clears 32 consecutive slots (of one query or two): the lanes
+// write consecutive words of the slots, so the stores are coalesced, and the
+// query is looked up once per warp.
 __global__ void qm_batch_init(const qm_bq *bq, const int64_t *slot0, int n, int64_t total) {
-  for (int64_t gs = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gs < total; gs += (int64_t)gridDim.x * blockDim.x) {
-    const int q = find_query(slot0, n, gs);
-    const qm_scan_args &a = bq[q].a;
-    const int64_t s = gs - slot0[q];
-    uint64_t *slot = a.table + s * a.stride;
-    slot[0] = a.key.mode == QK_HASH ? QM_EMPTY_KEY : 0ULL;
-    for (int w = 1; w < a.stride; ++w) slot[w] = a.agg.init[w - 1];
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t g = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; g < total; g += warps * 32) {
+    const int64_t g1 = min(total, g + 32);
+    int q = find_query(slot0, n, g);
+    for (int64_t s0 = g; s0 < g1;) {
+      while (q + 1 < n && slot0[q + 1] <= s0) ++q;
+      const int64_t qend = q + 1 < n ? slot0[q + 1] : total;
+      const int64_t s1 = min(g1, qend);
+      const qm_scan_args &a = bq[q].a;
+      const int stride = a.stride;
+      uint64_t *base = a.table + (s0 - slot0[q]) * stride;
+      const uint64_t key0 = a.key.mode == QK_HASH ? QM_EMPTY_KEY : 0ULL;
+      const int nw = (int)(s1 - s0) * stride;  // at most 32 slots
+      for (int j = lane; j < nw; j += 32) {
+        const int w = j % stride;
+        base[j] = w == 0 ? key0 : a.agg.init[w - 1];
+      }
+      s0 = s1;
+    }
   }
 }
 
@@ -174,9 +191,22 @@ __global__ void __launch_bounds__(QM_SCAN_THREADS)
 }
 
 // Set bit `first row` of each occupied group in its query's bitmap.
+// Slots go in warp-sized runs: a warp looks up the query of its run's first
+// slot once, and each lane moves on to the query of its own slot.
+__device__ __forceinline__ int run_query(const int64_t *slot0, int n, int64_t run, int64_t gs) {
+  int q = find_query(slot0, n, run);
+  while (q + 1 < n && slot0[q + 1] <= gs) ++q;
+  return q;
+}
+#define QM_SLOT_RUNS(total)                                                                          \
+  for (int64_t run = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; run < (total);    \
+       run += (int64_t)gridDim.x * (blockDim.x >> 5) * 32)
+
 __global__ void qm_batch_mark(const qm_bq *bq, const int64_t *slot0, int n, int64_t total, uint32_t *bitmap) {
-  for (int64_t gs = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gs < total; gs += (int64_t)gridDim.x * blockDim.x) {
-    const int q = find_query(slot0, n, gs);
+  QM_SLOT_RUNS(total) {
+    const int64_t gs = run + (threadIdx.x & 31);
+    if (gs >= total) continue;
+    const int q = run_query(slot0, n, run, gs);
     const qm_bq &b = bq[q];
     if (b.none) continue;
     const uint64_t *slot = b.a.table + (gs - slot0[q]) * b.a.stride + 1;
@@ -190,55 +220,135 @@ __global__ void qm_batch_mark(const qm_bq *bq, const int64_t *slot0, int n, int6
 __host__ __device__ inline int64_t align16(int64_t x) { return (x + 15) & ~(int64_t)15; }
 
 // One block: each query's group count, its packed region and the offsets of
-// its output columns, NULL byte maps and NULL bitmaps.
-__global__ void qm_batch_layout(qm_bq *bq, int n, const uint64_t *ranks, qm_batch_meta *meta) {
-  if (threadIdx.x != 0) return;
-  int64_t base = 0, nbase = 0;
-  for (int q = 0; q < n; ++q) {
-    qm_bq &b = bq[q];
-    const int64_t G = b.none ? 1 : (int64_t)(ranks[b.bm_word0 + b.bm_words] - ranks[b.bm_word0]);
-    meta->groups[q] = G;
-    meta->base[q] = base;
-    int64_t off = base;
-    for (int k = 0; k < b.outs.n_out; ++k) {
-      b.outs.o[k].offset = off;
-      off += align16(G * b.width[k]);
-      if (b.nullable[k]) {
-        b.outs.o[k].null_offset = off;  // packed bits (QMCB order)
-        off += align16(((G + 31) / 32) * 4);
-        b.nullbyte_off[k] = nbase;
-        nbase += align16(G);
-      } else {
-        b.outs.o[k].null_offset = -1;
-        b.nullbyte_off[k] = -1;
-      }
-    }
-    meta->bytes[q] = off - base;
-    base = off;
+// its output columns, NULL byte maps and NULL bitmaps.  The queries go in
+// chunks of blockDim.x, one per thread; a block-wide exclusive scan of their
+// region sizes gives their bases.
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t x, uint64_t *wsum, uint64_t &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+  uint64_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(QM_FULL, inc, o);
+    if (lane >= o) inc += y;
   }
-  meta->total = base;
-  meta->null_total = nbase;
+  if (lane == 31) wsum[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const uint64_t w = lane < nw ? wsum[lane] : 0;
+    uint64_t z = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(QM_FULL, z, o);
+      if (lane >= o) z += y;
+    }
+    if (lane < nw) wsum[lane] = z - w;
+    if (lane == 31) wsum[32] = z;
+  }
+  __syncthreads();
+  const uint64_t r = wsum[warp] + inc - x;
+  total = wsum[32];
+  __syncthreads();  // wsum is reused by the next chunk
+  return r;
 }
 
-// Write each occupied group of every query at its first-seen rank.
-__global__ void qm_batch_emit(const qm_bq *bq, const int64_t *slot0, int n, int64_t total, const uint32_t *bitmap,
-                              const uint64_t *ranks, unsigned char *packed, unsigned char *nullbytes) {
-  for (int64_t gs = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gs < total; gs += (int64_t)gridDim.x * blockDim.x) {
-    const int q = find_query(slot0, n, gs);
+__global__ void __launch_bounds__(256) qm_batch_layout(qm_bq *bq, int n, const uint64_t *ranks, qm_batch_meta *meta) {
+  __shared__ uint64_t wsum[33];
+  uint64_t base = 0, nbase = 0;
+  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+    const int q = c0 + (int)threadIdx.x;
+    int64_t G = 0, bytes = 0, nbytes = 0;
+    if (q < n) {
+      const qm_bq &b = bq[q];
+      G = b.none ? 1 : (int64_t)(ranks[b.bm_word0 + b.bm_words] - ranks[b.bm_word0]);
+      for (int k = 0; k < b.outs.n_out; ++k) {
+        bytes += align16(G * b.width[k]);
+        if (b.nullable[k]) {
+          bytes += align16(((G + 31) / 32) * 4);
+          nbytes += align16(G);
+        }
+      }
+    }
+    uint64_t tot, ntot;
+    const uint64_t off0 = base + block_exclusive_scan((uint64_t)bytes, wsum, tot);
+    const uint64_t noff0 = nbase + block_exclusive_scan((uint64_t)nbytes, wsum, ntot);
+    if (q < n) {
+      qm_bq &b = bq[q];
+      meta->groups[q] = G;
+      meta->base[q] = (int64_t)off0;
+      meta->bytes[q] = bytes;
+      int64_t off = (int64_t)off0, nb = (int64_t)noff0;
+      for (int k = 0; k < b.outs.n_out; ++k) {
+        b.outs.o[k].offset = off;
+        off += align16(G * b.width[k]);
+        if (b.nullable[k]) {
+          b.outs.o[k].null_offset = off;  // packed bits (QMCB order)
+          off += align16(((G + 31) / 32) * 4);
+          b.nullbyte_off[k] = nb;
+          nb += align16(G);
+        } else {
+          b.outs.o[k].null_offset = -1;
+          b.nullbyte_off[k] = -1;
+        }
+      }
+    }
+    base += tot;
+    nbase += ntot;
+  }
+  if (threadIdx.x == 0) {
+    meta->total = (int64_t)base;
+    meta->null_total = (int64_t)nbase;
+  }
+}
+
+// Output order in two steps.  First, every occupied slot writes its slot
+// number at its wave-wide first-seen rank (4-byte stores into an array that
+// stays in L2); a query without GROUP BY writes its one row directly.
+__global__ void qm_batch_order(const qm_bq *bq, const int64_t *slot0, int n, int64_t total, const uint32_t *bitmap,
+                               const uint64_t *ranks, uint32_t *perm, unsigned char *packed,
+                               unsigned char *nullbytes) {
+  QM_SLOT_RUNS(total) {
+    const int64_t gs = run + (threadIdx.x & 31);
+    if (gs >= total) continue;
+    const int q = run_query(slot0, n, run, gs);
     const qm_bq &b = bq[q];
     const int64_t s = gs - slot0[q];
-    int64_t rank;
     if (b.none) {
-      if (s != 0) continue;
-      rank = 0;
-    } else {
-      const uint64_t *slot = b.a.table + s * b.a.stride + 1;
-      if (slot[b.a.agg.w_count] == 0) continue;
-      const uint64_t first = slot[b.a.agg.w_first];
-      const int64_t w = b.bm_word0 + (int64_t)(first >> 5);
-      rank = (int64_t)(ranks[w] - ranks[b.bm_word0]) + __popc(bitmap[w] & ((1u << (first & 31)) - 1u));
+      if (s == 0)
+        emit_group_bytes(b.a.table, b.a.stride, 0, 0, b.a.key, b.a.n_slots, b.outs, packed, nullbytes,
+                         b.nullbyte_off);
+      continue;
     }
-    emit_group_bytes(b.a.table, b.a.stride, (uint64_t)s, rank, b.a.key, b.a.n_slots, b.outs, packed, nullbytes,
+    const uint64_t *slot = b.a.table + s * b.a.stride + 1;
+    if (slot[b.a.agg.w_count] == 0) continue;
+    const uint64_t first = slot[b.a.agg.w_first];
+    const int64_t w = b.bm_word0 + (int64_t)(first >> 5);
+    perm[ranks[w] + __popc(bitmap[w] & ((1u << (first & 31)) - 1u))] = (uint32_t)s;
+  }
+}
+
+// Then each output row, in order, reads its group's slot: the output
+// columns are written in runs instead of one scattered cell per column.
+// Warps take 32 consecutive rows; the query of a row is the last one whose
+// first rank is at or below it.
+__global__ void qm_batch_emit_ordered(const qm_bq *bq, int n, const uint64_t *ranks, int64_t bm_words,
+                                      const uint32_t *perm, unsigned char *packed, unsigned char *nullbytes) {
+  const int lane = threadIdx.x & 31;
+  const int64_t G = (int64_t)ranks[bm_words];
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < G; base += warps * 32) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((int64_t)ranks[bq[mid].bm_word0] <= base) lo = mid;
+      else hi = mid - 1;
+    }
+    const int64_t o = base + lane;
+    if (o >= G) continue;
+    int q = lo;
+    while (q + 1 < n && (int64_t)ranks[bq[q + 1].bm_word0] <= o) ++q;
+    const qm_bq &b = bq[q];
+    const int64_t i = o - (int64_t)ranks[b.bm_word0];
+    emit_group_bytes(b.a.table, b.a.stride, (uint64_t)perm[o], i, b.a.key, b.a.n_slots, b.outs, packed, nullbytes,
                      b.nullbyte_off);
   }
 }
@@ -348,9 +458,11 @@ cudaError_t qm_batch_launch_finalize(const qm_batch_dev &d, cudaStream_t st) {
   cudaError_t e;
   qm_batch_mark<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap);
   if ((e = qm_scan_popc_words(d.bitmap, d.bm_words, d.ranks, d.scan_temp, d.scan_temp_bytes, st))) return e;
-  qm_batch_layout<<<1, 32, 0, st>>>(d.bq, d.n, d.ranks, d.meta);
-  qm_batch_emit<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap,
-                                                                         d.ranks, d.packed, d.nullbytes);
+  qm_batch_layout<<<1, 256, 0, st>>>(d.bq, d.n, d.ranks, d.meta);
+  qm_batch_order<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.slot0, d.n, d.total_slots, d.bitmap,
+                                                                          d.ranks, d.perm, d.packed, d.nullbytes);
+  qm_batch_emit_ordered<<<grid_for(d.total_slots, d.sm_count, 8), 256, 0, st>>>(d.bq, d.n, d.ranks, d.bm_words, d.perm,
+                                                                                 d.packed, d.nullbytes);
   dim3 pg(8, d.n);
   qm_batch_pack_nulls<<<pg, 128, 0, st>>>(d.bq, d.n, d.meta, d.packed, d.nullbytes);
   if ((e = cudaMemcpyAsync(d.meta_host, d.meta, d.meta_bytes, cudaMemcpyDeviceToHost, st))) return e;

@@ -56,6 +56,7 @@ struct qm_batch_dev {
   size_t meta_bytes;
   unsigned char *packed;
   unsigned char *nullbytes;
+  uint32_t *perm;       // total_slots: slot of each ranked output row
 };
 
 size_t qm_batch_smem_bytes(int local_bytes);

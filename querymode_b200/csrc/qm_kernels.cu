@@ -246,16 +246,15 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
   }
 }
 
-// The same output in output order, for a direct-indexed table whose key
-// columns still hold every row the first-row bitmap indexes: output row i is
-// the group whose first row is the i-th set bit, and that row's key is the
-// group's slot.  Consecutive threads take consecutive bitmap words, so the
+// The same output in output order, for a table whose key columns still hold
+// every row the first-row bitmap indexes: output row i is the group whose
+// first row is the i-th set bit, and that row's key finds the group's slot
+// (a: the table, its key and slot layout).  Consecutive threads take consecutive bitmap words, so the
 // output columns are written in runs (the slot-order emit scatters every
 // 8-byte cell to its rank, and a result of millions of groups then costs a
 // partial-sector write per cell).
-__global__ void qm_emit_walk(const uint64_t *t, int stride, const uint32_t *bitmap, const uint64_t *ranks,
-                             int64_t words, const __grid_constant__ qm_keyspec K, int64_t n_slots,
-                             const __grid_constant__ qm_outspec O, unsigned char *out) {
+__global__ void qm_emit_walk(const __grid_constant__ qm_scan_args a, const uint32_t *bitmap, const uint64_t *ranks,
+                             int64_t words, const __grid_constant__ qm_outspec O, unsigned char *out) {
   for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
     uint32_t b = bitmap[w];
     if (b == 0) continue;
@@ -263,10 +262,10 @@ __global__ void qm_emit_walk(const uint64_t *t, int stride, const uint32_t *bitm
     for (; b; b &= b - 1, ++i) {
       const int64_t r = w * 32 + (__ffs(b) - 1);
       int special;
-      const uint64_t key = row_key<QM_KK_ANY>(K, r, special);
-      const uint64_t s = special == 2 ? (uint64_t)n_slots : key - (uint64_t)K.base;
-      if (s > (uint64_t)n_slots) continue;  // not a group of this table (a failed run's bitmap)
-      emit_group<false>(t, stride, s, i, K, n_slots, O, out, nullptr, nullptr);
+      const uint64_t key = row_key<QM_KK_ANY>(a.key, r, special);
+      const int64_t s = find_slot(a, key, special);
+      if (s < 0) continue;  // not a group of this table (a failed run's bitmap)
+      emit_group<false>(a.table, a.stride, (uint64_t)s, i, a.key, a.n_slots, O, out, nullptr, nullptr);
     }
   }
 }
@@ -1318,11 +1317,10 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
   return cudaGetLastError();
 }
 
-cudaError_t qm_launch_emit_walk(const uint64_t *t, int stride, const uint32_t *bitmap, const uint64_t *ranks,
-                                int64_t words, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
-                                unsigned char *out, int sm_count, cudaStream_t st) {
+cudaError_t qm_launch_emit_walk(const qm_scan_args &a, const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
+                                const qm_outspec &O, unsigned char *out, int sm_count, cudaStream_t st) {
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
-  qm_emit_walk<<<std::max(blocks, 1), 256, 0, st>>>(t, stride, bitmap, ranks, words, K, n_slots, O, out);
+  qm_emit_walk<<<std::max(blocks, 1), 256, 0, st>>>(a, bitmap, ranks, words, O, out);
   return cudaGetLastError();
 }
 

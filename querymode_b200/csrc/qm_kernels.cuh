@@ -542,6 +542,26 @@ __device__ __forceinline__ int64_t global_slot(const qm_scan_args &a, uint64_t k
   return s;
 }
 
+// A group's slot from its key, without inserting (the key is in the table).
+__device__ __forceinline__ int64_t find_slot(const qm_scan_args &a, uint64_t key, int special) {
+  if (a.key.mode == QK_NONE) return 0;
+  if (a.key.mode == QK_DIRECT) {
+    if (special == 2) return a.n_slots;
+    const uint64_t d = key - (uint64_t)a.key.base;
+    return d < (uint64_t)a.n_slots ? (int64_t)d : -1;
+  }
+  if (special) return a.n_slots + special - 1;
+  const uint64_t mask = (1ULL << a.log2cap) - 1;
+  uint64_t s = fmix64(key) & mask;
+  for (int p = 0; p < a.max_probe; ++p) {
+    const uint64_t k = a.table[s * a.stride];
+    if (k == key) return (int64_t)s;
+    if (k == QM_EMPTY_KEY) return -1;
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+
 // Block-local lookup.  New keys are admitted only while the table is at
 // most half full (`used` counts admissions), so a miss meets an empty slot
 // within a few probes and goes to the global table.

@@ -1,7 +1,8 @@
-"""Large direct-indexed results emitted in output order (the first-row bitmap
-walk used for resident tables of at least 2^20 group slots) against the
-oracle: keys and first-seen order, COUNT, integer SUM and float MIN / MAX
-bit-exact, float SUM / AVG within the path's tolerance (tests/helpers.py).
+"""Large results against the oracle — direct-indexed ones emitted in output
+order (the first-row bitmap walk used for resident tables of at least 2^20
+group slots), hashed ones at their ranks: keys and first-seen order, COUNT,
+integer SUM and float MIN / MAX bit-exact, float SUM / AVG within the path's
+tolerance (tests/helpers.py).
 Covers NULL keys (the direct table's NULL slot), digit-packed two-column keys
 with a nullable column, a filter that leaves most slots empty, and a
 post-aggregate ORDER BY / LIMIT over the walked result (finalizePartialAgg,
@@ -71,3 +72,19 @@ def test_order_by_limit_after_walk(ctx):
     want = post_aggregate(oracle.run_full(cols, q), "sum_w", True, 1000, 0)
     got = run(ctx, cols, dataclasses.replace(q, sort_column="sum_w", sort_desc=True, limit=1000))
     assert_same(got, want, ctx_msg="order by / limit")
+
+
+def test_hashed_keys_with_sentinel_and_nulls(ctx):
+    """A hash table of over 2^20 slots (800K distinct random int64 keys), the
+    empty-slot sentinel as a real key and NULL keys (the slot-order emit of
+    large hashed results, beside the walk of the direct ones)."""
+    rng = np.random.default_rng(15)
+    n = 5_000_000
+    universe = rng.integers(-(1 << 62), 1 << 62, 800_000).astype(np.int64)
+    universe[5] = np.iinfo(np.int64).min
+    key = Column(universe[rng.integers(0, len(universe), n)], rng.random(n) < 0.01)
+    cols = {"key": key, "v": rng.normal(size=n), "w": rng.integers(-3, 3, n).astype(np.int32)}
+    q = QueryDescriptor(group_by=["key"], aggregates=AGGS)
+    g = run(ctx, cols, q)
+    assert g.n_rows > 700_000
+    assert_same(g, oracle.run_full(cols, q), ctx_msg="hashed keys")
