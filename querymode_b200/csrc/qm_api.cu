@@ -157,6 +157,9 @@ struct DevPool {
 
 }  // namespace
 
+// Chunks of a large result emitted and copied to host memory in turn.
+#define QM_EMIT_CHUNKS 4
+
 struct qm_ctx {
   int device = 0;
   int sm_count = 0;
@@ -183,6 +186,10 @@ struct qm_ctx {
   // side stream for the statistics of columns being uploaded
   cudaStream_t aux = nullptr;
   cudaEvent_t aux_ev = nullptr;
+  // chunked copies of a large result while its later chunks are emitted
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copy_ev[QM_EMIT_CHUNKS + 1] = {};
+  DevBuf wbounds;
   DevBuf ustat;
 };
 
@@ -1515,6 +1522,8 @@ constexpr size_t SPEC_RESULT_BYTES = (size_t)8 << 20;
 // the slot-order emit: the walk's probes and its pass over every row's bitmap
 // word measured slower there, 0.73 -> 0.87 ms of finalize at 971K groups.)
 constexpr int64_t WALK_MIN_SLOTS = (int64_t)1 << 20;
+constexpr int64_t EMIT_CHUNK_MIN_ROWS = (int64_t)1 << 22;
+constexpr int EMIT_CHUNKS = QM_EMIT_CHUNKS;
 int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1,
                  qm_status *spec = nullptr, bool rows_resident = false) {
   const Plan &pl = gt.pl;
@@ -1591,7 +1600,48 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   for (int k = 0; k < O.n_out; k++)
     if (O.o[k].null_offset >= 0)
       CK(cudaMemsetAsync((char *)ctx->out.p + O.o[k].null_offset, 0, null_words_bytes, ctx->stream));
-  if (ranked && rows_resident && pl.key.mode == QK_DIRECT && ex.n_slots >= WALK_MIN_SLOTS) {
+  const bool walk = ranked && rows_resident && pl.key.mode == QK_DIRECT && ex.n_slots >= WALK_MIN_SLOTS;
+  // a large result laid out before its group count is known is emitted in
+  // chunks of rows, each chunk's copy to host memory running while the next
+  // chunk is emitted
+  const bool chunked = walk && spec && !pl.post && G >= EMIT_CHUNK_MIN_ROWS;
+  if (chunked) {
+    if ((rc = ensure(ctx, ctx->wbounds, sizeof(int64_t) * (EMIT_CHUNKS + 1)))) {
+      delete R;
+      return rc;
+    }
+    if (!ctx->copy) {
+      CK(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+      for (cudaEvent_t &e : ctx->copy_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    qm_scan_args a;
+    fill_args(gt, a, (qm_status *)ctx->status.p);
+    const int64_t per = ((G + EMIT_CHUNKS - 1) / EMIT_CHUNKS + 31) & ~(int64_t)31;  // whole NULL-bitmap words
+    const int64_t words = rank_words(gt);
+    const uint64_t *franks = (const uint64_t *)ctx->franks.p;
+    CK(qm_launch_walk_bounds(franks, words, per, EMIT_CHUNKS, (int64_t *)ctx->wbounds.p, ctx->stream));
+    for (int c = 0; c < EMIT_CHUNKS; c++) {
+      const int64_t r0 = std::min<int64_t>(G, c * per), r1 = std::min<int64_t>(G, r0 + per);
+      CK(qm_launch_emit_walk(a, (const uint32_t *)ctx->fbits.p, franks, words, O, (unsigned char *)ctx->out.p,
+                             ctx->sm_count, ctx->stream, (const int64_t *)ctx->wbounds.p, c));
+      CK(cudaEventRecord(ctx->copy_ev[c], ctx->stream));
+      CK(cudaStreamWaitEvent(ctx->copy, ctx->copy_ev[c], 0));
+      if (r1 <= r0) continue;
+      for (int k = 0; k < O.n_out; k++) {
+        const size_t wd = dtype_size(O.o[k].dtype);
+        const size_t at = (size_t)O.o[k].offset + (size_t)r0 * wd;
+        CK(cudaMemcpyAsync((char *)R->buf.p + at, (const char *)ctx->out.p + at, (size_t)(r1 - r0) * wd,
+                           cudaMemcpyDeviceToHost, ctx->copy));
+        if (O.o[k].null_offset >= 0) {
+          const size_t nat = (size_t)O.o[k].null_offset + (size_t)(r0 / 32) * 4;
+          CK(cudaMemcpyAsync((char *)R->buf.p + nat, (const char *)ctx->out.p + nat, (size_t)((r1 - r0 + 31) / 32) * 4,
+                             cudaMemcpyDeviceToHost, ctx->copy));
+        }
+      }
+    }
+    CK(cudaEventRecord(ctx->copy_ev[EMIT_CHUNKS], ctx->copy));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_ev[EMIT_CHUNKS], 0));
+  } else if (walk) {
     qm_scan_args a;
     fill_args(gt, a, (qm_status *)ctx->status.p);
     if (G > 0)
@@ -1624,7 +1674,7 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
     res_dev = ctx->out2.p;
     res_bytes = b2;
   }
-  CK(cudaMemcpyAsync(R->buf.p, res_dev, res_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!chunked) CK(cudaMemcpyAsync(R->buf.p, res_dev, res_bytes, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   cudaError_t se = cudaStreamSynchronize(ctx->stream);
   if (se != cudaSuccess) {
@@ -2226,6 +2276,9 @@ int qm_ctx_destroy(qm_ctx *ctx) {
   if (ctx->evs1) cudaEventDestroy(ctx->evs1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
+  if (ctx->copy) cudaStreamDestroy(ctx->copy);
+  for (cudaEvent_t e : ctx->copy_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->aux_ev) cudaEventDestroy(ctx->aux_ev);
   delete ctx;
   return QM_OK;

@@ -253,9 +253,12 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
 // output columns are written in runs (the slot-order emit scatters every
 // 8-byte cell to its rank, and a result of millions of groups then costs a
 // partial-sector write per cell).
+// bounds (optional): this launch walks words [bounds[chunk], bounds[chunk + 1]).
 __global__ void qm_emit_walk(const __grid_constant__ qm_scan_args a, const uint32_t *bitmap, const uint64_t *ranks,
-                             int64_t words, const __grid_constant__ qm_outspec O, unsigned char *out) {
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
+                             int64_t words, const __grid_constant__ qm_outspec O, unsigned char *out,
+                             const int64_t *bounds, int chunk) {
+  const int64_t w0 = bounds ? bounds[chunk] : 0, w1 = bounds ? bounds[chunk + 1] : words;
+  for (int64_t w = w0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < w1; w += (int64_t)gridDim.x * blockDim.x) {
     uint32_t b = bitmap[w];
     if (b == 0) continue;
     int64_t i = (int64_t)ranks[w];
@@ -268,6 +271,27 @@ __global__ void qm_emit_walk(const __grid_constant__ qm_scan_args a, const uint3
       emit_group<false>(a.table, a.stride, (uint64_t)s, i, a.key, a.n_slots, O, out, nullptr, nullptr);
     }
   }
+}
+
+// Bitmap word bounds of output chunks of `per` rows: bounds[c] = the first
+// word whose rank is at least c * per (lower bound over ranks[0..words]),
+// bounds[chunks] = words.  A word's later bits may fall into the next
+// chunk's rows; no word of a later chunk writes rows of an earlier one.
+__global__ void qm_walk_bounds(const uint64_t *ranks, int64_t words, int64_t per, int chunks, int64_t *bounds) {
+  const int c = threadIdx.x;
+  if (c > chunks) return;
+  if (c == chunks) {
+    bounds[c] = words;
+    return;
+  }
+  const uint64_t target = (uint64_t)c * (uint64_t)per;
+  int64_t lo = 0, hi = words;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (ranks[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  bounds[c] = lo;
 }
 
 // ---- Parquet PLAIN pages -> a column ----------------------------------------
@@ -1318,9 +1342,17 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
 }
 
 cudaError_t qm_launch_emit_walk(const qm_scan_args &a, const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
-                                const qm_outspec &O, unsigned char *out, int sm_count, cudaStream_t st) {
+                                const qm_outspec &O, unsigned char *out, int sm_count, cudaStream_t st,
+                                const int64_t *bounds, int chunk) {
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
-  qm_emit_walk<<<std::max(blocks, 1), 256, 0, st>>>(a, bitmap, ranks, words, O, out);
+  qm_emit_walk<<<std::max(blocks, 1), 256, 0, st>>>(a, bitmap, ranks, words, O, out, bounds, chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_walk_bounds(const uint64_t *ranks, int64_t words, int64_t per, int chunks, int64_t *bounds,
+                                  cudaStream_t st) {
+  if (chunks < 1 || chunks > 1023) return cudaErrorInvalidValue;
+  qm_walk_bounds<<<1, chunks + 1, 0, st>>>(ranks, words, per, chunks, bounds);
   return cudaGetLastError();
 }
 

@@ -70,8 +70,14 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
                                   int sm_count, cudaStream_t st);
 // Ranked emit in output order by walking the first-row bitmap: tables whose
 // key columns hold every row the bitmap indexes (a: table, key, slots).
+// bounds / chunk: walk only words [bounds[chunk], bounds[chunk + 1]) (bounds
+// from qm_launch_walk_bounds; null: every word).
 cudaError_t qm_launch_emit_walk(const qm_scan_args &a, const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
-                                const qm_outspec &O, unsigned char *out, int sm_count, cudaStream_t st);
+                                const qm_outspec &O, unsigned char *out, int sm_count, cudaStream_t st,
+                                const int64_t *bounds = nullptr, int chunk = 0);
+// Word bounds (chunks + 1 entries) of output chunks of `per` rows.
+cudaError_t qm_launch_walk_bounds(const uint64_t *ranks, int64_t words, int64_t per, int chunks, int64_t *bounds,
+                                  cudaStream_t st);
 // Post-aggregate ORDER BY / LIMIT over emitted result rows (see qm_kernels.cu).
 cudaError_t qm_launch_sort_keys(const unsigned char *data, const uint32_t *nulls, int dtype, int desc, int64_t G,
                                 uint32_t *last, uint64_t *hi, uint64_t *lo, uint32_t *idx, int sm_count, cudaStream_t st);
