@@ -158,7 +158,9 @@ struct DevPool {
 }  // namespace
 
 // Chunks of a large result emitted and copied to host memory in turn.
-#define QM_EMIT_CHUNKS 4
+#ifndef QM_EMIT_CHUNKS
+#define QM_EMIT_CHUNKS 8
+#endif
 
 struct qm_ctx {
   int device = 0;
