@@ -88,3 +88,20 @@ def test_hashed_keys_with_sentinel_and_nulls(ctx):
     g = run(ctx, cols, q)
     assert g.n_rows > 700_000
     assert_same(g, oracle.run_full(cols, q), ctx_msg="hashed keys")
+
+
+def test_chunked_dense_result_with_null_outputs(ctx):
+    """A dense direct table of 2^22 + 1 slots (4M groups of 12M rows): the
+    result is laid out before its group count is known and emitted and copied
+    in row chunks.  30 % NULL values leave some groups with NULL SUM / MIN /
+    AVG (the chunks' NULL-bitmap words), and 1 % NULL keys the NULL group."""
+    rng = np.random.default_rng(16)
+    n = 12_000_000
+    key = Column(rng.integers(0, 1 << 22, n).astype(np.int64), rng.random(n) < 0.01)
+    cols = {"key": key, "v": Column(rng.normal(size=n), rng.random(n) < 0.3),
+            "w": rng.integers(-100, 100, n).astype(np.int32)}
+    q = QueryDescriptor(group_by=["key"], aggregates=AGGS)
+    g = run(ctx, cols, q)
+    assert g.n_rows > 3_900_000
+    assert g.column("sum_v").nulls is not None and g.column("sum_v").nulls.any()
+    assert_same(g, oracle.run_full(cols, q), ctx_msg="chunked dense result")
