@@ -21,6 +21,7 @@
 #include <cstring>
 #include <memory>
 #include <unordered_map>
+#include <map>
 #include <mutex>
 #include <string>
 #include <deque>
@@ -44,6 +45,7 @@ struct DevBuf {
 struct HostBuf {
   void *p = nullptr;
   size_t bytes = 0;
+  bool carved = false;  // part of a pinned slab (returns to the pool, never freed alone)
 };
 
 // Pinned host buffers handed to results and recycled when they are
@@ -51,14 +53,25 @@ struct HostBuf {
 struct PinnedPool {
   std::mutex mu;
   std::vector<HostBuf> free;
+  std::vector<void *> slabs;  // page-locked slabs that small buffers are carved from
+  char *slab_cur = nullptr;
+  size_t slab_left = 0;
   ~PinnedPool() {
-    for (auto &b : free) cudaFreeHost(b.p);
+    for (auto &b : free)
+      if (!b.carved) cudaFreeHost(b.p);
+    for (void *s : slabs) cudaFreeHost(s);
   }
   // Buffers are power-of-two sized (results of similar size share them) and
   // kept up to a byte cap: allocating or freeing pinned memory costs far
-  // more than a query (and freeing synchronises the device).
+  // more than a query (page-locking takes milliseconds per buffer and holds
+  // up other threads' CUDA calls; freeing synchronises the device).  Buffers
+  // up to CARVE_MAX are carved from SLAB-sized page-locked slabs, so a burst
+  // of new small results costs one allocation per slab, not one per result;
+  // carved buffers stay in the pool.
   static constexpr size_t CACHE_CAP = (size_t)8 << 30;
-  static constexpr size_t MAX_BUFFERS = 256;
+  static constexpr size_t MAX_BUFFERS = 4096;
+  static constexpr size_t SLAB = (size_t)256 << 20;
+  static constexpr size_t CARVE_MAX = (size_t)16 << 20;
   static size_t class_of(size_t bytes) {
     size_t want = 64 * 1024;
     while (want < bytes) want <<= 1;
@@ -79,6 +92,26 @@ struct PinnedPool {
         free.erase(free.begin() + best);
         return true;
       }
+      if (want <= CARVE_MAX) {
+        if (slab_left < want) {
+          void *sp = nullptr;
+          if (cudaMallocHost(&sp, SLAB) == cudaSuccess) {
+            slabs.push_back(sp);
+            slab_cur = static_cast<char *>(sp);
+            slab_left = SLAB;
+          } else {
+            cudaGetLastError();
+          }
+        }
+        if (slab_left >= want) {
+          out.p = slab_cur;
+          out.bytes = want;
+          out.carved = true;
+          slab_cur += want;
+          slab_left -= want;
+          return true;
+        }
+      }
     }
     if (cudaMallocHost(&out.p, want) != cudaSuccess) {
       cudaGetLastError();
@@ -86,23 +119,29 @@ struct PinnedPool {
       return false;
     }
     out.bytes = want;
+    out.carved = false;
     return true;
   }
-  // Kept for reuse up to the caps; beyond them the smallest buffers go
-  // first (the large ones cost the most to page-lock again).
+  // Kept for reuse up to the caps; beyond them the smallest buffers of their
+  // own go first (the large ones cost the most to page-lock again).
   void release(HostBuf &b) {
     if (!b.p) return;
     std::vector<void *> drop;
     {
       std::lock_guard<std::mutex> lk(mu);
       free.push_back(b);
-      size_t cached = 0;
-      for (auto &f : free) cached += f.bytes;
-      while ((cached > CACHE_CAP || free.size() > MAX_BUFFERS) && !free.empty()) {
-        int s = 0;
-        for (int i = 1; i < (int)free.size(); i++)
-          if (free[i].bytes < free[s].bytes) s = i;
+      size_t cached = 0, own = 0;
+      for (auto &f : free)
+        if (!f.carved) {
+          cached += f.bytes;
+          own++;
+        }
+      while ((cached > CACHE_CAP || own > MAX_BUFFERS) && own > 0) {
+        int s = -1;
+        for (int i = 0; i < (int)free.size(); i++)
+          if (!free[i].carved && (s < 0 || free[i].bytes < free[s].bytes)) s = i;
         cached -= free[s].bytes;
+        own--;
         drop.push_back(free[s].p);
         free.erase(free.begin() + s);
       }
@@ -1040,15 +1079,30 @@ void choose_layout(const Plan &pl, int64_t est_groups, Exec &ex, const qm_tuning
 }
 
 std::mutex g_cfg_mu;
+// Occupancy answers are fixed per (device, kernel, shared memory) and the
+// runtime queries cost tens of microseconds under g_cfg_mu, which every
+// planning thread takes: they are cached.  Kernel ids: -1 / -2 the generic
+// scan (direct / staged), >= 0 a batched class.
+std::map<std::tuple<int, int, size_t>, int> g_occ;
+// The largest dynamic shared-memory limit set on each batched class kernel:
+// the limit is only ever raised, so a lane never lowers it under another
+// lane's larger launch.
+std::map<std::pair<int, int>, size_t> g_class_attr;
 
 // cap: blocks per SM for this launch unless the context's tuning sets them.
 int scan_blocks(qm_ctx *ctx, size_t smem, int64_t n, bool staged, int cap = 0) {
   int bps = 1;
   {
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    if (qm_scan_configure(smem, staged, &bps) != cudaSuccess) {
+    const auto key = std::make_tuple(ctx->device, staged ? -2 : -1, smem);
+    auto it = g_occ.find(key);
+    if (it != g_occ.end()) {
+      bps = it->second;
+    } else if (qm_scan_configure(smem, staged, &bps) != cudaSuccess) {
       cudaGetLastError();
       bps = 1;
+    } else {
+      g_occ[key] = bps;
     }
   }
   if (bps < 1) bps = 1;
@@ -3564,6 +3618,7 @@ struct qm_batch {
   cudaStream_t copy_stream = nullptr; // result copies
   cudaEvent_t ev_start = nullptr, ev_end = nullptr;
   std::vector<cudaEvent_t> q_ev;      // per-query copies landed (per-request completion)
+  std::vector<std::shared_ptr<SharedPinned>> q_host;  // per-request result buffers until completed
   int mode = 1;  // 0: one persistent kernel over (query, chunk) work items; 1: per-query launches
   std::vector<const qm_table *> tabs;  // query i's table and a copy of the
   std::vector<std::unique_ptr<OwnedQuery>> queries;  // query, to rerun it alone
@@ -3728,9 +3783,19 @@ int batch_layout(qm_batch *b) {
     int bps = 1;
     {
       std::lock_guard<std::mutex> lk(g_cfg_mu);
-      if (qm_batch_class_configure(c, class_smem[c], &bps) != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", class_smem[c]);
+      const auto key = std::make_tuple(ctx->device, c, class_smem[c]);
+      auto it = g_occ.find(key);
+      if (it != g_occ.end()) {
+        bps = it->second;
+      } else {
+        size_t &lim = g_class_attr[std::make_pair(ctx->device, c)];
+        const size_t raise = class_smem[c] > lim ? class_smem[c] : 0;
+        if (qm_batch_class_configure(c, raise, class_smem[c], &bps) != cudaSuccess) {
+          cudaGetLastError();
+          return set_err(ctx, QM_ERR_CUDA, "batched kernel: %zu bytes of shared memory rejected", class_smem[c]);
+        }
+        if (raise) lim = raise;
+        g_occ[key] = bps;
       }
     }
     if (bps < 1) bps = 1;
@@ -3825,8 +3890,8 @@ int batch_layout(qm_batch *b) {
     d.nullbytes = (unsigned char *)wv.d_nullbytes.p;
     d.perm = (uint32_t *)wv.d_perm.p;
   }
+  // (pageable source: the call returns once the bytes are staged, so dbq may go)
   CK(cudaMemcpyAsync(b->d_bq.p, dbq.data(), sizeof(qm_bq) * n, cudaMemcpyHostToDevice, st));
-  CK(cudaStreamSynchronize(st));
   // mode 1: each query's own specialised scan, with the planner's block-local
   // layout, on one of several stream branches
   b->launches.resize(n);
@@ -3941,17 +4006,21 @@ int batch_issue(qm_batch *b, bool use_graph) {
 }
 
 // Query i's result from its wave's packed results in host memory.
-qm_result *batch_result(qm_batch *b, int i, const BatchWave &wv, const qm_status &s, float scan_ms) {
+// own: the query's own buffer holding just its region (else the wave's
+// buffer of every region).
+qm_result *batch_result(qm_batch *b, int i, const BatchWave &wv, const qm_status &s, float scan_ms,
+                        const std::shared_ptr<SharedPinned> &own = nullptr) {
   const int j = b->pos[i];
   const qm_batch_meta *meta = (const qm_batch_meta *)wv.h_meta.p;
   const qm_bq &qb = b->bq[i];
   const Plan &pl = b->gts[i].pl;
   const int64_t G = meta->groups[j - wv.q0];
-  const uint8_t *h = (const uint8_t *)wv.host->buf.p;
+  const std::shared_ptr<SharedPinned> &hold = own ? own : wv.host;
+  const uint8_t *h = (const uint8_t *)hold->buf.p;
   qm_result *R = new qm_result();
-  R->shared = wv.host;
+  R->shared = hold;
   R->n_rows = G;
-  int64_t off = meta->base[j - wv.q0];
+  int64_t off = own ? 0 : meta->base[j - wv.q0];
   for (int k = 0; k < qb.outs.n_out; k++) {
     qm_result::Col c;
     c.name = pl.meta[k].name;
@@ -4002,6 +4071,7 @@ int batch_collect(qm_batch *b, qm_result **results, int *codes, bool per_query =
       b->q_ev.push_back(ev);
     }
   }
+  if (per_query) b->q_host.assign(n, nullptr);
   const qm_status *stv = (const qm_status *)b->h_status.p;
   for (auto &wp : b->waves) {
     BatchWave &wv = *wp;
@@ -4009,20 +4079,28 @@ int batch_collect(qm_batch *b, qm_result **results, int *codes, bool per_query =
     if (e != cudaSuccess) return set_err(ctx, QM_ERR_CUDA, "batched run: %s", cudaGetErrorString(e));
     const qm_batch_meta *meta = (const qm_batch_meta *)wv.h_meta.p;
     const size_t total = (size_t)meta->total;
-    auto holder = std::make_shared<SharedPinned>();
-    holder->pool = ctx->pool;
-    if (!ctx->pool->acquire(total + 16, holder->buf)) return set_err(ctx, QM_ERR_OOM, "pinned batch results");
-    wv.host = holder;
     CK(cudaStreamWaitEvent(b->copy_stream, wv.done, 0));
     if (!per_query) {
+      auto holder = std::make_shared<SharedPinned>();
+      holder->pool = ctx->pool;
+      if (!ctx->pool->acquire(total + 16, holder->buf)) return set_err(ctx, QM_ERR_OOM, "pinned batch results");
+      wv.host = holder;
       if (total)
         CK(cudaMemcpyAsync(holder->buf.p, wv.dev.packed, total, cudaMemcpyDeviceToHost, b->copy_stream));
       continue;
     }
+    // one pinned buffer per query: buffers of one query's size class are
+    // reused from request to request, where one buffer per batch would need
+    // ever larger ones as batches grow (page-locking a new buffer of
+    // gigabytes stalls every lane for most of a second)
     for (int j = wv.q0; j < wv.q1; j++) {
       const int64_t base = meta->base[j - wv.q0], bytes = meta->bytes[j - wv.q0];
+      auto holder = std::make_shared<SharedPinned>();
+      holder->pool = ctx->pool;
+      if (!ctx->pool->acquire((size_t)bytes + 16, holder->buf)) return set_err(ctx, QM_ERR_OOM, "pinned request result");
+      b->q_host[j] = holder;
       if (bytes > 0)
-        CK(cudaMemcpyAsync((char *)holder->buf.p + base, wv.dev.packed + base, (size_t)bytes, cudaMemcpyDeviceToHost,
+        CK(cudaMemcpyAsync(holder->buf.p, wv.dev.packed + base, (size_t)bytes, cudaMemcpyDeviceToHost,
                            b->copy_stream));
       CK(cudaEventRecord(b->q_ev[j], b->copy_stream));
     }
@@ -4036,7 +4114,8 @@ int batch_collect(qm_batch *b, qm_result **results, int *codes, bool per_query =
         if (e != cudaSuccess) return set_err(ctx, QM_ERR_CUDA, "batched results: %s", cudaGetErrorString(e));
         const int i = b->order[j];
         const int code = status_code(stv[j]);
-        qm_result *R = code == QM_OK ? batch_result(b, i, wv, stv[j], 0.f) : nullptr;
+        qm_result *R = code == QM_OK ? batch_result(b, i, wv, stv[j], 0.f, b->q_host[j]) : nullptr;
+        b->q_host[j].reset();
         if (results) results[i] = R;
         if (codes) codes[i] = code;
         if (on_done) on_done(i, code, R);

@@ -385,9 +385,10 @@ size_t qm_batch_smem_bytes(int local_bytes) { return batch_smem(local_bytes, QM_
 namespace {
 
 template <int DD, int NV, int KK>
-cudaError_t batch_class_configure(size_t smem, int *blocks_per_sm) {
-  cudaError_t e =
-      cudaFuncSetAttribute(qm_batch_scan<DD, NV, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t batch_class_configure(size_t attr_smem, size_t smem, int *blocks_per_sm) {
+  cudaError_t e = cudaSuccess;
+  if (attr_smem)
+    e = cudaFuncSetAttribute(qm_batch_scan<DD, NV, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)attr_smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, qm_batch_scan<DD, NV, KK>, QM_SCAN_THREADS,
                                                        smem);
@@ -414,13 +415,13 @@ int qm_batch_class_of(const qm_scan_args &a) {
   return 0;  // the run-time-plan kernel
 }
 
-cudaError_t qm_batch_class_configure(int cls, size_t smem, int *blocks_per_sm) {
+cudaError_t qm_batch_class_configure(int cls, size_t attr_smem, size_t smem, int *blocks_per_sm) {
   int c = 1;
 #define QM_CFG_(DD, NV, KK) \
-  if (cls == c++) return batch_class_configure<DD, NV, KK>(smem, blocks_per_sm);
+  if (cls == c++) return batch_class_configure<DD, NV, KK>(attr_smem, smem, blocks_per_sm);
   QM_BATCH_CLASSES(QM_CFG_)
 #undef QM_CFG_
-  return batch_class_configure<2, QM_NV_ANY, QM_KK_ANY>(smem, blocks_per_sm);
+  return batch_class_configure<2, QM_NV_ANY, QM_KK_ANY>(attr_smem, smem, blocks_per_sm);
 }
 
 cudaError_t qm_batch_launch_class(int cls, const qm_bq *bq, const qm_chunk *chunks, int n_chunks, int *counter,

@@ -67,7 +67,9 @@ size_t qm_batch_smem_bytes(int local_bytes);
 #define QM_BATCH_CLASS_SLOTS 16
 #define QM_BATCH_CLASSES_N 9
 int qm_batch_class_of(const qm_scan_args &a);
-cudaError_t qm_batch_class_configure(int cls, size_t smem, int *blocks_per_sm);
+// attr_smem: the class kernel's dynamic shared-memory limit to set (0: keep
+// it); smem: the launch's shared memory for the occupancy answer.
+cudaError_t qm_batch_class_configure(int cls, size_t attr_smem, size_t smem, int *blocks_per_sm);
 cudaError_t qm_batch_launch_class(int cls, const qm_bq *bq, const qm_chunk *chunks, int n_chunks, int *counter,
                                   int local_bytes, int blocks, size_t smem, cudaStream_t st);
 // The phases of a batched run: clear statuses, counters, bitmaps and group

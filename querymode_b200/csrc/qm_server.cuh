@@ -344,6 +344,21 @@ int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out) 
     ln->batch->waves_req = 1;
     s->lanes.push_back(std::move(ln));
   }
+  // Lanes grow their buffers with stream-ordered allocation from the
+  // device's memory pool, which keeps what is freed.  Growing the pool itself
+  // maps new memory (hundreds of milliseconds for a gigabyte, measured while
+  // the other lanes ran); taking a block of it up front and handing it back
+  // lets the lanes' first large batches reuse that memory instead.
+  {
+    const int64_t reserve = std::min<int64_t>((int64_t)L << 30, cfg->hbm_budget_bytes / 8);
+    void *blk = nullptr;
+    if (reserve > 0 && cudaMallocAsync(&blk, (size_t)reserve, ctx->stream) == cudaSuccess) {
+      cudaFreeAsync(blk, ctx->stream);
+      cudaStreamSynchronize(ctx->stream);
+    } else {
+      cudaGetLastError();
+    }
+  }
   for (auto &ln : s->lanes) {
     Lane *p = ln.get();
     p->th = std::thread([s, p] { s->lane_loop(*p); });
