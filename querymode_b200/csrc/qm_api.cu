@@ -53,9 +53,8 @@ struct HostBuf {
 struct PinnedPool {
   std::mutex mu;
   std::vector<HostBuf> free;
-  std::vector<void *> slabs;  // page-locked slabs that small buffers are carved from
-  char *slab_cur = nullptr;
-  size_t slab_left = 0;
+  std::vector<void *> slabs;                      // page-locked slabs buffers are carved from
+  std::vector<std::pair<char *, size_t>> space;   // the slabs' uncarved ends
   ~PinnedPool() {
     for (auto &b : free)
       if (!b.carved) cudaFreeHost(b.p);
@@ -63,19 +62,38 @@ struct PinnedPool {
   }
   // Buffers are power-of-two sized (results of similar size share them) and
   // kept up to a byte cap: allocating or freeing pinned memory costs far
-  // more than a query (page-locking takes milliseconds per buffer and holds
-  // up other threads' CUDA calls; freeing synchronises the device).  Buffers
-  // up to CARVE_MAX are carved from SLAB-sized page-locked slabs, so a burst
-  // of new small results costs one allocation per slab, not one per result;
-  // carved buffers stay in the pool.
-  static constexpr size_t CACHE_CAP = (size_t)8 << 30;
+  // more than a query (page-locking takes about 0.4 ms per MB and holds up
+  // every other thread's CUDA calls meanwhile; freeing synchronises the
+  // device).  Buffers up to CARVE_MAX are carved from SLAB-sized page-locked
+  // slabs, so new results cost one page-locking per slab, not one per
+  // buffer; carved buffers stay in the pool.
+  static constexpr size_t CACHE_CAP = (size_t)16 << 30;
   static constexpr size_t MAX_BUFFERS = 4096;
-  static constexpr size_t SLAB = (size_t)256 << 20;
-  static constexpr size_t CARVE_MAX = (size_t)16 << 20;
+  static constexpr size_t SLAB = (size_t)512 << 20;
+  static constexpr size_t CARVE_MAX = (size_t)64 << 20;
   static size_t class_of(size_t bytes) {
     size_t want = 64 * 1024;
     while (want < bytes) want <<= 1;
     return want;
+  }
+  // under mu: a new slab (false when page-locking fails)
+  bool add_slab() {
+    void *sp = nullptr;
+    if (cudaMallocHost(&sp, SLAB) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    slabs.push_back(sp);
+    space.emplace_back(static_cast<char *>(sp), SLAB);
+    return true;
+  }
+  // Page-lock slabs for at least `bytes` of buffers ahead of need (a server
+  // does this at creation, so its first requests pay no page-locking).
+  void reserve(size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    size_t have = 0;
+    for (auto &sp : space) have += sp.second;
+    while (have < bytes && add_slab()) have += SLAB;
   }
   bool acquire(size_t bytes, HostBuf &out) {
     const size_t want = class_of(bytes);
@@ -93,22 +111,16 @@ struct PinnedPool {
         return true;
       }
       if (want <= CARVE_MAX) {
-        if (slab_left < want) {
-          void *sp = nullptr;
-          if (cudaMallocHost(&sp, SLAB) == cudaSuccess) {
-            slabs.push_back(sp);
-            slab_cur = static_cast<char *>(sp);
-            slab_left = SLAB;
-          } else {
-            cudaGetLastError();
-          }
-        }
-        if (slab_left >= want) {
-          out.p = slab_cur;
+        int at = -1;
+        for (int i = 0; i < (int)space.size() && at < 0; i++)
+          if (space[i].second >= want) at = i;
+        if (at < 0 && add_slab()) at = (int)space.size() - 1;
+        if (at >= 0) {
+          out.p = space[at].first;
           out.bytes = want;
           out.carved = true;
-          slab_cur += want;
-          slab_left -= want;
+          space[at].first += want;
+          space[at].second -= want;
           return true;
         }
       }

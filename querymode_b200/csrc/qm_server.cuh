@@ -347,10 +347,11 @@ int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out) 
   // Lanes grow their buffers with stream-ordered allocation from the
   // device's memory pool, which keeps what is freed.  Growing the pool itself
   // maps new memory (hundreds of milliseconds for a gigabyte, measured while
-  // the other lanes ran); taking a block of it up front and handing it back
-  // lets the lanes' first large batches reuse that memory instead.
+  // the other lanes ran); taking a block of it up front (2 GB per lane, at
+  // most an eighth of the budget) and handing it back lets the lanes' large
+  // batches reuse that memory instead.
   {
-    const int64_t reserve = std::min<int64_t>((int64_t)L << 30, cfg->hbm_budget_bytes / 8);
+    const int64_t reserve = std::min<int64_t>((int64_t)L << 31, cfg->hbm_budget_bytes / 8);
     void *blk = nullptr;
     if (reserve > 0 && cudaMallocAsync(&blk, (size_t)reserve, ctx->stream) == cudaSuccess) {
       cudaFreeAsync(blk, ctx->stream);
@@ -359,6 +360,10 @@ int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out) 
       cudaGetLastError();
     }
   }
+  // and page-lock 256 MB of result buffers per lane (carved by size class)
+  // for the same reason: page-locking during serving holds up every lane's
+  // CUDA calls for tens of milliseconds per buffer
+  ctx->pool->reserve((size_t)L << 28);
   for (auto &ln : s->lanes) {
     Lane *p = ln.get();
     p->th = std::thread([s, p] { s->lane_loop(*p); });
