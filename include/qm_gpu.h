@@ -578,6 +578,11 @@ typedef struct {
   int64_t lanes;              /* lanes of the server                       */
 } qm_server_counters;
 
+/* Start the lanes.  At creation the server page-locks 256 MB of result
+ * buffers per lane (kept in the context's pinned pool) and takes up to 2 GB
+ * per lane (at most an eighth of hbm_budget_bytes) from the device's memory
+ * pool and hands it back, so that serving does not stall on page-locking or
+ * pool growth later; qm_ctx_trim returns the device memory. */
 int qm_server_create(qm_ctx *ctx, const qm_server_config *cfg, qm_server **out);
 /* Queue one request (the query is copied; the table must stay alive).
  * *ticket identifies it for cancel / wait.  Planning errors surface from
