@@ -228,6 +228,7 @@ struct qm_ctx {
   DevBuf masks, counts, offsets, sel_out, sel_in;
   DevBuf agg_spare;  // group table of a destroyed qm_agg, reused by the next one
   DevBuf fbits, fcounts, franks;  // first-row bitmap, its popcounts and prefix sums
+  DevBuf perm;                    // slot of each ranked output row (large results)
   DevBuf zstat, zones;           // zone-map statistics pass; the kept zones of a query
   DevBuf part_counts, part_offsets, part_bases, part_records;  // partitioned aggregation
   // post-aggregate ORDER BY / LIMIT: sort keys, row orders, scratch, result
@@ -1596,6 +1597,9 @@ constexpr size_t SPEC_RESULT_BYTES = (size_t)8 << 20;
 // word measured slower there, 0.73 -> 0.87 ms of finalize at 971K groups.)
 constexpr int64_t WALK_MIN_SLOTS = (int64_t)1 << 20;
 constexpr int64_t EMIT_CHUNK_MIN_ROWS = (int64_t)1 << 22;
+// Results of at least this many rows (hashed, or direct ones not walked) are
+// emitted in two ordered steps rather than cell by cell at their ranks.
+constexpr int64_t PERM_MIN_ROWS = (int64_t)1 << 18;
 constexpr int EMIT_CHUNKS = QM_EMIT_CHUNKS;
 int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_far, int64_t groups_known = -1,
                  qm_status *spec = nullptr, bool rows_resident = false) {
@@ -1720,6 +1724,15 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
     if (G > 0)
       CK(qm_launch_emit_walk(a, (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, rank_words(gt), O,
                              (unsigned char *)ctx->out.p, ctx->sm_count, ctx->stream));
+  } else if (ranked && G >= PERM_MIN_ROWS && ex.total_slots < ((int64_t)1 << 32)) {
+    if ((rc = ensure(ctx, ctx->perm, sizeof(uint32_t) * (size_t)ex.total_slots))) {
+      delete R;
+      return rc;
+    }
+    CK(qm_launch_emit_perm(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
+                           (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, rank_words(gt),
+                           (uint32_t *)ctx->perm.p, G, pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p,
+                           ctx->sm_count, ctx->stream));
   } else if (ranked) {
     if (G > 0)
       CK(qm_launch_emit_ranked(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word, first_word_o,
@@ -2338,7 +2351,8 @@ int qm_ctx_destroy(qm_ctx *ctx) {
                     &ctx->offsets, &ctx->sel_out, &ctx->sel_in, &ctx->agg_spare, &ctx->fbits, &ctx->fcounts,
                     &ctx->franks, &ctx->post_last, &ctx->post_hi, &ctx->post_lo, &ctx->post_idx,
                     &ctx->post_idx2, &ctx->post_k1, &ctx->post_k2, &ctx->post_l1, &ctx->post_l2,
-                    &ctx->post_temp, &ctx->out2, &ctx->zstat, &ctx->zones, &ctx->ustat};
+                    &ctx->post_temp, &ctx->out2, &ctx->zstat, &ctx->zones, &ctx->ustat, &ctx->perm,
+                    &ctx->wbounds, &ctx->part_counts, &ctx->part_offsets, &ctx->part_bases, &ctx->part_records};
   for (DevBuf *b : bufs) release(*b);
   for (auto &b : ctx->staged) release(b);
   ctx->dpool.trim();

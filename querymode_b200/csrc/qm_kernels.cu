@@ -246,6 +246,32 @@ __global__ void qm_emit_ranked(const uint64_t *t, int64_t n_slots_total, int str
   }
 }
 
+// The same output in two ordered steps, for large results of any table:
+// every occupied slot writes its number at its rank (4-byte stores into an
+// array that stays in L2), then each output row reads its slot, so the output
+// cells are written in runs instead of one scattered cell per column.
+__global__ void qm_rank_slots(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                              const uint32_t *bitmap, const uint64_t *ranks, int64_t words, uint32_t *perm) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots_total;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t *w = t + s * stride + 1;
+    if (w[count_word] == 0) continue;
+    const uint64_t f = w[first_word];
+    if ((f >> 5) >= (uint64_t)words) continue;  // not marked (see qm_mark_first)
+    const int64_t i = (int64_t)ranks[f >> 5] + __popc(bitmap[f >> 5] & ((1u << (f & 31)) - 1u));
+    if (i < n_slots_total) perm[i] = (uint32_t)s;
+  }
+}
+
+// rows: the layout's capacity (output rows past it are not written).
+__global__ void qm_emit_perm(const uint64_t *t, int stride, const uint32_t *perm, const uint64_t *ranks,
+                             int64_t words, int64_t rows, const __grid_constant__ qm_keyspec K, int64_t n_slots,
+                             const __grid_constant__ qm_outspec O, unsigned char *out) {
+  const int64_t G = min((int64_t)ranks[words], rows);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G; i += (int64_t)gridDim.x * blockDim.x)
+    emit_group<false>(t, stride, (uint64_t)perm[i], i, K, n_slots, O, out, nullptr, nullptr);
+}
+
 // The same output in output order, for a table whose key columns still hold
 // every row the first-row bitmap indexes: output row i is the group whose
 // first row is the i-th set bit, and that row's key finds the group's slot
@@ -1346,6 +1372,18 @@ cudaError_t qm_launch_emit_walk(const qm_scan_args &a, const uint32_t *bitmap, c
                                 const int64_t *bounds, int chunk) {
   const int blocks = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sm_count * 8);
   qm_emit_walk<<<std::max(blocks, 1), 256, 0, st>>>(a, bitmap, ranks, words, O, out, bounds, chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_emit_perm(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                                const uint32_t *bitmap, const uint64_t *ranks, int64_t words, uint32_t *perm,
+                                int64_t rows, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
+                                unsigned char *out, int sm_count, cudaStream_t st) {
+  const int b1 = (int)std::min<int64_t>((n_slots_total + 255) / 256, (int64_t)sm_count * 8);
+  qm_rank_slots<<<std::max(b1, 1), 256, 0, st>>>(t, n_slots_total, stride, count_word, first_word, bitmap, ranks, words,
+                                                  perm);
+  const int b2 = (int)std::min<int64_t>((rows + 255) / 256, (int64_t)sm_count * 8);
+  qm_emit_perm<<<std::max(b2, 1), 256, 0, st>>>(t, stride, perm, ranks, words, rows, K, n_slots, O, out);
   return cudaGetLastError();
 }
 

@@ -75,6 +75,12 @@ cudaError_t qm_launch_emit_ranked(const uint64_t *t, int64_t n_slots_total, int 
 cudaError_t qm_launch_emit_walk(const qm_scan_args &a, const uint32_t *bitmap, const uint64_t *ranks, int64_t words,
                                 const qm_outspec &O, unsigned char *out, int sm_count, cudaStream_t st,
                                 const int64_t *bounds = nullptr, int chunk = 0);
+// Ranked emit in two ordered steps (slot numbers to their ranks in perm,
+// n_slots_total entries; then rows in order, at most `rows` of them).
+cudaError_t qm_launch_emit_perm(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                                const uint32_t *bitmap, const uint64_t *ranks, int64_t words, uint32_t *perm,
+                                int64_t rows, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
+                                unsigned char *out, int sm_count, cudaStream_t st);
 // Word bounds (chunks + 1 entries) of output chunks of `per` rows.
 cudaError_t qm_launch_walk_bounds(const uint64_t *ranks, int64_t words, int64_t per, int chunks, int64_t *bounds,
                                   cudaStream_t st);
