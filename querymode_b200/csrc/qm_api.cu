@@ -1592,9 +1592,10 @@ constexpr size_t SPEC_RESULT_BYTES = (size_t)8 << 20;
 // regrows and runs again.
 // rows_resident: the plan's key columns hold every row the first-row bitmap
 // indexes (a query over a resident table), so a large direct-indexed result
-// can be emitted in output order by walking that bitmap.  (Hash tables keep
-// the slot-order emit: the walk's probes and its pass over every row's bitmap
-// word measured slower there, 0.73 -> 0.87 ms of finalize at 971K groups.)
+// can be emitted in output order by walking that bitmap.  (Not for hash
+// tables: the walk's probes and its pass over every row's bitmap word
+// measured slower there, 0.73 -> 0.87 ms of finalize at 971K groups; their
+// large results take the two ordered steps of qm_launch_emit_perm.)
 constexpr int64_t WALK_MIN_SLOTS = (int64_t)1 << 20;
 constexpr int64_t EMIT_CHUNK_MIN_ROWS = (int64_t)1 << 22;
 // Results of at least this many rows (hashed, or direct ones not walked) are
