@@ -970,13 +970,31 @@ __device__ __forceinline__ uint64_t scan_in(const uint32_t *in, int64_t i, int64
   return POPC ? (uint64_t)__popc(x) : (uint64_t)x;
 }
 
-template <bool POPC>
+// A thread's QM_SCAN_PER inputs; VEC: two 16-byte loads when all 8 are in range
+// (the caller checked that `in` is 16-byte aligned; base is a multiple of 8).
+template <bool POPC, bool VEC>
+__device__ __forceinline__ void scan_load8(const uint32_t *in, int64_t base, int64_t n, uint64_t (&v)[QM_SCAN_PER]) {
+  if (VEC && base + QM_SCAN_PER <= n) {
+    const uint4 a = reinterpret_cast<const uint4 *>(in + base)[0];
+    const uint4 b = reinterpret_cast<const uint4 *>(in + base)[1];
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int k = 0; k < QM_SCAN_PER; ++k) v[k] = POPC ? (uint64_t)__popc(w[k]) : (uint64_t)w[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < QM_SCAN_PER; ++k) v[k] = scan_in<POPC>(in, base + k, n);
+  }
+}
+
+template <bool POPC, bool VEC>
 __global__ void __launch_bounds__(QM_SCAN_BLOCK) qm_scan_tile_sums(const uint32_t *in, int64_t n, uint64_t *sums) {
   __shared__ uint64_t wsum[QM_SCAN_BLOCK / 32];
   const int64_t base = (int64_t)blockIdx.x * QM_SCAN_TILE + (int64_t)threadIdx.x * QM_SCAN_PER;
+  uint64_t v[QM_SCAN_PER];
+  scan_load8<POPC, VEC>(in, base, n, v);
   uint64_t t = 0;
 #pragma unroll
-  for (int k = 0; k < QM_SCAN_PER; ++k) t += scan_in<POPC>(in, base + k, n);
+  for (int k = 0; k < QM_SCAN_PER; ++k) t += v[k];
 #pragma unroll
   for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(QM_FULL, t, o);
   if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = t;
@@ -1030,19 +1048,19 @@ __global__ void __launch_bounds__(1024) qm_scan_tile_offsets(uint64_t *sums, int
     }
 }
 
-template <bool POPC>
+// VEC: 16-byte loads and stores for full runs of 8 (the caller checked that
+// `in` and `out` are 16-byte aligned).
+template <bool POPC, bool VEC>
 __global__ void __launch_bounds__(QM_SCAN_BLOCK)
     qm_scan_tiles(const uint32_t *in, int64_t n, const uint64_t *offsets, uint64_t *out, int write_total) {
   __shared__ uint64_t wsum[QM_SCAN_BLOCK / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * QM_SCAN_TILE + (int64_t)threadIdx.x * QM_SCAN_PER;
   uint64_t v[QM_SCAN_PER];
+  scan_load8<POPC, VEC>(in, base, n, v);
   uint64_t t = 0;
 #pragma unroll
-  for (int k = 0; k < QM_SCAN_PER; ++k) {
-    v[k] = scan_in<POPC>(in, base + k, n);
-    t += v[k];
-  }
+  for (int k = 0; k < QM_SCAN_PER; ++k) t += v[k];
   uint64_t x = t;  // inclusive scan of thread sums across the warp
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -1061,10 +1079,22 @@ __global__ void __launch_bounds__(QM_SCAN_BLOCK)
   }
   __syncthreads();
   uint64_t run = offsets[blockIdx.x] + wsum[warp] + x - t;  // exclusive offset of this thread's first input
+  if (VEC && base + QM_SCAN_PER <= n) {
+    uint64_t r[QM_SCAN_PER];
 #pragma unroll
-  for (int k = 0; k < QM_SCAN_PER; ++k) {
-    if (base + k < n) out[base + k] = run;
-    run += v[k];
+    for (int k = 0; k < QM_SCAN_PER; ++k) {
+      r[k] = run;
+      run += v[k];
+    }
+    ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + base);
+#pragma unroll
+    for (int k = 0; k < QM_SCAN_PER / 2; ++k) o[k] = make_ulonglong2(r[2 * k], r[2 * k + 1]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < QM_SCAN_PER; ++k) {
+      if (base + k < n) out[base + k] = run;
+      run += v[k];
+    }
   }
   if (write_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = offsets[gridDim.x];
 }
@@ -1082,9 +1112,12 @@ cudaError_t qm_scan_u64(const uint32_t *in, int64_t n, uint64_t *out, void *temp
   const int64_t tiles = std::max<int64_t>((n + QM_SCAN_TILE - 1) / QM_SCAN_TILE, 1);
   if (temp_bytes < qm_scan_temp_bytes_for(n)) return cudaErrorInvalidValue;
   uint64_t *sums = static_cast<uint64_t *>(temp);
-  qm_scan_tile_sums<POPC><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums);
+  const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+  if (vec) qm_scan_tile_sums<POPC, true><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums);
+  else qm_scan_tile_sums<POPC, false><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums);
   qm_scan_tile_offsets<<<1, 1024, 0, st>>>(sums, tiles);
-  qm_scan_tiles<POPC><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums, out, write_total ? 1 : 0);
+  if (vec) qm_scan_tiles<POPC, true><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums, out, write_total ? 1 : 0);
+  else qm_scan_tiles<POPC, false><<<(unsigned)tiles, QM_SCAN_BLOCK, 0, st>>>(in, n, sums, out, write_total ? 1 : 0);
   return cudaGetLastError();
 }
 
