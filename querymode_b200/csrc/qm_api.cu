@@ -1400,6 +1400,7 @@ struct GroupTable {
   int64_t sel_bound = -1;     // planner's sampled bound on selected rows, if taken
   const uint32_t *zones = nullptr;  // kept zones (device), or null: scan every tile
   int64_t n_zone_tiles = 0;
+  bool small_rank = false;  // ranked in one block (ctx->perm, the count in franks[0])
 };
 
 int read_status(qm_ctx *ctx, qm_status *out) {
@@ -1464,11 +1465,24 @@ int64_t rank_words(const GroupTable &gt) { return std::max<int64_t>(gt.rows_done
 // First-seen order: a bit per first row, prefix popcounts give the ranks.
 // Queues the ranking and a copy of the group count to ctx->hstatus + 32
 // (read after the caller's next synchronize).
-int launch_rank(qm_ctx *ctx, const GroupTable &gt) {
+int launch_rank(qm_ctx *ctx, GroupTable &gt) {
   const Plan &pl = gt.pl;
   const Exec &ex = gt.ex;
   const int64_t bm_words = rank_words(gt);
   int rc;
+  gt.small_rank = ex.total_slots <= QM_SMALL_RANK_SLOTS;
+  if (gt.small_rank) {
+    // a small table is sorted by first row in one block
+    if ((rc = ensure(ctx, ctx->perm, sizeof(uint32_t) * QM_SMALL_RANK_SLOTS)) ||
+        (rc = ensure(ctx, ctx->franks, 16)) || (rc = ensure_host(ctx, ctx->hstatus, 64)))
+      return rc;
+    CK(qm_launch_rank_small(gt.table, ex.total_slots, ex.stride, pl.agg.acc[pl.agg.acc_count].word,
+                            pl.agg.acc[pl.agg.acc_first].word, (uint32_t *)ctx->perm.p, (uint64_t *)ctx->franks.p,
+                            ctx->stream));
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync((char *)ctx->hstatus.p + 32, ctx->franks.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    return QM_OK;
+  }
   size_t tb = 0;
   CK(qm_rank_temp_bytes(bm_words, &tb));
   if ((rc = ensure(ctx, ctx->fbits, (bm_words + 1) * 4)) || (rc = ensure(ctx, ctx->fcounts, (bm_words + 1) * 4)) ||
@@ -1678,7 +1692,7 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
   for (int k = 0; k < O.n_out; k++)
     if (O.o[k].null_offset >= 0)
       CK(cudaMemsetAsync((char *)ctx->out.p + O.o[k].null_offset, 0, null_words_bytes, ctx->stream));
-  const bool walk = ranked && rows_resident && pl.key.mode == QK_DIRECT && ex.n_slots >= WALK_MIN_SLOTS;
+  const bool walk = ranked && !gt.small_rank && rows_resident && pl.key.mode == QK_DIRECT && ex.n_slots >= WALK_MIN_SLOTS;
   // a large result laid out before its group count is known is emitted in
   // chunks of rows, each chunk's copy to host memory running while the next
   // chunk is emitted
@@ -1725,6 +1739,10 @@ int finish_table(qm_ctx *ctx, GroupTable &gt, qm_result **out, float scan_ms_so_
     if (G > 0)
       CK(qm_launch_emit_walk(a, (const uint32_t *)ctx->fbits.p, (const uint64_t *)ctx->franks.p, rank_words(gt), O,
                              (unsigned char *)ctx->out.p, ctx->sm_count, ctx->stream));
+  } else if (ranked && gt.small_rank) {
+    if (G > 0)
+      CK(qm_launch_emit_sorted(gt.table, ex.stride, (const uint32_t *)ctx->perm.p, (const uint64_t *)ctx->franks.p, G,
+                               pl.key, ex.n_slots, O, (unsigned char *)ctx->out.p, ctx->sm_count, ctx->stream));
   } else if (ranked && G >= PERM_MIN_ROWS && ex.total_slots < ((int64_t)1 << 32)) {
     if ((rc = ensure(ctx, ctx->perm, sizeof(uint32_t) * (size_t)ex.total_slots))) {
       delete R;

@@ -263,6 +263,58 @@ __global__ void qm_rank_slots(const uint64_t *t, int64_t n_slots_total, int stri
   }
 }
 
+// First-seen order of a small table (at most QM_SMALL_RANK_SLOTS slots) in
+// one block: the occupied slots are collected with their first rows into
+// shared memory and sorted by first row (bitonic; first rows are distinct),
+// their slot numbers written in that order to perm and their count to
+// groups[0] (one launch where the bitmap ranking takes five).
+__global__ void __launch_bounds__(1024) qm_rank_small(const uint64_t *t, int64_t n_slots_total, int stride,
+                                                      int count_word, int first_word, uint32_t *perm,
+                                                      uint64_t *groups) {
+  __shared__ uint64_t fr[QM_SMALL_RANK_SLOTS];
+  __shared__ uint32_t sl[QM_SMALL_RANK_SLOTS];
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  for (int64_t s = threadIdx.x; s < n_slots_total && s < QM_SMALL_RANK_SLOTS; s += blockDim.x) {
+    const uint64_t *w = t + s * stride + 1;
+    if (w[count_word] == 0) continue;
+    const int i = atomicAdd(&cnt, 1);
+    fr[i] = w[first_word];
+    sl[i] = (uint32_t)s;
+  }
+  __syncthreads();
+  const int n = cnt;
+  int P = 1;
+  while (P < n) P <<= 1;
+  for (int i = n + (int)threadIdx.x; i < P; i += blockDim.x) {
+    fr[i] = ~0ULL;
+    sl[i] = 0;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const bool up = (i & k) == 0;
+          if ((fr[i] > fr[ixj]) == up) {
+            const uint64_t f = fr[i];
+            fr[i] = fr[ixj];
+            fr[ixj] = f;
+            const uint32_t v = sl[i];
+            sl[i] = sl[ixj];
+            sl[ixj] = v;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sl[i];
+  if (threadIdx.x == 0) groups[0] = (uint64_t)n;
+}
+
 // rows: the layout's capacity (output rows past it are not written).
 __global__ void qm_emit_perm(const uint64_t *t, int stride, const uint32_t *perm, const uint64_t *ranks,
                              int64_t words, int64_t rows, const __grid_constant__ qm_keyspec K, int64_t n_slots,
@@ -1417,6 +1469,21 @@ cudaError_t qm_launch_emit_perm(const uint64_t *t, int64_t n_slots_total, int st
                                                   perm);
   const int b2 = (int)std::min<int64_t>((rows + 255) / 256, (int64_t)sm_count * 8);
   qm_emit_perm<<<std::max(b2, 1), 256, 0, st>>>(t, stride, perm, ranks, words, rows, K, n_slots, O, out);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_rank_small(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                                 uint32_t *perm, uint64_t *groups, cudaStream_t st) {
+  if (n_slots_total > QM_SMALL_RANK_SLOTS) return cudaErrorInvalidValue;
+  qm_rank_small<<<1, 1024, 0, st>>>(t, n_slots_total, stride, count_word, first_word, perm, groups);
+  return cudaGetLastError();
+}
+
+cudaError_t qm_launch_emit_sorted(const uint64_t *t, int stride, const uint32_t *perm, const uint64_t *groups,
+                                  int64_t rows, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
+                                  unsigned char *out, int sm_count, cudaStream_t st) {
+  const int b = (int)std::min<int64_t>((rows + 255) / 256, (int64_t)sm_count * 8);
+  qm_emit_perm<<<std::max(b, 1), 256, 0, st>>>(t, stride, perm, groups, 0, rows, K, n_slots, O, out);
   return cudaGetLastError();
 }
 

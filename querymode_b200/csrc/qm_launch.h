@@ -81,6 +81,15 @@ cudaError_t qm_launch_emit_perm(const uint64_t *t, int64_t n_slots_total, int st
                                 const uint32_t *bitmap, const uint64_t *ranks, int64_t words, uint32_t *perm,
                                 int64_t rows, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
                                 unsigned char *out, int sm_count, cudaStream_t st);
+// First-seen order of a table of at most QM_SMALL_RANK_SLOTS slots in one
+// block (perm: slot of each output row; groups[0]: their count), then the
+// rows emitted in that order (at most `rows`).
+#define QM_SMALL_RANK_SLOTS 2048
+cudaError_t qm_launch_rank_small(const uint64_t *t, int64_t n_slots_total, int stride, int count_word, int first_word,
+                                 uint32_t *perm, uint64_t *groups, cudaStream_t st);
+cudaError_t qm_launch_emit_sorted(const uint64_t *t, int stride, const uint32_t *perm, const uint64_t *groups,
+                                  int64_t rows, const qm_keyspec &K, int64_t n_slots, const qm_outspec &O,
+                                  unsigned char *out, int sm_count, cudaStream_t st);
 // Word bounds (chunks + 1 entries) of output chunks of `per` rows.
 cudaError_t qm_launch_walk_bounds(const uint64_t *ranks, int64_t words, int64_t per, int chunks, int64_t *bounds,
                                   cudaStream_t st);
