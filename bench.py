@@ -384,9 +384,10 @@ def batch_tables_on_device(specs, device: int):
 
 
 def run_batched(ctx, stream, local: int, args) -> dict:
-    """256 filter -> GROUP BY queries of uneven sizes: one persistent fused
-    launch (autotuned, graph-replayed) against the same queries as sequential
-    per-query launches."""
+    """256 filter -> GROUP BY queries of uneven sizes as one batched run
+    (autotuned between per-query launches and per-class persistent kernels,
+    cut into waves, each wave graph-replayed) against the same queries as
+    sequential per-query runs; both end with every result in host memory."""
     import torch
 
     from querymode_b200 import autotune, datagen
