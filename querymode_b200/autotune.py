@@ -1,7 +1,7 @@
 """Autotuner for the batched launch.
 
-Times a batch run as per-query specialised launches (mode 1) and as one
-persistent kernel (mode 0) under a grid of launch shapes — tiles of 256 rows
+Times a batch run as per-query specialised launches (mode 1) and as
+per-class persistent kernels (mode 0) under a grid of launch shapes — tiles of 256 rows
 per work chunk, block-local table budget (KiB of shared memory; 0 places
 every group table in global memory only) and resident blocks per SM — each
 at several wave counts (the batch cut into waves whose result copies overlap
@@ -53,7 +53,7 @@ def tune_batch(batch, grid: dict | None = None, reps: int = 2, table_path: str |
         batch.set_waves(wv)
         trials.append({"mode": 1, "chunk_tiles": 0, "local_kb": 0, "blocks_per_sm": 0, "waves": wv,
                        "ms": _time(batch, reps)})
-    # the persistent kernel's shapes at the best wave count of mode 1
+    # the persistent kernels' shapes at the best wave count of mode 1
     wv = min(trials, key=lambda t: t["ms"])["waves"]
     batch.set_waves(wv)
     batch.set_mode(0)

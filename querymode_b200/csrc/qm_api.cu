@@ -3664,7 +3664,7 @@ struct qm_batch {
   cudaEvent_t ev_start = nullptr, ev_end = nullptr;
   std::vector<cudaEvent_t> q_ev;      // per-query copies landed (per-request completion)
   std::vector<std::shared_ptr<SharedPinned>> q_host;  // per-request result buffers until completed
-  int mode = 1;  // 0: one persistent kernel over (query, chunk) work items; 1: per-query launches
+  int mode = 1;  // 0: persistent kernels (one per query class) over (query, chunk) work items; 1: per-query launches
   std::vector<const qm_table *> tabs;  // query i's table and a copy of the
   std::vector<std::unique_ptr<OwnedQuery>> queries;  // query, to rerun it alone
   DevBuf arena, d_bq, d_counter, d_status;
@@ -3800,7 +3800,7 @@ int batch_layout(qm_batch *b) {
     gt.table = (uint64_t *)b->arena.p + table_off[i];
     qm_bq &q = b->bq[i];
     fill_args(gt, q.a, (qm_status *)b->d_status.p + b->pos[i]);
-    q.a.priv = 0;  // the persistent kernel keeps one block-local copy
+    q.a.priv = 0;  // the persistent kernels keep one block-local copy
     q.a.n = b->rows[i];
     q.a.sel = nullptr;
     q.a.row_offset = 0;

@@ -749,7 +749,7 @@ class Batch:
 
     def set_mode(self, mode: int) -> None:
         """1: one specialised scan launch per query on parallel graph
-        branches (default); 0: one persistent kernel over all queries."""
+        branches (default); 0: persistent kernels, one per query class."""
         self.ctx.check(self.ctx.lib.qm_batch_set_mode(self.h, mode))
 
     def set_waves(self, waves: int) -> None:
